@@ -1,0 +1,272 @@
+/*
+ * piro.h -- C ABI of piro_b200, a B200 (sm_100a) implementation of PIRO's
+ * sparse finite-difference time-stepping path.
+ *
+ * Two layers:
+ *   1. Kernel entry points on caller-owned device memory (plain pointers and
+ *      sizes, asynchronous on the given CUDA stream, which may be NULL for the
+ *      legacy default stream).  Each replaces one reference routine, cited as
+ *      file:line in the PIRO source tree.
+ *   2. A context API (piro_open ... piro_close) mirroring PIRO's operator API
+ *      (process::ddt_r / laplacian / gradient / vector, operator&, operator=,
+ *      scalarMatrix::Solve, Piro::solve) and its .ini case format; the library
+ *      owns all device memory of a context.
+ *
+ * Conventions, as in the reference: grid sizes nx, ny, nz include one ghost
+ * layer per side (src/preprocess.cpp:72-74); the linear index is
+ * i = x + y*nx + z*nx*ny (src/mathoperations.cpp:38-40); fields are float[N];
+ * a vector field is float[3N] stored x block, y block, z block (src/ic.cpp:84-95);
+ * CSR index arrays are int32.
+ *
+ * Every function returns a status code (PIRO_OK on success); no C++ exception
+ * crosses this boundary.  piro_last_error() gives a message for the calling
+ * thread's last failure.  Calls on one context are not thread-safe; separate
+ * contexts may be used from separate threads.
+ */
+#ifndef PIRO_H
+#define PIRO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PIRO_OK 0
+#define PIRO_ERR_ARG 1          /* invalid argument or size                     */
+#define PIRO_ERR_CONFIG 2       /* .ini missing a key or holding a bad value     */
+#define PIRO_ERR_DATATYPE 3     /* [Solve] Data not supported for this operator  */
+#define PIRO_ERR_TABLE_FULL 4   /* hash insert found no free slot (methods.cpp:106-116 exits) */
+#define PIRO_ERR_TABLE_SIZE 5   /* hash table size <= 0 (reference formula below N~18.6k only) */
+#define PIRO_ERR_CUDA 6         /* a CUDA runtime call failed                    */
+#define PIRO_STATUS_STALLED 7   /* iterative solve stopped making progress       */
+#define PIRO_ERR_NOT_CONVERGED 8 /* iteration cap reached                        */
+#define PIRO_ERR_SCHEME 9       /* TIMESCHEME / SOLVERSCHEME / space scheme unsupported */
+#define PIRO_ERR_NOMEM 10       /* device allocation failed                      */
+#define PIRO_ERR_STATE 11       /* call out of order (e.g. operator not built)  */
+
+typedef void *piro_stream_t; /* a cudaStream_t */
+
+const char *piro_status_string(int status);
+const char *piro_last_error(void);
+/* Version string of the library build. */
+const char *piro_version(void);
+
+/* ========================================================================
+ * 1. Kernel entry points (device pointers; asynchronous on `stream`)
+ * ======================================================================== */
+
+/* -- assembly ------------------------------------------------------------ */
+
+/* nnz of the 7-point Laplacian, 7N - 2(nx*ny + ny*nz + nx*nz), for every
+ * space scheme (the uw/dw duplicates and the 10.0 entries add no entries). */
+int piro_laplacian_nnz(int nx, int ny, int nz, int64_t *nnz);
+
+/* CSR Laplacian, bit-exact with CSR::stencils::laplacian_{uw,dw,cd}
+ * (src/stencils.cpp:233-429) called from CSR::laplacian
+ * (src/operatorlaplacian.cpp:14-63): per row self -6/norm then x-, x+, y-, y+,
+ * z-, z+ at +1/norm; scheme 1 (uw) replaces "+" columns by the row, scheme 2
+ * (dw) the "-" columns; the first occurrence of each boundary column is 10.0
+ * (stencils.cpp:278-291).  norm is the float (l0/(n0-2))^2 of
+ * operatorlaplacian.cpp:33.  rowptr[N+1], col/val[nnz]. */
+int piro_csr_laplacian(int nx, int ny, int nz, int space_scheme, float norm, int32_t *rowptr, int32_t *col,
+                       float *val, piro_stream_t stream);
+
+/* COO Laplacian, bit-exact with COO::stencils::laplacian_* (src/stencils.cpp:572-795)
+ * via COO::laplacian (src/operatorlaplacian.cpp:105-153): same entries and
+ * order as CSR with an explicit row array. */
+int piro_coo_laplacian(int nx, int ny, int nz, int space_scheme, float norm, int32_t *rows, int32_t *col,
+                       float *val, piro_stream_t stream);
+
+/* nnz of one gradient matrix: 2N - 2N/n_axis. */
+int piro_gradient_nnz(int nx, int ny, int nz, int axis, int64_t *nnz);
+
+/* One CSR gradient matrix (axis 0 x, 1 y, 2 z), bit-exact with
+ * CSR::stencils::gradient_{uw,dw,cd}_{x,y,z} (src/stencils.cpp:7-231) via
+ * CSR::gradient (src/operatorgradient.cpp:13-117, norm = 2*(l0/(n0-2)), :25). */
+int piro_csr_gradient(int nx, int ny, int nz, int space_scheme, int axis, float norm, int32_t *rowptr,
+                      int32_t *col, float *val, piro_stream_t stream);
+
+/* val[k] *= s[row(k)]: the row scale diag(s)*M that kernelmethods::csrscale
+ * (src/kernelcsrgeam.cpp:208-234) intends through SpMDSM.cl:20-31. */
+int piro_csr_rowscale(int64_t nrows, const int32_t *rowptr, float *val, const float *s, piro_stream_t stream);
+
+/* -- hash-table (HT) format ---------------------------------------------- */
+
+/* Table size.  policy 0: the reference formula of
+ * src/operatorlaplacian.cpp:184-185, (int)(nnz / ((a*N^b + c) * lf)) with
+ * float/double arithmetic as written (may be <= 0 above N ~ 18.6k, in which
+ * case PIRO_ERR_TABLE_SIZE is returned); policy 1: the smallest prime >=
+ * ceil(nnz/lf). */
+int piro_ht_table_size(int64_t nnz, int64_t N, int policy, float a, float b, float c, float lf, int64_t *ts);
+
+/* Bytes of device workspace piro_ht_build needs for a table of ts slots. */
+int piro_ht_build_workspace(int64_t ts, size_t *bytes);
+
+/* Insert a CSR matrix into an open-addressing table: key = row*N + col (int64;
+ * equal to the reference's int32 key while N <= 46340), slot = key % ts,
+ * linear probing, a repeated key keeps its first slot and takes the last
+ * value.  Slots match the reference's sequential row-major methods::sethash
+ * (src/methods.cpp:74-118, src/operatorlaplacian.cpp:190-203) exactly: keys
+ * are inserted in parallel with atomicCAS under insertion-time priority (a
+ * probe that meets a later-inserted key takes its slot and carries it on),
+ * which converges to the first-come-first-served layout whatever the thread
+ * interleaving.  keys[ts] get -1 for empty slots.  Returns PIRO_ERR_TABLE_FULL (synchronously checked) when an
+ * insert finds no slot. */
+int piro_ht_build(int64_t N, const int32_t *rowptr, const int32_t *col, const float *val, int64_t nnz, int64_t ts,
+                  int64_t *keys, float *vals, void *work, size_t work_bytes, piro_stream_t stream);
+
+/* -- time-step kernels ---------------------------------------------------- */
+
+/* SpMVCSR.cl:12-39 as launched by kernelsolve::CSR::TIMESCHEME_11
+ * (src/kernelprocess.cpp:10-40): for interior rows
+ * out[r] = u[r] + sum_k (dt*val[k])*u[col[k]], summed in storage order with
+ * no fused multiply-add; boundary rows of out are not written. */
+int piro_csr_fe_step(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val, float dt,
+                     const float *u, float *out, piro_stream_t stream);
+
+/* SpMVCSR_I1.cl:12-36 (backward-Euler residual form): interior rows get
+ * out[r] = u[r] - sum_k (dt*val[k])*u[col[k]]; boundary rows untouched. */
+int piro_csr_i1(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val, float dt,
+                const float *u, float *out, piro_stream_t stream);
+
+/* SpMVCOO.cl:12-24 semantics with a warp-segmented reduction: out[r] =
+ * dt * sum of vals*u[cols] over the entries of row r, for every row.  rows
+ * must be sorted ascending (the Laplacian assembly order).  Summation order
+ * differs from the sequential kernel (results agree to FP32 rounding). */
+int piro_coo_spmv(int64_t N, int64_t nnz, const int32_t *rows, const int32_t *cols, const float *vals, float dt,
+                  const float *u, float *out, piro_stream_t stream);
+
+/* kernelsolve::COO::TIMESCHEME_11 (src/kernelprocess.cpp:93-120) fused:
+ * out = u + dt*M*u on every row. */
+int piro_coo_fe_step(int64_t N, int64_t nnz, const int32_t *rows, const int32_t *cols, const float *vals, float dt,
+                     const float *u, float *out, piro_stream_t stream);
+
+/* SpMVHT.cl:22-40 semantics: out[r] = dt * sum over present keys (r, c) of
+ * H(r,c)*u[c] in ascending c, found by linear-probe lookups of the 7-point
+ * stencil's candidate columns of row r (the only columns a Laplacian table
+ * holds).  fe != 0 fuses addVectors: out = u + dt*H*u
+ * (kernelsolve::HT::TIMESCHEME_11, src/kernelprocess.cpp:68-91). */
+int piro_ht_spmv(int nx, int ny, int nz, const int64_t *keys, const float *vals, int64_t ts, float dt, int fe,
+                 const float *u, float *out, piro_stream_t stream);
+
+/* Matrix-free 7-point step, the comparison point for CSR (laplacianscalar.cl:1-21
+ * extended by alpha and the Euler update): interior cells
+ * out = u + dt*(alpha*((u[x+1]+u[x-1]-2u)*idx2 + (..y..)*idy2 + (..z..)*idz2)),
+ * boundary cells copied.  alpha may be NULL (1). */
+int piro_stencil_fe_step(int nx, int ny, int nz, float idx2, float idy2, float idz2, float dt, const float *alpha,
+                         const float *u, float *out, piro_stream_t stream);
+
+/* setBC.cl (launched by bc::opencl_setBC, src/bc.cpp:38-65): dst[idx[i]] = src[idx[i]]. */
+int piro_set_bc(int64_t q, const uint32_t *idx, const float *src, float *dst, piro_stream_t stream);
+
+/* Face-interior index lists of bc::initbc (src/bc.cpp:107-146): faces 0 x=nx-1,
+ * 1 x=0, 2 y=ny-1, 3 y=0, 4 z=0, 5 z=nz-1, each ascending, concatenated.
+ * piro_face_count gives Q and the 7 face offsets (host only); piro_face_lists
+ * writes idx[Q] on the device. */
+int piro_face_count(int nx, int ny, int nz, int64_t *q, int64_t face_start[7]);
+int piro_face_lists(int nx, int ny, int nz, uint32_t *idx, piro_stream_t stream);
+
+/* Elementwise kernels of 0_kernels_math.txt (operatoroverload.cpp:125-307):
+ * op 0 add (a = b + c), 1 subtract (b - c), 2 multiply, 3 divide. */
+int piro_vec_op(int op, int64_t n, const float *b, const float *c, float *a, piro_stream_t stream);
+/* *_constant.cl: op 0 a = s + c, 1 a = c - s, 2 a = s * c, 3 a = c / s. */
+int piro_vec_op_scalar(int op, int64_t n, float s, const float *c, float *a, piro_stream_t stream);
+/* addVectors_URF.cl: t = a; a += c*urf; c = a - t. */
+int piro_vec_urf(int64_t n, float *a, float *c, float urf, piro_stream_t stream);
+
+/* -- csrgeam ---------------------------------------------------------------- */
+
+/* Workspace bytes for the count/scan passes over nrows rows. */
+int piro_scan_workspace(int64_t nrows, size_t *bytes);
+
+/* operator& (src/operatoroverload.cpp:102-123) -> kernelmethods::csrgeam
+ * (src/kernelcsrgeam.cpp:9-86; csrgeam_1.cl, prefixsum.cl, csrgeam_3.cl):
+ * D = diag(v_x)*A (+) diag(v_y)*B (+) diag(v_z)*C as concatenated rows: a
+ * three-way column merge (ties A, B, C) while all three rows have entries,
+ * then the tails of A, B, C appended unmerged.  v is the 3N SoA vector.
+ * nnz(D) = nnz(A)+nnz(B)+nnz(C).  The N serial scan launches of the
+ * reference become one device scan. */
+int piro_csrgeam3(int64_t N, const int32_t *rpA, const int32_t *cA, const float *vA, const int32_t *rpB,
+                  const int32_t *cB, const float *vB, const int32_t *rpC, const int32_t *cC, const float *vC,
+                  const float *v, int32_t *rpD, int32_t *cD, float *vD, void *work, size_t work_bytes,
+                  piro_stream_t stream);
+
+/* D = A + beta*B, one union row per row with ascending columns; a column in
+ * both rows is A's value + beta*B's value.  Builds the backward-Euler matrix
+ * I - dt*diag(alpha)*L (no counterpart kernel in the reference, whose JLI
+ * applies dt inside SpMVCSR_I1.cl).  Two calls: _count writes rpD[N+1]
+ * (read rpD[N] for nnz), _fill writes cD/vD. */
+int piro_csrgeam2_count(int64_t N, const int32_t *rpA, const int32_t *cA, const int32_t *rpB, const int32_t *cB,
+                        int32_t *rpD, void *work, size_t work_bytes, piro_stream_t stream);
+int piro_csrgeam2_fill(int64_t N, const int32_t *rpA, const int32_t *cA, const float *vA, float beta,
+                       const int32_t *rpB, const int32_t *cB, const float *vB, const int32_t *rpD, int32_t *cD,
+                       float *vD, piro_stream_t stream);
+
+/* Identity CSR of N rows (the A of A + beta*B). */
+int piro_csr_identity(int64_t N, int32_t *rowptr, int32_t *col, float *val, piro_stream_t stream);
+
+/* -- norms and dots (FP64 accumulation, deterministic) -------------------- */
+
+/* Workspace bytes for a reduction over n elements. */
+int piro_reduce_workspace(int64_t n, size_t *bytes);
+/* *out (device double) = sum x[i]*y[i]; y == x gives the squared norm, which
+ * replaces the host sum of squares of extras.cpp:24-30. */
+int piro_dot_f64(int64_t n, const float *x, const float *y, double *out, void *work, size_t work_bytes,
+                 piro_stream_t stream);
+
+/* -- backward Euler (TIMESCHEME 12) ----------------------------------------- */
+
+typedef struct piro_be_solver piro_be_solver;
+
+typedef struct piro_be_info {
+    int status;            /* PIRO_OK, PIRO_STATUS_STALLED or PIRO_ERR_NOT_CONVERGED */
+    int outer_iterations;  /* FP64 refinement sweeps                               */
+    int inner_iterations;  /* FP32 Krylov iterations summed over sweeps            */
+    int fallbacks;         /* learned-preconditioner sweeps that reverted to Jacobi */
+    double rel_residual;   /* ||b - A x||_2 / ||b||_2 over interior rows, FP64     */
+} piro_be_info;
+
+/* Preconditioner kinds for piro_be_set_preconditioner. */
+#define PIRO_PRECOND_JACOBI 0
+#define PIRO_PRECOND_LEARNED 1
+
+/* Create a solver for A x = b with A = I - dt*diag(alpha)*L given as CSR over
+ * all N rows (device pointers, which must stay valid).  Interior rows are the
+ * unknowns; boundary values are held at b (Dirichlet).  The system is solved
+ * in its symmetric form diag(alpha)^-1 A on the interior (requires L
+ * symmetric there: space scheme 3), by FP32 Jacobi-PCG inside FP64 iterative
+ * refinement.  Replaces kernelsolve::CSR::TIMESCHEME_12_40
+ * (src/kernelprocess.cpp:123-209), whose Richardson iteration diverges for
+ * dt*lambda_max > 2.  The solver allocates its own workspace. */
+int piro_be_create(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val,
+                   const float *alpha, piro_stream_t stream, piro_be_solver **out);
+/* Solve: b, x device float[N]; x receives the FP32 solution (boundary = b).
+ * Stops when the FP64 relative residual <= rtol.  info may be NULL. */
+int piro_be_solve(piro_be_solver *s, const float *b, float *x, double rtol, int max_outer, int max_inner,
+                  piro_be_info *info);
+/* FP64 copy of the last solution (device double[N]) for error reporting. */
+int piro_be_solution_f64(piro_be_solver *s, const double **x64);
+/* Live timing of the solver's dominant kernel (the CG SpMV, q = A p): CUDA
+ * events recorded around each launch inside the solver's graph give the
+ * launches that did work since the last reset and their summed device time in
+ * ms; kernel_launches counts every kernel the solver launched.  Any output
+ * pointer may be NULL. */
+int piro_be_kernel_stats(piro_be_solver *s, int reset, long long *spmv_launches, double *spmv_ms,
+                         long long *kernel_launches);
+int piro_be_destroy(piro_be_solver *s);
+
+/* Reference JLI iteration (scheme 12 + solver 40, src/kernelprocess.cpp:123-209)
+ * on the device: x = b; repeat r = b - (I - dt*L)x on interior rows (b on the
+ * others), x += urf*r, r = dx; res = ||r||/sqrt(N); stop when
+ * (res - res_old)^2 < tol.  Residual sums are FP64.  *iters receives the count. */
+int piro_be_jli(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val, float dt,
+                const float *b, float *x, float *r_work, float tol, float urf, int maxiter, int *iters,
+                piro_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PIRO_H */

@@ -1,0 +1,114 @@
+"""ctypes binding of libpiro_b200.so (the C ABI declared in include/piro.h).
+
+The library is the product path: there is no CPU fallback.  `lib()` raises if
+the shared library is missing or does not export a declared symbol, and every
+wrapper in piro_b200.ops raises PiroError on a non-zero status.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+LIB_PATH = os.path.join(PKG, "libpiro_b200.so")
+HEADERS = [os.path.join(ROOT, "include", "piro.h")]
+
+i32, i64, f32, f64, vp, sz = C.c_int, C.c_int64, C.c_float, C.c_double, C.c_void_p, C.c_size_t
+pi64 = C.POINTER(C.c_int64)
+psz = C.POINTER(C.c_size_t)
+pint = C.POINTER(C.c_int)
+
+
+class BeInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("outer_iterations", C.c_int), ("inner_iterations", C.c_int),
+                ("fallbacks", C.c_int), ("rel_residual", C.c_double)]
+
+
+# name -> (restype, argtypes).  Pointers to device memory are passed as
+# integers (c_void_p).
+SIGNATURES = {
+    "piro_status_string": (C.c_char_p, [i32]),
+    "piro_last_error": (C.c_char_p, []),
+    "piro_version": (C.c_char_p, []),
+    "piro_laplacian_nnz": (i32, [i32, i32, i32, pi64]),
+    "piro_csr_laplacian": (i32, [i32, i32, i32, i32, f32, vp, vp, vp, vp]),
+    "piro_coo_laplacian": (i32, [i32, i32, i32, i32, f32, vp, vp, vp, vp]),
+    "piro_gradient_nnz": (i32, [i32, i32, i32, i32, pi64]),
+    "piro_csr_gradient": (i32, [i32, i32, i32, i32, i32, f32, vp, vp, vp, vp]),
+    "piro_csr_rowscale": (i32, [i64, vp, vp, vp, vp]),
+    "piro_ht_table_size": (i32, [i64, i64, i32, f32, f32, f32, f32, pi64]),
+    "piro_ht_build_workspace": (i32, [i64, psz]),
+    "piro_ht_build": (i32, [i64, vp, vp, vp, i64, i64, vp, vp, vp, sz, vp]),
+    "piro_csr_fe_step": (i32, [i32, i32, i32, vp, vp, vp, f32, vp, vp, vp]),
+    "piro_csr_i1": (i32, [i32, i32, i32, vp, vp, vp, f32, vp, vp, vp]),
+    "piro_coo_spmv": (i32, [i64, i64, vp, vp, vp, f32, vp, vp, vp]),
+    "piro_coo_fe_step": (i32, [i64, i64, vp, vp, vp, f32, vp, vp, vp]),
+    "piro_ht_spmv": (i32, [i32, i32, i32, vp, vp, i64, f32, i32, vp, vp, vp]),
+    "piro_stencil_fe_step": (i32, [i32, i32, i32, f32, f32, f32, f32, vp, vp, vp, vp]),
+    "piro_set_bc": (i32, [i64, vp, vp, vp, vp]),
+    "piro_face_count": (i32, [i32, i32, i32, pi64, pi64]),
+    "piro_face_lists": (i32, [i32, i32, i32, vp, vp]),
+    "piro_vec_op": (i32, [i32, i64, vp, vp, vp, vp]),
+    "piro_vec_op_scalar": (i32, [i32, i64, f32, vp, vp, vp]),
+    "piro_vec_urf": (i32, [i64, vp, vp, f32, vp]),
+    "piro_scan_workspace": (i32, [i64, psz]),
+    "piro_csrgeam3": (i32, [i64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
+    "piro_csrgeam2_count": (i32, [i64, vp, vp, vp, vp, vp, vp, sz, vp]),
+    "piro_csrgeam2_fill": (i32, [i64, vp, vp, vp, f32, vp, vp, vp, vp, vp, vp, vp]),
+    "piro_csr_identity": (i32, [i64, vp, vp, vp, vp]),
+    "piro_reduce_workspace": (i32, [i64, psz]),
+    "piro_dot_f64": (i32, [i64, vp, vp, vp, vp, sz, vp]),
+    "piro_be_create": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, C.POINTER(vp)]),
+    "piro_be_solve": (i32, [vp, vp, vp, f64, i32, i32, C.POINTER(BeInfo)]),
+    "piro_be_solution_f64": (i32, [vp, C.POINTER(vp)]),
+    "piro_be_kernel_stats": (i32, [vp, i32, C.POINTER(C.c_longlong), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_longlong)]),
+    "piro_be_destroy": (i32, [vp]),
+    "piro_be_jli": (i32, [i32, i32, i32, vp, vp, vp, f32, vp, vp, vp, f32, f32, i32, pint, vp]),
+}
+
+
+def declared_symbols() -> list[str]:
+    """Every function name declared in include/*.h."""
+    names = []
+    for h in HEADERS:
+        txt = open(h).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        names += re.findall(r"\b(piro_[a-z0-9_]+)\s*\(", txt)
+    return sorted(set(names))
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libpiro_b200.so; raise if it is missing or incomplete."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m piro_b200.build` "
+                           "(there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+class PiroError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        L = lib()
+        msg = L.piro_last_error().decode(errors="replace")
+        name = L.piro_status_string(status).decode()
+        super().__init__(f"{where}: {name} ({status}): {msg}")
+        self.status = status
+
+
+def check(status: int, where: str) -> None:
+    if status != 0:
+        raise PiroError(status, where)

@@ -1,0 +1,356 @@
+// assembly.cu -- Laplacian / gradient assembly on the device, bit-exact with
+// PIRO's serial host loops (src/stencils.cpp), plus the row scale, identity
+// and boundary face lists.
+//
+// The reference builds a matrix by pushing entries row by row and, for the
+// Laplacian, runs a std::find over the whole column array for every boundary
+// row (O(nnz * boundary), stencils.cpp:278-291).  Here each thread owns one
+// row: its rowptr comes from a closed-form prefix count of the 7-point
+// pattern, so there is no scan, and the "first occurrence of column c" rule is
+// decided locally from c's coordinates.  Rows are staged in shared memory per
+// block so that col/val/rows leave the SM as coalesced stores.
+#include "common.cuh"
+
+namespace piro {
+namespace {
+
+constexpr int kRowsPerBlock = 256;
+constexpr int kMaxPerRow = 7;
+
+struct Grid {
+    int nx, ny, nz;
+    int64_t sxy;
+};
+
+__device__ __forceinline__ void coords(int64_t i, const Grid &g, int &x, int &y, int &z)
+{
+    z = (int)(i / g.sxy);
+    int64_t rem = i - (int64_t)z * g.sxy;
+    y = (int)(rem / g.nx);
+    x = (int)(rem - (int64_t)y * g.nx);
+}
+
+// Sum of 7-point row lengths over all rows before (x, y, z) in row-major
+// order; a row has 7 - [x==0] - [x==nx-1] - [y==0] - [y==ny-1] - [z==0] - [z==nz-1]
+// entries.
+__device__ __forceinline__ int64_t lap_prefix(int x, int y, int z, const Grid &g)
+{
+    const int64_t nx = g.nx, ny = g.ny, nz = g.nz;
+    const int64_t by = (y == 0) + (y == ny - 1);
+    const int64_t bz = (z == 0) + (z == nz - 1);
+    int64_t p = (int64_t)z * (7 * nx * ny - 2 * ny - 2 * nx) - nx * ny * (z > 0);
+    p += (int64_t)y * (7 * nx - 2 - nx * bz) - nx * (y > 0);
+    p += (int64_t)x * (7 - by - bz) - (x > 0);
+    return p;
+}
+
+__device__ __forceinline__ bool is_bnd(int x, int y, int z, const Grid &g)
+{
+    return x == 0 || x == g.nx - 1 || y == 0 || y == g.ny - 1 || z == 0 || z == g.nz - 1;
+}
+
+// One row of the Laplacian: columns, values and count, in push order.
+__device__ __forceinline__ int lap_row(int64_t i, const Grid &g, int scheme, float vself, float vnb, int32_t *c,
+                                       float *v)
+{
+    int x, y, z;
+    coords(i, g, x, y, z);
+    const bool uw = scheme == 1, dw = scheme == 2;
+    int n = 0;
+    c[n] = (int32_t)i;
+    v[n] = vself;
+    // uw: the first occurrence of a boundary row's own column is its self
+    // entry (lower rows never reference higher columns); cd/dw: only cell 0.
+    if (is_bnd(x, y, z, g) && (uw || i == 0)) v[n] = 10.0f;
+    ++n;
+    if (x > 0) { c[n] = (int32_t)(dw ? i : i - 1); v[n] = vnb; ++n; }
+    if (x < g.nx - 1) {
+        c[n] = (int32_t)(uw ? i : i + 1);
+        v[n] = vnb;
+        // cd/dw: row i is the first referencer of column i+1 iff that cell
+        // has no lower z- or y-neighbour (z == 0 and y == 0).
+        if (!uw && z == 0 && y == 0 && is_bnd(x + 1, y, z, g)) v[n] = 10.0f;
+        ++n;
+    }
+    if (y > 0) { c[n] = (int32_t)(dw ? i : i - g.nx); v[n] = vnb; ++n; }
+    if (y < g.ny - 1) {
+        c[n] = (int32_t)(uw ? i : i + g.nx);
+        v[n] = vnb;
+        if (!uw && z == 0 && is_bnd(x, y + 1, z, g)) v[n] = 10.0f;
+        ++n;
+    }
+    if (z > 0) { c[n] = (int32_t)(dw ? i : i - g.sxy); v[n] = vnb; ++n; }
+    if (z < g.nz - 1) {
+        c[n] = (int32_t)(uw ? i : i + g.sxy);
+        v[n] = vnb;
+        if (!uw && is_bnd(x, y, z + 1, g)) v[n] = 10.0f;
+        ++n;
+    }
+    return n;
+}
+
+// Block = kRowsPerBlock consecutive rows.  rowptr may be NULL (COO), rows may
+// be NULL (CSR).
+__global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, int scheme, float vself, float vnb,
+                                                             int32_t *__restrict__ rowptr,
+                                                             int32_t *__restrict__ rows, int32_t *__restrict__ col,
+                                                             float *__restrict__ val)
+{
+    __shared__ int32_t s_col[kRowsPerBlock * kMaxPerRow];
+    __shared__ float s_val[kRowsPerBlock * kMaxPerRow];
+    __shared__ int32_t s_row[kRowsPerBlock * kMaxPerRow];
+    __shared__ int64_t s_base, s_end;
+    for (int64_t r0 = (int64_t)blockIdx.x * kRowsPerBlock; r0 < N; r0 += (int64_t)gridDim.x * kRowsPerBlock) {
+        const int64_t i = r0 + threadIdx.x;
+        const int64_t rlast = (r0 + kRowsPerBlock < N ? r0 + kRowsPerBlock : N) - 1;
+        if (threadIdx.x == 0) {
+            int x, y, z;
+            coords(r0, g, x, y, z);
+            s_base = lap_prefix(x, y, z, g);
+            int32_t c[kMaxPerRow];
+            float v[kMaxPerRow];
+            coords(rlast, g, x, y, z);
+            s_end = lap_prefix(x, y, z, g) + lap_row(rlast, g, scheme, vself, vnb, c, v);
+        }
+        __syncthreads();
+        if (i < N) {
+            int x, y, z;
+            coords(i, g, x, y, z);
+            const int64_t p = lap_prefix(x, y, z, g);
+            int32_t c[kMaxPerRow];
+            float v[kMaxPerRow];
+            const int n = lap_row(i, g, scheme, vself, vnb, c, v);
+            const int off = (int)(p - s_base);
+            for (int t = 0; t < n; ++t) {
+                s_col[off + t] = c[t];
+                s_val[off + t] = v[t];
+                s_row[off + t] = (int32_t)i;
+            }
+            if (rowptr) {
+                rowptr[i + 1] = (int32_t)(p + n);
+                if (i == 0) rowptr[0] = 0;
+            }
+        }
+        __syncthreads();
+        const int cnt = (int)(s_end - s_base);
+        for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+            col[s_base + t] = s_col[t];
+            val[s_base + t] = s_val[t];
+            if (rows) rows[s_base + t] = s_row[t];
+        }
+        __syncthreads();
+    }
+}
+
+// Gradient prefix: number of entries of rows before i for `axis`
+// (each row has [a > 0] + [a < n_a - 1] entries).
+__device__ __forceinline__ int64_t grad_prefix(int64_t i, int x, int y, int z, int axis, const Grid &g)
+{
+    int64_t c0, c1;  // rows before i with a == 0, with a == n_a - 1
+    if (axis == 0) {
+        int64_t r = (i - x) / g.nx;
+        c0 = r + (x > 0);
+        c1 = r;
+    } else if (axis == 1) {
+        c0 = (int64_t)g.nx * z + (y > 0 ? g.nx : x);
+        c1 = (int64_t)g.nx * z + (y == g.ny - 1 ? x : 0);
+    } else {
+        c0 = z > 0 ? g.sxy : i;
+        c1 = z == g.nz - 1 ? (int64_t)x + (int64_t)g.nx * y : 0;
+    }
+    return 2 * i - c0 - c1;
+}
+
+__global__ void __launch_bounds__(kRowsPerBlock) k_gradient(Grid g, int64_t N, int scheme, int axis, float vm, float vp,
+                                                            int32_t *__restrict__ rowptr, int32_t *__restrict__ col,
+                                                            float *__restrict__ val)
+{
+    const int64_t e = axis == 0 ? 1 : axis == 1 ? g.nx : g.sxy;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        int x, y, z;
+        coords(i, g, x, y, z);
+        const int a = axis == 0 ? x : axis == 1 ? y : z;
+        const int na = axis == 0 ? g.nx : axis == 1 ? g.ny : g.nz;
+        int64_t p = grad_prefix(i, x, y, z, axis, g);
+        if (a > 0) {
+            col[p] = (int32_t)(scheme == 2 ? i : i - e);
+            val[p] = vm;
+            ++p;
+        }
+        if (a < na - 1) {
+            col[p] = (int32_t)(scheme == 1 ? i : i + e);
+            val[p] = vp;
+            ++p;
+        }
+        rowptr[i + 1] = (int32_t)p;
+        if (i == 0) rowptr[0] = 0;
+    }
+}
+
+__global__ void k_rowscale(int64_t nrows, const int32_t *__restrict__ rowptr, float *__restrict__ val,
+                           const float *__restrict__ s)
+{
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += (int64_t)gridDim.x * blockDim.x) {
+        const float f = s[r];
+        for (int32_t k = rowptr[r]; k < rowptr[r + 1]; ++k) val[k] = __fmul_rn(val[k], f);
+    }
+}
+
+__global__ void k_identity(int64_t N, int32_t *__restrict__ rowptr, int32_t *__restrict__ col, float *__restrict__ val)
+{
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (int64_t)gridDim.x * blockDim.x) {
+        col[r] = (int32_t)r;
+        val[r] = 1.0f;
+        rowptr[r + 1] = (int32_t)(r + 1);
+        if (r == 0) rowptr[0] = 0;
+    }
+}
+
+// Face lists: faces 0/1 enumerate (z, y), 2/3 (z, x), 4/5 (y, x), each
+// over the interior range [1, n-2].
+__global__ void k_faces(Grid g, int64_t a, int64_t b, int64_t c, uint32_t *__restrict__ idx)
+{
+    const int64_t Q = 2 * (a + b + c);
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < Q; t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t u = t;
+        int face;
+        if (u < 2 * a) { face = (int)(u / a); u -= face * a; }
+        else if (u < 2 * a + 2 * b) { u -= 2 * a; face = 2 + (int)(u / b); u -= (face - 2) * b; }
+        else { u -= 2 * a + 2 * b; face = 4 + (int)(u / c); u -= (face - 4) * c; }
+        int x, y, z;
+        if (face <= 1) {
+            x = face == 0 ? g.nx - 1 : 0;
+            z = 1 + (int)(u / (g.ny - 2));
+            y = 1 + (int)(u % (g.ny - 2));
+        } else if (face <= 3) {
+            y = face == 2 ? g.ny - 1 : 0;
+            z = 1 + (int)(u / (g.nx - 2));
+            x = 1 + (int)(u % (g.nx - 2));
+        } else {
+            z = face == 4 ? 0 : g.nz - 1;
+            y = 1 + (int)(u / (g.nx - 2));
+            x = 1 + (int)(u % (g.nx - 2));
+        }
+        idx[t] = (uint32_t)(x + (int64_t)y * g.nx + (int64_t)z * g.sxy);
+    }
+}
+
+bool grid_ok(int nx, int ny, int nz)
+{
+    return nx >= 3 && ny >= 3 && nz >= 3 && (int64_t)nx * ny * nz < (int64_t)INT32_MAX / 8;
+}
+
+}  // namespace
+}  // namespace piro
+
+using namespace piro;
+
+extern "C" int piro_laplacian_nnz(int nx, int ny, int nz, int64_t *nnz)
+{
+    PIRO_ARG(nnz && grid_ok(nx, ny, nz), "piro_laplacian_nnz: grid sizes must be >= 3 (ghost-inclusive)");
+    const int64_t N = (int64_t)nx * ny * nz;
+    *nnz = 7 * N - 2 * ((int64_t)nx * ny + (int64_t)ny * nz + (int64_t)nx * nz);
+    return PIRO_OK;
+}
+
+static int launch_laplacian(int nx, int ny, int nz, int scheme, float norm, int32_t *rowptr, int32_t *rows,
+                            int32_t *col, float *val, piro_stream_t stream)
+{
+    PIRO_ARG(grid_ok(nx, ny, nz), "laplacian: grid sizes must be >= 3 (ghost-inclusive)");
+    PIRO_ARG(col && val, "laplacian: null output");
+    if (scheme < 1 || scheme > 3) {
+        piro::set_error("laplacian: space scheme %d not in {1 uw, 2 dw, 3 cd}", scheme);
+        return PIRO_ERR_SCHEME;
+    }
+    Grid g{nx, ny, nz, (int64_t)nx * ny};
+    const int64_t N = (int64_t)nx * ny * nz;
+    // The literals are double in stencils.cpp:245,250: (float)(-6.0/norm).
+    const float vself = (float)(-6.0 / (double)norm);
+    const float vnb = (float)(1.0 / (double)norm);
+    unsigned grid = grid_for(N, kRowsPerBlock, 4);
+    k_laplacian<<<grid, kRowsPerBlock, 0, as_stream(stream)>>>(g, N, scheme, vself, vnb, rowptr, rows, col, val);
+    PIRO_CHECK_LAUNCH("k_laplacian");
+    return PIRO_OK;
+}
+
+extern "C" int piro_csr_laplacian(int nx, int ny, int nz, int space_scheme, float norm, int32_t *rowptr, int32_t *col,
+                                  float *val, piro_stream_t stream)
+{
+    PIRO_ARG(rowptr, "piro_csr_laplacian: null rowptr");
+    return launch_laplacian(nx, ny, nz, space_scheme, norm, rowptr, nullptr, col, val, stream);
+}
+
+extern "C" int piro_coo_laplacian(int nx, int ny, int nz, int space_scheme, float norm, int32_t *rows, int32_t *col,
+                                  float *val, piro_stream_t stream)
+{
+    PIRO_ARG(rows, "piro_coo_laplacian: null rows");
+    return launch_laplacian(nx, ny, nz, space_scheme, norm, nullptr, rows, col, val, stream);
+}
+
+extern "C" int piro_gradient_nnz(int nx, int ny, int nz, int axis, int64_t *nnz)
+{
+    PIRO_ARG(nnz && grid_ok(nx, ny, nz) && axis >= 0 && axis <= 2, "piro_gradient_nnz: bad arguments");
+    const int64_t N = (int64_t)nx * ny * nz;
+    const int64_t na = axis == 0 ? nx : axis == 1 ? ny : nz;
+    *nnz = 2 * N - 2 * (N / na);
+    return PIRO_OK;
+}
+
+extern "C" int piro_csr_gradient(int nx, int ny, int nz, int space_scheme, int axis, float norm, int32_t *rowptr,
+                                 int32_t *col, float *val, piro_stream_t stream)
+{
+    PIRO_ARG(grid_ok(nx, ny, nz) && axis >= 0 && axis <= 2, "piro_csr_gradient: bad grid or axis");
+    PIRO_ARG(rowptr && col && val, "piro_csr_gradient: null output");
+    if (space_scheme < 1 || space_scheme > 3) {
+        piro::set_error("piro_csr_gradient: space scheme %d not in {1,2,3}", space_scheme);
+        return PIRO_ERR_SCHEME;
+    }
+    Grid g{nx, ny, nz, (int64_t)nx * ny};
+    const int64_t N = (int64_t)nx * ny * nz;
+    // -1/norm and 1/norm are float divisions (int operand promoted), stencils.cpp:17,24.
+    const float vm = -1 / norm, vp = 1 / norm;
+    k_gradient<<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(g, N, space_scheme, axis, vm, vp, rowptr, col, val);
+    PIRO_CHECK_LAUNCH("k_gradient");
+    return PIRO_OK;
+}
+
+extern "C" int piro_csr_rowscale(int64_t nrows, const int32_t *rowptr, float *val, const float *s, piro_stream_t stream)
+{
+    PIRO_ARG(nrows >= 0 && rowptr && val && s, "piro_csr_rowscale: bad arguments");
+    if (nrows == 0) return PIRO_OK;
+    k_rowscale<<<grid_for(nrows, 256, 8), 256, 0, as_stream(stream)>>>(nrows, rowptr, val, s);
+    PIRO_CHECK_LAUNCH("k_rowscale");
+    return PIRO_OK;
+}
+
+extern "C" int piro_csr_identity(int64_t N, int32_t *rowptr, int32_t *col, float *val, piro_stream_t stream)
+{
+    PIRO_ARG(N > 0 && rowptr && col && val, "piro_csr_identity: bad arguments");
+    k_identity<<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(N, rowptr, col, val);
+    PIRO_CHECK_LAUNCH("k_identity");
+    return PIRO_OK;
+}
+
+extern "C" int piro_face_count(int nx, int ny, int nz, int64_t *q, int64_t face_start[7])
+{
+    PIRO_ARG(q && grid_ok(nx, ny, nz), "piro_face_count: bad arguments");
+    const int64_t a = (int64_t)(ny - 2) * (nz - 2), b = (int64_t)(nx - 2) * (nz - 2), c = (int64_t)(nx - 2) * (ny - 2);
+    const int64_t len[6] = {a, a, b, b, c, c};
+    if (face_start) {
+        face_start[0] = 0;
+        for (int f = 0; f < 6; ++f) face_start[f + 1] = face_start[f] + len[f];
+    }
+    *q = 2 * (a + b + c);
+    return PIRO_OK;
+}
+
+extern "C" int piro_face_lists(int nx, int ny, int nz, uint32_t *idx, piro_stream_t stream)
+{
+    PIRO_ARG(idx && grid_ok(nx, ny, nz), "piro_face_lists: bad arguments");
+    Grid g{nx, ny, nz, (int64_t)nx * ny};
+    const int64_t a = (int64_t)(ny - 2) * (nz - 2), b = (int64_t)(nx - 2) * (nz - 2), c = (int64_t)(nx - 2) * (ny - 2);
+    const int64_t Q = 2 * (a + b + c);
+    k_faces<<<grid_for(Q, 256, 4), 256, 0, as_stream(stream)>>>(g, a, b, c, idx);
+    PIRO_CHECK_LAUNCH("k_faces");
+    return PIRO_OK;
+}

@@ -1,0 +1,95 @@
+// common.cuh -- shared helpers of the piro_b200 CUDA library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <string>
+
+#include "piro.h"
+
+namespace piro {
+
+// Per-thread message for piro_last_error().
+void set_error(const char *fmt, ...);
+
+inline cudaStream_t as_stream(piro_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// B200: 148 SMs; launch grids are sized against the device's SM count.
+int sm_count();
+
+inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Grid size for a grid-stride loop over n items with `per_block` items per block.
+inline unsigned grid_for(int64_t n, int64_t per_block, int blocks_per_sm = 8)
+{
+    int64_t want = cdiv(n, per_block);
+    int64_t cap = (int64_t)sm_count() * blocks_per_sm * 16;
+    if (want < 1) want = 1;
+    return (unsigned)(want < cap ? want : cap);
+}
+
+}  // namespace piro
+
+#define PIRO_CHECK_LAUNCH(what)                                                              \
+    do {                                                                                     \
+        cudaError_t e_ = cudaGetLastError();                                                 \
+        if (e_ != cudaSuccess) {                                                             \
+            piro::set_error("%s: %s", what, cudaGetErrorString(e_));                        \
+            return PIRO_ERR_CUDA;                                                            \
+        }                                                                                    \
+    } while (0)
+
+#define PIRO_CUDA(call)                                                                      \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            piro::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                            __LINE__);                                                       \
+            return PIRO_ERR_CUDA;                                                            \
+        }                                                                                    \
+    } while (0)
+
+#define PIRO_ARG(cond, msg)                         \
+    do {                                            \
+        if (!(cond)) {                              \
+            piro::set_error("%s", msg);             \
+            return PIRO_ERR_ARG;                    \
+        }                                           \
+    } while (0)
+
+// Device-side helpers --------------------------------------------------------
+namespace piro {
+
+// Reference arithmetic without contraction: (a*b) rounded, then +.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+
+// Interior test of SpMVCSR.cl:29-32 (grid sizes are ghost-inclusive).
+__device__ __forceinline__ bool interior(int64_t i, int nx, int ny, int nz)
+{
+    int64_t sxy = (int64_t)nx * ny;
+    int z = (int)(i / sxy);
+    int64_t rem = i - (int64_t)z * sxy;
+    int y = (int)(rem / nx);
+    int x = (int)(rem - (int64_t)y * nx);
+    return x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int warp_sum_i(int v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace piro

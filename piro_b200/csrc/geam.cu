@@ -1,0 +1,287 @@
+// geam.cu -- csrgeam (the v.grad merge of operator&), A + beta*B for the
+// backward-Euler matrix, and the device row-pointer scan they share.
+//
+// The reference computes row counts, then runs prefixsum.cl N times from the
+// host with a clFinish after each (src/kernelcsrgeam.cpp:55-62).  Here the
+// counts are written straight into rowptr[1..N] and scanned in place by a
+// three-pass block scan (block sums -> scan of block sums -> block-local scan
+// plus offset), two launches plus one small single-block launch regardless of
+// N.  The block sums live in caller-provided workspace.
+#include "common.cuh"
+
+namespace piro {
+namespace {
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanChunk = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int64_t block_inclusive_scan(int64_t v, int64_t *s_warp)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int64_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    if (lane == 31) s_warp[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        int64_t t = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int64_t q = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += q;
+        }
+        s_warp[lane] = t;
+    }
+    __syncthreads();
+    if (w > 0) v += s_warp[w - 1];
+    __syncthreads();
+    return v;
+}
+
+// Pass 1: per-chunk sums of a[0..n).
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(int64_t n, const int32_t *__restrict__ a,
+                                                            int64_t *__restrict__ sums)
+{
+    __shared__ int64_t s_warp[32];
+    const int64_t base = (int64_t)blockIdx.x * kScanChunk;
+    int64_t v = 0;
+#pragma unroll
+    for (int t = 0; t < kScanItems; ++t) {
+        const int64_t i = base + (int64_t)threadIdx.x * kScanItems + t;
+        if (i < n) v += a[i];
+    }
+    v = block_inclusive_scan(v, s_warp);
+    if (threadIdx.x == blockDim.x - 1) sums[blockIdx.x] = v;
+}
+
+// Pass 2: exclusive scan of the chunk sums, one block, carried across rounds.
+__global__ void __launch_bounds__(kScanThreads) k_scan_offsets(int64_t nb, int64_t *__restrict__ sums)
+{
+    __shared__ int64_t s_warp[32];
+    __shared__ int64_t s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (int64_t b0 = 0; b0 < nb; b0 += kScanThreads) {
+        const int64_t i = b0 + threadIdx.x;
+        const int64_t v = i < nb ? sums[i] : 0;
+        const int64_t inc = block_inclusive_scan(v, s_warp);
+        const int64_t carry = s_carry;
+        if (i < nb) sums[i] = carry + inc - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) s_carry = carry + inc;
+        __syncthreads();
+    }
+}
+
+// Pass 3: in-place inclusive scan of a[0..n) plus the chunk offset.
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(int64_t n, int32_t *__restrict__ a,
+                                                             const int64_t *__restrict__ offs)
+{
+    __shared__ int64_t s_warp[32];
+    const int64_t base = (int64_t)blockIdx.x * kScanChunk;
+    int64_t loc[kScanItems];
+    int64_t v = 0;
+#pragma unroll
+    for (int t = 0; t < kScanItems; ++t) {
+        const int64_t i = base + (int64_t)threadIdx.x * kScanItems + t;
+        loc[t] = i < n ? a[i] : 0;
+        v += loc[t];
+    }
+    int64_t run = block_inclusive_scan(v, s_warp) - v + offs[blockIdx.x];
+#pragma unroll
+    for (int t = 0; t < kScanItems; ++t) {
+        const int64_t i = base + (int64_t)threadIdx.x * kScanItems + t;
+        run += loc[t];
+        if (i < n) a[i] = (int32_t)run;
+    }
+}
+
+// Counts for csrgeam_1.cl: lenA + lenB + lenC (no dedup, csrgeam_1.cl:27-67).
+__global__ void k_geam3_count(int64_t N, const int32_t *__restrict__ rpA, const int32_t *__restrict__ rpB,
+                              const int32_t *__restrict__ rpC, int32_t *__restrict__ rpD)
+{
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (int64_t)gridDim.x * blockDim.x) {
+        rpD[r + 1] = (rpA[r + 1] - rpA[r]) + (rpB[r + 1] - rpB[r]) + (rpC[r + 1] - rpC[r]);
+        if (r == 0) rpD[0] = 0;
+    }
+}
+
+// csrgeam_3.cl:21-88: three-way merge, ties A before B before C, tails
+// appended A, B, C; values scaled by v[row + comp*N].
+__global__ void k_geam3_fill(int64_t N, const int32_t *__restrict__ rpA, const int32_t *__restrict__ cA,
+                             const float *__restrict__ vA, const int32_t *__restrict__ rpB,
+                             const int32_t *__restrict__ cB, const float *__restrict__ vB,
+                             const int32_t *__restrict__ rpC, const int32_t *__restrict__ cC,
+                             const float *__restrict__ vC, const float *__restrict__ v,
+                             const int32_t *__restrict__ rpD, int32_t *__restrict__ cD, float *__restrict__ vD)
+{
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < N;
+         row += (int64_t)gridDim.x * blockDim.x) {
+        int32_t i = rpA[row], ie = rpA[row + 1];
+        int32_t j = rpB[row], je = rpB[row + 1];
+        int32_t k = rpC[row], ke = rpC[row + 1];
+        int64_t d = rpD[row];
+        const float sa = v[row], sb = v[N + row], sc = v[2 * N + row];
+        while (i < ie && j < je && k < ke) {
+            const int32_t a = cA[i], b = cB[j], c = cC[k];
+            const int32_t m = min(a, min(c, b));
+            if (a == m) { cD[d] = a; vD[d] = __fmul_rn(vA[i], sa); ++i; }
+            else if (b == m) { cD[d] = b; vD[d] = __fmul_rn(vB[j], sb); ++j; }
+            else { cD[d] = c; vD[d] = __fmul_rn(vC[k], sc); ++k; }
+            ++d;
+        }
+        for (; i < ie; ++i, ++d) { cD[d] = cA[i]; vD[d] = __fmul_rn(vA[i], sa); }
+        for (; j < je; ++j, ++d) { cD[d] = cB[j]; vD[d] = __fmul_rn(vB[j], sb); }
+        for (; k < ke; ++k, ++d) { cD[d] = cC[k]; vD[d] = __fmul_rn(vC[k], sc); }
+    }
+}
+
+constexpr int kUnionMax = 64;
+
+// Sorted unique union of two rows' columns in a local array; -1 on overflow.
+__device__ __forceinline__ int row_union(const int32_t *__restrict__ ca, int na, const int32_t *__restrict__ cb, int nb,
+                                         int32_t *u)
+{
+    if (na + nb > kUnionMax) return -1;
+    int n = 0;
+    for (int t = 0; t < na + nb; ++t) {
+        const int32_t c = t < na ? ca[t] : cb[t - na];
+        int p = n;
+        bool dup = false;
+        for (int q = 0; q < n; ++q)
+            if (u[q] == c) { dup = true; break; }
+        if (dup) continue;
+        while (p > 0 && u[p - 1] > c) { u[p] = u[p - 1]; --p; }
+        u[p] = c;
+        ++n;
+    }
+    return n;
+}
+
+__global__ void k_geam2_count(int64_t N, const int32_t *__restrict__ rpA, const int32_t *__restrict__ cA,
+                              const int32_t *__restrict__ rpB, const int32_t *__restrict__ cB,
+                              int32_t *__restrict__ rpD, int *__restrict__ err)
+{
+    int32_t u[kUnionMax];
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (int64_t)gridDim.x * blockDim.x) {
+        const int n = row_union(cA + rpA[r], rpA[r + 1] - rpA[r], cB + rpB[r], rpB[r + 1] - rpB[r], u);
+        if (n < 0) { atomicExch(err, 1); rpD[r + 1] = 0; }
+        else rpD[r + 1] = n;
+        if (r == 0) rpD[0] = 0;
+    }
+}
+
+__global__ void k_geam2_fill(int64_t N, const int32_t *__restrict__ rpA, const int32_t *__restrict__ cA,
+                             const float *__restrict__ vA, float beta, const int32_t *__restrict__ rpB,
+                             const int32_t *__restrict__ cB, const float *__restrict__ vB,
+                             const int32_t *__restrict__ rpD, int32_t *__restrict__ cD, float *__restrict__ vD)
+{
+    int32_t u[kUnionMax];
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t a0 = rpA[r], a1 = rpA[r + 1], b0 = rpB[r], b1 = rpB[r + 1];
+        const int n = row_union(cA + a0, a1 - a0, cB + b0, b1 - b0, u);
+        if (n < 0) continue;
+        const int64_t d0 = rpD[r];
+        for (int t = 0; t < n; ++t) {
+            const int32_t c = u[t];
+            float acc = 0.0f;
+            bool have = false;
+            for (int32_t a = a0; a < a1; ++a)
+                if (cA[a] == c) { acc = have ? __fadd_rn(acc, vA[a]) : vA[a]; have = true; }
+            for (int32_t b = b0; b < b1; ++b)
+                if (cB[b] == c) {
+                    const float t2 = __fmul_rn(beta, vB[b]);
+                    acc = have ? __fadd_rn(acc, t2) : t2;
+                    have = true;
+                }
+            cD[d0 + t] = c;
+            vD[d0 + t] = acc;
+        }
+    }
+}
+
+}  // namespace
+
+// In-place scan of rowptr[1..N] (counts -> inclusive sums); rowptr[0] = 0
+// must already be set.  Exposed to the other translation units.
+int scan_rowptr_inplace(int64_t N, int32_t *rowptr, void *work, size_t work_bytes, cudaStream_t s)
+{
+    const int64_t nb = cdiv(N, kScanChunk);
+    PIRO_ARG(work && work_bytes >= sizeof(int64_t) * (size_t)nb, "scan: workspace too small");
+    int64_t *sums = static_cast<int64_t *>(work);
+    k_scan_sums<<<(unsigned)nb, kScanThreads, 0, s>>>(N, rowptr + 1, sums);
+    PIRO_CHECK_LAUNCH("k_scan_sums");
+    k_scan_offsets<<<1, kScanThreads, 0, s>>>(nb, sums);
+    PIRO_CHECK_LAUNCH("k_scan_offsets");
+    k_scan_apply<<<(unsigned)nb, kScanThreads, 0, s>>>(N, rowptr + 1, sums);
+    PIRO_CHECK_LAUNCH("k_scan_apply");
+    return PIRO_OK;
+}
+
+size_t scan_workspace_bytes(int64_t N) { return sizeof(int64_t) * (size_t)(cdiv(N, kScanChunk) + 1) + 256; }
+
+}  // namespace piro
+
+using namespace piro;
+
+extern "C" int piro_scan_workspace(int64_t nrows, size_t *bytes)
+{
+    PIRO_ARG(bytes && nrows >= 0, "piro_scan_workspace: bad arguments");
+    *bytes = scan_workspace_bytes(nrows);
+    return PIRO_OK;
+}
+
+extern "C" int piro_csrgeam3(int64_t N, const int32_t *rpA, const int32_t *cA, const float *vA, const int32_t *rpB,
+                             const int32_t *cB, const float *vB, const int32_t *rpC, const int32_t *cC,
+                             const float *vC, const float *v, int32_t *rpD, int32_t *cD, float *vD, void *work,
+                             size_t work_bytes, piro_stream_t stream)
+{
+    PIRO_ARG(N > 0 && rpA && cA && vA && rpB && cB && vB && rpC && cC && vC && v && rpD && cD && vD,
+             "piro_csrgeam3: null argument");
+    PIRO_ARG(N < INT32_MAX, "piro_csrgeam3: too many rows");
+    cudaStream_t s = as_stream(stream);
+    k_geam3_count<<<grid_for(N, 256, 8), 256, 0, s>>>(N, rpA, rpB, rpC, rpD);
+    PIRO_CHECK_LAUNCH("k_geam3_count");
+    int rc = scan_rowptr_inplace(N, rpD, work, work_bytes, s);
+    if (rc) return rc;
+    k_geam3_fill<<<grid_for(N, 128, 8), 128, 0, s>>>(N, rpA, cA, vA, rpB, cB, vB, rpC, cC, vC, v, rpD, cD, vD);
+    PIRO_CHECK_LAUNCH("k_geam3_fill");
+    return PIRO_OK;
+}
+
+extern "C" int piro_csrgeam2_count(int64_t N, const int32_t *rpA, const int32_t *cA, const int32_t *rpB,
+                                   const int32_t *cB, int32_t *rpD, void *work, size_t work_bytes,
+                                   piro_stream_t stream)
+{
+    PIRO_ARG(N > 0 && rpA && cA && rpB && cB && rpD, "piro_csrgeam2_count: null argument");
+    cudaStream_t s = as_stream(stream);
+    // the last 256 bytes of the workspace hold the overflow flag
+    PIRO_ARG(work && work_bytes >= scan_workspace_bytes(N), "piro_csrgeam2_count: workspace too small");
+    int *err = reinterpret_cast<int *>(static_cast<char *>(work) + work_bytes - sizeof(int));
+    PIRO_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    k_geam2_count<<<grid_for(N, 256, 8), 256, 0, s>>>(N, rpA, cA, rpB, cB, rpD, err);
+    PIRO_CHECK_LAUNCH("k_geam2_count");
+    int rc = scan_rowptr_inplace(N, rpD, work, work_bytes - 256, s);
+    if (rc) return rc;
+    int h_err = 0;
+    PIRO_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PIRO_CUDA(cudaStreamSynchronize(s));
+    if (h_err) {
+        piro::set_error("piro_csrgeam2_count: a row has more than %d combined entries", kUnionMax);
+        return PIRO_ERR_ARG;
+    }
+    return PIRO_OK;
+}
+
+extern "C" int piro_csrgeam2_fill(int64_t N, const int32_t *rpA, const int32_t *cA, const float *vA, float beta,
+                                  const int32_t *rpB, const int32_t *cB, const float *vB, const int32_t *rpD,
+                                  int32_t *cD, float *vD, piro_stream_t stream)
+{
+    PIRO_ARG(N > 0 && rpA && cA && vA && rpB && cB && vB && rpD && cD && vD, "piro_csrgeam2_fill: null argument");
+    k_geam2_fill<<<grid_for(N, 128, 8), 128, 0, as_stream(stream)>>>(N, rpA, cA, vA, beta, rpB, cB, vB, rpD, cD, vD);
+    PIRO_CHECK_LAUNCH("k_geam2_fill");
+    return PIRO_OK;
+}

@@ -1,0 +1,329 @@
+// spmv.cu -- time-step kernels: CSR SpMV with the forward-Euler update fused
+// in its epilogue, the backward-Euler residual form, COO SpMV by warp-segmented
+// reduction, HT SpMV by row lookups, the matrix-free 7-point stencil, setBC and
+// the elementwise kernels.
+//
+// CSR layout in HBM: rowptr int32[N+1], col int32[nnz], val float[nnz].  The
+// CSR kernels are HBM-bound (8 bytes per nonzero + 12 per row); a block takes
+// a tile of kTileRows consecutive rows, streams the tile's col/val range into
+// shared memory with 16-byte vector loads (fully coalesced, no reuse through
+// L1), then each thread reduces its own row from shared memory in storage
+// order -- the reference's summation order -- so results are bit-exact with
+// SpMVCSR.cl.  Field gathers u[col] hit L2 (the 7 neighbours of a tile lie in
+// five x-lines of three z-planes).
+#include "common.cuh"
+#include "csr_tile.cuh"
+
+namespace piro {
+namespace {
+
+// mode 0: SpMVCSR (out = u + sum), mode 1: SpMVCSR_I1 (out = u - sum).
+template <int kMode>
+__global__ void __launch_bounds__(kTileRows) k_csr_step(int nx, int ny, int nz, int64_t N,
+                                                        const int32_t *__restrict__ rowptr,
+                                                        const int32_t *__restrict__ col,
+                                                        const float *__restrict__ val, float dt,
+                                                        const float *__restrict__ u, float *__restrict__ out)
+{
+    __shared__ int32_t s_rp[kTileRows + 1];
+    __shared__ int32_t s_col[kTileCap];
+    __shared__ float s_val[kTileCap];
+    for (int64_t r0 = (int64_t)blockIdx.x * kTileRows; r0 < N; r0 += (int64_t)gridDim.x * kTileRows) {
+        const int nrows = (int)(N - r0 < kTileRows ? N - r0 : kTileRows);
+        for (int t = threadIdx.x; t <= nrows; t += blockDim.x) s_rp[t] = rowptr[r0 + t];
+        __syncthreads();
+        const int64_t s = s_rp[0], e = s_rp[nrows];
+        const bool staged = e - s <= kTileCap;
+        if (staged) stage_tile(col, val, s, e, s_col, s_val);
+        __syncthreads();
+        if (threadIdx.x < nrows) {
+            const int64_t row = r0 + threadIdx.x;
+            const int k0 = s_rp[threadIdx.x], k1 = s_rp[threadIdx.x + 1];
+            float result = 0.0f;
+            if (staged) {
+                for (int k = k0; k < k1; ++k) {
+                    const float t = mul_rn(dt, s_val[k - s]);
+                    result = add_rn(result, mul_rn(t, __ldg(u + s_col[k - s])));
+                }
+            } else {
+                for (int k = k0; k < k1; ++k) {
+                    const float t = mul_rn(dt, val[k]);
+                    result = add_rn(result, mul_rn(t, __ldg(u + col[k])));
+                }
+            }
+            if (interior(row, nx, ny, nz)) out[row] = kMode == 0 ? add_rn(result, u[row]) : sub_rn(u[row], result);
+        }
+        __syncthreads();
+    }
+}
+
+// COO: each warp takes 32 consecutive entries per pass; a segmented inclusive
+// scan over equal row ids gives each row's partial sum in the segment's last
+// lane.  Rows wholly inside the warp's span are stored; rows cut by the span
+// edges are atomically added (at most two contributions for rows of <= 32
+// entries, so the result does not depend on their order).  acc must be zero.
+__global__ void k_coo_segsum(int64_t nnz, const int32_t *__restrict__ rows, const int32_t *__restrict__ cols,
+                             const float *__restrict__ vals, const float *__restrict__ u, float *__restrict__ acc)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * 32; base < nnz; base += nwarps * 32) {
+        const int64_t k = base + lane;
+        const bool valid = k < nnz;
+        int r = valid ? __ldcs(rows + k) : -1;
+        float p = valid ? __fmul_rn(__ldcs(vals + k), __ldg(u + __ldcs(cols + k))) : 0.0f;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const float q = __shfl_up_sync(0xffffffffu, p, o);
+            const int rq = __shfl_up_sync(0xffffffffu, r, o);
+            if (lane >= o && rq == r) p = __fadd_rn(q, p);
+        }
+        const int rnext = __shfl_down_sync(0xffffffffu, r, 1);
+        const bool seg_end = valid && (lane == 31 || rnext != r);
+        if (seg_end) {
+            // segment start lane: first lane of this row within the warp
+            const bool cut_left = (k - lane > 0) && __ldg(rows + (base - 1)) == r &&
+                                  // the row reaches lane 0 of this span
+                                  __ldg(rows + base) == r;
+            const bool cut_right = (lane == 31) && (k + 1 < nnz) && __ldg(rows + k + 1) == r;
+            if (cut_left || cut_right) atomicAdd(acc + r, p);
+            else acc[r] = p;
+        }
+    }
+}
+
+// out = dt*acc (SpMVCOO's C[row] = deltat*result) or u + dt*acc.
+// acc and out may be the same buffer (element-wise, same index).
+__global__ void k_scale_add(int64_t n, float dt, const float *acc, const float *u, float *out)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float c = __fmul_rn(dt, acc[i]);
+        out[i] = u ? __fadd_rn(u[i], c) : c;
+    }
+}
+
+// HT lookup with linear probing (SpMVHT.cl:1-20); bounded by ts probes.
+__device__ __forceinline__ float ht_get(int64_t key, const int64_t *__restrict__ keys, const float *__restrict__ vals,
+                                        int64_t ts)
+{
+    int64_t h = key % ts;
+    for (int64_t a = 0; a < ts; ++a) {
+        const int64_t k = __ldg(keys + h);
+        if (k == key) return __ldg(vals + h);
+        if (k == -1) return 0.0f;
+        h = h + 1 == ts ? 0 : h + 1;
+    }
+    return 0.0f;
+}
+
+__global__ void k_ht_spmv(int nx, int ny, int nz, int64_t N, const int64_t *__restrict__ keys,
+                          const float *__restrict__ vals, int64_t ts, float dt, int fe, const float *__restrict__ u,
+                          float *__restrict__ out)
+{
+    const int64_t sxy = (int64_t)nx * ny;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int z = (int)(i / sxy);
+        const int64_t rem = i - (int64_t)z * sxy;
+        const int y = (int)(rem / nx);
+        const int x = (int)(rem - (int64_t)y * nx);
+        // candidate columns in ascending order
+        int64_t cand[7];
+        int n = 0;
+        if (z > 0) cand[n++] = i - sxy;
+        if (y > 0) cand[n++] = i - nx;
+        if (x > 0) cand[n++] = i - 1;
+        cand[n++] = i;
+        if (x < nx - 1) cand[n++] = i + 1;
+        if (y < ny - 1) cand[n++] = i + nx;
+        if (z < nz - 1) cand[n++] = i + sxy;
+        float sum = 0.0f;
+        for (int t = 0; t < n; ++t) {
+            // absent keys give 0, adding 0*u exactly as the reference's full column loop does
+            const float h = ht_get(i * N + cand[t], keys, vals, ts);
+            sum = __fadd_rn(sum, __fmul_rn(h, __ldg(u + cand[t])));
+        }
+        const float c = __fmul_rn(dt, sum);
+        out[i] = fe ? __fadd_rn(u[i], c) : c;
+    }
+}
+
+// Matrix-free 7-point update; one thread per x-cell, blocks tile (x, y) lines.
+__global__ void k_stencil(int nx, int ny, int nz, float idx2, float idy2, float idz2, float dt,
+                          const float *__restrict__ alpha, const float *__restrict__ u, float *__restrict__ out)
+{
+    const int64_t sxy = (int64_t)nx * ny;
+    const int64_t N = sxy * nz;
+    for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < N; id += (int64_t)gridDim.x * blockDim.x) {
+        const int z = (int)(id / sxy);
+        const int64_t rem = id - (int64_t)z * sxy;
+        const int y = (int)(rem / nx);
+        const int x = (int)(rem - (int64_t)y * nx);
+        const float c = __ldg(u + id);
+        if (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1) {
+            const float c2 = __fmul_rn(2.0f, c);
+            const float lx = __fmul_rn(__fsub_rn(__fadd_rn(__ldg(u + id + 1), __ldg(u + id - 1)), c2), idx2);
+            const float ly = __fmul_rn(__fsub_rn(__fadd_rn(__ldg(u + id + nx), __ldg(u + id - nx)), c2), idy2);
+            const float lz = __fmul_rn(__fsub_rn(__fadd_rn(__ldg(u + id + sxy), __ldg(u + id - sxy)), c2), idz2);
+            const float lap = __fadd_rn(__fadd_rn(lx, ly), lz);
+            const float a = alpha ? __ldg(alpha + id) : 1.0f;
+            out[id] = __fadd_rn(c, __fmul_rn(dt, __fmul_rn(a, lap)));
+        } else {
+            out[id] = c;
+        }
+    }
+}
+
+__global__ void k_set_bc(int64_t q, const uint32_t *__restrict__ idx, const float *__restrict__ src,
+                         float *__restrict__ dst)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < q; t += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t i = idx[t];
+        dst[i] = src[i];
+    }
+}
+
+__global__ void k_vec_op(int op, int64_t n, const float *__restrict__ b, const float *__restrict__ c,
+                         float *__restrict__ a)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float x = b[i], y = c[i];
+        a[i] = op == 0 ? __fadd_rn(x, y) : op == 1 ? __fsub_rn(x, y) : op == 2 ? __fmul_rn(x, y) : __fdiv_rn(x, y);
+    }
+}
+
+__global__ void k_vec_op_scalar(int op, int64_t n, float s, const float *__restrict__ c, float *__restrict__ a)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float y = c[i];
+        a[i] = op == 0 ? __fadd_rn(s, y) : op == 1 ? __fsub_rn(y, s) : op == 2 ? __fmul_rn(s, y) : __fdiv_rn(y, s);
+    }
+}
+
+__global__ void k_vec_urf(int64_t n, float *__restrict__ a, float *__restrict__ c, float urf)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float t = a[i];
+        const float an = __fadd_rn(t, __fmul_rn(c[i], urf));
+        a[i] = an;
+        c[i] = __fsub_rn(an, t);
+    }
+}
+
+bool grid_ok(int nx, int ny, int nz) { return nx >= 3 && ny >= 3 && nz >= 3; }
+
+template <int kMode>
+int launch_csr_step(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val, float dt,
+                    const float *u, float *out, piro_stream_t stream)
+{
+    PIRO_ARG(grid_ok(nx, ny, nz), "csr step: grid sizes must be >= 3");
+    PIRO_ARG(rowptr && col && val && u && out, "csr step: null pointer");
+    PIRO_ARG(u != out, "csr step: u and out must differ (the reference writes a fresh buffer)");
+    const int64_t N = (int64_t)nx * ny * nz;
+    k_csr_step<kMode><<<grid_for(N, kTileRows, 6), kTileRows, 0, as_stream(stream)>>>(nx, ny, nz, N, rowptr, col, val,
+                                                                                      dt, u, out);
+    PIRO_CHECK_LAUNCH("k_csr_step");
+    return PIRO_OK;
+}
+
+}  // namespace
+}  // namespace piro
+
+using namespace piro;
+
+extern "C" int piro_csr_fe_step(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val,
+                                float dt, const float *u, float *out, piro_stream_t stream)
+{
+    return launch_csr_step<0>(nx, ny, nz, rowptr, col, val, dt, u, out, stream);
+}
+
+extern "C" int piro_csr_i1(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val,
+                           float dt, const float *u, float *out, piro_stream_t stream)
+{
+    return launch_csr_step<1>(nx, ny, nz, rowptr, col, val, dt, u, out, stream);
+}
+
+static int coo_common(int64_t N, int64_t nnz, const int32_t *rows, const int32_t *cols, const float *vals, float dt,
+                      const float *u, float *out, bool fe, piro_stream_t stream)
+{
+    PIRO_ARG(N > 0 && nnz >= 0 && rows && cols && vals && u && out, "coo spmv: bad arguments");
+    PIRO_ARG(u != out, "coo spmv: u and out must differ");
+    cudaStream_t s = as_stream(stream);
+    // out doubles as the accumulator: zero it, sum into it, then scale in place.
+    PIRO_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * N, s));
+    if (nnz > 0) {
+        k_coo_segsum<<<grid_for(nnz, 256, 8), 256, 0, s>>>(nnz, rows, cols, vals, u, out);
+        PIRO_CHECK_LAUNCH("k_coo_segsum");
+    }
+    k_scale_add<<<grid_for(N, 256, 8), 256, 0, s>>>(N, dt, out, fe ? u : nullptr, out);
+    PIRO_CHECK_LAUNCH("k_scale_add");
+    return PIRO_OK;
+}
+
+extern "C" int piro_coo_spmv(int64_t N, int64_t nnz, const int32_t *rows, const int32_t *cols, const float *vals,
+                             float dt, const float *u, float *out, piro_stream_t stream)
+{
+    return coo_common(N, nnz, rows, cols, vals, dt, u, out, false, stream);
+}
+
+extern "C" int piro_coo_fe_step(int64_t N, int64_t nnz, const int32_t *rows, const int32_t *cols, const float *vals,
+                                float dt, const float *u, float *out, piro_stream_t stream)
+{
+    return coo_common(N, nnz, rows, cols, vals, dt, u, out, true, stream);
+}
+
+extern "C" int piro_ht_spmv(int nx, int ny, int nz, const int64_t *keys, const float *vals, int64_t ts, float dt, int fe,
+                            const float *u, float *out, piro_stream_t stream)
+{
+    PIRO_ARG(grid_ok(nx, ny, nz) && keys && vals && ts > 0 && u && out && u != out, "piro_ht_spmv: bad arguments");
+    const int64_t N = (int64_t)nx * ny * nz;
+    k_ht_spmv<<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(nx, ny, nz, N, keys, vals, ts, dt, fe, u, out);
+    PIRO_CHECK_LAUNCH("k_ht_spmv");
+    return PIRO_OK;
+}
+
+extern "C" int piro_stencil_fe_step(int nx, int ny, int nz, float idx2, float idy2, float idz2, float dt,
+                                    const float *alpha, const float *u, float *out, piro_stream_t stream)
+{
+    PIRO_ARG(grid_ok(nx, ny, nz) && u && out && u != out, "piro_stencil_fe_step: bad arguments");
+    const int64_t N = (int64_t)nx * ny * nz;
+    k_stencil<<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(nx, ny, nz, idx2, idy2, idz2, dt, alpha, u, out);
+    PIRO_CHECK_LAUNCH("k_stencil");
+    return PIRO_OK;
+}
+
+extern "C" int piro_set_bc(int64_t q, const uint32_t *idx, const float *src, float *dst, piro_stream_t stream)
+{
+    PIRO_ARG(q >= 0 && (q == 0 || (idx && src && dst)), "piro_set_bc: bad arguments");
+    if (q == 0) return PIRO_OK;
+    k_set_bc<<<grid_for(q, 256, 4), 256, 0, as_stream(stream)>>>(q, idx, src, dst);
+    PIRO_CHECK_LAUNCH("k_set_bc");
+    return PIRO_OK;
+}
+
+extern "C" int piro_vec_op(int op, int64_t n, const float *b, const float *c, float *a, piro_stream_t stream)
+{
+    PIRO_ARG(op >= 0 && op <= 3 && n >= 0 && (n == 0 || (a && b && c)), "piro_vec_op: bad arguments");
+    if (n == 0) return PIRO_OK;
+    k_vec_op<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(op, n, b, c, a);
+    PIRO_CHECK_LAUNCH("k_vec_op");
+    return PIRO_OK;
+}
+
+extern "C" int piro_vec_op_scalar(int op, int64_t n, float s, const float *c, float *a, piro_stream_t stream)
+{
+    PIRO_ARG(op >= 0 && op <= 3 && n >= 0 && (n == 0 || (a && c)), "piro_vec_op_scalar: bad arguments");
+    if (n == 0) return PIRO_OK;
+    k_vec_op_scalar<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(op, n, s, c, a);
+    PIRO_CHECK_LAUNCH("k_vec_op_scalar");
+    return PIRO_OK;
+}
+
+extern "C" int piro_vec_urf(int64_t n, float *a, float *c, float urf, piro_stream_t stream)
+{
+    PIRO_ARG(n >= 0 && (n == 0 || (a && c)), "piro_vec_urf: bad arguments");
+    if (n == 0) return PIRO_OK;
+    k_vec_urf<<<grid_for(n, 256, 8), 256, 0, as_stream(stream)>>>(n, a, c, urf);
+    PIRO_CHECK_LAUNCH("k_vec_urf");
+    return PIRO_OK;
+}

@@ -1,0 +1,289 @@
+"""Torch-facing wrappers of the C ABI (include/piro.h, layer 1).
+
+Device memory comes from torch; every call goes through libpiro_b200.so on
+torch's current CUDA stream.  Tensors must be contiguous CUDA tensors of the
+documented dtype.  There is no CPU path: a non-CUDA tensor is an error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from ._lib import BeInfo, check, lib
+
+i32, f32 = torch.int32, torch.float32
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _p(t: torch.Tensor | None) -> int | None:
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("piro_b200 kernels take CUDA tensors only (no CPU fallback)")
+    if not t.is_contiguous():
+        raise ValueError("tensor must be contiguous")
+    return t.data_ptr()
+
+
+def _need(t: torch.Tensor, dtype: torch.dtype, n: int | None = None, name: str = "tensor") -> None:
+    if t.dtype != dtype:
+        raise TypeError(f"{name}: expected {dtype}, got {t.dtype}")
+    if n is not None and t.numel() < n:
+        raise ValueError(f"{name}: expected at least {n} elements, got {t.numel()}")
+
+
+def cells(nx: int, ny: int, nz: int) -> int:
+    return int(nx) * int(ny) * int(nz)
+
+
+# ----------------------------------------------------------------- assembly
+def laplacian_nnz(nx, ny, nz) -> int:
+    v = C.c_int64()
+    check(lib().piro_laplacian_nnz(nx, ny, nz, C.byref(v)), "piro_laplacian_nnz")
+    return v.value
+
+
+def gradient_nnz(nx, ny, nz, axis) -> int:
+    v = C.c_int64()
+    check(lib().piro_gradient_nnz(nx, ny, nz, axis, C.byref(v)), "piro_gradient_nnz")
+    return v.value
+
+
+def csr_laplacian(nx, ny, nz, scheme, norm, device="cuda"):
+    N, nnz = cells(nx, ny, nz), laplacian_nnz(nx, ny, nz)
+    rp = torch.empty(N + 1, dtype=i32, device=device)
+    col = torch.empty(nnz, dtype=i32, device=device)
+    val = torch.empty(nnz, dtype=f32, device=device)
+    check(lib().piro_csr_laplacian(nx, ny, nz, scheme, float(norm), _p(rp), _p(col), _p(val), _stream()),
+          "piro_csr_laplacian")
+    return rp, col, val
+
+
+def coo_laplacian(nx, ny, nz, scheme, norm, device="cuda"):
+    nnz = laplacian_nnz(nx, ny, nz)
+    rows = torch.empty(nnz, dtype=i32, device=device)
+    col = torch.empty(nnz, dtype=i32, device=device)
+    val = torch.empty(nnz, dtype=f32, device=device)
+    check(lib().piro_coo_laplacian(nx, ny, nz, scheme, float(norm), _p(rows), _p(col), _p(val), _stream()),
+          "piro_coo_laplacian")
+    return rows, col, val
+
+
+def csr_gradient(nx, ny, nz, scheme, axis, norm, device="cuda"):
+    N, nnz = cells(nx, ny, nz), gradient_nnz(nx, ny, nz, axis)
+    rp = torch.empty(N + 1, dtype=i32, device=device)
+    col = torch.empty(nnz, dtype=i32, device=device)
+    val = torch.empty(nnz, dtype=f32, device=device)
+    check(lib().piro_csr_gradient(nx, ny, nz, scheme, axis, float(norm), _p(rp), _p(col), _p(val), _stream()),
+          "piro_csr_gradient")
+    return rp, col, val
+
+
+def csr_rowscale(rowptr, val, s):
+    """In place: val[k] *= s[row(k)]."""
+    _need(rowptr, i32, name="rowptr")
+    _need(val, f32, name="val")
+    _need(s, f32, rowptr.numel() - 1, "s")
+    check(lib().piro_csr_rowscale(rowptr.numel() - 1, _p(rowptr), _p(val), _p(s), _stream()), "piro_csr_rowscale")
+    return val
+
+
+def csr_identity(N, device="cuda"):
+    rp = torch.empty(N + 1, dtype=i32, device=device)
+    col = torch.empty(N, dtype=i32, device=device)
+    val = torch.empty(N, dtype=f32, device=device)
+    check(lib().piro_csr_identity(N, _p(rp), _p(col), _p(val), _stream()), "piro_csr_identity")
+    return rp, col, val
+
+
+# ---------------------------------------------------------------- hash table
+HT_A, HT_B, HT_C, HT_LF = 3.3608, -0.5552, -0.0143, 0.7  # assets/Data/hashtable.ini
+
+
+def ht_table_size(nnz, N, policy=0, a=HT_A, b=HT_B, c=HT_C, lf=HT_LF) -> int:
+    v = C.c_int64()
+    check(lib().piro_ht_table_size(nnz, N, policy, a, b, c, lf, C.byref(v)), "piro_ht_table_size")
+    return v.value
+
+
+def ht_build(N, rowptr, col, val, ts):
+    keys = torch.empty(ts, dtype=torch.int64, device=rowptr.device)
+    vals = torch.empty(ts, dtype=f32, device=rowptr.device)
+    wb = C.c_size_t()
+    check(lib().piro_ht_build_workspace(ts, C.byref(wb)), "piro_ht_build_workspace")
+    work = torch.empty(wb.value, dtype=torch.uint8, device=rowptr.device)
+    check(lib().piro_ht_build(N, _p(rowptr), _p(col), _p(val), val.numel(), ts, _p(keys), _p(vals), _p(work),
+                              wb.value, _stream()), "piro_ht_build")
+    return keys, vals
+
+
+# ----------------------------------------------------------------- steps
+def csr_fe_step(nx, ny, nz, A, dt, u, out):
+    check(lib().piro_csr_fe_step(nx, ny, nz, _p(A[0]), _p(A[1]), _p(A[2]), float(dt), _p(u), _p(out), _stream()),
+          "piro_csr_fe_step")
+    return out
+
+
+def csr_i1(nx, ny, nz, A, dt, u, out):
+    check(lib().piro_csr_i1(nx, ny, nz, _p(A[0]), _p(A[1]), _p(A[2]), float(dt), _p(u), _p(out), _stream()),
+          "piro_csr_i1")
+    return out
+
+
+def coo_spmv(N, coo, dt, u, out, fe=False):
+    fn = lib().piro_coo_fe_step if fe else lib().piro_coo_spmv
+    check(fn(N, coo[2].numel(), _p(coo[0]), _p(coo[1]), _p(coo[2]), float(dt), _p(u), _p(out), _stream()),
+          "piro_coo_spmv")
+    return out
+
+
+def ht_spmv(nx, ny, nz, keys, vals, dt, u, out, fe=False):
+    check(lib().piro_ht_spmv(nx, ny, nz, _p(keys), _p(vals), keys.numel(), float(dt), int(fe), _p(u), _p(out),
+                             _stream()), "piro_ht_spmv")
+    return out
+
+
+def stencil_fe_step(nx, ny, nz, dt, u, out, alpha=None, idx2=1.0, idy2=1.0, idz2=1.0):
+    check(lib().piro_stencil_fe_step(nx, ny, nz, idx2, idy2, idz2, float(dt), _p(alpha), _p(u), _p(out), _stream()),
+          "piro_stencil_fe_step")
+    return out
+
+
+def set_bc(idx, src, dst):
+    check(lib().piro_set_bc(idx.numel(), _p(idx), _p(src), _p(dst), _stream()), "piro_set_bc")
+    return dst
+
+
+def face_lists(nx, ny, nz, device="cuda"):
+    q = C.c_int64()
+    fs = (C.c_int64 * 7)()
+    check(lib().piro_face_count(nx, ny, nz, C.byref(q), fs), "piro_face_count")
+    idx = torch.empty(q.value, dtype=torch.int32, device=device)  # uint32 bits
+    check(lib().piro_face_lists(nx, ny, nz, _p(idx), _stream()), "piro_face_lists")
+    return idx, list(fs)
+
+
+def vec_op(op, b, c, out=None):
+    out = torch.empty_like(b) if out is None else out
+    check(lib().piro_vec_op(op, b.numel(), _p(b), _p(c), _p(out), _stream()), "piro_vec_op")
+    return out
+
+
+def vec_op_scalar(op, s, c, out=None):
+    out = torch.empty_like(c) if out is None else out
+    check(lib().piro_vec_op_scalar(op, c.numel(), float(s), _p(c), _p(out), _stream()), "piro_vec_op_scalar")
+    return out
+
+
+def vec_urf(a, c, urf):
+    check(lib().piro_vec_urf(a.numel(), _p(a), _p(c), float(urf), _stream()), "piro_vec_urf")
+
+
+# ----------------------------------------------------------------- csrgeam
+def _scan_work(N, device):
+    wb = C.c_size_t()
+    check(lib().piro_scan_workspace(N, C.byref(wb)), "piro_scan_workspace")
+    return torch.empty(wb.value, dtype=torch.uint8, device=device), wb.value
+
+
+def csrgeam3(N, A, B, Cm, v):
+    dev = A[0].device
+    nnz = A[2].numel() + B[2].numel() + Cm[2].numel()
+    rp = torch.empty(N + 1, dtype=i32, device=dev)
+    col = torch.empty(nnz, dtype=i32, device=dev)
+    val = torch.empty(nnz, dtype=f32, device=dev)
+    work, wb = _scan_work(N, dev)
+    check(lib().piro_csrgeam3(N, _p(A[0]), _p(A[1]), _p(A[2]), _p(B[0]), _p(B[1]), _p(B[2]), _p(Cm[0]), _p(Cm[1]),
+                              _p(Cm[2]), _p(v), _p(rp), _p(col), _p(val), _p(work), wb, _stream()), "piro_csrgeam3")
+    return rp, col, val
+
+
+def csrgeam2(N, A, beta, B):
+    dev = A[0].device
+    rp = torch.empty(N + 1, dtype=i32, device=dev)
+    work, wb = _scan_work(N, dev)
+    check(lib().piro_csrgeam2_count(N, _p(A[0]), _p(A[1]), _p(B[0]), _p(B[1]), _p(rp), _p(work), wb, _stream()),
+          "piro_csrgeam2_count")
+    nnz = int(rp[N].item())
+    col = torch.empty(nnz, dtype=i32, device=dev)
+    val = torch.empty(nnz, dtype=f32, device=dev)
+    check(lib().piro_csrgeam2_fill(N, _p(A[0]), _p(A[1]), _p(A[2]), float(beta), _p(B[0]), _p(B[1]), _p(B[2]),
+                                   _p(rp), _p(col), _p(val), _stream()), "piro_csrgeam2_fill")
+    return rp, col, val
+
+
+# ----------------------------------------------------------------- reductions
+class Reducer:
+    """Reusable FP64 dot-product workspace."""
+
+    def __init__(self, n, device="cuda"):
+        wb = C.c_size_t()
+        check(lib().piro_reduce_workspace(n, C.byref(wb)), "piro_reduce_workspace")
+        self.work = torch.zeros(wb.value, dtype=torch.uint8, device=device)
+        self.wb = wb.value
+        self.out = torch.zeros(1, dtype=torch.float64, device=device)
+
+    def dot(self, x, y):
+        check(lib().piro_dot_f64(x.numel(), _p(x), _p(y), _p(self.out), _p(self.work), self.wb, _stream()),
+              "piro_dot_f64")
+        return self.out
+
+
+def dot_f64(x, y):
+    return float(Reducer(x.numel(), x.device).dot(x, y).item())
+
+
+# ----------------------------------------------------------------- backward Euler
+class BESolver:
+    """FP32 Jacobi-PCG inside FP64 iterative refinement for A = I - dt*diag(alpha)*L."""
+
+    def __init__(self, nx, ny, nz, A, alpha):
+        self.keep = (A, alpha)
+        h = C.c_void_p()
+        check(lib().piro_be_create(nx, ny, nz, _p(A[0]), _p(A[1]), _p(A[2]), _p(alpha), _stream(), C.byref(h)),
+              "piro_be_create")
+        self.h = h
+        self.N = cells(nx, ny, nz)
+
+    def solve(self, b, x, rtol=1e-8, max_outer=20, max_inner=20000, strict=True):
+        info = BeInfo()
+        st = lib().piro_be_solve(self.h, _p(b), _p(x), rtol, max_outer, max_inner, C.byref(info))
+        if strict:
+            check(st, "piro_be_solve")
+        return info
+
+    def solution_f64(self):
+        p = C.c_void_p()
+        check(lib().piro_be_solution_f64(self.h, C.byref(p)), "piro_be_solution_f64")
+        return p.value
+
+    def kernel_stats(self, reset=False):
+        """(CG SpMV launches, their total ms by CUDA events, all kernel launches)."""
+        n, ms, k = C.c_longlong(), C.c_double(), C.c_longlong()
+        check(lib().piro_be_kernel_stats(self.h, int(reset), C.byref(n), C.byref(ms), C.byref(k)),
+              "piro_be_kernel_stats")
+        return n.value, ms.value, k.value
+
+    def close(self):
+        if self.h:
+            lib().piro_be_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def be_jli(nx, ny, nz, A, dt, b, tol=1e-5, urf=1.0, maxiter=1000):
+    x = torch.empty_like(b)
+    r = torch.empty_like(b)
+    it = C.c_int()
+    check(lib().piro_be_jli(nx, ny, nz, _p(A[0]), _p(A[1]), _p(A[2]), float(dt), _p(b), _p(x), _p(r), float(tol),
+                            float(urf), maxiter, C.byref(it), _stream()), "piro_be_jli")
+    return x, it.value
