@@ -383,10 +383,11 @@ static int be_capture_chunk(piro_be_solver *s)
     for (int it = 0; it < kChunk; ++it) {
         const float *p_old = s->p[it & 1];
         float *p_new = s->p[(it + 1) & 1];
-        cudaEventRecord(s->ev0[it], s->stream);
+        // External: the record becomes a node of the graph, observable from the host
+        cudaEventRecordWithFlags(s->ev0[it], s->stream, cudaEventRecordExternal);
         k_cg_spmv<<<s->grid_tiles, kTileRows, 0, s->stream>>>(s->nx, s->ny, s->nz, s->N, s->rowptr, s->col, s->val,
                                                               s->alpha, s->z, p_old, p_new, s->q, s->partials, s->st);
-        cudaEventRecord(s->ev1[it], s->stream);
+        cudaEventRecordWithFlags(s->ev1[it], s->stream, cudaEventRecordExternal);
         k_cg_update<<<s->grid_elem, 512, 0, s->stream>>>(s->nx, s->ny, s->nz, s->N, s->alpha, s->dinv, p_new, s->q,
                                                          s->d, s->r, s->z, s->partials, s->st);
     }
@@ -535,6 +536,8 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
                 if (cudaEventElapsedTime(&ms, s->ev0[i], s->ev1[i]) == cudaSuccess) {
                     s->spmv_ms += ms;
                     s->spmv_launches += 1;
+                } else {
+                    (void)cudaGetLastError();  // timing is best effort; do not leak the error
                 }
             }
             seen = s->h_st->iters;
