@@ -169,55 +169,78 @@ def run_piro(args):
     N = nx * ny * nz
     A, alpha = be_problem(torch, ops, cfg)
     nnzA = A[2].numel()
-    solver = ops.BESolver(nx, ny, nz, A, alpha)
+    # inner Krylov operator: matrix-free 7-point (checked against A) and CSR
+    solver = ops.BESolver(nx, ny, nz, A, alpha, stencil=(float(cfg["dt"]), 1.0))
+    solver_csr = ops.BESolver(nx, ny, nz, A, alpha)
+    inner_op = solver.inner_operator
     u0 = torch.from_numpy(cfg["u0"]).cuda()
-    u = u0.clone()
-    x = torch.empty_like(u)
     traj = cfg["steps"]
 
-    def step(i, u, x):
-        if i % traj == 0:
-            u.copy_(u0)
-        info = solver.solve(u, x, rtol=1e-8)
-        return x, u, info
+    def time_steps(sv, steps, warmup, sample_clocks):
+        u = u0.clone()
+        x = torch.empty_like(u)
+        for i in range(warmup):
+            if i % traj == 0:
+                u.copy_(u0)
+            sv.solve(u, x, rtol=1e-8)
+            u, x = x, u
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        sv.kernel_stats(reset=True)
+        clocks = ClockSampler(local) if sample_clocks else None
+        if clocks:
+            time.sleep(0.2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        iters, outers, worst = [], [], 0.0
+        for i in range(steps):
+            if i % traj == 0:
+                u.copy_(u0)
+            info = sv.solve(u, x, rtol=1e-8)
+            u, x = x, u
+            iters.append(info.inner_iterations)
+            outers.append(info.outer_iterations)
+            worst = max(worst, info.rel_residual)
+        e1.record()
+        torch.cuda.synchronize()
+        ck = clocks.stop() if clocks else None
+        ms = e0.elapsed_time(e1) / steps
+        pbytes = sv.persistent_bytes()
+        nsp, spms, nl = sv.kernel_stats(reset=True)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        return dict(ms=ms, iters=float(np.mean(iters)), outers=float(np.mean(outers)), worst=worst,
+                    spmv_launches=nsp, spmv_ms=spms, launches=nl, clocks=ck, pbytes=pbytes)
 
-    for i in range(args.warmup):
-        u, x, _ = step(i, u, x)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    solver.kernel_stats(reset=True)
-    clocks = ClockSampler(local)
-    time.sleep(0.2)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    iters, outers, worst = [], [], 0.0
-    for i in range(args.steps):
-        u, x, info = step(i, u, x)
-        iters.append(info.inner_iterations)
-        outers.append(info.outer_iterations)
-        worst = max(worst, info.rel_residual)
-    e1.record()
-    torch.cuda.synchronize()
-    ck = clocks.stop()
-    ms_step = e0.elapsed_time(e1) / args.steps
-    spmv_launches, spmv_ms, launches = solver.kernel_stats(reset=True)
-    if world > 1:
-        t = torch.tensor([ms_step], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
-        dist.barrier()
-
-    # roofline of the dominant kernel: CG SpMV q = A p with p = z + beta*p_old
-    bytes_spmv = 8 * nnzA + 4 * (N + 1) + 20 * N
-    avg_spmv_ms = spmv_ms / max(1, spmv_launches)
+    main = time_steps(solver, args.steps, args.warmup, True)
+    csr = time_steps(solver_csr, max(10, args.steps // 4), args.warmup, False)
+    ms_step = main["ms"]
+    ck = main["clocks"]
+    x = torch.empty_like(u0)
+    # roofline of the dominant kernel: the CG operator q = A p, p = z + beta*p_old
+    if inner_op == "stencil-persistent":
+        # one cooperative launch per step; bytes counted from its sweeps and iterations
+        k_name = "k_be_persistent"
+        bytes_spmv = main["pbytes"] / max(1, main["spmv_launches"])
+    elif inner_op == "stencil":
+        k_name, bytes_spmv = "k_cg_spmv_mf", 20 * N  # z, p_old, alpha read; p, q written
+    else:
+        k_name, bytes_spmv = "k_cg_spmv", 8 * nnzA + 4 * (N + 1) + 20 * N
+    avg_spmv_ms = main["spmv_ms"] / max(1, main["spmv_launches"])
     achieved = bytes_spmv / avg_spmv_ms / 1e6
+    csr_bytes = 8 * nnzA + 4 * (N + 1) + 20 * N
+    csr_avg = csr["spmv_ms"] / max(1, csr["spmv_launches"])
+    launches = main["launches"]
 
     # end to end through host buffers
     hb = torch.from_numpy(cfg["u0"]).pin_memory()
     hx = torch.empty(N, dtype=torch.float32).pin_memory()
-    db = torch.empty_like(u)
+    db = torch.empty_like(u0)
     torch.cuda.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record()
@@ -257,6 +280,7 @@ def run_piro(args):
         fp64 = {"step": 1, "max_abs_err_vs_fp64": err, "max_u": float(np.abs(u64b).max())}
 
     solver.close()
+    solver_csr.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -269,14 +293,18 @@ def run_piro(args):
         "config": {"workload": "heat backward Euler 128^3, smoothed log-normal alpha (sigma 1.5, filter 8, seed 2), "
                                "dt = 50x explicit limit, Jacobi-PCG FP32 + FP64 refinement to 1e-8",
                    "grid": [nx, ny, nz], "nnz_A": nnzA, "preconditioner": "jacobi",
+                   "inner_operator": inner_op,
                    "l2": "working set (A 117 MB + vectors) exceeds the 126 MB L2; no flush",
                    "parallelism": f"replicas x{world}"},
-        "solver": {"inner_iterations_mean": float(np.mean(iters)), "outer_sweeps_mean": float(np.mean(outers)),
-                   "worst_rel_residual": worst},
-        "roofline": {"kernel": "k_cg_spmv", "bound": "hbm", "achieved": round(achieved, 1),
+        "solver": {"inner_operator": inner_op, "inner_iterations_mean": main["iters"],
+                   "outer_sweeps_mean": main["outers"], "worst_rel_residual": main["worst"],
+                   "csr_inner_operator": {"ms_per_step": round(csr["ms"], 4), "inner_iterations_mean": csr["iters"],
+                                          "worst_rel_residual": csr["worst"], "k_cg_spmv_avg_ms": csr_avg,
+                                          "k_cg_spmv_gbs": round(csr_bytes / csr_avg / 1e6, 1)}},
+        "roofline": {"kernel": k_name, "bound": "hbm", "achieved": round(achieved, 1),
                      "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "peak_kind": peak_kind, "bytes_per_launch": bytes_spmv,
-                     "avg_launch_ms": avg_spmv_ms, "launches": spmv_launches, "traffic": None},
+                     "avg_launch_ms": avg_spmv_ms, "launches": main["spmv_launches"], "traffic": None},
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms/step", "h2d_bytes_per_step": 4 * N, "d2h_bytes_per_step": 4 * N},
         "gpu_launches": launches,
         "clocks": ck,

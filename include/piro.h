@@ -243,17 +243,33 @@ typedef struct piro_be_info {
  * dt*lambda_max > 2.  The solver allocates its own workspace. */
 int piro_be_create(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val,
                    const float *alpha, piro_stream_t stream, piro_be_solver **out);
+/* As piro_be_create, for A built as I - dt*diag(alpha)*L from the central
+ * 7-point Laplacian of the given norm (space scheme 3).  The inner Krylov
+ * operator is then applied matrix-free (alpha, dt and norm instead of the
+ * CSR stream: 20 instead of ~60 bytes per row) after a device check that A's
+ * interior block holds exactly those coefficients; if it does not, the CSR
+ * operator is used.  The FP64 residual always uses the CSR A. */
+int piro_be_create_stencil(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val,
+                           const float *alpha, float dt, float norm, piro_stream_t stream, piro_be_solver **out);
+/* Inner operator in use: 0 CSR SpMV (graph-launched CG), 1 matrix-free
+ * 7-point stencil (graph-launched CG), 2 matrix-free stencil with the whole
+ * solve in one persistent cooperative launch (FP64 refinement and CG phases
+ * separated by a grid barrier whose waits are bounded). */
+int piro_be_inner_operator(piro_be_solver *s, int *kind);
+/* Algorithmic bytes moved by the persistent launches counted in
+ * piro_be_kernel_stats (since its last reset). */
+int piro_be_persistent_bytes(piro_be_solver *s, double *bytes);
 /* Solve: b, x device float[N]; x receives the FP32 solution (boundary = b).
  * Stops when the FP64 relative residual <= rtol.  info may be NULL. */
 int piro_be_solve(piro_be_solver *s, const float *b, float *x, double rtol, int max_outer, int max_inner,
                   piro_be_info *info);
 /* FP64 copy of the last solution (device double[N]) for error reporting. */
 int piro_be_solution_f64(piro_be_solver *s, const double **x64);
-/* Live timing of the solver's dominant kernel (the CG SpMV, q = A p): CUDA
- * events recorded around each launch inside the solver's graph give the
- * launches that did work since the last reset and their summed device time in
- * ms; kernel_launches counts every kernel the solver launched.  Any output
- * pointer may be NULL. */
+/* Live timing of the solver's dominant kernel -- the CG SpMV q = A p, or the
+ * persistent solve kernel when inner operator kind 2 is in use: CUDA events
+ * recorded around each launch give the launches since the last reset and
+ * their summed device time in ms; kernel_launches counts every kernel the
+ * solver launched.  Any output pointer may be NULL. */
 int piro_be_kernel_stats(piro_be_solver *s, int reset, long long *spmv_launches, double *spmv_ms,
                          long long *kernel_launches);
 int piro_be_destroy(piro_be_solver *s);

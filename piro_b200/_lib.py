@@ -61,6 +61,9 @@ SIGNATURES = {
     "piro_reduce_workspace": (i32, [i64, psz]),
     "piro_dot_f64": (i32, [i64, vp, vp, vp, vp, sz, vp]),
     "piro_be_create": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, C.POINTER(vp)]),
+    "piro_be_create_stencil": (i32, [i32, i32, i32, vp, vp, vp, vp, f32, f32, vp, C.POINTER(vp)]),
+    "piro_be_inner_operator": (i32, [vp, pint]),
+    "piro_be_persistent_bytes": (i32, [vp, C.POINTER(C.c_double)]),
     "piro_be_solve": (i32, [vp, vp, vp, f64, i32, i32, C.POINTER(BeInfo)]),
     "piro_be_solution_f64": (i32, [vp, C.POINTER(vp)]),
     "piro_be_kernel_stats": (i32, [vp, i32, C.POINTER(C.c_longlong), C.POINTER(C.c_double),

@@ -19,6 +19,7 @@
 // launched as a CUDA graph and return at once when the flag is set.
 #include <cmath>
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
@@ -48,6 +49,11 @@ struct DevState {
     int max_iters;  // inner cap
     int broken;     // a non-finite scalar appeared
     unsigned ticket[4];
+    // persistent solve: grid barrier and results
+    unsigned bar_count, bar_gen;
+    int bar_err;
+    int p_status, p_outer, p_inner;
+    double p_rel;
 };
 
 __device__ __forceinline__ double block_sum(double v, double *s_warp)
@@ -91,7 +97,35 @@ __device__ __forceinline__ double gather_sum(const double *partials, double *s_w
 // r = b - A x in FP64 on interior rows, stored as float; z = r / A_rr;
 // partials of ||r64||^2, ||b||^2, <r/alpha, z>, ||r32||^2.  The last block
 // sets up the inner solve: rz, rr0, tol2, rel, done/iters reset, beta = 0.
-__global__ void __launch_bounds__(kTileRows) k_residual(int nx, int ny, int nz, int64_t N,
+struct ResidualRow {
+    GridDiv g;
+    const float *__restrict__ alpha, *__restrict__ dinv, *__restrict__ b;
+    const double *__restrict__ x;
+    float *__restrict__ r, *__restrict__ z;
+    double rr64, bb, rz, rr32;
+    __device__ __forceinline__ void operator()(int64_t row, const int32_t *c, const float *v, int n)
+    {
+        if (!g.interior(row)) {
+            r[row] = 0.0f;
+            z[row] = 0.0f;
+            return;
+        }
+        double q = 0.0;
+        for (int k = 0; k < n; ++k) q += (double)v[k] * x[c[k]];
+        const double bi = (double)b[row];
+        const double ri = bi - q;
+        const float rf = (float)ri;
+        const float zf = rf * dinv[row];
+        r[row] = rf;
+        z[row] = zf;
+        rr64 += ri * ri;
+        bb += bi * bi;
+        rz += (double)rf / (double)alpha[row] * (double)zf;
+        rr32 += (double)rf * (double)rf;
+    }
+};
+
+__global__ void __launch_bounds__(kTileRows) k_residual(GridDiv g, int64_t N,
                                                         const int32_t *__restrict__ rowptr,
                                                         const int32_t *__restrict__ col,
                                                         const float *__restrict__ val,
@@ -101,47 +135,14 @@ __global__ void __launch_bounds__(kTileRows) k_residual(int nx, int ny, int nz, 
                                                         float *__restrict__ z, double *__restrict__ partials,
                                                         DevState *__restrict__ st, double rtol, double inner_floor)
 {
-    __shared__ int32_t s_rp[kTileRows + 1];
-    __shared__ int32_t s_col[kTileCap];
-    __shared__ float s_val[kTileCap];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CsrStages &sm = *reinterpret_cast<CsrStages *>(smem_raw);
     __shared__ double s_warp[32];
     __shared__ bool s_last;
-    double rr64 = 0.0, bb = 0.0, rz = 0.0, rr32 = 0.0;
-    for (int64_t r0 = (int64_t)blockIdx.x * kTileRows; r0 < N; r0 += (int64_t)gridDim.x * kTileRows) {
-        const int nrows = (int)(N - r0 < kTileRows ? N - r0 : kTileRows);
-        for (int t = threadIdx.x; t <= nrows; t += blockDim.x) s_rp[t] = rowptr[r0 + t];
-        __syncthreads();
-        const int64_t s = s_rp[0], e = s_rp[nrows];
-        const bool staged = e - s <= kTileCap;
-        if (staged) stage_tile(col, val, s, e, s_col, s_val);
-        __syncthreads();
-        if (threadIdx.x < nrows) {
-            const int64_t row = r0 + threadIdx.x;
-            if (interior(row, nx, ny, nz)) {
-                double q = 0.0;
-                for (int k = s_rp[threadIdx.x]; k < s_rp[threadIdx.x + 1]; ++k) {
-                    const float v = staged ? s_val[k - s] : val[k];
-                    const int32_t c = staged ? s_col[k - s] : col[k];
-                    q += (double)v * x[c];
-                }
-                const double bi = (double)b[row];
-                const double ri = bi - q;
-                const float rf = (float)ri;
-                const float zf = rf * dinv[row];
-                r[row] = rf;
-                z[row] = zf;
-                rr64 += ri * ri;
-                bb += bi * bi;
-                rz += (double)rf / (double)alpha[row] * (double)zf;
-                rr32 += (double)rf * (double)rf;
-            } else {
-                r[row] = 0.0f;
-                z[row] = 0.0f;
-            }
-        }
-        __syncthreads();
-    }
-    double part[4] = {block_sum(rr64, s_warp), block_sum(bb, s_warp), block_sum(rz, s_warp), block_sum(rr32, s_warp)};
+    ResidualRow op{g, alpha, dinv, b, x, r, z, 0.0, 0.0, 0.0, 0.0};
+    csr_for_rows(sm, N, rowptr, col, val, op);
+    double part[4] = {block_sum(op.rr64, s_warp), block_sum(op.bb, s_warp), block_sum(op.rz, s_warp),
+                      block_sum(op.rr32, s_warp)};
     if (!publish_last(partials, kRedCap, 4, part, &st->ticket[0], &s_last)) return;
     double tot[4];
     for (int t = 0; t < 4; ++t) tot[t] = gather_sum(partials + t * kRedCap, s_warp);
@@ -167,7 +168,29 @@ __global__ void __launch_bounds__(kTileRows) k_residual(int nx, int ny, int nz, 
 }
 
 // p = z + beta*p_old (interior; 0 on boundary), q = A p, partial <p, q/alpha>.
-__global__ void __launch_bounds__(kTileRows) k_cg_spmv(int nx, int ny, int nz, int64_t N,
+struct CgSpmvRow {
+    GridDiv g;
+    float beta;
+    const float *__restrict__ alpha, *__restrict__ z, *__restrict__ p_old;
+    float *__restrict__ p_new, *__restrict__ q;
+    double pq;
+    __device__ __forceinline__ void operator()(int64_t row, const int32_t *c, const float *v, int n)
+    {
+        if (!g.interior(row)) {
+            p_new[row] = 0.0f;
+            q[row] = 0.0f;
+            return;
+        }
+        float acc = 0.0f;
+        for (int k = 0; k < n; ++k) acc += v[k] * (__ldg(z + c[k]) + beta * __ldg(p_old + c[k]));
+        const float pn = z[row] + beta * p_old[row];
+        p_new[row] = pn;
+        q[row] = acc;
+        pq += (double)pn * (double)acc / (double)alpha[row];
+    }
+};
+
+__global__ void __launch_bounds__(kTileRows) k_cg_spmv(GridDiv g, int64_t N,
                                                        const int32_t *__restrict__ rowptr,
                                                        const int32_t *__restrict__ col,
                                                        const float *__restrict__ val,
@@ -176,9 +199,8 @@ __global__ void __launch_bounds__(kTileRows) k_cg_spmv(int nx, int ny, int nz, i
                                                        float *__restrict__ q, double *__restrict__ partials,
                                                        DevState *__restrict__ st)
 {
-    __shared__ int32_t s_rp[kTileRows + 1];
-    __shared__ int32_t s_col[kTileCap];
-    __shared__ float s_val[kTileCap];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CsrStages &sm = *reinterpret_cast<CsrStages *>(smem_raw);
     __shared__ double s_warp[32];
     __shared__ bool s_last;
     __shared__ int s_done;
@@ -189,37 +211,9 @@ __global__ void __launch_bounds__(kTileRows) k_cg_spmv(int nx, int ny, int nz, i
     }
     __syncthreads();
     if (s_done) return;
-    const float beta = s_beta;
-    double pq = 0.0;
-    for (int64_t r0 = (int64_t)blockIdx.x * kTileRows; r0 < N; r0 += (int64_t)gridDim.x * kTileRows) {
-        const int nrows = (int)(N - r0 < kTileRows ? N - r0 : kTileRows);
-        for (int t = threadIdx.x; t <= nrows; t += blockDim.x) s_rp[t] = rowptr[r0 + t];
-        __syncthreads();
-        const int64_t s = s_rp[0], e = s_rp[nrows];
-        const bool staged = e - s <= kTileCap;
-        if (staged) stage_tile(col, val, s, e, s_col, s_val);
-        __syncthreads();
-        if (threadIdx.x < nrows) {
-            const int64_t row = r0 + threadIdx.x;
-            if (interior(row, nx, ny, nz)) {
-                float acc = 0.0f;
-                for (int k = s_rp[threadIdx.x]; k < s_rp[threadIdx.x + 1]; ++k) {
-                    const float v = staged ? s_val[k - s] : val[k];
-                    const int32_t c = staged ? s_col[k - s] : col[k];
-                    acc += v * (__ldg(z + c) + beta * __ldg(p_old + c));
-                }
-                const float pn = z[row] + beta * p_old[row];
-                p_new[row] = pn;
-                q[row] = acc;
-                pq += (double)pn * (double)acc / (double)alpha[row];
-            } else {
-                p_new[row] = 0.0f;
-                q[row] = 0.0f;
-            }
-        }
-        __syncthreads();
-    }
-    double part = block_sum(pq, s_warp);
+    CgSpmvRow op{g, s_beta, alpha, z, p_old, p_new, q, 0.0};
+    csr_for_rows(sm, N, rowptr, col, val, op);
+    double part = block_sum(op.pq, s_warp);
     if (!publish_last(partials, kRedCap, 1, &part, &st->ticket[1], &s_last)) return;
     const double tot = gather_sum(partials, s_warp);
     if (threadIdx.x == 0) {
@@ -235,8 +229,119 @@ __global__ void __launch_bounds__(kTileRows) k_cg_spmv(int nx, int ny, int nz, i
     }
 }
 
+// Matrix-free form of k_cg_spmv for A = I - dt*diag(alpha)*L with the
+// central 7-point L (space scheme 3): on interior rows A has the diagonal
+// fl(1 + fl(-dt*fl(alpha*vself))) and the six off-diagonals
+// fl(-dt*fl(alpha*vnb)), exactly the values csrgeam2 + rowscale produce, so
+// only the summation order differs from the CSR kernel.  One cell per
+// thread: the 14 loads of z and p_old at the cell and its six neighbours and
+// the alpha load are independent, so a warp has them all in flight; the
+// neighbour loads of adjacent threads hit L1/L2 (at 128^3 the whole working
+// set -- z, p, alpha, q, 40 MB -- stays in the 126 MB L2).
+constexpr int kMfThreads = 256;
+
+__global__ void __launch_bounds__(kMfThreads) k_cg_spmv_mf(GridDiv g, int64_t N, float mdt, float vself, float vnb,
+                                                            const float *__restrict__ alpha,
+                                                            const float *__restrict__ z,
+                                                            const float *__restrict__ p_old,
+                                                            float *__restrict__ p_new, float *__restrict__ q,
+                                                            double *__restrict__ partials, DevState *__restrict__ st)
+{
+    __shared__ double s_warp[32];
+    __shared__ bool s_last;
+    __shared__ int s_done;
+    __shared__ float s_beta;
+    if (threadIdx.x == 0) {
+        s_done = *((volatile int *)&st->done);
+        s_beta = (float)st->beta;
+    }
+    __syncthreads();
+    if (s_done) return;
+    const float beta = s_beta;
+    const int64_t sxy = (int64_t)g.nx * g.ny;
+    double pq = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        int x, y, zc;
+        g.coords((uint32_t)i, x, y, zc);
+        if (x > 0 && x < g.nx - 1 && y > 0 && y < g.ny - 1 && zc > 0 && zc < g.nz - 1) {
+            const float a = __ldg(alpha + i);
+            const float cur = __ldg(z + i) + beta * __ldg(p_old + i);
+            const float xm = __ldg(z + i - 1) + beta * __ldg(p_old + i - 1);
+            const float xp = __ldg(z + i + 1) + beta * __ldg(p_old + i + 1);
+            const float ym = __ldg(z + i - g.nx) + beta * __ldg(p_old + i - g.nx);
+            const float yp = __ldg(z + i + g.nx) + beta * __ldg(p_old + i + g.nx);
+            const float zm = __ldg(z + i - sxy) + beta * __ldg(p_old + i - sxy);
+            const float zp = __ldg(z + i + sxy) + beta * __ldg(p_old + i + sxy);
+            const float cd = __fadd_rn(1.0f, __fmul_rn(mdt, __fmul_rn(a, vself)));
+            const float co = __fmul_rn(mdt, __fmul_rn(a, vnb));
+            const float qv = cd * cur + co * (((xm + xp) + (ym + yp)) + (zm + zp));
+            p_new[i] = cur;
+            q[i] = qv;
+            pq += (double)cur * (double)qv / (double)a;
+        } else {
+            p_new[i] = 0.0f;
+            q[i] = 0.0f;
+        }
+    }
+    double part = block_sum(pq, s_warp);
+    if (!publish_last(partials, kRedCap, 1, &part, &st->ticket[1], &s_last)) return;
+    const double tot = gather_sum(partials, s_warp);
+    if (threadIdx.x == 0) {
+        const double aa = st->rz / tot;
+        if (!isfinite(aa) || tot <= 0.0) {
+            st->broken = 1;
+            st->done = 1;
+            st->a = 0.0;
+        } else {
+            st->a = aa;
+        }
+        st->ticket[1] = 0u;
+    }
+}
+
+// Check that every interior row of the CSR A is the central 7-point stencil
+// with the coefficients k_cg_spmv_mf uses; clears *ok otherwise.
+__global__ void k_check_stencil(GridDiv g, int64_t N, const int32_t *__restrict__ rowptr,
+                                const int32_t *__restrict__ col, const float *__restrict__ val,
+                                const float *__restrict__ alpha, float mdt, float vself, float vnb, int *ok)
+{
+    const int64_t sxy = (int64_t)g.nx * g.ny;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (int64_t)gridDim.x * blockDim.x) {
+        if (!g.interior(r)) continue;
+        const float a = alpha[r];
+        const float cd = __fadd_rn(1.0f, __fmul_rn(mdt, __fmul_rn(a, vself)));
+        const float co = __fmul_rn(mdt, __fmul_rn(a, vnb));
+        const int32_t k0 = rowptr[r], k1 = rowptr[r + 1];
+        bool good = k1 - k0 == 7;
+        for (int32_t k = k0; k < k1 && good; ++k) {
+            const int64_t d = (int64_t)col[k] - r;
+            const bool nb = d == 1 || d == -1 || d == g.nx || d == -g.nx || d == sxy || d == -sxy;
+            // entries in boundary columns meet p = 0 in the inner solve (they
+            // include the 10.0 entries of stencils.cpp:278-291): only the
+            // interior-interior block has to match
+            good = (d == 0 && val[k] == cd) || (nb && (!g.interior(col[k]) || val[k] == co));
+        }
+        if (!good) atomicExch(ok, 0);
+    }
+}
+
 // d += a p, r -= a q, z = r*dinv on interior rows; partials <r/alpha, z>, <r, r>.
-__global__ void __launch_bounds__(512) k_cg_update(int nx, int ny, int nz, int64_t N, const float *__restrict__ alpha,
+// Four consecutive rows per thread through 16-byte loads (N % 4 == 0 vectors
+// are 16-byte aligned; a scalar loop takes any remainder), one pass, all six
+// loads of a thread independent.  Boundary rows carry dinv = 0 and are left
+// untouched (their r, z, d stay 0).
+__device__ __forceinline__ void cg_update_one(float a, float di, float al, float pp, float qq, float &dd, float &rr_,
+                                              float &zz, double &rz, double &rr)
+{
+    if (di == 0.0f) return;
+    dd += a * pp;
+    rr_ -= a * qq;
+    zz = rr_ * di;
+    rz += (double)rr_ / (double)al * (double)zz;
+    rr += (double)rr_ * (double)rr_;
+}
+
+__global__ void __launch_bounds__(256) k_cg_update(int64_t N, int64_t n4, const float *__restrict__ alpha,
                                                    const float *__restrict__ dinv, const float *__restrict__ p,
                                                    const float *__restrict__ q, float *__restrict__ d,
                                                    float *__restrict__ r, float *__restrict__ z,
@@ -254,16 +359,30 @@ __global__ void __launch_bounds__(512) k_cg_update(int nx, int ny, int nz, int64
     if (s_done) return;
     const float a = s_a;
     double rz = 0.0, rr = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
-        const float di = dinv[i];
-        if (di == 0.0f) continue;  // boundary rows carry dinv = 0
-        d[i] += a * p[i];
-        const float ri = r[i] - a * q[i];
-        const float zi = ri * di;
-        r[i] = ri;
-        z[i] = zi;
-        rz += (double)ri / (double)alpha[i] * (double)zi;
-        rr += (double)ri * (double)ri;
+
+    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n4; v += (int64_t)gridDim.x * blockDim.x) {
+        const float4 di = __ldg(reinterpret_cast<const float4 *>(dinv) + v);
+        const float4 al = __ldg(reinterpret_cast<const float4 *>(alpha) + v);
+        const float4 pp = __ldg(reinterpret_cast<const float4 *>(p) + v);
+        const float4 qq = __ldg(reinterpret_cast<const float4 *>(q) + v);
+        float4 dd = reinterpret_cast<const float4 *>(d)[v];
+        float4 r4 = reinterpret_cast<const float4 *>(r)[v];
+        float4 z4 = reinterpret_cast<const float4 *>(z)[v];
+        cg_update_one(a, di.x, al.x, pp.x, qq.x, dd.x, r4.x, z4.x, rz, rr);
+        cg_update_one(a, di.y, al.y, pp.y, qq.y, dd.y, r4.y, z4.y, rz, rr);
+        cg_update_one(a, di.z, al.z, pp.z, qq.z, dd.z, r4.z, z4.z, rz, rr);
+        cg_update_one(a, di.w, al.w, pp.w, qq.w, dd.w, r4.w, z4.w, rz, rr);
+        reinterpret_cast<float4 *>(d)[v] = dd;
+        reinterpret_cast<float4 *>(r)[v] = r4;
+        reinterpret_cast<float4 *>(z)[v] = z4;
+    }
+    for (int64_t i = 4 * n4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        float dd = d[i], r1 = r[i], z1 = z[i];
+        cg_update_one(a, dinv[i], alpha[i], p[i], q[i], dd, r1, z1, rz, rr);
+        d[i] = dd;
+        r[i] = r1;
+        z[i] = z1;
     }
     double part[2] = {block_sum(rz, s_warp), block_sum(rr, s_warp)};
     if (!publish_last(partials, kRedCap, 2, part, &st->ticket[2], &s_last)) return;
@@ -283,6 +402,424 @@ __global__ void __launch_bounds__(512) k_cg_update(int nx, int ny, int nz, int64
             st->done = 1;
         }
         st->ticket[2] = 0u;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent solve.  For a stencil A the whole backward-Euler solve -- FP64
+// refinement sweeps and the FP32 CG inside them -- runs in one cooperative
+// launch.  Phases are separated by a grid barrier; every block reduces the
+// per-block partials itself in the same fixed order, so all blocks hold
+// identical scalars and take identical branches.  Data written inside the
+// kernel by other blocks is read with ld.global.cg (L2), never through L1.
+// At 128^3 the working set (x64, beff, r, z, q, d, p0, p1, alpha, dinv: about
+// 90 MB) stays in the 126 MB L2.
+//
+// The interior-boundary coupling of A (including the 10.0 entries of
+// stencils.cpp:278-291) is taken exactly from the CSR into a small side matrix
+// (ib_ptr/ib_col/ib_val) and folded into beff = b_I - A_IB b_B once per solve.
+constexpr int kPT = 256;
+constexpr int kPMaxBlocks = 2048;
+constexpr int kPSlots = 8;
+
+struct PArgs {
+    GridDiv g;
+    int64_t N;
+    float mdt, vself, vnb;
+    const float *alpha, *dinv, *b;
+    const int32_t *ib_ptr, *ib_col;
+    const float *ib_val;
+    double *x64, *beff;
+    float *r, *z, *q, *d, *p0, *p1;
+    float *xout;
+    double *partials;
+    DevState *st;
+    double rtol, inner_floor;
+    int max_outer, max_inner;
+    long long spin_limit;
+    int vec_a, vec_b;  // float4 paths usable (alignment and divisibility checked on the host)
+};
+
+// Loads of data written earlier in the same launch by other blocks: ordinary
+// (L1-cacheable, never the read-only .nc path) loads, ordered after the grid
+// barrier's release/acquire fences, so that the 7-point neighbour reuse is
+// served by L1 within a phase.
+template <class T>
+__device__ __forceinline__ T ld_(const T *p)
+{
+    return *p;
+}
+
+// Grid barrier with a bounded wait: false if the wait ran out or another block
+// reported an error (every block then leaves the kernel).
+__device__ __forceinline__ bool grid_barrier(DevState *st, long long spin_limit, int *s_ok)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *vgen = &st->bar_gen;
+        volatile int *verr = &st->bar_err;
+        const unsigned g = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(&st->bar_count, 1u) + 1u;
+        int ok = 1;
+        if (arrived == gridDim.x) {
+            atomicExch(&st->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&st->bar_gen, 1u);
+        } else {
+            long long spins = 0;
+            while (*vgen == g) {
+                if (*verr || ++spins > spin_limit) {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        if (*verr) ok = 0;
+        if (!ok) atomicExch(&st->bar_err, 1);
+        __threadfence();
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+// Sum of one partial slot over all blocks, identical in every block.
+__device__ __forceinline__ double all_sum(const double *partials, int slot, double *s_warp, double *s_b)
+{
+    double v = 0.0;
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) v += __ldcg(partials + slot * kPMaxBlocks + k);
+    v = block_sum(v, s_warp);
+    if (threadIdx.x == 0) *s_b = v;
+    __syncthreads();
+    const double out = *s_b;
+    __syncthreads();
+    return out;
+}
+
+__device__ __forceinline__ void put_partial(double *partials, int slot, double v, double *s_warp)
+{
+    v = block_sum(v, s_warp);
+    if (threadIdx.x == 0) partials[slot * kPMaxBlocks + blockIdx.x] = v;
+}
+
+// n block sums at once (one shared-memory round): s_red holds 32 * kN doubles.
+template <int kN>
+__device__ __forceinline__ void block_sums(double (&v)[kN], double *s_red)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int t = 0; t < kN; ++t) v[t] = warp_sum(v[t]);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int t = 0; t < kN; ++t) s_red[t * 32 + w] = v[t];
+    __syncthreads();
+    if (w == 0)
+#pragma unroll
+        for (int t = 0; t < kN; ++t) v[t] = warp_sum(lane < nw ? s_red[t * 32 + lane] : 0.0);
+}
+
+// Publish kN partials of this block into slots first..first+kN-1.
+template <int kN>
+__device__ __forceinline__ void put_partials(double *partials, int first, double (&v)[kN], double *s_red)
+{
+    block_sums<kN>(v, s_red);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int t = 0; t < kN; ++t) partials[(first + t) * kPMaxBlocks + blockIdx.x] = v[t];
+}
+
+// Sums of slots first..first+kN-1 over all blocks, identical in every block.
+template <int kN>
+__device__ __forceinline__ void all_sums(const double *partials, int first, double (&out)[kN], double *s_red,
+                                         double *s_b)
+{
+#pragma unroll
+    for (int t = 0; t < kN; ++t) out[t] = 0.0;
+    for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x)
+#pragma unroll
+        for (int t = 0; t < kN; ++t) out[t] += __ldcg(partials + (first + t) * kPMaxBlocks + k);
+    block_sums<kN>(out, s_red);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int t = 0; t < kN; ++t) s_b[t] = out[t];
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < kN; ++t) out[t] = s_b[t];
+    __syncthreads();
+}
+
+// Phase A on groups of 4 x-adjacent cells (nx % 4 == 0: a group never spans
+// two x-lines, and every row offset keeps 16-byte alignment).  Per group:
+// 11 float4 loads + 4 scalar halo loads instead of 60 scalar loads.
+__device__ __forceinline__ double cg_phase_a_vec(const PArgs &P, const float *pold, float *pnew, float fb, int64_t v0,
+                                                 int64_t dv)
+{
+    const GridDiv &g = P.g;
+    const int64_t nv = P.N >> 2, rx = g.nx >> 2, rxy = ((int64_t)g.nx * g.ny) >> 2;
+    const float4 *Z = reinterpret_cast<const float4 *>(P.z);
+    const float4 *Po = reinterpret_cast<const float4 *>(pold);
+    const float4 *Al = reinterpret_cast<const float4 *>(P.alpha);
+    double pq = 0.0;
+    for (int64_t v = v0; v < nv; v += dv) {
+        const int64_t i = v << 2;
+        int x0, y, z;
+        g.coords((uint32_t)i, x0, y, z);
+        if (!(y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1)) continue;  // boundary row: p, q stay 0
+        const float4 zc = ld_(Z + v), pc = ld_(Po + v);
+        const float4 zym = ld_(Z + v - rx), pym = ld_(Po + v - rx), zyp = ld_(Z + v + rx), pyp = ld_(Po + v + rx);
+        const float4 zzm = ld_(Z + v - rxy), pzm = ld_(Po + v - rxy), zzp = ld_(Z + v + rxy), pzp = ld_(Po + v + rxy);
+        const float zl = x0 > 0 ? ld_(P.z + i - 1) : 0.0f, pl = x0 > 0 ? ld_(pold + i - 1) : 0.0f;
+        const float zr = x0 + 4 < g.nx ? ld_(P.z + i + 4) : 0.0f, pr = x0 + 4 < g.nx ? ld_(pold + i + 4) : 0.0f;
+        const float4 al = __ldg(Al + v);
+        const float c[6] = {zl + fb * pl, zc.x + fb * pc.x, zc.y + fb * pc.y, zc.z + fb * pc.z, zc.w + fb * pc.w,
+                            zr + fb * pr};
+        const float ym[4] = {zym.x + fb * pym.x, zym.y + fb * pym.y, zym.z + fb * pym.z, zym.w + fb * pym.w};
+        const float yp[4] = {zyp.x + fb * pyp.x, zyp.y + fb * pyp.y, zyp.z + fb * pyp.z, zyp.w + fb * pyp.w};
+        const float zm[4] = {zzm.x + fb * pzm.x, zzm.y + fb * pzm.y, zzm.z + fb * pzm.z, zzm.w + fb * pzm.w};
+        const float zp[4] = {zzp.x + fb * pzp.x, zzp.y + fb * pzp.y, zzp.z + fb * pzp.z, zzp.w + fb * pzp.w};
+        const float a[4] = {al.x, al.y, al.z, al.w};
+        float pn[4], qv[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int x = x0 + k;
+            if (x > 0 && x < g.nx - 1) {
+                const float cd = __fadd_rn(1.0f, __fmul_rn(P.mdt, __fmul_rn(a[k], P.vself)));
+                const float co = __fmul_rn(P.mdt, __fmul_rn(a[k], P.vnb));
+                pn[k] = c[k + 1];
+                qv[k] = cd * c[k + 1] + co * (((c[k] + c[k + 2]) + (ym[k] + yp[k])) + (zm[k] + zp[k]));
+                pq += (double)pn[k] * (double)qv[k] / (double)a[k];
+            } else {
+                pn[k] = 0.0f;
+                qv[k] = 0.0f;
+            }
+        }
+        reinterpret_cast<float4 *>(pnew)[v] = make_float4(pn[0], pn[1], pn[2], pn[3]);
+        reinterpret_cast<float4 *>(P.q)[v] = make_float4(qv[0], qv[1], qv[2], qv[3]);
+    }
+    return pq;
+}
+
+// Phase B on float4 groups (N % 4 == 0).  Boundary lanes carry p = q = r = 0
+// and dinv = 0, so the update leaves them at zero without a branch; only the
+// dot products are masked.
+__device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const float *pnew, float fa, int64_t v0, int64_t dv,
+                                               double &rzn, double &rr)
+{
+    const int64_t nv = P.N >> 2;
+    for (int64_t v = v0; v < nv; v += dv) {
+        const float4 di = __ldg(reinterpret_cast<const float4 *>(P.dinv) + v);
+        const float4 al = __ldg(reinterpret_cast<const float4 *>(P.alpha) + v);
+        const float4 pp = ld_(reinterpret_cast<const float4 *>(pnew) + v);
+        const float4 qq = ld_(reinterpret_cast<const float4 *>(P.q) + v);
+        float4 dd = ld_(reinterpret_cast<const float4 *>(P.d) + v);
+        float4 r4 = ld_(reinterpret_cast<const float4 *>(P.r) + v);
+        dd.x += fa * pp.x; dd.y += fa * pp.y; dd.z += fa * pp.z; dd.w += fa * pp.w;
+        r4.x -= fa * qq.x; r4.y -= fa * qq.y; r4.z -= fa * qq.z; r4.w -= fa * qq.w;
+        const float4 z4 = make_float4(r4.x * di.x, r4.y * di.y, r4.z * di.z, r4.w * di.w);
+        reinterpret_cast<float4 *>(P.d)[v] = dd;
+        reinterpret_cast<float4 *>(P.r)[v] = r4;
+        reinterpret_cast<float4 *>(P.z)[v] = z4;
+        if (di.x != 0.0f) { rzn += (double)r4.x / (double)al.x * (double)z4.x; rr += (double)r4.x * (double)r4.x; }
+        if (di.y != 0.0f) { rzn += (double)r4.y / (double)al.y * (double)z4.y; rr += (double)r4.y * (double)r4.y; }
+        if (di.z != 0.0f) { rzn += (double)r4.z / (double)al.z * (double)z4.z; rr += (double)r4.z * (double)r4.z; }
+        if (di.w != 0.0f) { rzn += (double)r4.w / (double)al.w * (double)z4.w; rr += (double)r4.w * (double)r4.w; }
+    }
+}
+
+__global__ void __launch_bounds__(kPT, 4) k_be_persistent(PArgs P)
+{
+    __shared__ double s_warp[32];
+    __shared__ double s_red[4 * 32];
+    __shared__ double s_b;
+    __shared__ double s_bn[4];
+    __shared__ int s_ok;
+    const GridDiv g = P.g;
+    const int64_t N = P.N;
+    const int64_t sxy = (int64_t)g.nx * g.ny;
+    const int64_t i0 = (int64_t)blockIdx.x * kPT + threadIdx.x, di = (int64_t)gridDim.x * kPT;
+    auto inter = [&](int64_t i) {
+        int x, y, z;
+        g.coords((uint32_t)i, x, y, z);
+        return x > 0 && x < g.nx - 1 && y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1;
+    };
+    // P0: x = b on the interior (0 on the boundary), beff = b_I - A_IB b_B, d = p = 0
+    for (int64_t i = i0; i < N; i += di) {
+        if (inter(i)) {
+            const float bi = P.b[i];
+            double be = (double)bi;
+            for (int32_t k = P.ib_ptr[i]; k < P.ib_ptr[i + 1]; ++k) be -= (double)P.ib_val[k] * (double)P.b[P.ib_col[k]];
+            P.x64[i] = (double)bi;
+            P.beff[i] = be;
+        } else {
+            P.x64[i] = 0.0;
+            P.beff[i] = 0.0;
+        }
+        P.d[i] = 0.0f;
+        P.p0[i] = 0.0f;
+        P.p1[i] = 0.0f;
+    }
+    int status = PIRO_ERR_NOT_CONVERGED, outer = 0, inner_total = 0;
+    double rel = INFINITY, prev_rel = INFINITY;
+    bool ok = grid_barrier(P.st, P.spin_limit, &s_ok);
+    for (int sweep = 0; ok; ++sweep) {
+        // R: r = beff - A_II x in FP64, z = r / A_rr
+        double rr64 = 0.0, bb = 0.0, rz = 0.0, rr32 = 0.0;
+        for (int64_t i = i0; i < N; i += di) {
+            if (!inter(i)) continue;
+            const float a = __ldg(P.alpha + i);
+            const double cd = (double)__fadd_rn(1.0f, __fmul_rn(P.mdt, __fmul_rn(a, P.vself)));
+            const double co = (double)__fmul_rn(P.mdt, __fmul_rn(a, P.vnb));
+            const double nb = (ld_(P.x64 + i - 1) + ld_(P.x64 + i + 1)) +
+                              (ld_(P.x64 + i - g.nx) + ld_(P.x64 + i + g.nx)) +
+                              (ld_(P.x64 + i - sxy) + ld_(P.x64 + i + sxy));
+            const double ri = ld_(P.beff + i) - (cd * ld_(P.x64 + i) + co * nb);
+            const float rf = (float)ri;
+            const float zf = rf * __ldg(P.dinv + i);
+            P.r[i] = rf;
+            P.z[i] = zf;
+            const double bi = (double)P.b[i];
+            rr64 += ri * ri;
+            bb += bi * bi;
+            rz += (double)rf / (double)a * (double)zf;
+            rr32 += (double)rf * (double)rf;
+        }
+        double rsum[4] = {rr64, bb, rz, rr32};
+        put_partials<4>(P.partials, 0, rsum, s_red);
+        if (!(ok = grid_barrier(P.st, P.spin_limit, &s_ok))) break;
+        double rt[4];
+        all_sums<4>(P.partials, 0, rt, s_red, s_bn);
+        const double t_rr64 = rt[0], t_bb = rt[1];
+        double t_rz = rt[2];
+        const double rr0 = rt[3];
+        const double bn = t_bb > 0.0 ? sqrt(t_bb) : 1.0;
+        rel = sqrt(t_rr64) / bn;
+        if (!isfinite(rel)) { status = PIRO_STATUS_STALLED; break; }
+        if (rel <= P.rtol) { status = PIRO_OK; break; }
+        if (sweep >= P.max_outer || inner_total >= P.max_inner) break;
+        if (sweep > 0 && rel > 0.5 * prev_rel) { status = PIRO_STATUS_STALLED; break; }
+        prev_rel = rel;
+        outer = sweep + 1;
+        double itol = rel > 0.0 ? 0.5 * P.rtol / rel : 1.0;
+        itol = itol > 0.1 ? 0.1 : itol;
+        itol = itol < P.inner_floor ? P.inner_floor : itol;
+        const double tol2 = itol * itol;
+        double beta = 0.0;
+        float *pold = P.p0, *pnew = P.p1;
+        bool broken = false;
+        while (rr0 > 0.0) {
+            // A: p = z + beta*p_old, q = A_II p, <p, q/alpha>
+            const float fb = (float)beta;
+            double pq = 0.0;
+            if (P.vec_a) {
+                pq = cg_phase_a_vec(P, pold, pnew, fb, i0, di);
+            } else {
+                for (int64_t i = i0; i < N; i += di) {
+                    if (!inter(i)) continue;
+                    const float a = __ldg(P.alpha + i);
+                    const float cur = ld_(P.z + i) + fb * ld_(pold + i);
+                    const float xm = ld_(P.z + i - 1) + fb * ld_(pold + i - 1);
+                    const float xp = ld_(P.z + i + 1) + fb * ld_(pold + i + 1);
+                    const float ym = ld_(P.z + i - g.nx) + fb * ld_(pold + i - g.nx);
+                    const float yp = ld_(P.z + i + g.nx) + fb * ld_(pold + i + g.nx);
+                    const float zm = ld_(P.z + i - sxy) + fb * ld_(pold + i - sxy);
+                    const float zp = ld_(P.z + i + sxy) + fb * ld_(pold + i + sxy);
+                    const float cd = __fadd_rn(1.0f, __fmul_rn(P.mdt, __fmul_rn(a, P.vself)));
+                    const float co = __fmul_rn(P.mdt, __fmul_rn(a, P.vnb));
+                    const float qv = cd * cur + co * (((xm + xp) + (ym + yp)) + (zm + zp));
+                    pnew[i] = cur;
+                    P.q[i] = qv;
+                    pq += (double)cur * (double)qv / (double)a;
+                }
+            }
+            put_partial(P.partials, 4, pq, s_warp);
+            if (!(ok = grid_barrier(P.st, P.spin_limit, &s_ok))) break;
+            const double t_pq = all_sum(P.partials, 4, s_warp, &s_b);
+            const double alpha_k = t_rz / t_pq;
+            if (!isfinite(alpha_k) || t_pq <= 0.0) { broken = true; break; }
+            const float fa = (float)alpha_k;
+            // B: d += a p, r -= a q, z = r / A_rr
+            double bsum[2] = {0.0, 0.0};
+            if (P.vec_b) {
+                cg_phase_b_vec(P, pnew, fa, i0, di, bsum[0], bsum[1]);
+            } else {
+                for (int64_t i = i0; i < N; i += di) {
+                    const float dv = __ldg(P.dinv + i);
+                    if (dv == 0.0f) continue;
+                    P.d[i] += fa * pnew[i];
+                    const float ri = P.r[i] - fa * P.q[i];
+                    const float zi = ri * dv;
+                    P.r[i] = ri;
+                    P.z[i] = zi;
+                    bsum[0] += (double)ri / (double)__ldg(P.alpha + i) * (double)zi;
+                    bsum[1] += (double)ri * (double)ri;
+                }
+            }
+            put_partials<2>(P.partials, 5, bsum, s_red);
+            if (!(ok = grid_barrier(P.st, P.spin_limit, &s_ok))) break;
+            double bt[2];
+            all_sums<2>(P.partials, 5, bt, s_red, s_bn);
+            const double t_rzn = bt[0], t_rr = bt[1];
+            beta = t_rzn / t_rz;
+            t_rz = t_rzn;
+            ++inner_total;
+            float *t = pold;
+            pold = pnew;
+            pnew = t;
+            if (!isfinite(t_rr) || !isfinite(beta)) { broken = true; break; }
+            if (t_rr <= tol2 * rr0 || inner_total >= P.max_inner) break;
+        }
+        if (!ok) break;
+        if (broken) { status = PIRO_STATUS_STALLED; break; }
+        // X: x += d, d = 0
+        for (int64_t i = i0; i < N; i += di) {
+            const float dv = P.d[i];
+            if (dv != 0.0f) {
+                P.x64[i] += (double)dv;
+                P.d[i] = 0.0f;
+            }
+        }
+        if (!(ok = grid_barrier(P.st, P.spin_limit, &s_ok))) break;
+    }
+    // output: interior from x, boundary from b
+    for (int64_t i = i0; i < N; i += di) P.xout[i] = inter(i) ? (float)P.x64[i] : P.b[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        P.st->p_status = ok ? status : PIRO_ERR_CUDA;
+        P.st->p_outer = outer;
+        P.st->p_inner = inner_total;
+        P.st->p_rel = rel;
+    }
+}
+
+// Interior-boundary coupling of A: per row, the entries of interior rows whose
+// column is a boundary cell.  Count pass writes ib_ptr[r+1]; fill after scan.
+__global__ void k_ib_count(GridDiv g, int64_t N, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
+                           int32_t *__restrict__ ib_ptr)
+{
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (int64_t)gridDim.x * blockDim.x) {
+        int n = 0;
+        if (g.interior(r))
+            for (int32_t k = rowptr[r]; k < rowptr[r + 1]; ++k) n += !g.interior(col[k]);
+        ib_ptr[r + 1] = n;
+        if (r == 0) ib_ptr[0] = 0;
+    }
+}
+
+__global__ void k_ib_fill(GridDiv g, int64_t N, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
+                          const float *__restrict__ val, const int32_t *__restrict__ ib_ptr,
+                          int32_t *__restrict__ ib_col, float *__restrict__ ib_val)
+{
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (int64_t)gridDim.x * blockDim.x) {
+        if (!g.interior(r)) continue;
+        int32_t o = ib_ptr[r];
+        for (int32_t k = rowptr[r]; k < rowptr[r + 1]; ++k)
+            if (!g.interior(col[k])) {
+                ib_col[o] = col[k];
+                ib_val[o] = val[k];
+                ++o;
+            }
     }
 }
 
@@ -337,6 +874,7 @@ struct piro_be_solver {
     cudaStream_t stream;  // the solver's own non-blocking stream (graph capture needs one)
     cudaEvent_t ev_in;
     unsigned grid_tiles, grid_elem;
+    int64_t n4;  // float4 groups handled by the vector path of k_cg_update (0: scalar only)
     float *dinv, *r, *z, *q, *d, *p[2];
     double *x64;
     double *partials;
@@ -345,6 +883,19 @@ struct piro_be_solver {
     cudaGraph_t graph;
     cudaGraphExec_t exec;
     double inner_floor;
+    int op_mf;                 // inner operator: 0 CSR, 1 matrix-free 7-point
+    float mdt, vself, vnb;     // its coefficients
+    unsigned grid_mf;
+    // persistent single-launch solve (stencil operator, cooperative launch)
+    int persist;
+    unsigned grid_p;
+    int32_t *ib_ptr, *ib_col;
+    float *ib_val;
+    double *beff;
+    cudaEvent_t pev0, pev1;
+    double persist_ms;
+    long long persist_launches;
+    double persist_bytes;  // algorithmic bytes of the timed launches
     // event pairs around each k_cg_spmv of the captured chunk: live kernel times
     cudaEvent_t ev0[kChunk], ev1[kChunk];
     double spmv_ms;
@@ -362,6 +913,12 @@ static void be_free(piro_be_solver *s)
     if (s->exec) cudaGraphExecDestroy(s->exec);
     if (s->ev_in) cudaEventDestroy(s->ev_in);
     if (s->graph) cudaGraphDestroy(s->graph);
+    if (s->pev0) cudaEventDestroy(s->pev0);
+    if (s->pev1) cudaEventDestroy(s->pev1);
+    cudaFree(s->ib_ptr);
+    cudaFree(s->ib_col);
+    cudaFree(s->ib_val);
+    cudaFree(s->beff);
     cudaFree(s->dinv);
     cudaFree(s->x64);
     cudaFree(s->partials);
@@ -385,11 +942,17 @@ static int be_capture_chunk(piro_be_solver *s)
         float *p_new = s->p[(it + 1) & 1];
         // External: the record becomes a node of the graph, observable from the host
         cudaEventRecordWithFlags(s->ev0[it], s->stream, cudaEventRecordExternal);
-        k_cg_spmv<<<s->grid_tiles, kTileRows, 0, s->stream>>>(s->nx, s->ny, s->nz, s->N, s->rowptr, s->col, s->val,
-                                                              s->alpha, s->z, p_old, p_new, s->q, s->partials, s->st);
+        if (s->op_mf)
+            k_cg_spmv_mf<<<s->grid_mf, kMfThreads, 0, s->stream>>>(GridDiv(s->nx, s->ny, s->nz), s->N, s->mdt,
+                                                                   s->vself, s->vnb, s->alpha, s->z, p_old, p_new,
+                                                                   s->q, s->partials, s->st);
+        else
+            k_cg_spmv<<<s->grid_tiles, kTileRows, sizeof(CsrStages), s->stream>>>(
+                GridDiv(s->nx, s->ny, s->nz), s->N, s->rowptr, s->col, s->val, s->alpha, s->z, p_old, p_new, s->q,
+                s->partials, s->st);
         cudaEventRecordWithFlags(s->ev1[it], s->stream, cudaEventRecordExternal);
-        k_cg_update<<<s->grid_elem, 512, 0, s->stream>>>(s->nx, s->ny, s->nz, s->N, s->alpha, s->dinv, p_new, s->q,
-                                                         s->d, s->r, s->z, s->partials, s->st);
+        k_cg_update<<<s->grid_elem, 256, 0, s->stream>>>(s->N, s->n4, s->alpha, s->dinv, p_new, s->q, s->d, s->r,
+                                                         s->z, s->partials, s->st);
     }
     cudaError_t e = cudaStreamEndCapture(s->stream, &s->graph);
     if (e != cudaSuccess) {
@@ -400,10 +963,59 @@ static int be_capture_chunk(piro_be_solver *s)
     return PIRO_OK;
 }
 
-extern "C" int piro_be_create(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val,
-                              const float *alpha, piro_stream_t stream, piro_be_solver **out)
+namespace piro {
+int scan_rowptr_inplace(int64_t N, int32_t *rowptr, void *work, size_t work_bytes, cudaStream_t s);
+size_t scan_workspace_bytes(int64_t N);
+}  // namespace piro
+
+// Extract A's interior-boundary coupling and size the cooperative grid.  On
+// any failure the solver keeps the multi-kernel path (persist = 0).
+static int be_setup_persistent(piro_be_solver *s)
+{
+    int dev = 0, coop = 0, per_sm = 0;
+    PIRO_CUDA(cudaGetDevice(&dev));
+    PIRO_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_be_persistent, kPT, 0));
+    if (!coop || per_sm < 1) return PIRO_OK;
+    const int64_t N = s->N;
+    const GridDiv g(s->nx, s->ny, s->nz);
+    PIRO_CUDA(cudaMalloc(&s->ib_ptr, sizeof(int32_t) * (size_t)(N + 1)));
+    PIRO_CUDA(cudaMalloc(&s->beff, sizeof(double) * (size_t)N));
+    void *work = nullptr;
+    const size_t wb = scan_workspace_bytes(N);
+    PIRO_CUDA(cudaMalloc(&work, wb));
+    k_ib_count<<<grid_for(N, 256, 8), 256, 0, s->stream>>>(g, N, s->rowptr, s->col, s->ib_ptr);
+    PIRO_CHECK_LAUNCH("k_ib_count");
+    int rc = scan_rowptr_inplace(N, s->ib_ptr, work, wb, s->stream);
+    int32_t nib = 0;
+    if (!rc && (cudaMemcpyAsync(&nib, s->ib_ptr + N, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+                cudaStreamSynchronize(s->stream) != cudaSuccess))
+        rc = PIRO_ERR_CUDA;
+    cudaFree(work);
+    if (rc) return rc;
+    PIRO_CUDA(cudaMalloc(&s->ib_col, sizeof(int32_t) * (size_t)(nib > 0 ? nib : 1)));
+    PIRO_CUDA(cudaMalloc(&s->ib_val, sizeof(float) * (size_t)(nib > 0 ? nib : 1)));
+    k_ib_fill<<<grid_for(N, 256, 8), 256, 0, s->stream>>>(g, N, s->rowptr, s->col, s->val, s->ib_ptr, s->ib_col,
+                                                          s->ib_val);
+    PIRO_CHECK_LAUNCH("k_ib_fill");
+    PIRO_CUDA(cudaEventCreate(&s->pev0));
+    PIRO_CUDA(cudaEventCreate(&s->pev1));
+    int nsm = sm_count();
+    int64_t grid = (int64_t)nsm * per_sm;
+    if (grid > kPMaxBlocks) grid = kPMaxBlocks;
+    const int64_t need = cdiv(N, kPT);
+    if (grid > need) grid = need;
+    s->grid_p = (unsigned)grid;
+    s->persist = 1;
+    return PIRO_OK;
+}
+
+static int be_create(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val,
+                     const float *alpha, bool stencil, float dt, float norm, piro_stream_t stream,
+                     piro_be_solver **out)
 {
     PIRO_ARG(out && rowptr && col && val && alpha && nx >= 3 && ny >= 3 && nz >= 3, "piro_be_create: bad arguments");
+    PIRO_ARG((int64_t)nx * ny * nz < ((int64_t)1 << 31), "piro_be_create: grid too large");
     *out = nullptr;
     piro_be_solver *s = new piro_be_solver();
     s->nx = nx;
@@ -424,16 +1036,25 @@ extern "C" int piro_be_create(int nx, int ny, int nz, const int32_t *rowptr, con
         return PIRO_ERR_CUDA;
     }
     const int64_t N = s->N;
-    s->grid_tiles = (unsigned)std::min<int64_t>(cdiv(N, kTileRows), (int64_t)sm_count() * 6);
-    s->grid_elem = (unsigned)std::min<int64_t>(cdiv(N, 512 * 4), (int64_t)sm_count() * 4);
+    s->grid_tiles = (unsigned)std::min<int64_t>(cdiv(N, kTileRows), (int64_t)sm_count() * 4);
+    if (cudaFuncSetAttribute(k_cg_spmv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CsrStages)) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CsrStages)) !=
+            cudaSuccess) {
+        be_free(s);
+        piro::set_error("piro_be_create: cannot raise the shared-memory limit");
+        return PIRO_ERR_CUDA;
+    }
+    s->grid_elem = (unsigned)std::min<int64_t>(std::max<int64_t>(1, cdiv(N / 4, 256)), (int64_t)kRedCap);
     if (s->grid_tiles > (unsigned)kRedCap || s->grid_elem > (unsigned)kRedCap) {
         be_free(s);
         piro::set_error("piro_be_create: reduction grid exceeds %d blocks", kRedCap);
         return PIRO_ERR_ARG;
     }
-    // one allocation for the seven FP32 work vectors
+    // one allocation for the seven FP32 work vectors, each 256-byte aligned
+    const int64_t Np = cdiv(N, 64) * 64;
     float *fbuf = nullptr;
-    cudaError_t e = cudaMalloc(&fbuf, sizeof(float) * (size_t)N * 7);
+    cudaError_t e = cudaMalloc(&fbuf, sizeof(float) * (size_t)Np * 7);
     if (e == cudaSuccess) e = cudaMalloc(&s->x64, sizeof(double) * (size_t)N);
     if (e == cudaSuccess) e = cudaMalloc(&s->partials, sizeof(double) * kRedCap * 4);
     if (e == cudaSuccess) e = cudaMalloc(&s->st, sizeof(DevState));
@@ -445,13 +1066,15 @@ extern "C" int piro_be_create(int nx, int ny, int nz, const int32_t *rowptr, con
         return PIRO_ERR_NOMEM;
     }
     s->dinv = fbuf;
-    s->r = fbuf + N;
-    s->z = fbuf + 2 * N;
-    s->q = fbuf + 3 * N;
-    s->d = fbuf + 4 * N;
-    s->p[0] = fbuf + 5 * N;
-    s->p[1] = fbuf + 6 * N;
-    if (cudaMemsetAsync(fbuf, 0, sizeof(float) * (size_t)N * 7, s->stream) != cudaSuccess ||
+    s->r = fbuf + Np;
+    s->z = fbuf + 2 * Np;
+    s->q = fbuf + 3 * Np;
+    s->d = fbuf + 4 * Np;
+    s->p[0] = fbuf + 5 * Np;
+    s->p[1] = fbuf + 6 * Np;
+    // 16-byte vector path of k_cg_update: needs N % 4 == 0 and an aligned alpha
+    s->n4 = (N % 4 == 0 && (reinterpret_cast<uintptr_t>(alpha) & 15) == 0) ? N / 4 : 0;
+    if (cudaMemsetAsync(fbuf, 0, sizeof(float) * (size_t)Np * 7, s->stream) != cudaSuccess ||
         cudaMemsetAsync(s->st, 0, sizeof(DevState), s->stream) != cudaSuccess) {
         be_free(s);
         piro::set_error("piro_be_create: memset failed");
@@ -462,6 +1085,39 @@ extern "C" int piro_be_create(int nx, int ny, int nz, const int32_t *rowptr, con
         be_free(s);
         piro::set_error("k_diag_inv launch failed");
         return PIRO_ERR_CUDA;
+    }
+    if (stencil) {
+        // use the matrix-free inner operator only if A's interior block is
+        // exactly the stencil it computes
+        s->mdt = -dt;
+        s->vself = (float)(-6.0 / (double)norm);
+        s->vnb = (float)(1.0 / (double)norm);
+        s->grid_mf = (unsigned)std::min<int64_t>(cdiv(N, kMfThreads), (int64_t)kRedCap);
+        int *d_ok = reinterpret_cast<int *>(s->partials);  // scratch before first use
+        int h_ok = 0;
+        const int one = 1;
+        if (cudaMemcpyAsync(d_ok, &one, sizeof(int), cudaMemcpyHostToDevice, s->stream) != cudaSuccess) {
+            be_free(s);
+            return PIRO_ERR_CUDA;
+        }
+        k_check_stencil<<<grid_for(N, 256, 8), 256, 0, s->stream>>>(GridDiv(nx, ny, nz), N, rowptr, col, val, alpha,
+                                                                     s->mdt, s->vself, s->vnb, d_ok);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(&h_ok, d_ok, sizeof(int), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+            cudaStreamSynchronize(s->stream) != cudaSuccess) {
+            be_free(s);
+            piro::set_error("piro_be_create_stencil: structure check failed to run");
+            return PIRO_ERR_CUDA;
+        }
+        s->op_mf = h_ok ? 1 : 0;
+    }
+    const char *env = getenv("PIRO_BE_PERSISTENT");  // "0" keeps the graph-launched CG (testing, tuning)
+    if (s->op_mf && !(env && env[0] == '0')) {
+        int rc = be_setup_persistent(s);
+        if (rc) {
+            be_free(s);
+            return rc;
+        }
     }
     int rc = be_capture_chunk(s);
     if (rc) {
@@ -477,6 +1133,33 @@ extern "C" int piro_be_create(int nx, int ny, int nz, const int32_t *rowptr, con
     return PIRO_OK;
 }
 
+extern "C" int piro_be_create(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val,
+                              const float *alpha, piro_stream_t stream, piro_be_solver **out)
+{
+    return be_create(nx, ny, nz, rowptr, col, val, alpha, false, 0.0f, 1.0f, stream, out);
+}
+
+extern "C" int piro_be_create_stencil(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col,
+                                      const float *val, const float *alpha, float dt, float norm, piro_stream_t stream,
+                                      piro_be_solver **out)
+{
+    return be_create(nx, ny, nz, rowptr, col, val, alpha, true, dt, norm, stream, out);
+}
+
+extern "C" int piro_be_inner_operator(piro_be_solver *s, int *kind)
+{
+    PIRO_ARG(s && kind, "piro_be_inner_operator: bad arguments");
+    *kind = s->op_mf ? (s->persist ? 2 : 1) : 0;
+    return PIRO_OK;
+}
+
+extern "C" int piro_be_persistent_bytes(piro_be_solver *s, double *bytes)
+{
+    PIRO_ARG(s && bytes, "piro_be_persistent_bytes: bad arguments");
+    *bytes = s->persist_bytes;
+    return PIRO_OK;
+}
+
 extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double rtol, int max_outer, int max_inner,
                              piro_be_info *info)
 {
@@ -489,13 +1172,75 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
     PIRO_CUDA(cudaStreamWaitEvent(st, s->ev_in, 0));
     piro_be_info inf{};
     inf.status = PIRO_ERR_NOT_CONVERGED;
+    if (s->persist) {
+        PArgs P;
+        P.g = GridDiv(s->nx, s->ny, s->nz);
+        P.N = N;
+        P.mdt = s->mdt;
+        P.vself = s->vself;
+        P.vnb = s->vnb;
+        P.alpha = s->alpha;
+        P.dinv = s->dinv;
+        P.b = b;
+        P.ib_ptr = s->ib_ptr;
+        P.ib_col = s->ib_col;
+        P.ib_val = s->ib_val;
+        P.x64 = s->x64;
+        P.beff = s->beff;
+        P.r = s->r;
+        P.z = s->z;
+        P.q = s->q;
+        P.d = s->d;
+        P.p0 = s->p[0];
+        P.p1 = s->p[1];
+        P.xout = x;
+        P.partials = s->partials;
+        P.st = s->st;
+        P.rtol = rtol;
+        P.inner_floor = s->inner_floor;
+        P.max_outer = max_outer;
+        P.max_inner = max_inner;
+        P.spin_limit = 1ll << 22;  // ~2 s of polling: a stuck barrier ends with an error, not a hang
+        const bool al16 = ((reinterpret_cast<uintptr_t>(s->alpha) | reinterpret_cast<uintptr_t>(s->dinv)) & 15) == 0;
+        P.vec_b = (N % 4 == 0) && al16;
+        P.vec_a = P.vec_b && (s->nx % 4 == 0);
+        void *args[] = {&P};
+        PIRO_CUDA(cudaMemsetAsync(s->st, 0, sizeof(DevState), st));
+        PIRO_CUDA(cudaEventRecord(s->pev0, st));
+        PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_be_persistent, dim3(s->grid_p), dim3(kPT), args, 0, st));
+        PIRO_CUDA(cudaEventRecord(s->pev1, st));
+        s->kernel_launches += 1;
+        PIRO_CUDA(cudaMemcpyAsync(s->h_st, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, st));
+        PIRO_CUDA(cudaStreamSynchronize(st));
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, s->pev0, s->pev1) == cudaSuccess) {
+            s->persist_ms += ms;
+            s->persist_launches += 1;
+            // algorithmic bytes: P0 32, residual sweep 32 + update 24, CG iteration 20 + 36 bytes per cell
+            const double n = (double)N;
+            s->persist_bytes += n * (32.0 + 56.0 * (s->h_st->p_outer + 1) + 56.0 * s->h_st->p_inner + 8.0);
+        } else {
+            (void)cudaGetLastError();
+        }
+        inf.status = s->h_st->p_status;
+        inf.outer_iterations = s->h_st->p_outer;
+        inf.inner_iterations = s->h_st->p_inner;
+        inf.rel_residual = s->h_st->p_rel;
+        if (s->h_st->bar_err) {
+            piro::set_error("piro_be_solve: grid barrier timed out");
+            inf.status = PIRO_ERR_CUDA;
+        }
+        if (info) *info = inf;
+        return inf.status;
+    }
     k_promote<<<grid_for(N, 256, 8), 256, 0, st>>>(N, b, s->x64);
     PIRO_CHECK_LAUNCH("k_promote");
     s->kernel_launches += 1;
     PIRO_CUDA(cudaMemsetAsync(s->d, 0, sizeof(float) * (size_t)N, st));
     double prev_rel = INFINITY;
     for (int outer = 0; outer <= max_outer; ++outer) {
-        k_residual<<<s->grid_tiles, kTileRows, 0, st>>>(s->nx, s->ny, s->nz, N, s->rowptr, s->col, s->val, s->alpha,
+        k_residual<<<s->grid_tiles, kTileRows, sizeof(CsrStages), st>>>(GridDiv(s->nx, s->ny, s->nz), N, s->rowptr,
+                                                                        s->col, s->val, s->alpha,
                                                        s->dinv, b, s->x64, s->r, s->z, s->partials, s->st, rtol,
                                                        s->inner_floor);
         PIRO_CHECK_LAUNCH("k_residual");
@@ -571,13 +1316,16 @@ extern "C" int piro_be_kernel_stats(piro_be_solver *s, int reset, long long *spm
                                     long long *kernel_launches)
 {
     PIRO_ARG(s, "piro_be_kernel_stats: null solver");
-    if (spmv_launches) *spmv_launches = s->spmv_launches;
-    if (spmv_ms) *spmv_ms = s->spmv_ms;
+    if (spmv_launches) *spmv_launches = s->persist ? s->persist_launches : s->spmv_launches;
+    if (spmv_ms) *spmv_ms = s->persist ? s->persist_ms : s->spmv_ms;
     if (kernel_launches) *kernel_launches = s->kernel_launches;
     if (reset) {
         s->spmv_launches = 0;
         s->spmv_ms = 0.0;
         s->kernel_launches = 0;
+        s->persist_launches = 0;
+        s->persist_ms = 0.0;
+        s->persist_bytes = 0.0;
     }
     return PIRO_OK;
 }

@@ -19,7 +19,7 @@ inline cudaStream_t as_stream(piro_stream_t s) { return reinterpret_cast<cudaStr
 // B200: 148 SMs; launch grids are sized against the device's SM count.
 int sm_count();
 
-inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+__host__ __device__ inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 // Grid size for a grid-stride loop over n items with `per_block` items per block.
 inline unsigned grid_for(int64_t n, int64_t per_block, int blocks_per_sm = 8)
@@ -67,7 +67,50 @@ __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, 
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
 
-// Interior test of SpMVCSR.cl:29-32 (grid sizes are ghost-inclusive).
+// Division by a runtime constant for numerators below 2^31: with
+// l = ceil(log2 d) and m = ceil(2^(31+l) / d) (< 2^32), n / d =
+// (n * m) >> (31 + l) exactly, since n*(m - 2^(31+l)/d) / 2^(31+l) < 1/d
+// (round-up reciprocal method, Granlund & Montgomery 1994).
+struct FastDiv {
+    uint32_t d, m, sh;  // sh = l - 1 applied after the high-word multiply; d == 1 handled apart
+    FastDiv() = default;
+    __host__ explicit FastDiv(uint32_t div) : d(div), m(0), sh(0)
+    {
+        uint32_t l = 0;
+        while ((1ull << l) < div) ++l;
+        if (div > 1) {
+            m = (uint32_t)(((1ull << (31 + l)) + div - 1) / div);
+            sh = l - 1;
+        }
+    }
+    __device__ __forceinline__ uint32_t div(uint32_t n) const { return d == 1 ? n : __umulhi(n, m) >> sh; }
+};
+
+// Grid with fast coordinate decomposition of a linear index i < 2^31.
+struct GridDiv {
+    int nx, ny, nz;
+    FastDiv fx, fxy;
+    GridDiv() = default;
+    __host__ GridDiv(int x, int y, int z) : nx(x), ny(y), nz(z), fx((uint32_t)x), fxy((uint32_t)x * (uint32_t)y) {}
+    __device__ __forceinline__ void coords(uint32_t i, int &x, int &y, int &z) const
+    {
+        const uint32_t zz = fxy.div(i);
+        const uint32_t rem = i - zz * fxy.d;
+        const uint32_t yy = fx.div(rem);
+        z = (int)zz;
+        y = (int)yy;
+        x = (int)(rem - yy * fx.d);
+    }
+    // interior test of SpMVCSR.cl:29-32 (ghost-inclusive sizes)
+    __device__ __forceinline__ bool interior(int64_t i) const
+    {
+        int x, y, z;
+        coords((uint32_t)i, x, y, z);
+        return x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1;
+    }
+};
+
+// Interior test of SpMVCSR.cl:29-32 with general 64-bit division (one-off use).
 __device__ __forceinline__ bool interior(int64_t i, int nx, int ny, int nz)
 {
     int64_t sxy = (int64_t)nx * ny;

@@ -14,47 +14,37 @@
 #include "common.cuh"
 #include "csr_tile.cuh"
 
+#include <algorithm>
+
 namespace piro {
 namespace {
 
 // mode 0: SpMVCSR (out = u + sum), mode 1: SpMVCSR_I1 (out = u - sum).
 template <int kMode>
-__global__ void __launch_bounds__(kTileRows) k_csr_step(int nx, int ny, int nz, int64_t N,
+struct FeRow {
+    GridDiv g;
+    float dt;
+    const float *__restrict__ u;
+    float *__restrict__ out;
+    __device__ __forceinline__ void operator()(int64_t row, const int32_t *c, const float *v, int n) const
+    {
+        float result = 0.0f;
+        for (int k = 0; k < n; ++k) result = add_rn(result, mul_rn(mul_rn(dt, v[k]), __ldg(u + c[k])));
+        if (g.interior(row)) out[row] = kMode == 0 ? add_rn(result, u[row]) : sub_rn(u[row], result);
+    }
+};
+
+template <int kMode>
+__global__ void __launch_bounds__(kTileRows) k_csr_step(GridDiv g, int64_t N,
                                                         const int32_t *__restrict__ rowptr,
                                                         const int32_t *__restrict__ col,
                                                         const float *__restrict__ val, float dt,
                                                         const float *__restrict__ u, float *__restrict__ out)
 {
-    __shared__ int32_t s_rp[kTileRows + 1];
-    __shared__ int32_t s_col[kTileCap];
-    __shared__ float s_val[kTileCap];
-    for (int64_t r0 = (int64_t)blockIdx.x * kTileRows; r0 < N; r0 += (int64_t)gridDim.x * kTileRows) {
-        const int nrows = (int)(N - r0 < kTileRows ? N - r0 : kTileRows);
-        for (int t = threadIdx.x; t <= nrows; t += blockDim.x) s_rp[t] = rowptr[r0 + t];
-        __syncthreads();
-        const int64_t s = s_rp[0], e = s_rp[nrows];
-        const bool staged = e - s <= kTileCap;
-        if (staged) stage_tile(col, val, s, e, s_col, s_val);
-        __syncthreads();
-        if (threadIdx.x < nrows) {
-            const int64_t row = r0 + threadIdx.x;
-            const int k0 = s_rp[threadIdx.x], k1 = s_rp[threadIdx.x + 1];
-            float result = 0.0f;
-            if (staged) {
-                for (int k = k0; k < k1; ++k) {
-                    const float t = mul_rn(dt, s_val[k - s]);
-                    result = add_rn(result, mul_rn(t, __ldg(u + s_col[k - s])));
-                }
-            } else {
-                for (int k = k0; k < k1; ++k) {
-                    const float t = mul_rn(dt, val[k]);
-                    result = add_rn(result, mul_rn(t, __ldg(u + col[k])));
-                }
-            }
-            if (interior(row, nx, ny, nz)) out[row] = kMode == 0 ? add_rn(result, u[row]) : sub_rn(u[row], result);
-        }
-        __syncthreads();
-    }
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CsrStages &sm = *reinterpret_cast<CsrStages *>(smem_raw);
+    FeRow<kMode> op{g, dt, u, out};
+    csr_for_rows(sm, N, rowptr, col, val, op);
 }
 
 // COO: each warp takes 32 consecutive entries per pass; a segmented inclusive
@@ -148,29 +138,69 @@ __global__ void k_ht_spmv(int nx, int ny, int nz, int64_t N, const int64_t *__re
     }
 }
 
-// Matrix-free 7-point update; one thread per x-cell, blocks tile (x, y) lines.
-__global__ void k_stencil(int nx, int ny, int nz, float idx2, float idy2, float idz2, float dt,
-                          const float *__restrict__ alpha, const float *__restrict__ u, float *__restrict__ out)
+// Matrix-free 7-point update.  A block owns a 32 x 8 tile of (x, y) columns
+// and a run of kZRun planes.  Every load the block needs -- its columns at
+// z0-1 .. z0+kZRun, alpha, and the x/y halo cells of each plane -- is issued
+// up front into registers, so a thread has ~30 independent loads in flight;
+// the planes are then swept with the x/y neighbours exchanged through a
+// shared-memory plane tile.  Algorithmic traffic is 12 bytes per cell (u read,
+// alpha read, out written); the column halo and the two extra planes of each
+// run are served mostly by L2.
+constexpr int kStX = 32, kStY = 8, kZRun = 8;
+
+__global__ void __launch_bounds__(kStX *kStY) k_stencil(int nx, int ny, int nz, float idx2, float idy2, float idz2,
+                                                        float dt, const float *__restrict__ alpha,
+                                                        const float *__restrict__ u, float *__restrict__ out)
 {
+    __shared__ float tile[kStY + 2][kStX + 2];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x = blockIdx.x * kStX + tx, y = blockIdx.y * kStY + ty;
+    const int z0 = blockIdx.z * kZRun;
     const int64_t sxy = (int64_t)nx * ny;
-    const int64_t N = sxy * nz;
-    for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < N; id += (int64_t)gridDim.x * blockDim.x) {
-        const int z = (int)(id / sxy);
-        const int64_t rem = id - (int64_t)z * sxy;
-        const int y = (int)(rem / nx);
-        const int x = (int)(rem - (int64_t)y * nx);
-        const float c = __ldg(u + id);
-        if (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1) {
-            const float c2 = __fmul_rn(2.0f, c);
-            const float lx = __fmul_rn(__fsub_rn(__fadd_rn(__ldg(u + id + 1), __ldg(u + id - 1)), c2), idx2);
-            const float ly = __fmul_rn(__fsub_rn(__fadd_rn(__ldg(u + id + nx), __ldg(u + id - nx)), c2), idy2);
-            const float lz = __fmul_rn(__fsub_rn(__fadd_rn(__ldg(u + id + sxy), __ldg(u + id - sxy)), c2), idz2);
-            const float lap = __fadd_rn(__fadd_rn(lx, ly), lz);
-            const float a = alpha ? __ldg(alpha + id) : 1.0f;
-            out[id] = __fadd_rn(c, __fmul_rn(dt, __fmul_rn(a, lap)));
-        } else {
-            out[id] = c;
+    const bool in_xy = x < nx && y < ny;
+    const int64_t colm = (int64_t)y * nx + x;
+    // halo role of this thread (at most one x and one y halo cell)
+    const int hxo = tx == 0 ? -1 : tx == kStX - 1 ? 1 : 0;
+    const int hyo = ty == 0 ? -1 : ty == kStY - 1 ? 1 : 0;
+    const bool hx_ok = hxo != 0 && y < ny && x + hxo >= 0 && x + hxo < nx;
+    const bool hy_ok = hyo != 0 && x < nx && y + hyo >= 0 && y + hyo < ny;
+    float c[kZRun + 2], a[kZRun], hx[kZRun], hy[kZRun];
+#pragma unroll
+    for (int j = 0; j < kZRun + 2; ++j) {
+        const int zz = z0 - 1 + j;
+        c[j] = (in_xy && zz >= 0 && zz < nz) ? __ldcs(u + zz * sxy + colm) : 0.0f;
+    }
+#pragma unroll
+    for (int j = 0; j < kZRun; ++j) {
+        const int zz = z0 + j;
+        const bool zok = zz < nz;
+        a[j] = (alpha && in_xy && zok) ? __ldcs(alpha + zz * sxy + colm) : 1.0f;
+        hx[j] = (hx_ok && zok) ? __ldg(u + zz * sxy + colm + hxo) : 0.0f;
+        hy[j] = (hy_ok && zok) ? __ldg(u + zz * sxy + colm + (int64_t)hyo * nx) : 0.0f;
+    }
+#pragma unroll
+    for (int j = 0; j < kZRun; ++j) {
+        const int z = z0 + j;
+        if (z >= nz) break;  // uniform across the block
+        const float cur = c[j + 1];
+        tile[ty + 1][tx + 1] = cur;
+        if (hxo) tile[ty + 1][tx + 1 + hxo] = hx[j];
+        if (hyo) tile[ty + 1 + hyo][tx + 1] = hy[j];
+        __syncthreads();
+        if (in_xy) {
+            const int64_t id = z * sxy + colm;
+            if (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1) {
+                const float c2 = __fmul_rn(2.0f, cur);
+                const float lx = __fmul_rn(__fsub_rn(__fadd_rn(tile[ty + 1][tx + 2], tile[ty + 1][tx]), c2), idx2);
+                const float ly = __fmul_rn(__fsub_rn(__fadd_rn(tile[ty + 2][tx + 1], tile[ty][tx + 1]), c2), idy2);
+                const float lz = __fmul_rn(__fsub_rn(__fadd_rn(c[j + 2], c[j]), c2), idz2);
+                const float lap = __fadd_rn(__fadd_rn(lx, ly), lz);
+                __stcs(out + id, __fadd_rn(cur, __fmul_rn(dt, __fmul_rn(a[j], lap))));
+            } else {
+                __stcs(out + id, cur);
+            }
         }
+        __syncthreads();
     }
 }
 
@@ -210,7 +240,10 @@ __global__ void k_vec_urf(int64_t n, float *__restrict__ a, float *__restrict__ 
     }
 }
 
-bool grid_ok(int nx, int ny, int nz) { return nx >= 3 && ny >= 3 && nz >= 3; }
+bool grid_ok(int nx, int ny, int nz)
+{
+    return nx >= 3 && ny >= 3 && nz >= 3 && (int64_t)nx * ny * nz < ((int64_t)1 << 31);
+}
 
 template <int kMode>
 int launch_csr_step(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val, float dt,
@@ -220,8 +253,15 @@ int launch_csr_step(int nx, int ny, int nz, const int32_t *rowptr, const int32_t
     PIRO_ARG(rowptr && col && val && u && out, "csr step: null pointer");
     PIRO_ARG(u != out, "csr step: u and out must differ (the reference writes a fresh buffer)");
     const int64_t N = (int64_t)nx * ny * nz;
-    k_csr_step<kMode><<<grid_for(N, kTileRows, 6), kTileRows, 0, as_stream(stream)>>>(nx, ny, nz, N, rowptr, col, val,
-                                                                                      dt, u, out);
+    static bool attr_set[2] = {false, false};
+    if (!attr_set[kMode]) {
+        PIRO_CUDA(cudaFuncSetAttribute(k_csr_step<kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(CsrStages)));
+        attr_set[kMode] = true;
+    }
+    const unsigned grid = (unsigned)std::min<int64_t>(cdiv(N, kTileRows), (int64_t)sm_count() * 4);
+    k_csr_step<kMode><<<grid, kTileRows, sizeof(CsrStages), as_stream(stream)>>>(GridDiv(nx, ny, nz), N, rowptr, col,
+                                                                                val, dt, u, out);
     PIRO_CHECK_LAUNCH("k_csr_step");
     return PIRO_OK;
 }
@@ -286,8 +326,9 @@ extern "C" int piro_stencil_fe_step(int nx, int ny, int nz, float idx2, float id
                                     const float *alpha, const float *u, float *out, piro_stream_t stream)
 {
     PIRO_ARG(grid_ok(nx, ny, nz) && u && out && u != out, "piro_stencil_fe_step: bad arguments");
-    const int64_t N = (int64_t)nx * ny * nz;
-    k_stencil<<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(nx, ny, nz, idx2, idy2, idz2, dt, alpha, u, out);
+    const dim3 block(kStX, kStY);
+    const dim3 grid((unsigned)cdiv(nx, kStX), (unsigned)cdiv(ny, kStY), (unsigned)cdiv(nz, kZRun));
+    k_stencil<<<grid, block, 0, as_stream(stream)>>>(nx, ny, nz, idx2, idy2, idz2, dt, alpha, u, out);
     PIRO_CHECK_LAUNCH("k_stencil");
     return PIRO_OK;
 }

@@ -241,13 +241,31 @@ def dot_f64(x, y):
 class BESolver:
     """FP32 Jacobi-PCG inside FP64 iterative refinement for A = I - dt*diag(alpha)*L."""
 
-    def __init__(self, nx, ny, nz, A, alpha):
+    def __init__(self, nx, ny, nz, A, alpha, stencil=None):
+        """stencil=(dt, norm): A = I - dt*diag(alpha)*L(norm) from the central
+        scheme; the inner operator then runs matrix-free when A matches."""
         self.keep = (A, alpha)
         h = C.c_void_p()
-        check(lib().piro_be_create(nx, ny, nz, _p(A[0]), _p(A[1]), _p(A[2]), _p(alpha), _stream(), C.byref(h)),
-              "piro_be_create")
+        if stencil is None:
+            check(lib().piro_be_create(nx, ny, nz, _p(A[0]), _p(A[1]), _p(A[2]), _p(alpha), _stream(), C.byref(h)),
+                  "piro_be_create")
+        else:
+            dt, norm = stencil
+            check(lib().piro_be_create_stencil(nx, ny, nz, _p(A[0]), _p(A[1]), _p(A[2]), _p(alpha), float(dt),
+                                               float(norm), _stream(), C.byref(h)), "piro_be_create_stencil")
         self.h = h
         self.N = cells(nx, ny, nz)
+
+    @property
+    def inner_operator(self):
+        k = C.c_int()
+        check(lib().piro_be_inner_operator(self.h, C.byref(k)), "piro_be_inner_operator")
+        return ["csr", "stencil", "stencil-persistent"][k.value]
+
+    def persistent_bytes(self):
+        v = C.c_double()
+        check(lib().piro_be_persistent_bytes(self.h, C.byref(v)), "piro_be_persistent_bytes")
+        return v.value
 
     def solve(self, b, x, rtol=1e-8, max_outer=20, max_inner=20000, strict=True):
         info = BeInfo()

@@ -246,17 +246,21 @@ def test_fe_steps_match_oracle(cuda, oracle, n):
     np.testing.assert_allclose(h(u), ref_coo, rtol=1e-5, atol=1e-6)
 
 
-def test_stencil_matches_oracle(cuda, oracle):
+@pytest.mark.parametrize("n", [(48, 40, 36), (33, 9, 17), (3, 3, 3), (70, 12, 5)])
+def test_stencil_matches_oracle(cuda, oracle, n):
     import torch
     from piro_b200 import ops
-    nx, ny, nz = 48, 40, 36
+    nx, ny, nz = n
     N = nx * ny * nz
     rng = np.random.default_rng(1)
     u = rng.random(N, dtype=np.float32)
     alpha = np.exp(rng.standard_normal(N)).astype(np.float32)
-    ref = oracle.stencil_fe(nx, ny, nz, 0.01, u, alpha)
+    ref = oracle.stencil_fe(nx, ny, nz, 0.01, u, alpha, idx2=1.0, idy2=0.25, idz2=4.0)
     out = torch.empty(N, dtype=torch.float32, device="cuda")
-    ops.stencil_fe_step(nx, ny, nz, 0.01, dev(torch, u), out, alpha=dev(torch, alpha))
+    ops.stencil_fe_step(nx, ny, nz, 0.01, dev(torch, u), out, alpha=dev(torch, alpha), idx2=1.0, idy2=0.25, idz2=4.0)
+    assert f32_bits_equal(h(out), ref)
+    ref = oracle.stencil_fe(nx, ny, nz, 0.01, u)
+    ops.stencil_fe_step(nx, ny, nz, 0.01, dev(torch, u), out)
     assert f32_bits_equal(h(out), ref)
 
 
