@@ -356,13 +356,53 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_case(args):
+    """Small fixed cases for ncu captures (no timing, no JSON): `be` solves the
+    128^3 backward-Euler step twice, `spmv` runs each 256^3 forward-Euler
+    kernel four times."""
+    import torch
+
+    from piro_b200 import ops
+    from piro_b200 import workloads as W
+    torch.cuda.set_device(0)
+    if args.profile == "be":
+        cfg = W.heat_be_128()
+        nx, ny, nz = cfg["n"]
+        A, alpha = be_problem(torch, ops, cfg)
+        s = ops.BESolver(nx, ny, nz, A, alpha, stencil=(float(cfg["dt"]), 1.0))
+        b = torch.from_numpy(cfg["u0"]).cuda()
+        x = torch.empty_like(b)
+        for _ in range(2):
+            info = s.solve(b, x, rtol=1e-8)
+        print("be", s.inner_operator, info.inner_iterations, info.rel_residual)
+        s.close()
+    else:
+        cfg = W.spmv_256()
+        nx, ny, nz = cfg["n"]
+        u = torch.from_numpy(cfg["u"]).cuda()
+        alpha = torch.from_numpy(cfg["alpha"]).cuda()
+        out = torch.empty_like(u)
+        A = ops.csr_laplacian(nx, ny, nz, 3, 1.0)
+        ops.csr_rowscale(A[0], A[2], alpha)
+        for _ in range(4):
+            ops.csr_fe_step(nx, ny, nz, A, 0.01, u, out)
+        for _ in range(4):
+            ops.stencil_fe_step(nx, ny, nz, 0.01, u, out, alpha=alpha)
+        torch.cuda.synchronize()
+        print("spmv ok")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="piro", choices=["piro", "reference"])
+    ap.add_argument("--profile", choices=["be", "spmv"], help="run a small fixed case for ncu, print no JSON")
     args = ap.parse_args()
+    if args.profile:
+        run_profile_case(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
