@@ -194,6 +194,21 @@ int piro_csrgeam3(int64_t N, const int32_t *rpA, const int32_t *cA, const float 
                   const float *v, int32_t *rpD, int32_t *cD, float *vD, void *work, size_t work_bytes,
                   piro_stream_t stream);
 
+/* piro_csrgeam3 for callers that cannot allocate device memory (a host that
+ * fixes its whole device-memory budget before the time loop, or one that only
+ * owns the buffers it passes in).  No counterpart in the reference: it is an
+ * addition of this library.  Same arguments and results as piro_csrgeam3,
+ * without the workspace: the scan scratch is a fixed 36 KB array inside the
+ * library, held on every GPU that loads it until exit.  Serves 1 to 16,777,216
+ * rows (PIRO_ERR_ARG beyond).  Allocates nothing.  All calls share the array:
+ * calls whose GPU work overlaps (other streams or threads on the same device)
+ * race and must be serialised by the caller.  The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before starting any stream capture. */
+int piro_csrgeam3_noalloc(int64_t N, const int32_t *rpA, const int32_t *cA, const float *vA, const int32_t *rpB,
+                          const int32_t *cB, const float *vB, const int32_t *rpC, const int32_t *cC, const float *vC,
+                          const float *v, int32_t *rpD, int32_t *cD, float *vD, piro_stream_t stream);
+
 /* D = A + beta*B, one union row per row with ascending columns; a column in
  * both rows is A's value + beta*B's value.  Builds the backward-Euler matrix
  * I - dt*diag(alpha)*L (no counterpart kernel in the reference, whose JLI

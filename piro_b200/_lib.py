@@ -55,6 +55,7 @@ SIGNATURES = {
     "piro_vec_urf": (i32, [i64, vp, vp, f32, vp]),
     "piro_scan_workspace": (i32, [i64, psz]),
     "piro_csrgeam3": (i32, [i64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
+    "piro_csrgeam3_noalloc": (i32, [i64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "piro_csrgeam2_count": (i32, [i64, vp, vp, vp, vp, vp, vp, sz, vp]),
     "piro_csrgeam2_fill": (i32, [i64, vp, vp, vp, f32, vp, vp, vp, vp, vp, vp, vp]),
     "piro_csr_identity": (i32, [i64, vp, vp, vp, vp]),
