@@ -297,6 +297,89 @@ int piro_be_jli(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *co
                 const float *b, float *x, float *r_work, float tol, float urf, int maxiter, int *iters,
                 piro_stream_t stream);
 
+/* ========================================================================
+ * 2. Context API: PIRO's operator interface over a case .ini
+ * ======================================================================== */
+
+typedef struct piro_ctx piro_ctx;
+
+/* A field handle (CLBuffer of operatoroverload.hpp:9-17): index of the field
+ * in creation order (constants, scalars, vectors) and its length. */
+typedef struct piro_buf {
+    int32_t id;
+    int64_t n;
+} piro_buf;
+
+/* An operator handle (the std::vector<CLBuffer> the reference returns). */
+typedef struct piro_op {
+    int32_t kind;
+} piro_op;
+
+#define PIRO_OP_LAPLACIAN 1
+#define PIRO_OP_GRADIENT 2
+#define PIRO_OP_DOT 3        /* vector & gradient (csrgeam result) */
+#define PIRO_EQN_RESULT (-1) /* piro_buf id of the operator= result (partD) */
+
+typedef struct piro_case_info {
+    int32_t nx, ny, nz; /* ghost-inclusive */
+    int64_t n_cells;
+    int32_t timescheme, spacescheme, solverscheme, datatype, simindex;
+    float timestep, totaltime;
+    int64_t steps_done;
+    int32_t n_fields;
+    int64_t bc_cells;
+} piro_case_info;
+
+/* Piro::preprocess (src/preprocess.cpp:20-208) + bc::readbc: read
+ * <assets_dir>/<case_name> ([File] [Mesh] [Simulation] [IC] [Schemes]
+ * [Solve]), solver.ini ([JLI], when Solver = 40), Data/hashtable.ini ([Table],
+ * when Data = 2), IC/distribution.ini and setup.ini ([BC]); add the ghost
+ * layers; create the fields with their initial conditions (src/ic.cpp) on the
+ * device; compute the boundary values of field 1 (src/bc.cpp:107-157).
+ * PIRO_ERR_CONFIG names a missing or malformed key (the reference throws). */
+int piro_open(const char *assets_dir, const char *case_name, piro_ctx **out);
+void piro_close(piro_ctx *ctx);
+int piro_ctx_query(piro_ctx *ctx, piro_case_info *info);
+/* 0 (default): alpha applied as SpMDSM intends; 1: alpha dropped, as the
+ * reference's csrscale actually behaves (src/kernelcsrgeam.cpp:224-231).
+ * Must be set before the Laplacian is assembled. */
+int piro_set_alpha_mode(piro_ctx *ctx, int mode);
+
+/* process::ddt_r / process::vector / matchscalartovar (src/process.cpp:20-58,
+ * 154-166): the handle of the named field (field 0 when no name matches, as
+ * in the reference). */
+int piro_ddt_r(piro_ctx *ctx, const char *var, piro_buf *out);
+int piro_vector(piro_ctx *ctx, const char *var, piro_buf *out);
+int piro_field(piro_ctx *ctx, const char *var, piro_buf *out);
+/* Host <-> device copies of a field (synchronous). */
+int piro_field_upload(piro_ctx *ctx, piro_buf f, const float *host, int64_t n);
+int piro_field_download(piro_ctx *ctx, piro_buf f, float *host, int64_t n);
+int piro_field_device_ptr(piro_ctx *ctx, piro_buf f, float **dptr);
+
+/* process::laplacian (src/process.cpp:60-122): assembled on the first call
+ * per [Solve] Data (0 CSR, 2 HT, 3 COO; 1 DENSE gives PIRO_ERR_DATATYPE) and
+ * cached; for CSR the rows are scaled by the field named `coeff`. */
+int piro_laplacian(piro_ctx *ctx, const char *var, const char *coeff, piro_op *out);
+/* process::gradient (src/process.cpp:124-152): the three CSR matrices. */
+int piro_gradient(piro_ctx *ctx, const char *var, piro_op *out);
+/* operator& (src/operatoroverload.cpp:102-123): csrgeam of a vector field
+ * with the gradient, merged once and cached. */
+int piro_dot(piro_ctx *ctx, piro_buf v, piro_op grad, piro_op *out);
+/* CLBuffer::operator= (src/operatoroverload.cpp:20-100): one time step of
+ * lhs by [Schemes] Time: 11 forward Euler (CSR, HT or COO), 12 backward
+ * Euler with Solver 40 (JLI, as written) or 39 (FP32 PCG in FP64
+ * refinement to 1e-8).  *out is the new field (partD, PIRO_EQN_RESULT). */
+int piro_assign(piro_ctx *ctx, piro_buf lhs, piro_op rhs, piro_buf *out);
+/* scalarMatrix::Solve (src/process.cpp:221-236): copy the result into field
+ * 1 and apply the Dirichlet face values (setBC). */
+int piro_step_solve(piro_ctx *ctx, piro_buf eqn, float time);
+/* Piro::solve (src/solve.cpp:11-48): while (time < TotalTime) with float
+ * time, the equation of [File] simindex (0 heat, 1 advection) per step. */
+int piro_solve(piro_ctx *ctx, int64_t *steps_taken);
+/* Download an assembled operator in CSR form (nnz only when rowptr is NULL). */
+int piro_op_export_csr(piro_ctx *ctx, piro_op op, int32_t *rowptr, int32_t *col, float *val, int64_t cap,
+                       int64_t *nnz);
+
 #ifdef __cplusplus
 }
 #endif

@@ -69,6 +69,9 @@ def _load():
         "or_be_jli": (i32, [i64, i32, i32, _i32p, _i32p, _f32p, f32, _f32p, _f32p, _f32p, f32, f32, i32]),
         "or_be_cg_f64": (i32, [i64, i32, i32, i32, _i32p, _i32p, _f32p, _f32p, _f32p, _f64p, f64, i32,
                                C.POINTER(C.c_double)]),
+        "or_ic_gaussian": (None, [i32, i32, i32, f32, f32, f32, f32, _f32p, _f32p, _f32p]),
+        "or_ic_coulomb": (None, [i32, i32, i32, f32, f32, f32, _f32p, f32, f64, f64, _f32p]),
+        "or_ic_uniform_vector": (None, [i64, _f32p, f32, _f32p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -319,6 +322,27 @@ def be_cg_f64(nx, ny, nz, A, alpha, b, rtol=1e-12, maxiter=100000):
     return u, it, rel.value
 
 
+def ic_gaussian(nx, ny, nz, l, scale, sigma, mean):
+    out = np.zeros(n_cells(nx, ny, nz), np.float32)
+    lib().or_ic_gaussian(nx, ny, nz, *map(np.float32, l), np.float32(scale), np.asarray(sigma, np.float32),
+                         np.asarray(mean, np.float32), out)
+    return out
+
+
+def ic_coulomb(nx, ny, nz, l, center, Z, e, eps0):
+    """e and eps0 as the reference holds them: parsed to float, widened to double."""
+    out = np.zeros(n_cells(nx, ny, nz), np.float32)
+    lib().or_ic_coulomb(nx, ny, nz, *map(np.float32, l), np.asarray(center, np.float32), np.float32(Z),
+                        float(np.float32(e)), float(np.float32(eps0)), out)
+    return out
+
+
+def ic_uniform_vector(N, direction, value):
+    out = np.zeros(3 * N, np.float32)
+    lib().or_ic_uniform_vector(N, np.asarray(direction, np.float32), np.float32(value), out)
+    return out
+
+
 def set_threads(n):
     lib().or_set_threads(int(n))
 
@@ -344,6 +368,8 @@ class Ref:
         L.ref_gradient.argtypes = [i32, i32, i32, i32, f32, _i32p, _i32p, _f32p, np.ctypeslib.ndpointer(np.int64)]
         L.ref_ht_insert_all.restype = i32
         L.ref_ht_insert_all.argtypes = [i32, _i32p, _i32p, _f32p, i32, _i32p, _f32p]
+        L.ref_initialcondition.restype = ll
+        L.ref_initialcondition.argtypes = [i32, i32, i32, f32, f32, f32, C.c_char_p, C.c_char_p, _f32p]
         L.ref_initbc.restype = ll
         L.ref_initbc.argtypes = [i32, i32, i32, C.c_char_p, C.c_char_p, _i32p, _i32p, _f32p]
         L.refcl_spmvcsr.argtypes = [i32, _f32p, _i32p, _i32p, f32, _f32p, _f32p, C.c_uint, C.c_uint, C.c_uint]
@@ -404,6 +430,12 @@ class Ref:
         field = np.zeros(N, np.float32)
         q = self.lib.ref_initbc(nx, ny, nz, assets_root.encode(), scalar.encode(), idx, flen, field)
         return idx[:q].copy(), flen, field
+
+    def initialcondition(self, nx, ny, nz, l, assets_root, ic_name):
+        out = np.zeros(3 * n_cells(nx, ny, nz), np.float32)
+        n = self.lib.ref_initialcondition(nx, ny, nz, *map(np.float32, l), assets_root.encode(), ic_name.encode(),
+                                          out)
+        return out[:n].copy()
 
     def spmvcsr(self, nx, ny, nz, A, dt, B, C_in):
         N = n_cells(nx, ny, nz)

@@ -24,6 +24,9 @@
 #include <stdlib.h>
 #include <string.h>
 #include <math.h>
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -691,4 +694,46 @@ int or_be_cg_f64(int64_t N, int nx, int ny, int nz, const int32_t *rp, const int
     if (final_rel) *final_rel = sqrt(rr) / bnorm;
     free(interior); free(r); free(z); free(p); free(q); free(dinv); free(bb); free(s);
     return ok ? it : -1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Initial conditions (src/ic.cpp:16-99), host float/double arithmetic as the
+ * C++ evaluates it.  Coordinates are x*l0/(float)nx with ghost-inclusive n
+ * (ic.cpp:53-55).  std::exp(float) is expf; std::pow with a double or int
+ * argument is the double pow. */
+void or_ic_gaussian(int nx, int ny, int nz, float l0, float l1, float l2, float scale, const float *sigma,
+                    const float *mean, float *out)
+{
+    const float norm = (float)(1.0f / (pow(2.0f * M_PI, 1.5f) * sigma[0] * sigma[1] * sigma[2]));
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                const float c0 = x * l0 / (float)nx, c1 = y * l1 / (float)ny, c2 = z * l2 / (float)nz;
+                const float a = (c0 - mean[0]) / sigma[0], b = (c1 - mean[1]) / sigma[1], c = (c2 - mean[2]) / sigma[2];
+                const float e = -0.5f * (a * a + b * b + c * c);
+                out[idx3(x, y, z, nx, ny)] = scale * (norm * expf(e));
+            }
+}
+
+void or_ic_coulomb(int nx, int ny, int nz, float l0, float l1, float l2, const float *center, float Z, double e,
+                   double eps0, float *out)
+{
+    for (int x = 0; x < nx; ++x)
+        for (int y = 0; y < ny; ++y)
+            for (int z = 0; z < nz; ++z) {
+                const float c0 = x * l0 / (float)nx, c1 = y * l1 / (float)ny, c2 = z * l2 / (float)nz;
+                /* math_operations::calc_length_3d (src/mathoperations.cpp:42-46) */
+                const float r = (float)pow(pow((double)(c0 - center[0]), 2.0) + pow((double)(c1 - center[1]), 2.0) +
+                                               pow((double)(c2 - center[2]), 2.0),
+                                           0.5);
+                out[idx3(x, y, z, nx, ny)] =
+                    (float)(-((double)Z * 1E15 * pow(e, 2.0)) / (4 * M_PI * eps0 * ((double)r + 1E-10)));
+            }
+}
+
+/* UniformVector (ic.cpp:80-96): 3N values, block d = dir[d]*value. */
+void or_ic_uniform_vector(int64_t N, const float *dir, float value, float *out)
+{
+    for (int d = 0; d < 3; ++d)
+        for (int64_t i = 0; i < N; ++i) out[d * N + i] = dir[d] * value;
 }

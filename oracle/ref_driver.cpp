@@ -8,6 +8,7 @@
 // C restatement in piro_oracle.c and to generate tests/golden/ fixtures.
 #include <filesystem>
 #include <bc.hpp>
+#include <ic.hpp>
 #include <datatypes.hpp>
 #include <fileutilities.hpp>
 #include <methods.hpp>
@@ -159,6 +160,22 @@ long long ref_initbc(int nx, int ny, int nz, const char *assets_root, const char
     auto &cd1 = MP.getvalue<std::vector<Piro::AMR>>(Piro::MeshParams::AMR)[0].CD[1];
     std::memcpy(field, cd1.values.data(), sizeof(float) * N);
     return q;
+}
+
+// Piro::initialcondition(0) (src/ic.cpp:34-99) for one field whose [IC]
+// filename entry is `ic_name`, reading <assets_root>/assets/IC/distribution.ini.
+// out must hold 3N floats; returns the number of values produced.
+long long ref_initialcondition(int nx, int ny, int nz, float l0, float l1, float l2, const char *assets_root,
+                               const char *ic_name, float *out)
+{
+    set_grid(nx, ny, nz);
+    Piro::file_utilities::current_path = std::string(assets_root);
+    Piro::MeshParams &MP = Piro::MeshParams::getInstance();
+    MP.setvalue(Piro::MeshParams::L, std::vector<float>{l0, l1, l2});
+    MP.setvalue(Piro::MeshParams::ICFILES, std::vector<std::string>{std::string(ic_name)});
+    std::vector<float> v = Piro::initialcondition(0);
+    std::memcpy(out, v.data(), sizeof(float) * v.size());
+    return (long long)v.size();
 }
 
 }  // extern "C"

@@ -21,6 +21,21 @@ psz = C.POINTER(C.c_size_t)
 pint = C.POINTER(C.c_int)
 
 
+class Buf(C.Structure):
+    _fields_ = [("id", C.c_int32), ("n", C.c_int64)]
+
+
+class Op(C.Structure):
+    _fields_ = [("kind", C.c_int32)]
+
+
+class CaseInfo(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("n_cells", C.c_int64),
+                ("timescheme", C.c_int32), ("spacescheme", C.c_int32), ("solverscheme", C.c_int32),
+                ("datatype", C.c_int32), ("simindex", C.c_int32), ("timestep", C.c_float), ("totaltime", C.c_float),
+                ("steps_done", C.c_int64), ("n_fields", C.c_int32), ("bc_cells", C.c_int64)]
+
+
 class BeInfo(C.Structure):
     _fields_ = [("status", C.c_int), ("outer_iterations", C.c_int), ("inner_iterations", C.c_int),
                 ("fallbacks", C.c_int), ("rel_residual", C.c_double)]
@@ -71,6 +86,23 @@ SIGNATURES = {
                                    C.POINTER(C.c_longlong)]),
     "piro_be_destroy": (i32, [vp]),
     "piro_be_jli": (i32, [i32, i32, i32, vp, vp, vp, f32, vp, vp, vp, f32, f32, i32, pint, vp]),
+    "piro_open": (i32, [C.c_char_p, C.c_char_p, C.POINTER(vp)]),
+    "piro_close": (None, [vp]),
+    "piro_ctx_query": (i32, [vp, C.POINTER(CaseInfo)]),
+    "piro_set_alpha_mode": (i32, [vp, i32]),
+    "piro_ddt_r": (i32, [vp, C.c_char_p, C.POINTER(Buf)]),
+    "piro_vector": (i32, [vp, C.c_char_p, C.POINTER(Buf)]),
+    "piro_field": (i32, [vp, C.c_char_p, C.POINTER(Buf)]),
+    "piro_field_upload": (i32, [vp, Buf, vp, i64]),
+    "piro_field_download": (i32, [vp, Buf, vp, i64]),
+    "piro_field_device_ptr": (i32, [vp, Buf, C.POINTER(vp)]),
+    "piro_laplacian": (i32, [vp, C.c_char_p, C.c_char_p, C.POINTER(Op)]),
+    "piro_gradient": (i32, [vp, C.c_char_p, C.POINTER(Op)]),
+    "piro_dot": (i32, [vp, Buf, Op, C.POINTER(Op)]),
+    "piro_assign": (i32, [vp, Buf, Op, C.POINTER(Buf)]),
+    "piro_step_solve": (i32, [vp, Buf, f32]),
+    "piro_solve": (i32, [vp, C.POINTER(C.c_int64)]),
+    "piro_op_export_csr": (i32, [vp, Op, vp, vp, vp, i64, C.POINTER(C.c_int64)]),
 }
 
 

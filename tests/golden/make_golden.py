@@ -107,6 +107,19 @@ def main() -> None:
         name = f"grid_{nx}x{ny}x{nz}.npz"
         np.savez_compressed(os.path.join(HERE, name), **data)
         manifest["grids"].append({"file": name, "n": [nx, ny, nz]})
+    # Initial conditions from Piro::initialcondition (src/ic.cpp), with the
+    # test cases' IC/distribution.ini.
+    ic = {}
+    with tempfile.TemporaryDirectory() as td:
+        os.makedirs(os.path.join(td, "assets", "IC"))
+        src = os.path.join(os.path.dirname(HERE), "cases", "IC", "distribution.ini")
+        with open(src) as f, open(os.path.join(td, "assets", "IC", "distribution.ini"), "w") as g:
+            g.write(f.read())
+        for (nx, ny, nz), l in [((16, 14, 12), (14, 12, 10)), ((11, 10, 9), (9, 8, 7)), ((7, 6, 5), (5, 4, 3.5))]:
+            for kind in ("Gaussian", "Coulomb", "UniformVector"):
+                ic[f"ic_{kind}_{nx}x{ny}x{nz}"] = R.initialcondition(nx, ny, nz, l, td, kind)
+                ic[f"l_{nx}x{ny}x{nz}"] = np.asarray(l, np.float32)
+    np.savez_compressed(os.path.join(HERE, "initial_conditions.npz"), **ic)
     # Large grids: only hashes and counts (arrays would bloat the repository).
     for (nx, ny, nz) in HASH_GRIDS:
         for s in (1, 2, 3):

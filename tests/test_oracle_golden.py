@@ -136,3 +136,44 @@ def test_ht_table_size_reference_sign(oracle):
     # the reference formula turns negative above N ~ 18.6k (27^3 = 19683)
     assert oracle.ht_table_size_reference(7 * 125 - 150, 125) == 4795
     assert oracle.ht_table_size_reference(7 * 19683, 19683) <= 0
+
+
+def test_initial_conditions_bit_exact(oracle):
+    """Gaussian / Coulomb / UniformVector against Piro::initialcondition."""
+    import os
+    from case_oracle import floats, read_ini
+    from conftest import GOLDEN, ROOT
+    g = dict(np.load(os.path.join(GOLDEN, "initial_conditions.npz")))
+    dist = read_ini(os.path.join(ROOT, "tests", "cases", "IC", "distribution.ini"))
+    for key in g:
+        if not key.startswith("ic_"):
+            continue
+        _, kind, dims = key.split("_")
+        nx, ny, nz = map(int, dims.split("x"))
+        l = g[f"l_{dims}"]
+        if kind == "Gaussian":
+            d = dist["Gaussian"]
+            got = oracle.ic_gaussian(nx, ny, nz, l, np.float32(d["Scalefactor"]), floats(d["Sigma"]), floats(d["Median"]))
+        elif kind == "Coulomb":
+            d = dist["Coulomb"]
+            got = oracle.ic_coulomb(nx, ny, nz, l, floats(d["center"]), np.float32(d["Z"]), np.float32(d["e"]),
+                                    np.float32(d["epsilon_0"]))
+        else:
+            d = dist["Vector"]
+            got = oracle.ic_uniform_vector(nx * ny * nz, floats(d["Direction"]), floats(d["Value"])[0])
+        assert f32_bits_equal(got, g[key]), key
+
+
+def test_case_oracle_runs_every_test_case(oracle):
+    """The oracle-composed case runner itself (used by the GPU case tests)."""
+    import os
+    from case_oracle import run_case
+    from conftest import ROOT
+    assets = os.path.join(ROOT, "tests", "cases")
+    r = run_case(assets, "heat_fe_csr.ini")
+    assert r["steps"] == 10 and r["n"] == (16, 14, 12)
+    # the face values of field 1 are restored by setBC every step; edges stay 0
+    idx, fs = oracle.face_lists(16, 14, 12)
+    T = r["fields"][1]
+    assert np.all(T[idx[fs[5]:fs[6]]] == np.float32(1.0))
+    assert T[0] == 0.0
