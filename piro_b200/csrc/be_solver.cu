@@ -103,15 +103,16 @@ struct ResidualRow {
     const double *__restrict__ x;
     float *__restrict__ r, *__restrict__ z;
     double rr64, bb, rz, rr32;
-    __device__ __forceinline__ void operator()(int64_t row, const int32_t *c, const float *v, int n)
+    double q;
+    __device__ __forceinline__ void begin(int64_t) { q = 0.0; }
+    __device__ __forceinline__ void add(int32_t c, float v) { q += (double)v * x[c]; }
+    __device__ __forceinline__ void end(int64_t row)
     {
         if (!g.interior(row)) {
             r[row] = 0.0f;
             z[row] = 0.0f;
             return;
         }
-        double q = 0.0;
-        for (int k = 0; k < n; ++k) q += (double)v[k] * x[c[k]];
         const double bi = (double)b[row];
         const double ri = bi - q;
         const float rf = (float)ri;
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(kTileRows) k_residual(GridDiv g, int64_t N,
     CsrStages &sm = *reinterpret_cast<CsrStages *>(smem_raw);
     __shared__ double s_warp[32];
     __shared__ bool s_last;
-    ResidualRow op{g, alpha, dinv, b, x, r, z, 0.0, 0.0, 0.0, 0.0};
+    ResidualRow op{g, alpha, dinv, b, x, r, z, 0.0, 0.0, 0.0, 0.0, 0.0};
     csr_for_rows(sm, N, rowptr, col, val, op);
     double part[4] = {block_sum(op.rr64, s_warp), block_sum(op.bb, s_warp), block_sum(op.rz, s_warp),
                       block_sum(op.rr32, s_warp)};
@@ -174,15 +175,16 @@ struct CgSpmvRow {
     const float *__restrict__ alpha, *__restrict__ z, *__restrict__ p_old;
     float *__restrict__ p_new, *__restrict__ q;
     double pq;
-    __device__ __forceinline__ void operator()(int64_t row, const int32_t *c, const float *v, int n)
+    float acc;
+    __device__ __forceinline__ void begin(int64_t) { acc = 0.0f; }
+    __device__ __forceinline__ void add(int32_t c, float v) { acc += v * (__ldg(z + c) + beta * __ldg(p_old + c)); }
+    __device__ __forceinline__ void end(int64_t row)
     {
         if (!g.interior(row)) {
             p_new[row] = 0.0f;
             q[row] = 0.0f;
             return;
         }
-        float acc = 0.0f;
-        for (int k = 0; k < n; ++k) acc += v[k] * (__ldg(z + c[k]) + beta * __ldg(p_old + c[k]));
         const float pn = z[row] + beta * p_old[row];
         p_new[row] = pn;
         q[row] = acc;
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(kTileRows) k_cg_spmv(GridDiv g, int64_t N,
     }
     __syncthreads();
     if (s_done) return;
-    CgSpmvRow op{g, s_beta, alpha, z, p_old, p_new, q, 0.0};
+    CgSpmvRow op{g, s_beta, alpha, z, p_old, p_new, q, 0.0, 0.0f};
     csr_for_rows(sm, N, rowptr, col, val, op);
     double part = block_sum(op.pq, s_warp);
     if (!publish_last(partials, kRedCap, 1, &part, &st->ticket[1], &s_last)) return;

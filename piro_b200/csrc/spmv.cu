@@ -26,10 +26,11 @@ struct FeRow {
     float dt;
     const float *__restrict__ u;
     float *__restrict__ out;
-    __device__ __forceinline__ void operator()(int64_t row, const int32_t *c, const float *v, int n) const
+    float result;
+    __device__ __forceinline__ void begin(int64_t) { result = 0.0f; }
+    __device__ __forceinline__ void add(int32_t c, float v) { result = add_rn(result, mul_rn(mul_rn(dt, v), __ldg(u + c))); }
+    __device__ __forceinline__ void end(int64_t row)
     {
-        float result = 0.0f;
-        for (int k = 0; k < n; ++k) result = add_rn(result, mul_rn(mul_rn(dt, v[k]), __ldg(u + c[k])));
         if (g.interior(row)) out[row] = kMode == 0 ? add_rn(result, u[row]) : sub_rn(u[row], result);
     }
 };
@@ -43,7 +44,7 @@ __global__ void __launch_bounds__(kTileRows) k_csr_step(GridDiv g, int64_t N,
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CsrStages &sm = *reinterpret_cast<CsrStages *>(smem_raw);
-    FeRow<kMode> op{g, dt, u, out};
+    FeRow<kMode> op{g, dt, u, out, 0.0f};
     csr_for_rows(sm, N, rowptr, col, val, op);
 }
 
@@ -138,69 +139,43 @@ __global__ void k_ht_spmv(int nx, int ny, int nz, int64_t N, const int64_t *__re
     }
 }
 
-// Matrix-free 7-point update.  A block owns a 32 x 8 tile of (x, y) columns
-// and a run of kZRun planes.  Every load the block needs -- its columns at
-// z0-1 .. z0+kZRun, alpha, and the x/y halo cells of each plane -- is issued
-// up front into registers, so a thread has ~30 independent loads in flight;
-// the planes are then swept with the x/y neighbours exchanged through a
-// shared-memory plane tile.  Algorithmic traffic is 12 bytes per cell (u read,
-// alpha read, out written); the column halo and the two extra planes of each
-// run are served mostly by L2.
-constexpr int kStX = 32, kStY = 8, kZRun = 8;
+// Matrix-free 7-point update: one (x, y) column per thread over a run of
+// kStZ planes, 32 x 8 columns per block.  u at z-1, z, z+1 rolls through
+// registers, so a cell costs six new loads (x and y neighbours from L1/L2,
+// z+1, alpha) and HBM sees each u and alpha value about once: 12 bytes per
+// cell.  Coordinates come from the block indices (no division).
+constexpr int kStX = 32, kStY = 8, kStZ = 8;
 
 __global__ void __launch_bounds__(kStX *kStY) k_stencil(int nx, int ny, int nz, float idx2, float idy2, float idz2,
                                                         float dt, const float *__restrict__ alpha,
                                                         const float *__restrict__ u, float *__restrict__ out)
 {
-    __shared__ float tile[kStY + 2][kStX + 2];
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int x = blockIdx.x * kStX + tx, y = blockIdx.y * kStY + ty;
-    const int z0 = blockIdx.z * kZRun;
+    const int x = blockIdx.x * kStX + threadIdx.x, y = blockIdx.y * kStY + threadIdx.y;
+    if (x >= nx || y >= ny) return;
+    const int z0 = blockIdx.z * kStZ;
+    const int z1 = min(z0 + kStZ, nz);
     const int64_t sxy = (int64_t)nx * ny;
-    const bool in_xy = x < nx && y < ny;
-    const int64_t colm = (int64_t)y * nx + x;
-    // halo role of this thread (at most one x and one y halo cell)
-    const int hxo = tx == 0 ? -1 : tx == kStX - 1 ? 1 : 0;
-    const int hyo = ty == 0 ? -1 : ty == kStY - 1 ? 1 : 0;
-    const bool hx_ok = hxo != 0 && y < ny && x + hxo >= 0 && x + hxo < nx;
-    const bool hy_ok = hyo != 0 && x < nx && y + hyo >= 0 && y + hyo < ny;
-    float c[kZRun + 2], a[kZRun], hx[kZRun], hy[kZRun];
-#pragma unroll
-    for (int j = 0; j < kZRun + 2; ++j) {
-        const int zz = z0 - 1 + j;
-        c[j] = (in_xy && zz >= 0 && zz < nz) ? __ldcs(u + zz * sxy + colm) : 0.0f;
-    }
-#pragma unroll
-    for (int j = 0; j < kZRun; ++j) {
-        const int zz = z0 + j;
-        const bool zok = zz < nz;
-        a[j] = (alpha && in_xy && zok) ? __ldcs(alpha + zz * sxy + colm) : 1.0f;
-        hx[j] = (hx_ok && zok) ? __ldg(u + zz * sxy + colm + hxo) : 0.0f;
-        hy[j] = (hy_ok && zok) ? __ldg(u + zz * sxy + colm + (int64_t)hyo * nx) : 0.0f;
-    }
-#pragma unroll
-    for (int j = 0; j < kZRun; ++j) {
-        const int z = z0 + j;
-        if (z >= nz) break;  // uniform across the block
-        const float cur = c[j + 1];
-        tile[ty + 1][tx + 1] = cur;
-        if (hxo) tile[ty + 1][tx + 1 + hxo] = hx[j];
-        if (hyo) tile[ty + 1 + hyo][tx + 1] = hy[j];
-        __syncthreads();
-        if (in_xy) {
-            const int64_t id = z * sxy + colm;
-            if (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1) {
-                const float c2 = __fmul_rn(2.0f, cur);
-                const float lx = __fmul_rn(__fsub_rn(__fadd_rn(tile[ty + 1][tx + 2], tile[ty + 1][tx]), c2), idx2);
-                const float ly = __fmul_rn(__fsub_rn(__fadd_rn(tile[ty + 2][tx + 1], tile[ty][tx + 1]), c2), idy2);
-                const float lz = __fmul_rn(__fsub_rn(__fadd_rn(c[j + 2], c[j]), c2), idz2);
-                const float lap = __fadd_rn(__fadd_rn(lx, ly), lz);
-                __stcs(out + id, __fadd_rn(cur, __fmul_rn(dt, __fmul_rn(a[j], lap))));
-            } else {
-                __stcs(out + id, cur);
-            }
+    const bool in_xy = x > 0 && x < nx - 1 && y > 0 && y < ny - 1;
+    int64_t id = (int64_t)z0 * sxy + (int64_t)y * nx + x;
+    float zm = z0 > 0 ? __ldg(u + id - sxy) : 0.0f;
+    float c = __ldg(u + id);
+    for (int z = z0; z < z1; ++z, id += sxy) {
+        const float zp = z + 1 < nz ? __ldg(u + id + sxy) : 0.0f;
+        if (in_xy && z > 0 && z < nz - 1) {
+            const float xm = __ldg(u + id - 1), xp = __ldg(u + id + 1);
+            const float ym = __ldg(u + id - nx), yp = __ldg(u + id + nx);
+            const float a = alpha ? __ldg(alpha + id) : 1.0f;
+            const float c2 = __fmul_rn(2.0f, c);
+            const float lx = __fmul_rn(__fsub_rn(__fadd_rn(xp, xm), c2), idx2);
+            const float ly = __fmul_rn(__fsub_rn(__fadd_rn(yp, ym), c2), idy2);
+            const float lz = __fmul_rn(__fsub_rn(__fadd_rn(zp, zm), c2), idz2);
+            const float lap = __fadd_rn(__fadd_rn(lx, ly), lz);
+            __stcs(out + id, __fadd_rn(c, __fmul_rn(dt, __fmul_rn(a, lap))));
+        } else {
+            __stcs(out + id, c);
         }
-        __syncthreads();
+        zm = c;
+        c = zp;
     }
 }
 
@@ -327,7 +302,7 @@ extern "C" int piro_stencil_fe_step(int nx, int ny, int nz, float idx2, float id
 {
     PIRO_ARG(grid_ok(nx, ny, nz) && u && out && u != out, "piro_stencil_fe_step: bad arguments");
     const dim3 block(kStX, kStY);
-    const dim3 grid((unsigned)cdiv(nx, kStX), (unsigned)cdiv(ny, kStY), (unsigned)cdiv(nz, kZRun));
+    const dim3 grid((unsigned)cdiv(nx, kStX), (unsigned)cdiv(ny, kStY), (unsigned)cdiv(nz, kStZ));
     k_stencil<<<grid, block, 0, as_stream(stream)>>>(nx, ny, nz, idx2, idy2, idz2, dt, alpha, u, out);
     PIRO_CHECK_LAUNCH("k_stencil");
     return PIRO_OK;
