@@ -146,6 +146,49 @@ def spmv_section(torch, ops, steps, warmup, peak):
     return res
 
 
+def config_sections(torch, peak):
+    """Configuration 1 (32^3 forward-Euler heat, 100 steps) and the advection
+    part of configuration 2 (256^3 upwind, csrgeam-merged operator, 1000
+    steps), each replayed from a CUDA graph of two steps."""
+    from piro_b200 import fe
+    from piro_b200 import workloads as W
+    out = {}
+    c = W.heat_fe_32()
+    nx, ny, nz = c["n"]
+    N = nx * ny * nz
+    run = fe.FeRunner(nx, ny, nz, torch.from_numpy(c["alpha"]).cuda(), float(c["dt"]))
+    u0 = torch.from_numpy(c["u0"]).cuda()
+    run.run(u0, 10, graph=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run.run(u0, c["steps"], graph=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out["heat_fe_32"] = {"steps": c["steps"], "ms_total": round(ms, 4), "us_per_step": round(1e3 * ms / c["steps"], 2),
+                         "note": "includes the one-off graph capture; 32^3 = 2.3 MB per step is launch-bound"}
+    c = W.advection(256)
+    nx, ny, nz = c["n"]
+    N = nx * ny * nz
+    run = fe.AdvectionRunner(nx, ny, nz, torch.from_numpy(c["v"]).cuda(), float(c["dt"]), float(c["gnorm"]))
+    nnz = run.A[2].numel()
+    u0 = torch.from_numpy(c["u0"]).cuda()
+    run.run(u0, 4, graph=True)
+    steps = c["steps"]
+    e0.record()
+    run.run(u0, steps, graph=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    byt = 8 * nnz + 4 * (N + 1) + 8 * N
+    out["advection_256"] = {"steps": steps, "ms_per_step": round(ms, 4), "nnz": nnz, "gbs": round(byt / ms / 1e6, 1),
+                            "frac": round(byt / ms / 1e6 / peak, 4),
+                            "note": "per step: memset + SpMVCSR-order step + setBC; bytes counted for the step kernel"}
+    del run
+    torch.cuda.empty_cache()
+    return out
+
+
 # ------------------------------------------------------------------ arms
 def run_piro(args):
     import torch
@@ -260,6 +303,7 @@ def run_piro(args):
         e2e_ms = float(t.item())
 
     spmv = spmv_section(torch, ops, steps=20, warmup=3, peak=peak) if rank == 0 else None
+    configs = config_sections(torch, peak) if rank == 0 else None
 
     cpu = None
     fp64 = None
@@ -309,6 +353,7 @@ def run_piro(args):
         "gpu_launches": launches,
         "clocks": ck,
         "spmv_256": spmv,
+        "configs": configs,
         "fp64_check": fp64,
         "cpu_baseline": cpu,
     }

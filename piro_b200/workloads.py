@@ -73,3 +73,22 @@ def spmv_256(seed: int = 1, n: int = 256):
     f = np.sin(2 * np.pi * (k[0] * ax[None, None, :] + k[1] * ax[None, :, None] + k[2] * ax[:, None, None]) / n + phi)
     u = f.astype(np.float32).reshape(-1)
     return dict(n=(n, n, n), u=u, alpha=alpha)
+
+
+def advection(n: int, seed: int = 1):
+    """Upwind advection (space scheme 1): velocity w = (1.0, 0.5, 0.25) passed
+    as v = -w because the upwind gradient rows are a backward difference over
+    2h (stencils.cpp:78-154); dt = 0.5 * 2h / |w|_1, i.e. CFL 0.5 in the
+    reference's scaling.  Field: sin(2 pi (k . x) / n + phi), k and phi from
+    default_rng(seed)."""
+    rng = np.random.default_rng(seed)
+    k = rng.integers(1, 4, size=3)
+    phi = rng.uniform(0, 2 * np.pi)
+    ax = np.arange(n, dtype=np.float64)
+    f = np.sin(2 * np.pi * (k[0] * ax[None, None, :] + k[1] * ax[None, :, None] + k[2] * ax[:, None, None]) / n + phi)
+    u0 = f.astype(np.float32).reshape(-1)
+    w = np.array([1.0, 0.5, 0.25])
+    N = n ** 3
+    v = np.concatenate([np.full(N, -w[d], np.float32) for d in range(3)])
+    dt = np.float32(0.5 * 2.0 / np.abs(w).sum())
+    return dict(n=(n, n, n), u0=u0, v=v, dt=dt, steps=1000, gnorm=np.float32(2.0))
