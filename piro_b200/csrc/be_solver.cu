@@ -126,7 +126,7 @@ struct ResidualRow {
     }
 };
 
-__global__ void __launch_bounds__(kTileRows) k_residual(GridDiv g, int64_t N,
+__global__ void __launch_bounds__(kRowThreads) k_residual(GridDiv g, int64_t N,
                                                         const int32_t *__restrict__ rowptr,
                                                         const int32_t *__restrict__ col,
                                                         const float *__restrict__ val,
@@ -136,12 +136,10 @@ __global__ void __launch_bounds__(kTileRows) k_residual(GridDiv g, int64_t N,
                                                         float *__restrict__ z, double *__restrict__ partials,
                                                         DevState *__restrict__ st, double rtol, double inner_floor)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    CsrStages &sm = *reinterpret_cast<CsrStages *>(smem_raw);
     __shared__ double s_warp[32];
     __shared__ bool s_last;
     ResidualRow op{g, alpha, dinv, b, x, r, z, 0.0, 0.0, 0.0, 0.0, 0.0};
-    csr_for_rows(sm, N, rowptr, col, val, op);
+    csr_for_rows(N, rowptr, col, val, op);
     double part[4] = {block_sum(op.rr64, s_warp), block_sum(op.bb, s_warp), block_sum(op.rz, s_warp),
                       block_sum(op.rr32, s_warp)};
     if (!publish_last(partials, kRedCap, 4, part, &st->ticket[0], &s_last)) return;
@@ -192,7 +190,7 @@ struct CgSpmvRow {
     }
 };
 
-__global__ void __launch_bounds__(kTileRows) k_cg_spmv(GridDiv g, int64_t N,
+__global__ void __launch_bounds__(kRowThreads) k_cg_spmv(GridDiv g, int64_t N,
                                                        const int32_t *__restrict__ rowptr,
                                                        const int32_t *__restrict__ col,
                                                        const float *__restrict__ val,
@@ -201,8 +199,6 @@ __global__ void __launch_bounds__(kTileRows) k_cg_spmv(GridDiv g, int64_t N,
                                                        float *__restrict__ q, double *__restrict__ partials,
                                                        DevState *__restrict__ st)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    CsrStages &sm = *reinterpret_cast<CsrStages *>(smem_raw);
     __shared__ double s_warp[32];
     __shared__ bool s_last;
     __shared__ int s_done;
@@ -214,7 +210,7 @@ __global__ void __launch_bounds__(kTileRows) k_cg_spmv(GridDiv g, int64_t N,
     __syncthreads();
     if (s_done) return;
     CgSpmvRow op{g, s_beta, alpha, z, p_old, p_new, q, 0.0, 0.0f};
-    csr_for_rows(sm, N, rowptr, col, val, op);
+    csr_for_rows(N, rowptr, col, val, op);
     double part = block_sum(op.pq, s_warp);
     if (!publish_last(partials, kRedCap, 1, &part, &st->ticket[1], &s_last)) return;
     const double tot = gather_sum(partials, s_warp);
@@ -949,7 +945,7 @@ static int be_capture_chunk(piro_be_solver *s)
                                                                    s->vself, s->vnb, s->alpha, s->z, p_old, p_new,
                                                                    s->q, s->partials, s->st);
         else
-            k_cg_spmv<<<s->grid_tiles, kTileRows, sizeof(CsrStages), s->stream>>>(
+            k_cg_spmv<<<s->grid_tiles, kRowThreads, 0, s->stream>>>(
                 GridDiv(s->nx, s->ny, s->nz), s->N, s->rowptr, s->col, s->val, s->alpha, s->z, p_old, p_new, s->q,
                 s->partials, s->st);
         cudaEventRecordWithFlags(s->ev1[it], s->stream, cudaEventRecordExternal);
@@ -1038,15 +1034,7 @@ static int be_create(int nx, int ny, int nz, const int32_t *rowptr, const int32_
         return PIRO_ERR_CUDA;
     }
     const int64_t N = s->N;
-    s->grid_tiles = (unsigned)std::min<int64_t>(cdiv(N, kTileRows), (int64_t)sm_count() * 4);
-    if (cudaFuncSetAttribute(k_cg_spmv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CsrStages)) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(k_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(CsrStages)) !=
-            cudaSuccess) {
-        be_free(s);
-        piro::set_error("piro_be_create: cannot raise the shared-memory limit");
-        return PIRO_ERR_CUDA;
-    }
+    s->grid_tiles = csr_rows_grid(N);
     s->grid_elem = (unsigned)std::min<int64_t>(std::max<int64_t>(1, cdiv(N / 4, 256)), (int64_t)kRedCap);
     if (s->grid_tiles > (unsigned)kRedCap || s->grid_elem > (unsigned)kRedCap) {
         be_free(s);
@@ -1241,7 +1229,7 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
     PIRO_CUDA(cudaMemsetAsync(s->d, 0, sizeof(float) * (size_t)N, st));
     double prev_rel = INFINITY;
     for (int outer = 0; outer <= max_outer; ++outer) {
-        k_residual<<<s->grid_tiles, kTileRows, sizeof(CsrStages), st>>>(GridDiv(s->nx, s->ny, s->nz), N, s->rowptr,
+        k_residual<<<s->grid_tiles, kRowThreads, 0, st>>>(GridDiv(s->nx, s->ny, s->nz), N, s->rowptr,
                                                                         s->col, s->val, s->alpha,
                                                        s->dinv, b, s->x64, s->r, s->z, s->partials, s->st, rtol,
                                                        s->inner_floor);

@@ -4,13 +4,9 @@
 // the elementwise kernels.
 //
 // CSR layout in HBM: rowptr int32[N+1], col int32[nnz], val float[nnz].  The
-// CSR kernels are HBM-bound (8 bytes per nonzero + 12 per row); a block takes
-// a tile of kTileRows consecutive rows, streams the tile's col/val range into
-// shared memory with 16-byte vector loads (fully coalesced, no reuse through
-// L1), then each thread reduces its own row from shared memory in storage
-// order -- the reference's summation order -- so results are bit-exact with
-// SpMVCSR.cl.  Field gathers u[col] hit L2 (the 7 neighbours of a tile lie in
-// five x-lines of three z-planes).
+// CSR kernels are HBM-bound (8 bytes per nonzero + 12 per row) and share the
+// row loop of csr_tile.cuh: one row per thread in storage order -- the
+// reference's summation order -- so results are bit-exact with SpMVCSR.cl.
 #include "common.cuh"
 #include "csr_tile.cuh"
 
@@ -36,16 +32,13 @@ struct FeRow {
 };
 
 template <int kMode>
-__global__ void __launch_bounds__(kTileRows) k_csr_step(GridDiv g, int64_t N,
-                                                        const int32_t *__restrict__ rowptr,
-                                                        const int32_t *__restrict__ col,
-                                                        const float *__restrict__ val, float dt,
-                                                        const float *__restrict__ u, float *__restrict__ out)
+__global__ void __launch_bounds__(kRowThreads) k_csr_step(GridDiv g, int64_t N, const int32_t *__restrict__ rowptr,
+                                                          const int32_t *__restrict__ col,
+                                                          const float *__restrict__ val, float dt,
+                                                          const float *__restrict__ u, float *__restrict__ out)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    CsrStages &sm = *reinterpret_cast<CsrStages *>(smem_raw);
     FeRow<kMode> op{g, dt, u, out, 0.0f};
-    csr_for_rows(sm, N, rowptr, col, val, op);
+    csr_for_rows(N, rowptr, col, val, op);
 }
 
 // COO: each warp takes 32 consecutive entries per pass; a segmented inclusive
@@ -228,15 +221,8 @@ int launch_csr_step(int nx, int ny, int nz, const int32_t *rowptr, const int32_t
     PIRO_ARG(rowptr && col && val && u && out, "csr step: null pointer");
     PIRO_ARG(u != out, "csr step: u and out must differ (the reference writes a fresh buffer)");
     const int64_t N = (int64_t)nx * ny * nz;
-    static bool attr_set[2] = {false, false};
-    if (!attr_set[kMode]) {
-        PIRO_CUDA(cudaFuncSetAttribute(k_csr_step<kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sizeof(CsrStages)));
-        attr_set[kMode] = true;
-    }
-    const unsigned grid = (unsigned)std::min<int64_t>(cdiv(N, kTileRows), (int64_t)sm_count() * 4);
-    k_csr_step<kMode><<<grid, kTileRows, sizeof(CsrStages), as_stream(stream)>>>(GridDiv(nx, ny, nz), N, rowptr, col,
-                                                                                val, dt, u, out);
+    k_csr_step<kMode><<<csr_rows_grid(N), kRowThreads, 0, as_stream(stream)>>>(GridDiv(nx, ny, nz), N, rowptr, col,
+                                                                              val, dt, u, out);
     PIRO_CHECK_LAUNCH("k_csr_step");
     return PIRO_OK;
 }
