@@ -247,6 +247,7 @@ typedef struct piro_be_info {
 /* Preconditioner kinds for piro_be_set_preconditioner. */
 #define PIRO_PRECOND_JACOBI 0
 #define PIRO_PRECOND_LEARNED 1
+#define PIRO_PRECOND_JACOBI_FLEX 2 /* Jacobi inside the flexible-CG iteration (checks that path) */
 
 /* Create a solver for A x = b with A = I - dt*diag(alpha)*L given as CSR over
  * all N rows (device pointers, which must stay valid).  Interior rows are the
@@ -288,6 +289,56 @@ int piro_be_solution_f64(piro_be_solver *s, const double **x64);
 int piro_be_kernel_stats(piro_be_solver *s, int reset, long long *spmv_launches, double *spmv_ms,
                          long long *kernel_launches);
 int piro_be_destroy(piro_be_solver *s);
+
+/* -- learned preconditioner (flexible CG inside the backward-Euler solve) -----
+ *
+ * A 3-D convolutional net z = M(r, f): four 3x3x3 convolutions, channels
+ * 2 -> 16 -> 16 -> 16 -> 1, GELU after the first three, zero padding outside
+ * the interior, BF16 weights and activations with FP32 accumulation.  Input
+ * channels per cell: the residual r (scaled to unit RMS over the interior by
+ * the solver) and r*f with the feature f = log(dt * alpha / h^2); output: an
+ * approximation of the error A^-1 r.  With no biases M(0) = 0.  It is trained on the device with the library's own
+ * forward and backward kernels (masked MSE against the error, Adam).  PIRO has
+ * no learned component: this extends TIMESCHEME 12
+ * (src/kernelprocess.cpp:123-209), with Jacobi-PCG kept as the fallback. */
+typedef struct piro_pcnet piro_pcnet;
+
+/* Number of parameters (one flat FP32 vector: per layer W[tap][ci][co],
+ * tap = (dz+1)*9 + (dy+1)*3 + (dx+1); the convolutions have no bias, so a
+ * zero residual maps to a zero correction). */
+int piro_pcnet_num_params(int64_t *n);
+/* New network with deterministic He-normal weights from `seed`. */
+int piro_pcnet_create(uint64_t seed, piro_pcnet **out);
+/* Host copies of the parameters: FP32 master values, or (rounded != 0) the
+ * BF16-rounded values the kernels use.  set_params also resets Adam. */
+int piro_pcnet_get_params(piro_pcnet *n, float *host, int64_t count, int rounded);
+int piro_pcnet_set_params(piro_pcnet *n, const float *host, int64_t count);
+/* out[b][c] = M(r[b], feat[b]) over `batch` grids of nx*ny*nz cells (device
+ * float arrays, batch-major; feat may be NULL = 0).  Boundary outputs are 0. */
+int piro_pcnet_forward(piro_pcnet *n, int batch, int nx, int ny, int nz, const float *r, const float *feat,
+                       float *out, piro_stream_t stream);
+/* Forward + backward: loss = sum mask*(M(r,f) - target)^2 / sum mask; the
+ * parameter gradient is kept on the device for piro_pcnet_adam_step.  loss
+ * (host double) and grad (host float[num_params]) may be NULL; when either is
+ * given the call synchronizes the stream. */
+int piro_pcnet_loss_grad(piro_pcnet *n, int batch, int nx, int ny, int nz, const float *r, const float *feat,
+                         const float *target, const float *mask, double *loss, float *grad, piro_stream_t stream);
+/* Adam (beta1 0.9, beta2 0.999, eps 1e-8) with the last computed gradient. */
+int piro_pcnet_adam_step(piro_pcnet *n, float lr, piro_stream_t stream);
+/* Kernels launched by this network so far. */
+int piro_pcnet_stats(piro_pcnet *n, long long *launches);
+int piro_pcnet_destroy(piro_pcnet *n);
+
+/* Select the inner preconditioner of a stencil solver (piro_be_create_stencil):
+ * PIRO_PRECOND_JACOBI, or PIRO_PRECOND_LEARNED with a network (not owned; it
+ * must outlive the solver's use of it).  With the learned preconditioner the
+ * inner solve is flexible CG (Notay's FCG(1)) on the graph-launched path; a
+ * refinement sweep that stalls (FP64 residual not halved) or breaks down
+ * reverts to Jacobi-PCG for the rest of the solve (piro_be_info.fallbacks). */
+int piro_be_set_preconditioner(piro_be_solver *s, int kind, piro_pcnet *net);
+/* Live timing of the learned preconditioner: network applies since the last
+ * reset and their summed device time in ms (CUDA events around each apply). */
+int piro_be_pc_stats(piro_be_solver *s, int reset, long long *applies, double *ms);
 
 /* Reference JLI iteration (scheme 12 + solver 40, src/kernelprocess.cpp:123-209)
  * on the device: x = b; repeat r = b - (I - dt*L)x on interior rows (b on the

@@ -86,6 +86,17 @@ SIGNATURES = {
                                    C.POINTER(C.c_longlong)]),
     "piro_be_destroy": (i32, [vp]),
     "piro_be_jli": (i32, [i32, i32, i32, vp, vp, vp, f32, vp, vp, vp, f32, f32, i32, pint, vp]),
+    "piro_pcnet_num_params": (i32, [pi64]),
+    "piro_pcnet_create": (i32, [C.c_uint64, C.POINTER(vp)]),
+    "piro_pcnet_get_params": (i32, [vp, vp, i64, i32]),
+    "piro_pcnet_set_params": (i32, [vp, vp, i64]),
+    "piro_pcnet_forward": (i32, [vp, i32, i32, i32, i32, vp, vp, vp, vp]),
+    "piro_pcnet_loss_grad": (i32, [vp, i32, i32, i32, i32, vp, vp, vp, vp, C.POINTER(C.c_double), vp, vp]),
+    "piro_pcnet_adam_step": (i32, [vp, f32, vp]),
+    "piro_pcnet_stats": (i32, [vp, C.POINTER(C.c_longlong)]),
+    "piro_pcnet_destroy": (i32, [vp]),
+    "piro_be_set_preconditioner": (i32, [vp, i32, vp]),
+    "piro_be_pc_stats": (i32, [vp, i32, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]),
     "piro_open": (i32, [C.c_char_p, C.c_char_p, C.POINTER(vp)]),
     "piro_close": (None, [vp]),
     "piro_ctx_query": (i32, [vp, C.POINTER(CaseInfo)]),

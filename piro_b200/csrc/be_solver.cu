@@ -29,10 +29,15 @@ namespace piro {
 
 int dot_f64(int64_t n, const float *x, const float *y, double *out, void *work, size_t work_bytes, cudaStream_t s);
 size_t reduce_workspace_bytes(int64_t n);
+size_t pcnet_apply_bytes(int64_t N);
+int pcnet_apply(const piro_pcnet *n, void *work, const GridDiv &g, int64_t N, const float *r, const float *feat,
+                const double *rr, double n_int, float *z, const int *skip, cudaStream_t st);
 
 namespace {
 
 constexpr int kChunk = 8;       // CG iterations per graph launch (even: p buffers alternate)
+constexpr int kChunkF = 4;      // flexible-CG (Jacobi) iterations per graph launch (even)
+constexpr int kLearnedIters = 2;  // iterations per sweep preconditioned by the network (even)
 constexpr int kRedCap = 4096;   // max blocks of a reducing kernel
 
 struct DevState {
@@ -54,6 +59,7 @@ struct DevState {
     int bar_err;
     int p_status, p_outer, p_inner;
     double p_rel;
+    double pq;      // flexible CG: <p, S p> of the last direction
 };
 
 __device__ __forceinline__ double block_sum(double v, double *s_warp)
@@ -401,6 +407,206 @@ __global__ void __launch_bounds__(256) k_cg_update(int64_t N, int64_t n4, const 
         }
         st->ticket[2] = 0u;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Flexible CG (Notay's FCG(1)) for a preconditioner that changes from one
+// iteration to the next.  In the symmetric form S = diag(alpha)^-1 A_II with
+// s = r / alpha and z approximating S^-1 s = A^-1 r:
+//   beta = -<z, S p_old> / <p_old, S p_old>   (0 on a sweep's first iteration)
+//   p = z + beta p_old,  q = A p,  a = <p, s> / <p, S p>
+//   d += a p,  r -= a q
+// With the learned preconditioner the first kLearnedIters iterations of a
+// sweep take z = zt + D^-1 (r - A zt), zt = M(r) the network's output
+// followed by one Jacobi correction; the later iterations take z = D^-1 r.
+// A 9^3 receptive field resolves the error well where dt*alpha/h^2 is small
+// but not where the coupling length sqrt(dt*alpha)/h approaches the field's
+// radius: there the network's output for its own later residuals is no
+// better than zero, so it is used only where it pays, at the start.
+// Kernels: k_fcg_hybrid (learned iterations), k_fcg_beta (computes the Jacobi
+// z itself when asked), k_fcg_spmv_mf (matrix-free 7-point A) and k_fcg_update.
+__global__ void __launch_bounds__(256) k_fcg_beta(int64_t N, const float *__restrict__ alpha,
+                                                  const float *__restrict__ dinv, const float *__restrict__ r,
+                                                  float *__restrict__ z, const float *__restrict__ q, int jacobi,
+                                                  double *__restrict__ partials, DevState *__restrict__ st)
+{
+    __shared__ double s_warp[32];
+    __shared__ bool s_last;
+    __shared__ int s_done, s_first;
+    if (threadIdx.x == 0) {
+        s_done = *((volatile int *)&st->done);
+        s_first = *((volatile int *)&st->iters) == 0;
+    }
+    __syncthreads();
+    if (s_done) return;
+    double zq = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const float di = dinv[i];
+        float zi;
+        if (jacobi) {
+            zi = r[i] * di;
+            z[i] = zi;
+        } else {
+            zi = z[i];
+        }
+        if (!s_first && di != 0.0f) zq += (double)zi * (double)q[i] / (double)alpha[i];
+    }
+    if (s_first) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->beta = 0.0;
+        return;
+    }
+    double part = block_sum(zq, s_warp);
+    if (!publish_last(partials, kRedCap, 1, &part, &st->ticket[3], &s_last)) return;
+    const double tot = gather_sum(partials, s_warp);
+    if (threadIdx.x == 0) {
+        const double beta = -tot / st->pq;
+        if (!isfinite(beta)) {
+            st->broken = 1;
+            st->done = 1;
+        } else {
+            st->beta = beta;
+        }
+        st->ticket[3] = 0u;
+    }
+}
+
+// z = zt + D^-1 (r - A zt) on interior cells (matrix-free 7-point A, zt = 0
+// on the boundary): one Jacobi correction of the network's output.
+__global__ void __launch_bounds__(kMfThreads) k_fcg_hybrid(GridDiv g, int64_t N, float mdt, float vself, float vnb,
+                                                            const float *__restrict__ alpha,
+                                                            const float *__restrict__ dinv,
+                                                            const float *__restrict__ zt, const float *__restrict__ r,
+                                                            float *__restrict__ z, const DevState *__restrict__ st)
+{
+    if (*((volatile const int *)&st->done)) return;
+    const int64_t sxy = (int64_t)g.nx * g.ny;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        int x, y, zc;
+        g.coords((uint32_t)i, x, y, zc);
+        if (x > 0 && x < g.nx - 1 && y > 0 && y < g.ny - 1 && zc > 0 && zc < g.nz - 1) {
+            const float a = __ldg(alpha + i);
+            const float cur = __ldg(zt + i);
+            const float nb = ((__ldg(zt + i - 1) + __ldg(zt + i + 1)) + (__ldg(zt + i - g.nx) + __ldg(zt + i + g.nx))) +
+                             (__ldg(zt + i - sxy) + __ldg(zt + i + sxy));
+            const float cd = __fadd_rn(1.0f, __fmul_rn(mdt, __fmul_rn(a, vself)));
+            const float co = __fmul_rn(mdt, __fmul_rn(a, vnb));
+            z[i] = cur + dinv[i] * (r[i] - (cd * cur + co * nb));
+        } else {
+            z[i] = 0.0f;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kMfThreads) k_fcg_spmv_mf(GridDiv g, int64_t N, float mdt, float vself, float vnb,
+                                                             const float *__restrict__ alpha,
+                                                             const float *__restrict__ z,
+                                                             const float *__restrict__ p_old,
+                                                             const float *__restrict__ r, float *__restrict__ p_new,
+                                                             float *__restrict__ q, double *__restrict__ partials,
+                                                             DevState *__restrict__ st)
+{
+    __shared__ double s_warp[32];
+    __shared__ bool s_last;
+    __shared__ int s_done;
+    __shared__ float s_beta;
+    if (threadIdx.x == 0) {
+        s_done = *((volatile int *)&st->done);
+        s_beta = (float)st->beta;
+    }
+    __syncthreads();
+    if (s_done) return;
+    const float beta = s_beta;
+    const int64_t sxy = (int64_t)g.nx * g.ny;
+    double pq = 0.0, pr = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        int x, y, zc;
+        g.coords((uint32_t)i, x, y, zc);
+        if (x > 0 && x < g.nx - 1 && y > 0 && y < g.ny - 1 && zc > 0 && zc < g.nz - 1) {
+            const float a = __ldg(alpha + i);
+            const float cur = __ldg(z + i) + beta * __ldg(p_old + i);
+            const float xm = __ldg(z + i - 1) + beta * __ldg(p_old + i - 1);
+            const float xp = __ldg(z + i + 1) + beta * __ldg(p_old + i + 1);
+            const float ym = __ldg(z + i - g.nx) + beta * __ldg(p_old + i - g.nx);
+            const float yp = __ldg(z + i + g.nx) + beta * __ldg(p_old + i + g.nx);
+            const float zm = __ldg(z + i - sxy) + beta * __ldg(p_old + i - sxy);
+            const float zp = __ldg(z + i + sxy) + beta * __ldg(p_old + i + sxy);
+            const float cd = __fadd_rn(1.0f, __fmul_rn(mdt, __fmul_rn(a, vself)));
+            const float co = __fmul_rn(mdt, __fmul_rn(a, vnb));
+            const float qv = cd * cur + co * (((xm + xp) + (ym + yp)) + (zm + zp));
+            p_new[i] = cur;
+            q[i] = qv;
+            pq += (double)cur * (double)qv / (double)a;
+            pr += (double)cur * (double)__ldg(r + i) / (double)a;
+        } else {
+            p_new[i] = 0.0f;
+            q[i] = 0.0f;
+        }
+    }
+    double part[2] = {block_sum(pq, s_warp), block_sum(pr, s_warp)};
+    if (!publish_last(partials, kRedCap, 2, part, &st->ticket[1], &s_last)) return;
+    double tot[2];
+    for (int t = 0; t < 2; ++t) tot[t] = gather_sum(partials + t * kRedCap, s_warp);
+    if (threadIdx.x == 0) {
+        const double aa = tot[1] / tot[0];
+        st->pq = tot[0];
+        if (!isfinite(aa) || tot[0] <= 0.0) {
+            st->broken = 1;
+            st->done = 1;
+            st->a = 0.0;
+        } else {
+            st->a = aa;
+        }
+        st->ticket[1] = 0u;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_fcg_update(int64_t N, const float *__restrict__ dinv,
+                                                    const float *__restrict__ p, const float *__restrict__ q,
+                                                    float *__restrict__ d, float *__restrict__ r,
+                                                    double *__restrict__ partials, DevState *__restrict__ st)
+{
+    __shared__ double s_warp[32];
+    __shared__ bool s_last;
+    __shared__ int s_done;
+    __shared__ float s_a;
+    if (threadIdx.x == 0) {
+        s_done = *((volatile int *)&st->done);
+        s_a = (float)st->a;
+    }
+    __syncthreads();
+    if (s_done) return;
+    const float a = s_a;
+    double rr = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        if (dinv[i] == 0.0f) continue;
+        d[i] += a * p[i];
+        const float ri = r[i] - a * q[i];
+        r[i] = ri;
+        rr += (double)ri * (double)ri;
+    }
+    double part = block_sum(rr, s_warp);
+    if (!publish_last(partials, kRedCap, 1, &part, &st->ticket[2], &s_last)) return;
+    const double tot = gather_sum(partials, s_warp);
+    if (threadIdx.x == 0) {
+        st->rr = tot;
+        const int it = st->iters + 1;
+        st->iters = it;
+        if (!isfinite(tot)) {
+            st->broken = 1;
+            st->done = 1;
+        } else if (tot <= st->tol2 * st->rr0 || it >= st->max_iters) {
+            st->done = 1;
+        }
+        st->ticket[2] = 0u;
+    }
+}
+
+// Network feature log(dt * alpha / h^2) on interior cells (0 elsewhere).
+__global__ void k_pc_feature(GridDiv g, int64_t N, const float *__restrict__ alpha, float dt_vnb,
+                             float *__restrict__ feat)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        feat[i] = g.interior(i) ? logf(dt_vnb * alpha[i]) : 0.0f;
 }
 
 // ---------------------------------------------------------------------------
@@ -899,6 +1105,18 @@ struct piro_be_solver {
     double spmv_ms;
     long long spmv_launches;
     long long kernel_launches;  // every kernel this solver launched
+    // learned preconditioner (flexible CG on the graph-launched path)
+    int pc_kind;
+    piro_pcnet *net;
+    float *feat;
+    void *pc_work;
+    float *zt;                  // network output before the Jacobi correction
+    cudaGraph_t graph_f, graph_l;
+    cudaGraphExec_t exec_f;     // kChunkF flexible-CG iterations with Jacobi z
+    cudaGraphExec_t exec_l;     // kLearnedIters iterations with the network
+    cudaEvent_t evf0[kLearnedIters], evf1[kLearnedIters];
+    double pc_ms;
+    long long pc_applies;
 };
 
 static void be_free(piro_be_solver *s)
@@ -912,6 +1130,17 @@ static void be_free(piro_be_solver *s)
     if (s->ev_in) cudaEventDestroy(s->ev_in);
     if (s->graph) cudaGraphDestroy(s->graph);
     if (s->pev0) cudaEventDestroy(s->pev0);
+    for (int i = 0; i < kLearnedIters; ++i) {
+        if (s->evf0[i]) cudaEventDestroy(s->evf0[i]);
+        if (s->evf1[i]) cudaEventDestroy(s->evf1[i]);
+    }
+    if (s->exec_f) cudaGraphExecDestroy(s->exec_f);
+    if (s->graph_f) cudaGraphDestroy(s->graph_f);
+    if (s->exec_l) cudaGraphExecDestroy(s->exec_l);
+    if (s->graph_l) cudaGraphDestroy(s->graph_l);
+    cudaFree(s->zt);
+    cudaFree(s->feat);
+    cudaFree(s->pc_work);
     if (s->pev1) cudaEventDestroy(s->pev1);
     cudaFree(s->ib_ptr);
     cudaFree(s->ib_col);
@@ -958,6 +1187,67 @@ static int be_capture_chunk(piro_be_solver *s)
         return PIRO_ERR_CUDA;
     }
     PIRO_CUDA(cudaGraphInstantiate(&s->exec, s->graph, 0));
+    return PIRO_OK;
+}
+
+// Capture flexible-CG iterations: with the network (kLearnedIters of them,
+// events around each network apply give its live device time) or with the
+// Jacobi z (kChunkF).  Both start on p[0] and end on p[0].
+static int be_capture_fcg(piro_be_solver *s, bool with_net)
+{
+    const GridDiv g(s->nx, s->ny, s->nz);
+    const double n_int = (double)(s->nx - 2) * (double)(s->ny - 2) * (double)(s->nz - 2);
+    const int iters = with_net ? kLearnedIters : kChunkF;
+    if (with_net)
+        for (int i = 0; i < kLearnedIters; ++i) {
+            if (!s->evf0[i]) PIRO_CUDA(cudaEventCreate(&s->evf0[i]));
+            if (!s->evf1[i]) PIRO_CUDA(cudaEventCreate(&s->evf1[i]));
+        }
+    PIRO_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = PIRO_OK;
+    for (int it = 0; it < iters && rc == PIRO_OK; ++it) {
+        const float *p_old = s->p[it & 1];
+        float *p_new = s->p[(it + 1) & 1];
+        if (with_net) {
+            cudaEventRecordWithFlags(s->evf0[it], s->stream, cudaEventRecordExternal);
+            rc = pcnet_apply(s->net, s->pc_work, g, s->N, s->r, s->feat, &s->st->rr, n_int, s->zt, &s->st->done,
+                             s->stream);
+            cudaEventRecordWithFlags(s->evf1[it], s->stream, cudaEventRecordExternal);
+            if (rc != PIRO_OK) break;
+            k_fcg_hybrid<<<s->grid_mf, kMfThreads, 0, s->stream>>>(g, s->N, s->mdt, s->vself, s->vnb, s->alpha,
+                                                                   s->dinv, s->zt, s->r, s->z, s->st);
+        }
+        k_fcg_beta<<<s->grid_elem, 256, 0, s->stream>>>(s->N, s->alpha, s->dinv, s->r, s->z, s->q, with_net ? 0 : 1,
+                                                        s->partials, s->st);
+        k_fcg_spmv_mf<<<s->grid_mf, kMfThreads, 0, s->stream>>>(g, s->N, s->mdt, s->vself, s->vnb, s->alpha, s->z,
+                                                                 p_old, s->r, p_new, s->q, s->partials, s->st);
+        k_fcg_update<<<s->grid_elem, 256, 0, s->stream>>>(s->N, s->dinv, p_new, s->q, s->d, s->r, s->partials,
+                                                          s->st);
+    }
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    if (rc != PIRO_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        piro::set_error("flexible-CG graph capture: %s", cudaGetErrorString(e));
+        return PIRO_ERR_CUDA;
+    }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        piro::set_error("flexible-CG graph instantiate: %s", cudaGetErrorString(e));
+        return PIRO_ERR_CUDA;
+    }
+    if (with_net) {
+        s->graph_l = graph;
+        s->exec_l = exec;
+    } else {
+        s->graph_f = graph;
+        s->exec_f = exec;
+    }
     return PIRO_OK;
 }
 
@@ -1136,6 +1426,66 @@ extern "C" int piro_be_create_stencil(int nx, int ny, int nz, const int32_t *row
     return be_create(nx, ny, nz, rowptr, col, val, alpha, true, dt, norm, stream, out);
 }
 
+extern "C" int piro_be_set_preconditioner(piro_be_solver *s, int kind, piro_pcnet *net)
+{
+    PIRO_ARG(s && (kind == PIRO_PRECOND_JACOBI || kind == PIRO_PRECOND_JACOBI_FLEX ||
+                   (kind == PIRO_PRECOND_LEARNED && net)),
+             "piro_be_set_preconditioner: bad arguments");
+    if (kind == PIRO_PRECOND_JACOBI) {
+        s->pc_kind = PIRO_PRECOND_JACOBI;
+        return PIRO_OK;
+    }
+    if (kind == PIRO_PRECOND_JACOBI_FLEX) net = nullptr;
+    if (!s->op_mf) {
+        piro::set_error("piro_be_set_preconditioner: flexible CG needs the matrix-free stencil operator "
+                        "(piro_be_create_stencil on a verified central-scheme A)");
+        return PIRO_ERR_STATE;
+    }
+    const int64_t N = s->N;
+    if (!s->exec_f) {
+        int rc = be_capture_fcg(s, false);
+        if (rc != PIRO_OK) return rc;
+    }
+    if (net) {
+        if (!s->feat) {
+            PIRO_CUDA(cudaMalloc(&s->feat, sizeof(float) * (size_t)N));
+            PIRO_CUDA(cudaMalloc(&s->zt, sizeof(float) * (size_t)N));
+            PIRO_CUDA(cudaMalloc(&s->pc_work, pcnet_apply_bytes(N)));
+            PIRO_CUDA(cudaMemsetAsync(s->zt, 0, sizeof(float) * (size_t)N, s->stream));
+            k_pc_feature<<<grid_for(N, 256, 8), 256, 0, s->stream>>>(GridDiv(s->nx, s->ny, s->nz), N, s->alpha,
+                                                                     -s->mdt * s->vnb, s->feat);
+            PIRO_CHECK_LAUNCH("k_pc_feature");
+        }
+        if (s->net != net || !s->exec_l) {
+            if (s->exec_l) cudaGraphExecDestroy(s->exec_l);
+            if (s->graph_l) cudaGraphDestroy(s->graph_l);
+            s->exec_l = nullptr;
+            s->graph_l = nullptr;
+            s->net = net;
+            int rc = be_capture_fcg(s, true);
+            if (rc != PIRO_OK) {
+                s->net = nullptr;
+                return rc;
+            }
+        }
+    }
+    PIRO_CUDA(cudaStreamSynchronize(s->stream));
+    s->pc_kind = kind;
+    return PIRO_OK;
+}
+
+extern "C" int piro_be_pc_stats(piro_be_solver *s, int reset, long long *applies, double *ms)
+{
+    PIRO_ARG(s, "piro_be_pc_stats: null solver");
+    if (applies) *applies = s->pc_applies;
+    if (ms) *ms = s->pc_ms;
+    if (reset) {
+        s->pc_applies = 0;
+        s->pc_ms = 0.0;
+    }
+    return PIRO_OK;
+}
+
 extern "C" int piro_be_inner_operator(piro_be_solver *s, int *kind)
 {
     PIRO_ARG(s && kind, "piro_be_inner_operator: bad arguments");
@@ -1162,7 +1512,10 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
     PIRO_CUDA(cudaStreamWaitEvent(st, s->ev_in, 0));
     piro_be_info inf{};
     inf.status = PIRO_ERR_NOT_CONVERGED;
-    if (s->persist) {
+    // flexible CG: the learned preconditioner, or Jacobi run through FCG
+    bool learned = s->pc_kind != PIRO_PRECOND_JACOBI && s->exec_f &&
+                   (s->pc_kind != PIRO_PRECOND_LEARNED || s->exec_l);
+    if (s->persist && !learned) {
         PArgs P;
         P.g = GridDiv(s->nx, s->ny, s->nz);
         P.N = N;
@@ -1237,7 +1590,6 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
         s->kernel_launches += 1;
         // cap for this sweep
         int cap = max_inner - inf.inner_iterations;
-        PIRO_CUDA(cudaMemcpyAsync(&s->st->max_iters, &cap, sizeof(int), cudaMemcpyHostToDevice, st));
         PIRO_CUDA(cudaMemcpyAsync(s->h_st, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, st));
         PIRO_CUDA(cudaStreamSynchronize(st));
         const double rel = s->h_st->rel;
@@ -1252,27 +1604,46 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
         }
         if (outer == max_outer || cap <= 0) break;
         if (outer > 0 && rel > 0.5 * prev_rel) {
-            inf.status = PIRO_STATUS_STALLED;  // refinement no longer contracts
-            break;
+            if (!learned) {
+                inf.status = PIRO_STATUS_STALLED;  // refinement no longer contracts
+                break;
+            }
+            // the learned sweep stalled: Jacobi-PCG from here on (k_residual
+            // has already set up its z and <s, z> for this sweep)
+            learned = false;
+            inf.fallbacks += 1;
         }
         prev_rel = rel;
         inf.outer_iterations = outer + 1;
+        PIRO_CUDA(cudaMemcpyAsync(&s->st->max_iters, &cap, sizeof(int), cudaMemcpyHostToDevice, st));
         // inner CG: launch graph chunks until the device flag says done
         int seen = 0;
+        bool net_iters = learned && s->pc_kind == PIRO_PRECOND_LEARNED;
         while (true) {
-            PIRO_CUDA(cudaGraphLaunch(s->exec, st));
-            s->kernel_launches += 2 * kChunk;
+            const bool with_net = net_iters;
+            net_iters = false;
+            const int chunk = learned ? (with_net ? kLearnedIters : kChunkF) : kChunk;
+            PIRO_CUDA(cudaGraphLaunch(learned ? (with_net ? s->exec_l : s->exec_f) : s->exec, st));
+            s->kernel_launches += learned ? (with_net ? 9 * kLearnedIters : 3 * kChunkF) : 2 * kChunk;
             PIRO_CUDA(cudaMemcpyAsync(s->h_st, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, st));
             PIRO_CUDA(cudaStreamSynchronize(st));
             // kernel times of the iterations that ran in this chunk
-            const int ran = std::min(kChunk, s->h_st->iters - seen);
-            for (int i = 0; i < ran; ++i) {
-                float ms = 0.0f;
-                if (cudaEventElapsedTime(&ms, s->ev0[i], s->ev1[i]) == cudaSuccess) {
-                    s->spmv_ms += ms;
-                    s->spmv_launches += 1;
-                } else {
-                    (void)cudaGetLastError();  // timing is best effort; do not leak the error
+            const int ran = std::min(chunk, s->h_st->iters - seen);
+            if (!learned || with_net) {
+                for (int i = 0; i < ran; ++i) {
+                    float ms = 0.0f;
+                    cudaEvent_t e0 = with_net ? s->evf0[i] : s->ev0[i], e1 = with_net ? s->evf1[i] : s->ev1[i];
+                    if (cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) {
+                        if (with_net) {
+                            s->pc_ms += ms;
+                            s->pc_applies += 1;
+                        } else {
+                            s->spmv_ms += ms;
+                            s->spmv_launches += 1;
+                        }
+                    } else {
+                        (void)cudaGetLastError();  // timing is best effort; do not leak the error
+                    }
                 }
             }
             seen = s->h_st->iters;
@@ -1280,6 +1651,18 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
         }
         inf.inner_iterations += s->h_st->iters;
         if (s->h_st->broken) {
+            if (learned) {
+                // discard the broken correction (and directions that may hold
+                // non-finite values) and redo the sweep with Jacobi-PCG
+                learned = false;
+                inf.fallbacks += 1;
+                PIRO_CUDA(cudaMemsetAsync(s->d, 0, sizeof(float) * (size_t)N, st));
+                PIRO_CUDA(cudaMemsetAsync(s->p[0], 0, sizeof(float) * (size_t)N, st));
+                PIRO_CUDA(cudaMemsetAsync(s->p[1], 0, sizeof(float) * (size_t)N, st));
+                PIRO_CUDA(cudaMemsetAsync(s->q, 0, sizeof(float) * (size_t)N, st));
+                prev_rel = INFINITY;
+                continue;
+            }
             inf.status = PIRO_STATUS_STALLED;
             break;
         }

@@ -279,6 +279,26 @@ class BESolver:
         check(lib().piro_be_solution_f64(self.h, C.byref(p)), "piro_be_solution_f64")
         return p.value
 
+    def set_preconditioner(self, net=None, flexible_jacobi=False):
+        """Learned preconditioner (flexible CG) with a PCNet, or Jacobi with None
+        (flexible_jacobi: Jacobi run through the flexible-CG iteration)."""
+        if flexible_jacobi:
+            check(lib().piro_be_set_preconditioner(self.h, 2, None), "piro_be_set_preconditioner")
+            self.net = None
+            return
+        if net is None:
+            check(lib().piro_be_set_preconditioner(self.h, 0, None), "piro_be_set_preconditioner")
+            self.net = None
+        else:
+            check(lib().piro_be_set_preconditioner(self.h, 1, net.h), "piro_be_set_preconditioner")
+            self.net = net  # keep the network alive while the solver may use it
+
+    def pc_stats(self, reset=False):
+        """(network applies, their total ms by CUDA events)."""
+        n, ms = C.c_longlong(), C.c_double()
+        check(lib().piro_be_pc_stats(self.h, int(reset), C.byref(n), C.byref(ms)), "piro_be_pc_stats")
+        return n.value, ms.value
+
     def kernel_stats(self, reset=False):
         """(CG SpMV launches, their total ms by CUDA events, all kernel launches)."""
         n, ms, k = C.c_longlong(), C.c_double(), C.c_longlong()
@@ -305,3 +325,68 @@ def be_jli(nx, ny, nz, A, dt, b, tol=1e-5, urf=1.0, maxiter=1000):
     check(lib().piro_be_jli(nx, ny, nz, _p(A[0]), _p(A[1]), _p(A[2]), float(dt), _p(b), _p(x), _p(r), float(tol),
                             float(urf), maxiter, C.byref(it), _stream()), "piro_be_jli")
     return x, it.value
+
+
+# ----------------------------------------------------------------- learned preconditioner
+class PCNet:
+    """The learned preconditioner network (include/piro.h, piro_pcnet_*)."""
+
+    def __init__(self, seed: int = 0):
+        h = C.c_void_p()
+        check(lib().piro_pcnet_create(int(seed), C.byref(h)), "piro_pcnet_create")
+        self.h = h
+
+    @staticmethod
+    def num_params() -> int:
+        n = C.c_int64()
+        check(lib().piro_pcnet_num_params(C.byref(n)), "piro_pcnet_num_params")
+        return n.value
+
+    def get_params(self, rounded: bool = False):
+        import numpy as np
+        out = np.empty(self.num_params(), np.float32)
+        check(lib().piro_pcnet_get_params(self.h, out.ctypes.data_as(C.c_void_p), out.size, int(rounded)),
+              "piro_pcnet_get_params")
+        return out
+
+    def set_params(self, params) -> None:
+        import numpy as np
+        p = np.ascontiguousarray(params, np.float32)
+        check(lib().piro_pcnet_set_params(self.h, p.ctypes.data_as(C.c_void_p), p.size), "piro_pcnet_set_params")
+
+    def forward(self, nx, ny, nz, r, feat, out=None, batch=1):
+        if out is None:
+            out = torch.empty_like(r)
+        check(lib().piro_pcnet_forward(self.h, batch, nx, ny, nz, _p(r), _p(feat), _p(out), _stream()),
+              "piro_pcnet_forward")
+        return out
+
+    def loss_grad(self, nx, ny, nz, r, feat, target, mask, batch=1, want_loss=True, want_grad=False):
+        """Forward + backward; returns (loss or None, gradient array or None)."""
+        import numpy as np
+        loss = C.c_double()
+        g = np.empty(self.num_params(), np.float32) if want_grad else None
+        check(lib().piro_pcnet_loss_grad(self.h, batch, nx, ny, nz, _p(r), _p(feat), _p(target), _p(mask),
+                                         C.byref(loss) if want_loss else None,
+                                         g.ctypes.data_as(C.c_void_p) if want_grad else None, _stream()),
+              "piro_pcnet_loss_grad")
+        return (loss.value if want_loss else None), g
+
+    def adam_step(self, lr: float) -> None:
+        check(lib().piro_pcnet_adam_step(self.h, float(lr), _stream()), "piro_pcnet_adam_step")
+
+    def launches(self) -> int:
+        n = C.c_longlong()
+        check(lib().piro_pcnet_stats(self.h, C.byref(n)), "piro_pcnet_stats")
+        return n.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().piro_pcnet_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
