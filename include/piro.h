@@ -325,6 +325,14 @@ int piro_pcnet_loss_grad(piro_pcnet *n, int batch, int nx, int ny, int nz, const
                          const float *target, const float *mask, double *loss, float *grad, piro_stream_t stream);
 /* Adam (beta1 0.9, beta2 0.999, eps 1e-8) with the last computed gradient. */
 int piro_pcnet_adam_step(piro_pcnet *n, float lr, piro_stream_t stream);
+/* Engine of the inference forward pass (piro_pcnet_forward and the solver's
+ * preconditioner apply): CUDA-core kernels, or all four layers as tcgen05
+ * implicit GEMMs (TMA-staged BF16 operands with the channels padded to 16,
+ * FP32 accumulation in tensor memory).  Training always uses the CUDA-core
+ * kernels. */
+#define PIRO_PCNET_CUDA_CORES 0
+#define PIRO_PCNET_TENSOR_CORES 1
+int piro_pcnet_set_engine(piro_pcnet *n, int engine);
 /* Kernels launched by this network so far. */
 int piro_pcnet_stats(piro_pcnet *n, long long *launches);
 int piro_pcnet_destroy(piro_pcnet *n);

@@ -94,6 +94,7 @@ SIGNATURES = {
     "piro_pcnet_loss_grad": (i32, [vp, i32, i32, i32, i32, vp, vp, vp, vp, C.POINTER(C.c_double), vp, vp]),
     "piro_pcnet_adam_step": (i32, [vp, f32, vp]),
     "piro_pcnet_stats": (i32, [vp, C.POINTER(C.c_longlong)]),
+    "piro_pcnet_set_engine": (i32, [vp, i32]),
     "piro_pcnet_destroy": (i32, [vp]),
     "piro_be_set_preconditioner": (i32, [vp, i32, vp]),
     "piro_be_pc_stats": (i32, [vp, i32, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]),

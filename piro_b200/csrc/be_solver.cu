@@ -32,6 +32,7 @@ size_t reduce_workspace_bytes(int64_t n);
 size_t pcnet_apply_bytes(int64_t N);
 int pcnet_apply(const piro_pcnet *n, void *work, const GridDiv &g, int64_t N, const float *r, const float *feat,
                 const double *rr, double n_int, float *z, const int *skip, cudaStream_t st);
+int pcnet_take_error(const piro_pcnet *n, cudaStream_t st);
 
 namespace {
 
@@ -1451,6 +1452,7 @@ extern "C" int piro_be_set_preconditioner(piro_be_solver *s, int kind, piro_pcne
             PIRO_CUDA(cudaMalloc(&s->feat, sizeof(float) * (size_t)N));
             PIRO_CUDA(cudaMalloc(&s->zt, sizeof(float) * (size_t)N));
             PIRO_CUDA(cudaMalloc(&s->pc_work, pcnet_apply_bytes(N)));
+            PIRO_CUDA(cudaMemsetAsync(s->pc_work, 0, pcnet_apply_bytes(N), s->stream));
             PIRO_CUDA(cudaMemsetAsync(s->zt, 0, sizeof(float) * (size_t)N, s->stream));
             k_pc_feature<<<grid_for(N, 256, 8), 256, 0, s->stream>>>(GridDiv(s->nx, s->ny, s->nz), N, s->alpha,
                                                                      -s->mdt * s->vnb, s->feat);
@@ -1674,6 +1676,10 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
     PIRO_CHECK_LAUNCH("k_demote");
     s->kernel_launches += 1;
     PIRO_CUDA(cudaStreamSynchronize(st));
+    if (s->pc_kind == PIRO_PRECOND_LEARNED && s->net) {
+        const int rc = pcnet_take_error(s->net, st);
+        if (rc) inf.status = rc;
+    }
     if (info) *info = inf;
     return inf.status == PIRO_OK ? PIRO_OK : inf.status;
 }

@@ -25,13 +25,16 @@
 // (data gradient = the transposed convolution times GELU'; weight gradient =
 // per-block partial correlations reduced in a fixed order, so gradients are
 // deterministic), and Adam.
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "common.cuh"
+#include "conv_tc.cuh"
 
 namespace piro {
 namespace {
@@ -40,6 +43,7 @@ typedef __nv_bfloat16 bf16;
 
 constexpr int kTaps = 27;
 constexpr int kLayers = 4;
+constexpr int kTcZChunk = 16;  // z-planes per CTA of the tensor-core layers
 constexpr int kCi[kLayers] = {2, 16, 16, 16};
 constexpr int kCo[kLayers] = {16, 16, 16, 1};
 
@@ -422,6 +426,49 @@ __global__ void k_round_bf16(int64_t n, const float *__restrict__ w, float *__re
         wq[i] = bfr(w[i]);
 }
 
+// BF16 weights of the four layers in the tensor-core operand layout: per
+// layer and tap [channel group 2][co 16][8 ci] (the no-swizzle K-major core
+// matrices of conv_tc.cuh), input channels beyond 2 (layer 1) and output
+// channels beyond 1 (layer 4) zero.
+__global__ void k_pack_wtc(const float *__restrict__ wq, Layout L, bf16 *__restrict__ wpk)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kLayers * kTaps * 256; i += gridDim.x * blockDim.x) {
+        const int l = i / (kTaps * 256), rem = i % (kTaps * 256);
+        const int tap = rem / 256, r2 = rem % 256;
+        const int ci = (r2 / 128) * 8 + (r2 % 8), co = (r2 / 8) % 16;
+        const int CI = l == 0 ? 2 : 16, CO = l == kLayers - 1 ? 1 : 16;  // kCi[l], kCo[l]
+        const float v = (ci < CI && co < CO) ? wq[L.w[l] + (tap * CI + ci) * CO + co] : 0.0f;
+        wpk[i] = __float2bfloat16_rn(v);
+    }
+}
+
+// Tensor-core input: x16[b][c] = (r s_b, r s_b f, 0 x 14) on interior cells,
+// zeros elsewhere (32 bytes per cell, the layout of the hidden activations).
+__global__ void k_pack_input16(GridDiv g, int64_t N, const float *__restrict__ r, const float *__restrict__ feat,
+                               const double *__restrict__ rr, double n_int, bf16 *__restrict__ x16,
+                               const int *__restrict__ skip)
+{
+    if (skip && *((volatile const int *)skip)) return;
+    const int b = blockIdx.y;
+    float s = 1.0f;
+    if (rr) {
+        const double v = rr[b];
+        s = v > 0.0 ? (float)(1.0 / sqrt(v / n_int)) : 0.0f;
+    }
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < N; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = (int64_t)b * N + c;
+        uint32_t w0 = 0;
+        if (g.interior(c)) {
+            const float rs = r[o] * s;
+            const __nv_bfloat162 h = __floats2bfloat162_rn(rs, feat ? rs * feat[o] : 0.0f);
+            w0 = *reinterpret_cast<const uint32_t *>(&h);
+        }
+        uint4 *dst = reinterpret_cast<uint4 *>(x16 + o * 16);
+        dst[0] = make_uint4(w0, 0, 0, 0);
+        dst[1] = make_uint4(0, 0, 0, 0);
+    }
+}
+
 // Deterministic host RNG for the initial weights (splitmix64 + Box-Muller).
 struct HostRng {
     uint64_t s;
@@ -448,6 +495,9 @@ using namespace piro;
 struct piro_pcnet {
     Layout L;
     float *w = nullptr, *wq = nullptr, *m = nullptr, *v = nullptr, *g = nullptr;
+    bf16 *wpk = nullptr;  // BF16 tensor-core operands of the four layers
+    int *d_err = nullptr; // raised by a tensor-core launch whose bounded wait ran out
+    int engine = PIRO_PCNET_CUDA_CORES;
     float *partials = nullptr;
     double *red = nullptr;
     int64_t adam_t = 0;
@@ -490,6 +540,7 @@ static int net_reserve(piro_pcnet *n, int64_t cells, bool training)
         for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMalloc(&n->g16[i], c * 16 * sizeof(bf16));
         if (e == cudaSuccess) e = cudaMalloc(&n->gout, c * sizeof(float));
     }
+    for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaMemset(n->a[i], 0, c * 16 * sizeof(bf16));
     if (e != cudaSuccess) {
         net_free_ws(n);
         set_error("piro_pcnet: workspace allocation failed: %s", cudaGetErrorString(e));
@@ -557,6 +608,89 @@ static Acts infer_acts(void *work, int64_t cells)
     return Acts{x0, {nullptr, nullptr, nullptr}, {b0, b1, b0}};
 }
 
+// TMA descriptor of an activation array of `rows` cells (16 BF16 channels
+// each) as the 3-D view (8 channels, rows at 32 bytes, 2 groups at 16 bytes)
+// with box {8, 130, 2}: the line blocks of conv_tc.cuh.
+static int encode_rows_map(CUtensorMap *m, const void *base, int64_t rows)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            set_error("cuTensorMapEncodeTiled is not available");
+            return PIRO_ERR_CUDA;
+        }
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[3] = {8, (cuuint64_t)rows, 2};
+    const cuuint64_t strides[2] = {32, 16};
+    const cuuint32_t box[3] = {8, (cuuint32_t)tc::kLineRows, 2};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void *>(base), dims, strides, box,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return PIRO_ERR_CUDA;
+    }
+    return PIRO_OK;
+}
+
+// One layer on the tensor cores over `batch` grids of N cells: in (16 BF16
+// channels per cell) -> out (GELU, 16 BF16 channels) or, for the last layer,
+// zout (FP32 channel 0 times sqrt(rr / n_int)).  Cells of the boundary planes
+// z = 0 and nz - 1 are not written (they must already be zero).
+template <int kEpi>
+static int conv_tc(const bf16 *in, bf16 *out, float *zout, const bf16 *wpk, const GridDiv &g, int64_t N, int batch,
+                   const double *rr, double n_int, const int *skip, int *err, cudaStream_t st)
+{
+    static bool attr = false;
+    if (!attr) {
+        PIRO_CUDA(cudaFuncSetAttribute(tc::k_conv16_tc<kEpi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       tc::kSmemBytes));
+        attr = true;
+    }
+    CUtensorMap map;
+    int rc = encode_rows_map(&map, in, N * batch);
+    if (rc) return rc;
+    const int64_t nxy = (int64_t)g.nx * g.ny;
+    const int ncol = (int)cdiv(nxy, tc::kRows);
+    const int planes = g.nz - 2;
+    const int zchunk = planes < kTcZChunk ? planes : kTcZChunk;
+    const int nzc = (int)cdiv(planes, zchunk);
+    tc::Args a{g, N, nxy, ncol, zchunk, wpk, out, zout, rr, n_int, skip, err};
+    tc::k_conv16_tc<kEpi><<<dim3((unsigned)(ncol * nzc), (unsigned)batch), tc::kThreads, tc::kSmemBytes, st>>>(map, a);
+    PIRO_CHECK_LAUNCH("k_conv16_tc");
+    return PIRO_OK;
+}
+
+// Inference forward with all four layers on the tensor cores.  A.a[0] and
+// A.a[1] ping-pong: input -> a[1], layer 1 -> a[0], 2 -> a[1], 3 -> a[0],
+// layer 4 -> out.
+static int net_forward_tc(const piro_pcnet *n, const Acts &A, int batch, const GridDiv &g, int64_t N,
+                          const float *r, const float *feat, float *out, const double *rr, double n_int,
+                          const int *skip, cudaStream_t st)
+{
+    bf16 *ping = A.a[0], *pong = A.a[1];
+    const int64_t W = (int64_t)kTaps * 256;
+    k_pack_input16<<<dim3(net_grid(N, 256), batch), 256, 0, st>>>(g, N, r, feat, rr, n_int, pong, skip);
+    PIRO_CHECK_LAUNCH("k_pack_input16");
+    int rc = conv_tc<0>(pong, ping, nullptr, n->wpk, g, N, batch, nullptr, 0.0, skip, n->d_err, st);
+    if (!rc) rc = conv_tc<0>(ping, pong, nullptr, n->wpk + W, g, N, batch, nullptr, 0.0, skip, n->d_err, st);
+    if (!rc) rc = conv_tc<0>(pong, ping, nullptr, n->wpk + 2 * W, g, N, batch, nullptr, 0.0, skip, n->d_err, st);
+    if (!rc) rc = conv_tc<1>(ping, nullptr, out, n->wpk + 3 * W, g, N, batch, rr, n_int, skip, n->d_err, st);
+    return rc;
+}
+
+static int net_pack(piro_pcnet *n, cudaStream_t st)
+{
+    k_pack_wtc<<<cdiv(kLayers * kTaps * 256, 256), 256, 0, st>>>(n->wq, n->L, n->wpk);
+    PIRO_CHECK_LAUNCH("k_pack_wtc");
+    return PIRO_OK;
+}
+
 template <int CI, int CO, typename GT>
 static int launch_bwd_w(piro_pcnet *n, const GridDiv &g, int64_t N, int batch, const bf16 *x, const GT *gy,
                         float *grad_w, cudaStream_t st)
@@ -599,6 +733,9 @@ extern "C" int piro_pcnet_create(uint64_t seed, piro_pcnet **out)
     if (e == cudaSuccess) e = cudaMalloc(&n->g, P * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&n->partials, (size_t)pmax * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&n->red, (kRedBlocks + 8) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&n->wpk, sizeof(bf16) * kLayers * kTaps * 256);
+    if (e == cudaSuccess) e = cudaMalloc(&n->d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(n->d_err, 0, sizeof(int));
     if (e != cudaSuccess) {
         piro_pcnet_destroy(n);
         set_error("piro_pcnet_create: allocation failed: %s", cudaGetErrorString(e));
@@ -632,6 +769,8 @@ extern "C" int piro_pcnet_set_params(piro_pcnet *n, const float *host, int64_t c
     PIRO_CUDA(cudaMemset(n->g, 0, P * sizeof(float)));
     k_round_bf16<<<cdiv(count, 256), 256>>>(count, n->w, n->wq);
     PIRO_CHECK_LAUNCH("k_round_bf16");
+    int rc = net_pack(n, 0);
+    if (rc) return rc;
     PIRO_CUDA(cudaDeviceSynchronize());
     n->adam_t = 0;
     return PIRO_OK;
@@ -656,26 +795,70 @@ extern "C" int piro_pcnet_forward(piro_pcnet *n, int batch, int nx, int ny, int 
     int rc = net_reserve(n, N * batch, false);
     if (rc) return rc;
     const GridDiv g(nx, ny, nz);
-    k_pack_input<<<dim3(net_grid(N, 256), batch), 256, 0, st>>>(g, N, r, feat, nullptr, 1.0, n->x0, nullptr);
-    PIRO_CHECK_LAUNCH("k_pack_input");
     n->launches += 5;
     const Acts A{n->x0, {nullptr, nullptr, nullptr}, {n->a[0], n->a[1], n->a[2]}};
+    if (n->engine == PIRO_PCNET_TENSOR_CORES) {
+        // the tensor-core layers leave the boundary planes of out unwritten
+        const int64_t nxy = (int64_t)nx * ny;
+        for (int b = 0; b < batch; ++b) {
+            PIRO_CUDA(cudaMemsetAsync(out + b * N, 0, sizeof(float) * nxy, st));
+            PIRO_CUDA(cudaMemsetAsync(out + b * N + N - nxy, 0, sizeof(float) * nxy, st));
+        }
+        rc = net_forward_tc(n, A, batch, g, N, r, feat, out, nullptr, 1.0, nullptr, st);
+        if (rc) return rc;
+        int err = 0;
+        PIRO_CUDA(cudaMemcpyAsync(&err, n->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        PIRO_CUDA(cudaStreamSynchronize(st));
+        if (err) {
+            set_error("piro_pcnet_forward: a tensor-core pipeline wait timed out");
+            return PIRO_ERR_CUDA;
+        }
+        return PIRO_OK;
+    }
+    k_pack_input<<<dim3(net_grid(N, 256), batch), 256, 0, st>>>(g, N, r, feat, nullptr, 1.0, n->x0, nullptr);
+    PIRO_CHECK_LAUNCH("k_pack_input");
     return net_forward(n->wq, A, batch, g, N, false, out, nullptr, 1.0, nullptr, st);
 }
 
+extern "C" int piro_pcnet_set_engine(piro_pcnet *n, int engine)
+{
+    PIRO_ARG(n && (engine == PIRO_PCNET_CUDA_CORES || engine == PIRO_PCNET_TENSOR_CORES),
+             "piro_pcnet_set_engine: bad arguments");
+    n->engine = engine;
+    return PIRO_OK;
+}
+
 namespace piro {
-// Device bytes of the caller-owned workspace of pcnet_apply for N cells.
+// Device bytes of the caller-owned workspace of pcnet_apply for N cells; the
+// caller zeroes it once (boundary planes of the tensor-core layers' outputs
+// are never written).
 size_t pcnet_apply_bytes(int64_t N) { return sizeof(bf16) * (size_t)(cdiv(N * 2, 128) * 128 + 2 * N * 16); }
+
+// Tensor-core pipeline error of the network (a bounded wait ran out); clears it.
+int pcnet_take_error(const piro_pcnet *n, cudaStream_t st)
+{
+    int err = 0;
+    PIRO_CUDA(cudaMemcpyAsync(&err, n->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PIRO_CUDA(cudaStreamSynchronize(st));
+    if (err) {
+        PIRO_CUDA(cudaMemset(n->d_err, 0, sizeof(int)));
+        set_error("learned preconditioner: a tensor-core pipeline wait timed out");
+        return PIRO_ERR_CUDA;
+    }
+    return PIRO_OK;
+}
 
 // Preconditioner apply for the solver: z = sqrt(rr/n_int) * M(r / sqrt(rr/n_int), f),
 // every launch returning at once when *skip is set.  Reads only the net's
-// BF16 weight vector (allocated once per network), so a CUDA graph that
-// captured it stays valid while the network is trained or reloaded.  Five
-// kernel launches.
+// weight vectors (allocated once per network), so a CUDA graph that captured
+// it stays valid while the network is trained or reloaded.  Five kernel
+// launches.  z's boundary planes must be zero already (the tensor-core
+// engine does not write them).
 int pcnet_apply(const piro_pcnet *n, void *work, const GridDiv &g, int64_t N, const float *r, const float *feat,
                 const double *rr, double n_int, float *z, const int *skip, cudaStream_t st)
 {
     const Acts A = infer_acts(work, N);
+    if (n->engine == PIRO_PCNET_TENSOR_CORES) return net_forward_tc(n, A, 1, g, N, r, feat, z, rr, n_int, skip, st);
     k_pack_input<<<dim3(net_grid(N, 256), 1), 256, 0, st>>>(g, N, r, feat, rr, n_int, A.x0, skip);
     PIRO_CHECK_LAUNCH("k_pack_input");
     return net_forward(n->wq, A, 1, g, N, false, z, rr, n_int, skip, st);
@@ -741,9 +924,9 @@ extern "C" int piro_pcnet_adam_step(piro_pcnet *n, float lr, piro_stream_t strea
     const int64_t P = n->L.total;
     k_adam<<<cdiv(P, 256), 256, 0, as_stream(stream)>>>(P, n->w, n->m, n->v, n->g, n->wq, lr, b1, b2, eps, bc1,
                                                          bc2);
-    n->launches += 1;
+    n->launches += 2;
     PIRO_CHECK_LAUNCH("k_adam");
-    return PIRO_OK;
+    return net_pack(n, as_stream(stream));
 }
 
 extern "C" int piro_pcnet_stats(piro_pcnet *n, long long *launches)
@@ -764,6 +947,8 @@ extern "C" int piro_pcnet_destroy(piro_pcnet *n)
     cudaFree(n->g);
     cudaFree(n->partials);
     cudaFree(n->red);
+    cudaFree(n->wpk);
+    cudaFree(n->d_err);
     delete n;
     return PIRO_OK;
 }

@@ -35,9 +35,33 @@ RADIUS = 4
 SNAP_ITERS = (0, 1, 2, 3, 5, 8, 12, 17, 23, 30)
 
 
+_ALPHA: dict = {}
+
+
+def _alpha_field(n: int, seed: int) -> np.ndarray:
+    return W.smoothed_lognormal(n, 1.5, 8.0, seed)
+
+
+def prefetch_alpha(n: int, seeds, workers: int | None = None) -> None:
+    """Generate the alpha fields of `seeds` in a process pool (started with
+    spawn, so it is safe after CUDA initialisation) and keep them for
+    be_family."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    todo = [s for s in seeds if (n, s) not in _ALPHA]
+    if not todo:
+        return
+    workers = workers or min(len(todo), os.cpu_count() or 1)
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        for s, a in zip(todo, ex.map(_alpha_field, [n] * len(todo), todo)):
+            _ALPHA[(n, s)] = a
+
+
 def be_family(n: int, seed: int):
     """One member of the backward-Euler family on an n^3 grid (ghost-inclusive)."""
-    alpha = W.smoothed_lognormal(n, 1.5, 8.0, seed)
+    alpha = _ALPHA.get((n, seed))
+    if alpha is None:
+        alpha = _alpha_field(n, seed)
     dt = np.float32(50.0 / (6.0 * float(alpha.max())))
     s = n / 32.0
     b = W.gaussian_bump(n, 4.0 * s, (n - 1) / 2.0)
@@ -192,6 +216,33 @@ def compare(torch, ops, net, n, seeds, rtol=1e-8):
     return rows
 
 
+def summary(rows):
+    """Mean iterations and ms of the plain and learned solves over `rows`."""
+    out = {}
+    for k in ("jacobi", "learned"):
+        out[k] = {"iters": float(np.mean([r[k]["iters"] for r in rows])),
+                  "ms": float(np.mean([r[k]["ms"] for r in rows])),
+                  "worst_rel": float(max(r[k]["rel"] for r in rows)),
+                  "fallbacks": int(sum(r[k]["fallbacks"] for r in rows))}
+    out["iteration_ratio"] = out["jacobi"]["iters"] / out["learned"]["iters"]
+    out["time_ratio"] = out["jacobi"]["ms"] / out["learned"]["ms"]
+    return out
+
+
+def fit(torch, ops, n, seeds, crop, crops_per_pair, steps, batch, lr, rounds, log=None):
+    """Train a network: one round on Jacobi-PCG iterates, then `rounds` more
+    that add the iterates of flexible CG with the network being trained."""
+    data = make_dataset(torch, ops, n, seeds, crop, crops_per_pair, log=log)
+    net = ops.PCNet(seed=0)
+    hist = [train(torch, ops, net, data, crop, steps, batch, lr, log=log)]
+    for rnd in range(1, rounds + 1):
+        more = make_dataset(torch, ops, n, seeds, crop, crops_per_pair, seed=rnd, net=net, log=log)
+        data = tuple(torch.cat([a, b]) for a, b in zip(data, more))
+        del more
+        hist.append(train(torch, ops, net, data, crop, steps, batch, lr * 0.5, seed=rnd, log=log))
+    return net, int(data[0].shape[0]), hist
+
+
 def main():
     ap = argparse.ArgumentParser(description="train the learned preconditioner on the device")
     ap.add_argument("--n", type=int, default=128)
@@ -199,31 +250,31 @@ def main():
     ap.add_argument("--eval-seeds", type=str, default="200:210")
     ap.add_argument("--crop", type=int, default=32)
     ap.add_argument("--crops-per-pair", type=int, default=10)
-    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--steps", type=int, default=1500)
     ap.add_argument("--batch", type=int, default=16)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--rounds", type=int, default=2, help="on-policy rounds after the first")
     ap.add_argument("--out", type=str, required=True, help="weights file (.npy, float32)")
     ap.add_argument("--report", type=str, default=None, help="JSON report")
     args = ap.parse_args()
-    import torch
-
-    from . import ops
     lo, hi = (int(v) for v in args.seeds.split(":"))
     elo, ehi = (int(v) for v in args.eval_seeds.split(":"))
     t0 = time.time()
-    data = make_dataset(torch, ops, args.n, range(lo, hi), args.crop, args.crops_per_pair,
-                        log=lambda s: print(s, flush=True))
+    prefetch_alpha(args.n, list(range(lo, hi)) + list(range(elo, ehi)))
+    import torch
+
+    from . import ops
     t1 = time.time()
-    net = ops.PCNet(seed=0)
-    hist = train(torch, ops, net, data, args.crop, args.steps, args.batch, args.lr,
-                 log=lambda s: print(s, flush=True))
+    log = lambda s: print(s, flush=True)  # noqa: E731
+    net, pairs, hist = fit(torch, ops, args.n, range(lo, hi), args.crop, args.crops_per_pair, args.steps,
+                           args.batch, args.lr, args.rounds, log=log)
     torch.cuda.synchronize()
     t2 = time.time()
-    w = net.get_params()
-    np.save(args.out, w)
+    np.save(args.out, net.get_params())
     rows = compare(torch, ops, net, args.n, range(elo, ehi))
-    rep = {"pairs": int(data[0].shape[0]), "gen_s": t1 - t0, "train_s": t2 - t1, "loss": hist, "eval": rows}
-    print(json.dumps(rep["eval"]), flush=True)
+    rep = {"n": args.n, "train_seeds": [lo, hi], "eval_seeds": [elo, ehi], "pairs": pairs,
+           "alpha_s": t1 - t0, "train_s": t2 - t1, "loss": hist, "eval": rows, "summary": summary(rows)}
+    print(json.dumps(rep["summary"]), flush=True)
     if args.report:
         with open(args.report, "w") as f:
             json.dump(rep, f, indent=1)

@@ -372,6 +372,10 @@ class PCNet:
               "piro_pcnet_loss_grad")
         return (loss.value if want_loss else None), g
 
+    def set_engine(self, tensor_cores: bool) -> None:
+        """Inference engine: tcgen05 tensor cores for the 16 -> 16 layers, or CUDA cores."""
+        check(lib().piro_pcnet_set_engine(self.h, 1 if tensor_cores else 0), "piro_pcnet_set_engine")
+
     def adam_step(self, lr: float) -> None:
         check(lib().piro_pcnet_adam_step(self.h, float(lr), _stream()), "piro_pcnet_adam_step")
 

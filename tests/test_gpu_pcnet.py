@@ -161,3 +161,48 @@ def test_learned_fcg_gains_over_jacobi(cuda):
         assert row["learned"]["fallbacks"] == 0
         assert row["learned"]["iters"] < row["jacobi"]["iters"], rows
     netw.close()
+
+
+@pytest.mark.parametrize("n,B", [((10, 9, 8), 2), ((7, 12, 9), 1), ((40, 33, 21), 1)])
+def test_tensor_core_forward_matches_oracle(cuda, n, B):
+    """The tcgen05 implicit-GEMM layers (TMA-staged BF16 operands, FP32 in
+    tensor memory) give the oracle's network output to the same tolerance
+    as the CUDA-core kernels."""
+    import torch
+    from piro_b200 import ops
+    net = ops.PCNet(seed=0)
+    p = P.init_params(12).astype(np.float32)
+    net.set_params(p)
+    net.set_engine(True)
+    r, f, _, _ = _inputs(4, n, B)
+    rt, ft = torch.from_numpy(r.reshape(-1)).cuda(), torch.from_numpy(f.reshape(-1)).cuda()
+    got = net.forward(*n, rt, ft, batch=B).cpu().numpy().reshape(B, -1).astype(np.float64)
+    ref = P.forward(p.astype(np.float64), n, r, f, emulate=True)
+    scale = np.abs(ref).max()
+    assert np.abs(got - ref).max() <= 2e-2 * scale
+    assert np.sqrt(((got - ref) ** 2).sum() / (ref ** 2).sum()) < 5e-3
+    net.set_engine(False)
+    cc = net.forward(*n, rt, ft, batch=B).cpu().numpy().reshape(B, -1).astype(np.float64)
+    assert np.sqrt(((got - cc) ** 2).sum() / (cc ** 2).sum()) < 5e-3
+    net.close()
+
+
+def test_tensor_core_preconditioner_in_solver(cuda):
+    """The solver with the tensor-core network converges like the CUDA-core one."""
+    import torch
+    from piro_b200 import ops
+    n = 34
+    a_t, b_t, A, dt = _family(n, 203)
+    net = ops.PCNet(seed=3)
+    its = []
+    for tcore in (False, True):
+        net.set_engine(tcore)
+        sv = ops.BESolver(n, n, n, A, a_t, stencil=(float(dt), 1.0))
+        sv.set_preconditioner(net)
+        x = torch.empty_like(b_t)
+        info = sv.solve(b_t, x, rtol=1e-8)
+        assert info.status == 0 and info.rel_residual <= 1e-8
+        its.append(info.inner_iterations)
+        sv.close()
+    assert abs(its[0] - its[1]) <= 2, its
+    net.close()
