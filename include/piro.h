@@ -293,7 +293,7 @@ int piro_be_destroy(piro_be_solver *s);
 /* -- learned preconditioner (flexible CG inside the backward-Euler solve) -----
  *
  * A 3-D convolutional net z = M(r, f): four 3x3x3 convolutions, channels
- * 2 -> 16 -> 16 -> 16 -> 1, GELU after the first three, zero padding outside
+ * 2 -> 16 -> 16 -> 16 -> 1, GELU (tanh form) after the first three, zero padding outside
  * the interior, BF16 weights and activations with FP32 accumulation.  Input
  * channels per cell: the residual r (scaled to unit RMS over the interior by
  * the solver) and r*f with the feature f = log(dt * alpha / h^2); output: an
@@ -325,7 +325,7 @@ int piro_pcnet_loss_grad(piro_pcnet *n, int batch, int nx, int ny, int nz, const
                          const float *target, const float *mask, double *loss, float *grad, piro_stream_t stream);
 /* Adam (beta1 0.9, beta2 0.999, eps 1e-8) with the last computed gradient. */
 int piro_pcnet_adam_step(piro_pcnet *n, float lr, piro_stream_t stream);
-/* Engine of the inference forward pass (piro_pcnet_forward and the solver's
+/* Engine of the inference forward pass (default: tensor cores) of piro_pcnet_forward and the solver's
  * preconditioner apply): CUDA-core kernels, or all four layers as tcgen05
  * implicit GEMMs (TMA-staged BF16 operands with the channels padded to 16,
  * FP32 accumulation in tensor memory).  Training always uses the CUDA-core

@@ -5,7 +5,7 @@ never does.  It restates, in numpy float64, the network of
 piro_b200/csrc/pcnet.cu:
 
   input channels (r, r*f); four bias-free 3x3x3 convolutions, channels
-  2 -> 16 -> 16 -> 16 -> 1, GELU after the first three, zero padding outside
+  2 -> 16 -> 16 -> 16 -> 1, GELU (tanh form) after the first three, zero padding outside
   the interior of the ghost-inclusive grid; parameters one flat vector, per
   layer W[tap][ci][co], tap = (dz+1)*9 + (dy+1)*3 + (dx+1);
 
@@ -54,16 +54,18 @@ def bf16(x):
     return r.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-def _erf(x):
-    return np.vectorize(math.erf, otypes=[np.float64])(x)
+_C = math.sqrt(2.0 / math.pi)
+_A = 0.044715
 
 
 def gelu(x):
-    return 0.5 * x * (1.0 + _erf(x / math.sqrt(2.0)))
+    """GELU, tanh form (Hendrycks & Gimpel 2016): 0.5 x (1 + tanh(c (x + a x^3)))."""
+    return 0.5 * x * (1.0 + np.tanh(_C * (x + _A * x ** 3)))
 
 
 def gelu_d(x):
-    return 0.5 * (1.0 + _erf(x / math.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(_C * (x + _A * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * _C * (1.0 + 3.0 * _A * x * x)
 
 
 def interior(nx, ny, nz):

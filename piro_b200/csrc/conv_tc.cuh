@@ -161,7 +161,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-__device__ __forceinline__ float gelu_tc(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel 2016): 0.5 x (1 + tanh(sqrt(2/pi)
+// (x + 0.044715 x^3))), with the hardware tanh.approx (one instruction; the
+// erf form costs several special-function operations per element and made
+// this epilogue the kernel's bottleneck).
+__device__ __forceinline__ float gelu_tc(float x)
+{
+    float t;
+    const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+    return 0.5f * x * (1.0f + t);
+}
 
 // kEpi 0: GELU, 16 BF16 channels out (hidden layers); 1: output channel 0 in
 // FP32 times the batch member's scale (the last layer, N padded to 16).

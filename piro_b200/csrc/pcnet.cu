@@ -6,7 +6,7 @@
 // (TIMESCHEME 12, src/kernelprocess.cpp:123-209).
 //
 // Network: four 3x3x3 convolutions, channels 2 -> 16 -> 16 -> 16 -> 1, GELU
-// after the first three, zero padding outside the interior (boundary cells
+// (tanh form) after the first three, zero padding outside the interior (boundary cells
 // of the ghost-inclusive grid hold zero activations, so an interior cell's
 // 27 neighbours are always inside the array).  BF16 weights and activations,
 // FP32 accumulation.  Activations are stored channels-last (16 bf16 = 32 bytes
@@ -60,11 +60,23 @@ struct Layout {
     }
 };
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
-// d/dx [x Phi(x)] = Phi(x) + x phi(x)
+// GELU in its tanh form (Hendrycks & Gimpel 2016), g(x) = 0.5 x (1 + t),
+// t = tanh(c (x + a x^3)), c = sqrt(2/pi), a = 0.044715, with the hardware
+// tanh.approx; g'(x) = 0.5 (1 + t) + 0.5 x (1 - t^2) c (1 + 3 a x^2).
+__device__ __forceinline__ float tanh_hw(float u)
+{
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+    return t;
+}
+__device__ __forceinline__ float gelu(float x)
+{
+    return 0.5f * x * (1.0f + tanh_hw(0.7978845608028654f * (x + 0.044715f * x * x * x)));
+}
 __device__ __forceinline__ float gelu_d(float x)
 {
-    return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+    const float t = tanh_hw(0.7978845608028654f * (x + 0.044715f * x * x * x));
+    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * 0.7978845608028654f * (1.0f + 0.134145f * x * x);
 }
 
 __device__ __forceinline__ float bfr(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
@@ -497,7 +509,7 @@ struct piro_pcnet {
     float *w = nullptr, *wq = nullptr, *m = nullptr, *v = nullptr, *g = nullptr;
     bf16 *wpk = nullptr;  // BF16 tensor-core operands of the four layers
     int *d_err = nullptr; // raised by a tensor-core launch whose bounded wait ran out
-    int engine = PIRO_PCNET_CUDA_CORES;
+    int engine = PIRO_PCNET_TENSOR_CORES;
     float *partials = nullptr;
     double *red = nullptr;
     int64_t adam_t = 0;
