@@ -39,6 +39,15 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def load_tflops_peak():
+    """Dense BF16 TFLOP/s (burst: the network applies are short kernels)."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["bf16_tflops"])
+    return 1590.0
+
+
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during a region."""
@@ -189,6 +198,65 @@ def config_sections(torch, peak):
     return out
 
 
+def learned_section(torch, ops, cfg, A, alpha, plain_ms, plain_iters, steps, tflops_peak):
+    """Configuration 4: the backward-Euler step with the learned preconditioner
+    (the network trained on the device on seeds 100-199 by
+    `python -m piro_b200.learned`, weights in piro_b200/data) inside flexible
+    CG, against plain Jacobi-PCG on the same step; plus held-out fields
+    (seeds 200-202) solved both ways."""
+    from piro_b200 import learned as LP
+    nx, ny, nz = cfg["n"]
+    N = nx * ny * nz
+    w = np.load(os.path.join(ROOT, "piro_b200", "data", "pcnet_be128.npy"))
+    net = ops.PCNet(seed=0)
+    net.set_params(w)
+    sv = ops.BESolver(nx, ny, nz, A, alpha, stencil=(float(cfg["dt"]), 1.0))
+    sv.set_preconditioner(net)
+    u0 = torch.from_numpy(cfg["u0"]).cuda()
+    u, x = u0.clone(), torch.empty_like(u0)
+    for _ in range(2):
+        sv.solve(u, x, rtol=1e-8)
+    sv.pc_stats(reset=True)
+    sv.kernel_stats(reset=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    iters, fb, worst = [], 0, 0.0
+    u.copy_(u0)
+    for i in range(steps):
+        if i % cfg["steps"] == 0:
+            u.copy_(u0)
+        info = sv.solve(u, x, rtol=1e-8)
+        u, x = x, u
+        iters.append(info.inner_iterations)
+        fb += info.fallbacks
+        worst = max(worst, info.rel_residual)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    napply, apply_ms = sv.pc_stats(reset=True)
+    _, _, launches = sv.kernel_stats(reset=True)
+    sv.close()
+    n_int = (nx - 2) * (ny - 2) * (nz - 2)
+    alg_flops = 2 * 27 * (2 * 16 + 16 * 16 + 16 * 16 + 16 * 1) * n_int  # the network's multiply-adds
+    avg_apply = apply_ms / max(1, napply)
+    held = LP.compare(torch, ops, net, nx, [200, 201, 202])
+    net.close()
+    return {
+        "ms_per_step": round(ms, 4), "inner_iterations_mean": float(np.mean(iters)), "fallbacks": fb,
+        "worst_rel_residual": worst, "plain_ms_per_step": plain_ms, "plain_iterations_mean": plain_iters,
+        "speedup_vs_plain": round(plain_ms / ms, 4), "iteration_ratio": round(plain_iters / float(np.mean(iters)), 3),
+        "network_applies_per_step": napply / steps, "apply_ms": round(avg_apply, 4),
+        "apply_tflops": round(alg_flops / avg_apply / 1e9, 1),
+        "apply_frac_of_bf16_peak": round(alg_flops / avg_apply / 1e9 / tflops_peak, 4),
+        "kernel_launches_per_step": launches / steps,
+        "held_out": LP.summary(held),
+        "note": "network applies on the tensor cores (tcgen05, 4 layers); the network preconditions the first 2 "
+                "flexible-CG iterations of each refinement sweep, Jacobi the rest; plain = Jacobi-PCG in the "
+                "persistent single-launch solver",
+    }
+
+
 # ------------------------------------------------------------------ arms
 def run_piro(args):
     import torch
@@ -206,6 +274,7 @@ def run_piro(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     peak, peak_kind = load_peaks()
+    tf_peak = load_tflops_peak()
 
     cfg = W.heat_be_128()
     nx, ny, nz = cfg["n"]
@@ -304,6 +373,8 @@ def run_piro(args):
 
     spmv = spmv_section(torch, ops, steps=20, warmup=3, peak=peak) if rank == 0 else None
     configs = config_sections(torch, peak) if rank == 0 else None
+    learned = (learned_section(torch, ops, cfg, A, alpha, ms_step, main["iters"], min(args.steps, 40), tf_peak)
+               if rank == 0 else None)
 
     cpu = None
     fp64 = None
@@ -354,6 +425,7 @@ def run_piro(args):
         "clocks": ck,
         "spmv_256": spmv,
         "configs": configs,
+        "learned": learned,
         "fp64_check": fp64,
         "cpu_baseline": cpu,
     }
