@@ -348,6 +348,44 @@ int piro_be_set_preconditioner(piro_be_solver *s, int kind, piro_pcnet *net);
  * reset and their summed device time in ms (CUDA events around each apply). */
 int piro_be_pc_stats(piro_be_solver *s, int reset, long long *applies, double *ms);
 
+/* -- batched stepping: many independent problems in one persistent launch ----
+ *
+ * `count` independent heat problems, member k a constant-alpha cube of n[k]^3
+ * ghost-inclusive cells (h = 1, homogeneous boundary values held fixed) with
+ * its own dt and scheme (0: forward Euler as SpMVCSR.cl + setBC with the
+ * matrix-free 7-point arithmetic; 1: backward Euler, (I - dt*alpha*L) u' = u
+ * by FP32 CG inside FP64 iterative refinement to a relative residual).  The
+ * fields sit back to back in one device array (member k at offset[k], offsets
+ * 64-cell aligned).  One step advances every member with ONE cooperative
+ * persistent kernel launch: forward-Euler members in its first pass, the
+ * backward-Euler members as a lockstep state machine of FP64-residual and CG
+ * phases separated by grid barriers (bounded waits), with per-member
+ * reductions in a fixed order.  PIRO steps one grid per process
+ * (src/solve.cpp:11-48); this is the build's batched form of that loop. */
+typedef struct piro_batch piro_batch;
+int piro_batch_create(int count, const int *n, const float *alpha, const float *dt, const int *scheme,
+                      piro_stream_t stream, piro_batch **out);
+/* offsets (int64[count], may be NULL) and the total cells of the field array. */
+int piro_batch_layout(piro_batch *s, int64_t *offsets, int64_t *total_cells);
+/* Copy all fields in (out): host (from_host/to_host != 0) or device memory. */
+int piro_batch_set_fields(piro_batch *s, const float *u, int from_host);
+int piro_batch_get_fields(piro_batch *s, float *u, int to_host);
+/* Device pointer of the current fields (valid until the next step). */
+int piro_batch_field_ptr(piro_batch *s, float **u);
+/* Advance every member `steps` times (one launch per step); backward-Euler
+ * members solve to the FP64 relative residual rtol.  *ms (may be NULL) gets
+ * the device time (CUDA events). */
+int piro_batch_step(piro_batch *s, int steps, double rtol, double *ms);
+/* Per-member result of the last step (host arrays of count; any may be NULL):
+ * status (PIRO_OK, PIRO_STATUS_STALLED, PIRO_ERR_NOT_CONVERGED), refinement
+ * sweeps, CG iterations, FP64 relative residual (0 for forward Euler). */
+int piro_batch_member_info(piro_batch *s, int *status, int *sweeps, int *inner, double *rel);
+/* Autotuner: times one step from the current fields (result discarded) for
+ * each tile size (2048 .. 16384 cells) and blocks-per-SM (1, 2, 4) the
+ * occupancy allows and keeps the fastest. */
+int piro_batch_autotune(piro_batch *s, double rtol, int *tile, int *blocks_per_sm);
+int piro_batch_destroy(piro_batch *s);
+
 /* Reference JLI iteration (scheme 12 + solver 40, src/kernelprocess.cpp:123-209)
  * on the device: x = b; repeat r = b - (I - dt*L)x on interior rows (b on the
  * others), x += urf*r, r = dx; res = ||r||/sqrt(N); stop when

@@ -98,6 +98,15 @@ SIGNATURES = {
     "piro_pcnet_destroy": (i32, [vp]),
     "piro_be_set_preconditioner": (i32, [vp, i32, vp]),
     "piro_be_pc_stats": (i32, [vp, i32, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]),
+    "piro_batch_create": (i32, [i32, vp, vp, vp, vp, vp, C.POINTER(vp)]),
+    "piro_batch_layout": (i32, [vp, vp, pi64]),
+    "piro_batch_set_fields": (i32, [vp, vp, i32]),
+    "piro_batch_get_fields": (i32, [vp, vp, i32]),
+    "piro_batch_field_ptr": (i32, [vp, C.POINTER(vp)]),
+    "piro_batch_step": (i32, [vp, i32, f64, C.POINTER(C.c_double)]),
+    "piro_batch_member_info": (i32, [vp, vp, vp, vp, vp]),
+    "piro_batch_autotune": (i32, [vp, f64, pint, pint]),
+    "piro_batch_destroy": (i32, [vp]),
     "piro_open": (i32, [C.c_char_p, C.c_char_p, C.POINTER(vp)]),
     "piro_close": (None, [vp]),
     "piro_ctx_query": (i32, [vp, C.POINTER(CaseInfo)]),

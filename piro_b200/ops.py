@@ -394,3 +394,77 @@ class PCNet:
             self.close()
         except Exception:
             pass
+
+
+# ----------------------------------------------------------------- batched stepping
+class Batch:
+    """Many independent heat problems stepped in one persistent launch per step
+    (include/piro.h, piro_batch_*)."""
+
+    def __init__(self, n, alpha, dt, scheme):
+        import numpy as np
+        self.n = np.ascontiguousarray(n, np.int32)
+        self.alpha = np.ascontiguousarray(alpha, np.float32)
+        self.dt = np.ascontiguousarray(dt, np.float32)
+        self.scheme = np.ascontiguousarray(scheme, np.int32)
+        self.count = int(self.n.size)
+        h = C.c_void_p()
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        check(lib().piro_batch_create(self.count, vp(self.n), vp(self.alpha), vp(self.dt), vp(self.scheme),
+                                      _stream(), C.byref(h)), "piro_batch_create")
+        self.h = h
+        self.offsets = np.empty(self.count, np.int64)
+        tot = C.c_int64()
+        check(lib().piro_batch_layout(self.h, vp(self.offsets), C.byref(tot)), "piro_batch_layout")
+        self.total = tot.value
+
+    def set_fields(self, u) -> None:
+        """u: host numpy float32 array of total cells, or a CUDA tensor."""
+        import numpy as np
+        if isinstance(u, np.ndarray):
+            a = np.ascontiguousarray(u, np.float32)
+            check(lib().piro_batch_set_fields(self.h, a.ctypes.data_as(C.c_void_p), 1), "piro_batch_set_fields")
+        else:
+            check(lib().piro_batch_set_fields(self.h, _p(u), 0), "piro_batch_set_fields")
+
+    def get_fields(self):
+        import numpy as np
+        out = np.empty(self.total, np.float32)
+        check(lib().piro_batch_get_fields(self.h, out.ctypes.data_as(C.c_void_p), 1), "piro_batch_get_fields")
+        return out
+
+    def member(self, fields, k):
+        n = int(self.n[k])
+        o = int(self.offsets[k])
+        return fields[o:o + n ** 3]
+
+    def step(self, steps=1, rtol=1e-8) -> float:
+        ms = C.c_double()
+        check(lib().piro_batch_step(self.h, int(steps), float(rtol), C.byref(ms)), "piro_batch_step")
+        return ms.value
+
+    def member_info(self):
+        import numpy as np
+        st = np.empty(self.count, np.int32)
+        sw = np.empty(self.count, np.int32)
+        it = np.empty(self.count, np.int32)
+        rel = np.empty(self.count, np.float64)
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        check(lib().piro_batch_member_info(self.h, vp(st), vp(sw), vp(it), vp(rel)), "piro_batch_member_info")
+        return dict(status=st, sweeps=sw, inner=it, rel=rel)
+
+    def autotune(self, rtol=1e-8):
+        t, b = C.c_int(), C.c_int()
+        check(lib().piro_batch_autotune(self.h, float(rtol), C.byref(t), C.byref(b)), "piro_batch_autotune")
+        return t.value, b.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().piro_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

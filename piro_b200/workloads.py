@@ -92,3 +92,30 @@ def advection(n: int, seed: int = 1):
     v = np.concatenate([np.full(N, -w[d], np.float32) for d in range(3)])
     dt = np.float32(0.5 * 2.0 / np.abs(w).sum())
     return dict(n=(n, n, n), u0=u0, v=v, dt=dt, steps=1000, gnorm=np.float32(2.0))
+
+
+def batched(seed: int = 3, count: int = 512, lo: int = 16, hi: int = 96):
+    """Batched heat problems: cube sides uniform in [lo, hi] (ghost-inclusive),
+    alpha log-uniform in [1e-3, 1e-1], forward or backward Euler, all drawn
+    from default_rng(seed); dt = 0.2 h^2/(6 alpha) (forward) or 50 times the
+    explicit limit h^2/(6 alpha) (backward), h = 1.  Field: a centred Gaussian
+    bump (sigma n/8) plus U[0, 1e-3) noise, zero boundary."""
+    rng = np.random.default_rng(seed)
+    n = rng.integers(lo, hi + 1, size=count).astype(np.int32)
+    alpha = (10.0 ** rng.uniform(-3.0, -1.0, size=count)).astype(np.float32)
+    scheme = rng.integers(0, 2, size=count).astype(np.int32)
+    dt = np.where(scheme == 0, 0.2 / (6.0 * alpha), 50.0 / (6.0 * alpha)).astype(np.float32)
+    fields = []
+    for k in range(count):
+        m = int(n[k])
+        f = gaussian_bump(m, m / 8.0, (m - 1) / 2.0) + rng.uniform(0.0, 1e-3, m ** 3).astype(np.float32)
+        fields.append(zero_boundary(f, m, m, m).astype(np.float32))
+    return dict(n=n, alpha=alpha, dt=dt, scheme=scheme, fields=fields)
+
+
+def pack_batch(fields, offsets, total):
+    """Member fields into one array at the given offsets."""
+    u = np.zeros(total, np.float32)
+    for f, o in zip(fields, offsets):
+        u[int(o):int(o) + f.size] = f
+    return u
