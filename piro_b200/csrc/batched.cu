@@ -1,6 +1,6 @@
 // batched.cu -- many independent heat problems of uneven sizes stepped
-// together: one persistent cooperative launch per time step (captured in a
-// CUDA graph), each member a constant-alpha problem on its own ghost-inclusive
+// together: one persistent cooperative launch per time step (two steps per
+// replayed CUDA graph), each member a constant-alpha problem on its own ghost-inclusive
 // cube, forward Euler (TIMESCHEME 11, src/kernelprocess.cpp:10-40) or
 // backward Euler (TIMESCHEME 12, solved as the single-grid solver does:
 // FP32 Jacobi-PCG inside FP64 iterative refinement to a relative residual).
@@ -433,13 +433,23 @@ struct piro_batch {
     unsigned grid = 0;
     int blocks_per_sm = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStream_t own = nullptr;      // non-blocking stream for graph capture
+    cudaGraphExec_t pair = nullptr;  // two steps (f[0] -> f[1] -> f[0]) as one graph
+    double pair_rtol = 0.0;
     double step_ms = 0.0;
     long long steps = 0;
     double rtol = 1e-8;
 };
 
+static void batch_drop_graph(piro_batch *s)
+{
+    if (s->pair) cudaGraphExecDestroy(s->pair);
+    s->pair = nullptr;
+}
+
 static void batch_free_tiles(piro_batch *s)
 {
+    batch_drop_graph(s);
     cudaFree(s->d_fe_m);
     cudaFree(s->d_be_m);
     cudaFree(s->d_fe_s);
@@ -607,7 +617,7 @@ extern "C" int piro_batch_field_ptr(piro_batch *s, float **u)
     return PIRO_OK;
 }
 
-static int batch_launch(piro_batch *s, const float *u, float *out)
+static int batch_launch(piro_batch *s, const float *u, float *out, cudaStream_t st)
 {
     BArgs A;
     A.mem = s->d_mem;
@@ -638,8 +648,37 @@ static int batch_launch(piro_batch *s, const float *u, float *out)
     A.max_rounds = 40000;
     A.spin_limit = 1ll << 22;  // ~2 s of polling per barrier wait
     void *args[] = {&A};
-    PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_batch_step, dim3(s->grid), dim3(kThreads), args, 0,
-                                          s->stream));
+    PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_batch_step, dim3(s->grid), dim3(kThreads), args, 0, st));
+    return PIRO_OK;
+}
+
+// Two steps, f[0] -> f[1] -> f[0], captured once as a CUDA graph (two
+// cooperative kernel nodes) and replayed; re-captured when the tiling or the
+// tolerance changes.
+static int batch_pair_graph(piro_batch *s)
+{
+    if (s->pair && s->pair_rtol == s->rtol) return PIRO_OK;
+    batch_drop_graph(s);
+    if (!s->own) PIRO_CUDA(cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking));
+    PIRO_CUDA(cudaStreamBeginCapture(s->own, cudaStreamCaptureModeThreadLocal));
+    int rc = batch_launch(s, s->f[0], s->f[1], s->own);
+    if (!rc) rc = batch_launch(s, s->f[1], s->f[0], s->own);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s->own, &g);
+    if (rc || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        (void)cudaGetLastError();
+        set_error("piro_batch: graph capture of the step failed");
+        return rc ? rc : PIRO_ERR_CUDA;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&s->pair, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+        s->pair = nullptr;
+        set_error("piro_batch: graph instantiation failed: %s", cudaGetErrorString(ei));
+        return PIRO_ERR_CUDA;
+    }
+    s->pair_rtol = s->rtol;
     return PIRO_OK;
 }
 
@@ -647,11 +686,23 @@ extern "C" int piro_batch_step(piro_batch *s, int steps, double rtol, double *ms
 {
     PIRO_ARG(s && steps >= 0 && rtol > 0.0, "piro_batch_step: bad arguments");
     s->rtol = rtol;
-    PIRO_CUDA(cudaEventRecord(s->e0, s->stream));
-    for (int k = 0; k < steps; ++k) {
-        int rc = batch_launch(s, s->f[s->cur], s->f[s->cur ^ 1]);
+    int k = 0;
+    if (steps >= 2) {
+        int rc = batch_pair_graph(s);
         if (rc) return rc;
-        s->cur ^= 1;
+    }
+    PIRO_CUDA(cudaEventRecord(s->e0, s->stream));
+    if (s->cur == 1 && k < steps) {  // realign to f[0] so the pair graph applies
+        int rc = batch_launch(s, s->f[1], s->f[0], s->stream);
+        if (rc) return rc;
+        s->cur = 0;
+        ++k;
+    }
+    for (; k + 2 <= steps; k += 2) PIRO_CUDA(cudaGraphLaunch(s->pair, s->stream));
+    if (k < steps) {
+        int rc = batch_launch(s, s->f[0], s->f[1], s->stream);
+        if (rc) return rc;
+        s->cur = 1;
     }
     PIRO_CUDA(cudaEventRecord(s->e1, s->stream));
     PIRO_CUDA(cudaStreamSynchronize(s->stream));
@@ -701,7 +752,7 @@ extern "C" int piro_batch_autotune(piro_batch *s, double rtol, int *tile_out, in
             float ms = INFINITY;
             for (int rep = 0; rep < 2; ++rep) {  // second run timed
                 PIRO_CUDA(cudaEventRecord(s->e0, s->stream));
-                rc = batch_launch(s, s->f[s->cur], s->f[s->cur ^ 1]);
+                rc = batch_launch(s, s->f[s->cur], s->f[s->cur ^ 1], s->stream);
                 if (rc) return rc;
                 PIRO_CUDA(cudaEventRecord(s->e1, s->stream));
                 PIRO_CUDA(cudaStreamSynchronize(s->stream));
@@ -733,6 +784,7 @@ extern "C" int piro_batch_destroy(piro_batch *s)
     cudaFree(s->bar);
     if (s->e0) cudaEventDestroy(s->e0);
     if (s->e1) cudaEventDestroy(s->e1);
+    if (s->own) cudaStreamDestroy(s->own);
     delete s;
     return PIRO_OK;
 }
