@@ -348,6 +348,48 @@ int piro_be_set_preconditioner(piro_be_solver *s, int kind, piro_pcnet *net);
  * reset and their summed device time in ms (CUDA events around each apply). */
 int piro_be_pc_stats(piro_be_solver *s, int reset, long long *applies, double *ms);
 
+/* -- z-slab decomposition of one grid over ranks ------------------------------
+ *
+ * A rank owns grid planes [z0, z1) and keeps arrays of planes z0-1 .. z1 (one
+ * halo plane each side; local cell l = grid cell l + (z0-1)*nx*ny).  The host
+ * exchanges halo planes between neighbouring ranks and all-reduces the FP64
+ * partial sums these entry points return (device double[]); see
+ * piro_b200/slab.py.  Forward Euler: the owned rows of the assembled CSR
+ * matrix (column indices local) stepped exactly as SpMVCSR.cl, so a sharded
+ * step equals the single-grid step bit for bit.  Backward Euler: the
+ * single-grid solver's method (FP32 Jacobi-PCG in FP64 refinement on
+ * A = I - dt*diag(alpha)*L, central scheme) with a matrix-free operator whose
+ * couplings to boundary cells carry the stencil value. */
+/* nnz of grid rows [row0, row0 + nrows) of the Laplacian. */
+int piro_laplacian_nnz_rows(int nx, int ny, int nz, int64_t row0, int64_t nrows, int64_t *nnz);
+/* Those rows of PIRO's CSR Laplacian (entries, order and 10.0 rule of
+ * stencils.cpp:233-429): rowptr[nrows+1] from 0, columns minus col_shift. */
+int piro_csr_laplacian_rows(int nx, int ny, int nz, int space_scheme, float norm, int64_t row0, int64_t nrows,
+                            int64_t col_shift, int32_t *rowptr, int32_t *col, float *val, piro_stream_t stream);
+/* SpMVCSR.cl on rows [row0, row0 + nrows): out[ubase + i] = u[ubase + i] +
+ * sum_k (dt*val[k])*u[col[k]] for interior grid rows row0 + i. */
+int piro_csr_fe_step_rows(int nx, int ny, int nz, int64_t row0, int64_t nrows, const int32_t *rowptr,
+                          const int32_t *col, const float *val, float dt, const float *u, int64_t ubase, float *out,
+                          piro_stream_t stream);
+/* Doubles of the `work` array the slab solver kernels need. */
+int piro_slab_workspace(int64_t *doubles);
+/* r = b - A x64 (FP64), z = r / A_rr on owned interior cells; sums[4] =
+ * |r64|^2, |b|^2, <r/alpha, z>, |r32|^2 over the owned interior. */
+int piro_slab_be_residual(int nx, int ny, int nz, int z0, int z1, float dt, float norm, const float *alpha,
+                          const float *b, const double *x64, float *r, float *z, double *work, double *sums,
+                          piro_stream_t stream);
+/* p_new = z + beta p_old (owned and halo planes), q = A p_new (owned);
+ * sums[0] = <p_new, q/alpha>.  z's halo planes must be current. */
+int piro_slab_cg_spmv(int nx, int ny, int nz, int z0, int z1, float dt, float norm, float beta, const float *alpha,
+                      const float *z, const float *p_old, float *p_new, float *q, double *work, double *sums,
+                      piro_stream_t stream);
+/* d += a p, r -= a q, z = r / A_rr (owned); sums[0..1] = <r/alpha, z>, |r|^2. */
+int piro_slab_cg_update(int nx, int ny, int nz, int z0, int z1, float dt, float norm, float a, const float *alpha,
+                        const float *p, const float *q, float *d, float *r, float *z, double *work, double *sums,
+                        piro_stream_t stream);
+/* x64 += d, d = 0 on owned interior cells. */
+int piro_slab_x_update(int nx, int ny, int nz, int z0, int z1, double *x64, float *d, piro_stream_t stream);
+
 /* -- batched stepping: many independent problems in one persistent launch ----
  *
  * `count` independent heat problems, member k a constant-alpha cube of n[k]^3

@@ -98,6 +98,14 @@ SIGNATURES = {
     "piro_pcnet_destroy": (i32, [vp]),
     "piro_be_set_preconditioner": (i32, [vp, i32, vp]),
     "piro_be_pc_stats": (i32, [vp, i32, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]),
+    "piro_laplacian_nnz_rows": (i32, [i32, i32, i32, i64, i64, pi64]),
+    "piro_csr_laplacian_rows": (i32, [i32, i32, i32, i32, f32, i64, i64, i64, vp, vp, vp, vp]),
+    "piro_csr_fe_step_rows": (i32, [i32, i32, i32, i64, i64, vp, vp, vp, f32, vp, i64, vp, vp]),
+    "piro_slab_workspace": (i32, [pi64]),
+    "piro_slab_be_residual": (i32, [i32, i32, i32, i32, i32, f32, f32, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "piro_slab_cg_spmv": (i32, [i32, i32, i32, i32, i32, f32, f32, f32, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "piro_slab_cg_update": (i32, [i32, i32, i32, i32, i32, f32, f32, f32, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "piro_slab_x_update": (i32, [i32, i32, i32, i32, i32, vp, vp, vp]),
     "piro_batch_create": (i32, [i32, vp, vp, vp, vp, vp, C.POINTER(vp)]),
     "piro_batch_layout": (i32, [vp, vp, pi64]),
     "piro_batch_set_fields": (i32, [vp, vp, i32]),

@@ -33,7 +33,7 @@ __device__ __forceinline__ void coords(int64_t i, const Grid &g, int &x, int &y,
 // Sum of 7-point row lengths over all rows before (x, y, z) in row-major
 // order; a row has 7 - [x==0] - [x==nx-1] - [y==0] - [y==ny-1] - [z==0] - [z==nz-1]
 // entries.
-__device__ __forceinline__ int64_t lap_prefix(int x, int y, int z, const Grid &g)
+__host__ __device__ __forceinline__ int64_t lap_prefix(int x, int y, int z, const Grid &g)
 {
     const int64_t nx = g.nx, ny = g.ny, nz = g.nz;
     const int64_t by = (y == 0) + (y == ny - 1);
@@ -90,19 +90,29 @@ __device__ __forceinline__ int lap_row(int64_t i, const Grid &g, int scheme, flo
 }
 
 // Block = kRowsPerBlock consecutive rows.  rowptr may be NULL (COO), rows may
-// be NULL (CSR).
+// be NULL (CSR).  Rows [row0, row0 + N) of the grid's matrix: rowptr starts at
+// 0, entries are stored from 0 and columns (and COO rows) are shifted by
+// -col_shift (the whole matrix: row0 = 0, N = all rows, col_shift = 0).
 __global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, int scheme, float vself, float vnb,
                                                              int32_t *__restrict__ rowptr,
                                                              int32_t *__restrict__ rows, int32_t *__restrict__ col,
-                                                             float *__restrict__ val)
+                                                             float *__restrict__ val, int64_t row0,
+                                                             int64_t col_shift)
 {
     __shared__ int32_t s_col[kRowsPerBlock * kMaxPerRow];
     __shared__ float s_val[kRowsPerBlock * kMaxPerRow];
     __shared__ int32_t s_row[kRowsPerBlock * kMaxPerRow];
     __shared__ int64_t s_base, s_end;
-    for (int64_t r0 = (int64_t)blockIdx.x * kRowsPerBlock; r0 < N; r0 += (int64_t)gridDim.x * kRowsPerBlock) {
+    int64_t base0;
+    {
+        int x, y, z;
+        coords(row0, g, x, y, z);
+        base0 = lap_prefix(x, y, z, g);
+    }
+    const int64_t R1 = row0 + N;
+    for (int64_t r0 = row0 + (int64_t)blockIdx.x * kRowsPerBlock; r0 < R1; r0 += (int64_t)gridDim.x * kRowsPerBlock) {
         const int64_t i = r0 + threadIdx.x;
-        const int64_t rlast = (r0 + kRowsPerBlock < N ? r0 + kRowsPerBlock : N) - 1;
+        const int64_t rlast = (r0 + kRowsPerBlock < R1 ? r0 + kRowsPerBlock : R1) - 1;
         if (threadIdx.x == 0) {
             int x, y, z;
             coords(r0, g, x, y, z);
@@ -113,7 +123,7 @@ __global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, 
             s_end = lap_prefix(x, y, z, g) + lap_row(rlast, g, scheme, vself, vnb, c, v);
         }
         __syncthreads();
-        if (i < N) {
+        if (i < R1) {
             int x, y, z;
             coords(i, g, x, y, z);
             const int64_t p = lap_prefix(x, y, z, g);
@@ -122,21 +132,21 @@ __global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, 
             const int n = lap_row(i, g, scheme, vself, vnb, c, v);
             const int off = (int)(p - s_base);
             for (int t = 0; t < n; ++t) {
-                s_col[off + t] = c[t];
+                s_col[off + t] = (int32_t)(c[t] - col_shift);
                 s_val[off + t] = v[t];
-                s_row[off + t] = (int32_t)i;
+                s_row[off + t] = (int32_t)(i - col_shift);
             }
             if (rowptr) {
-                rowptr[i + 1] = (int32_t)(p + n);
-                if (i == 0) rowptr[0] = 0;
+                rowptr[i - row0 + 1] = (int32_t)(p + n - base0);
+                if (i == row0) rowptr[0] = 0;
             }
         }
         __syncthreads();
         const int cnt = (int)(s_end - s_base);
         for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-            col[s_base + t] = s_col[t];
-            val[s_base + t] = s_val[t];
-            if (rows) rows[s_base + t] = s_row[t];
+            col[s_base - base0 + t] = s_col[t];
+            val[s_base - base0 + t] = s_val[t];
+            if (rows) rows[s_base - base0 + t] = s_row[t];
         }
         __syncthreads();
     }
@@ -268,7 +278,48 @@ static int launch_laplacian(int nx, int ny, int nz, int scheme, float norm, int3
     const float vself = (float)(-6.0 / (double)norm);
     const float vnb = (float)(1.0 / (double)norm);
     unsigned grid = grid_for(N, kRowsPerBlock, 4);
-    k_laplacian<<<grid, kRowsPerBlock, 0, as_stream(stream)>>>(g, N, scheme, vself, vnb, rowptr, rows, col, val);
+    k_laplacian<<<grid, kRowsPerBlock, 0, as_stream(stream)>>>(g, N, scheme, vself, vnb, rowptr, rows, col, val, 0,
+                                                               0);
+    PIRO_CHECK_LAUNCH("k_laplacian");
+    return PIRO_OK;
+}
+
+extern "C" int piro_laplacian_nnz_rows(int nx, int ny, int nz, int64_t row0, int64_t nrows, int64_t *nnz)
+{
+    const int64_t N = (int64_t)nx * ny * nz;
+    PIRO_ARG(nnz && grid_ok(nx, ny, nz) && row0 >= 0 && nrows >= 0 && row0 + nrows <= N,
+             "piro_laplacian_nnz_rows: bad arguments");
+    const Grid g{nx, ny, nz, (int64_t)nx * ny};
+    auto prefix = [&](int64_t i) -> int64_t {
+        if (i >= N) return 7 * N - 2 * ((int64_t)nx * ny + (int64_t)ny * nz + (int64_t)nx * nz);
+        const int z = (int)(i / g.sxy);
+        const int64_t rem = i - (int64_t)z * g.sxy;
+        const int y = (int)(rem / nx);
+        return lap_prefix((int)(rem - (int64_t)y * nx), y, z, g);
+    };
+    *nnz = prefix(row0 + nrows) - prefix(row0);
+    return PIRO_OK;
+}
+
+extern "C" int piro_csr_laplacian_rows(int nx, int ny, int nz, int space_scheme, float norm, int64_t row0,
+                                       int64_t nrows, int64_t col_shift, int32_t *rowptr, int32_t *col, float *val,
+                                       piro_stream_t stream)
+{
+    const int64_t N = (int64_t)nx * ny * nz;
+    // columns of rows >= row0 reach down to row0 - nx*ny: local columns stay >= 0
+    PIRO_ARG(grid_ok(nx, ny, nz) && rowptr && col && val && row0 >= 0 && nrows > 0 && row0 + nrows <= N &&
+                 col_shift <= row0 - (row0 > 0 ? (int64_t)nx * ny : 0),
+             "piro_csr_laplacian_rows: bad arguments");
+    if (space_scheme < 1 || space_scheme > 3) {
+        piro::set_error("laplacian: space scheme %d not in {1 uw, 2 dw, 3 cd}", space_scheme);
+        return PIRO_ERR_SCHEME;
+    }
+    Grid g{nx, ny, nz, (int64_t)nx * ny};
+    const float vself = (float)(-6.0 / (double)norm);
+    const float vnb = (float)(1.0 / (double)norm);
+    unsigned grid = grid_for(nrows, kRowsPerBlock, 4);
+    k_laplacian<<<grid, kRowsPerBlock, 0, as_stream(stream)>>>(g, nrows, space_scheme, vself, vnb, rowptr, nullptr,
+                                                               col, val, row0, col_shift);
     PIRO_CHECK_LAUNCH("k_laplacian");
     return PIRO_OK;
 }

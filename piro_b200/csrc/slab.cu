@@ -1,0 +1,266 @@
+// slab.cu -- z-slab domain decomposition of one grid over ranks: the kernels
+// of the backward-Euler solve on one slab (FP64 residual, FP32 CG steps,
+// refinement update) for A = I - dt*diag(alpha)*L with the central 7-point L.
+//
+// Slab layout: a rank owns grid planes [z0, z1); its arrays hold planes
+// z0-1 .. z1 (one halo plane each side, nz_l = z1 - z0 + 2 planes; the halo
+// below plane 0 and above plane nz-1 of the grid is never read by an owned
+// interior row).  Local cell l is grid cell l + (z0 - 1)*nx*ny.  The host
+// exchanges halo planes (z before each CG operator apply, x64 after each
+// refinement update) and all-reduces the FP64 partial sums each kernel
+// returns; these kernels only touch owned cells (and, for p, the halo planes,
+// which every rank forms identically from the exchanged z).
+//
+// Coefficients per cell are the FP32 values csrgeam2 gives the assembled A
+// (diagonal fl(1 + fl(-dt*fl(alpha*vself))), off-diagonal fl(-dt*fl(alpha*vnb)))
+// promoted to FP64 for the residual, as the single-grid solver's CSR residual.
+// Couplings to boundary cells use the stencil value (PIRO's 10.0 entries,
+// stencils.cpp:278-291, only meet nonzero boundary values).
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace piro {
+namespace {
+
+constexpr int kSlabThreads = 256;
+constexpr int kSlabBlocks = 1184;  // at most 8 per SM on a 148-SM part: per-block partial sums
+
+struct Slab {
+    GridDiv g;           // the whole grid
+    int64_t lbase;       // grid index of local cell 0: (z0 - 1) * nx * ny (may be negative)
+    int64_t own0, own1;  // local cell range of the owned planes
+    float mdt, vself, vnb;
+};
+
+__device__ __forceinline__ void coef(const Slab &S, float a, float &cd, float &co)
+{
+    cd = __fadd_rn(1.0f, __fmul_rn(S.mdt, __fmul_rn(a, S.vself)));
+    co = __fmul_rn(S.mdt, __fmul_rn(a, S.vnb));
+}
+
+// Block sums of nvals values into out[k * gridDim.x + blockIdx.x].
+__device__ __forceinline__ void block_partials(double *out, int nvals, const double (&v)[4])
+{
+    __shared__ double s_w[4][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int k = 0; k < nvals; ++k) {
+        const double t = warp_sum(v[k]);
+        if (lane == 0) s_w[k][w] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        for (int k = 0; k < nvals; ++k) {
+            double t = threadIdx.x < (blockDim.x >> 5) ? s_w[k][threadIdx.x] : 0.0;
+            t = warp_sum(t);
+            if (threadIdx.x == 0) out[(int64_t)k * gridDim.x + blockIdx.x] = t;
+        }
+    }
+}
+
+// r = b - A x64 (FP64) and z = r / A_rr on owned interior cells, 0 on the
+// owned boundary; partials: |r64|^2, |b|^2, <r/alpha, z>, |r32|^2.
+__global__ void __launch_bounds__(kSlabThreads) k_slab_residual(Slab S, const float *__restrict__ alpha,
+                                                                const float *__restrict__ b,
+                                                                const double *__restrict__ x, float *__restrict__ r,
+                                                                float *__restrict__ z, double *__restrict__ part)
+{
+    const int64_t sxy = (int64_t)S.g.nx * S.g.ny;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int64_t l = S.own0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < S.own1;
+         l += (int64_t)gridDim.x * blockDim.x) {
+        if (!S.g.interior(l + S.lbase)) {
+            r[l] = 0.0f;
+            z[l] = 0.0f;
+            continue;
+        }
+        const float a = alpha[l];
+        float cd, co;
+        coef(S, a, cd, co);
+        const int nx = S.g.nx;
+        const double nb = ((x[l - 1] + x[l + 1]) + (x[l - nx] + x[l + nx])) + (x[l - sxy] + x[l + sxy]);
+        const double bi = (double)b[l];
+        const double ri = bi - ((double)cd * x[l] + (double)co * nb);
+        const float rf = (float)ri;
+        const float zf = rf / cd;
+        r[l] = rf;
+        z[l] = zf;
+        v[0] += ri * ri;
+        v[1] += bi * bi;
+        v[2] += (double)rf / (double)a * (double)zf;
+        v[3] += (double)rf * (double)rf;
+    }
+    block_partials(part, 4, v);
+}
+
+// p = z + beta*p_old on interior cells of the owned and halo planes (0 on the
+// boundary); q = A p on owned interior cells; partial <p, q/alpha>.
+__global__ void __launch_bounds__(kSlabThreads) k_slab_cg_spmv(Slab S, float beta, const float *__restrict__ alpha,
+                                                               const float *__restrict__ z,
+                                                               const float *__restrict__ p_old,
+                                                               float *__restrict__ p_new, float *__restrict__ q,
+                                                               double *__restrict__ part)
+{
+    const int64_t sxy = (int64_t)S.g.nx * S.g.ny;
+    const int64_t N = sxy * S.g.nz;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    const int64_t lo = max(S.own0 - sxy, -S.lbase), hi = min(S.own1 + sxy, N - S.lbase);
+    for (int64_t l = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < hi;
+         l += (int64_t)gridDim.x * blockDim.x) {
+        const bool in = S.g.interior(l + S.lbase);
+        const float pc = in ? z[l] + beta * p_old[l] : 0.0f;
+        p_new[l] = pc;
+        if (!in || l < S.own0 || l >= S.own1) continue;
+        const int nx = S.g.nx;
+        // neighbours' p formed from z and p_old (p_new of other threads is not read)
+        auto pv = [&](int64_t j) { return S.g.interior(j + S.lbase) ? z[j] + beta * p_old[j] : 0.0f; };
+        const float a = alpha[l];
+        float cd, co;
+        coef(S, a, cd, co);
+        const float qv =
+            cd * pc + co * (((pv(l - 1) + pv(l + 1)) + (pv(l - nx) + pv(l + nx))) + (pv(l - sxy) + pv(l + sxy)));
+        q[l] = qv;
+        v[0] += (double)pc * (double)qv / (double)a;
+    }
+    block_partials(part, 1, v);
+}
+
+// d += a p, r -= a q, z = r / A_rr on owned interior cells; partials
+// <r/alpha, z>, |r|^2.
+__global__ void __launch_bounds__(kSlabThreads) k_slab_cg_update(Slab S, float a, const float *__restrict__ alpha,
+                                                                 const float *__restrict__ p,
+                                                                 const float *__restrict__ q, float *__restrict__ d,
+                                                                 float *__restrict__ r, float *__restrict__ z,
+                                                                 double *__restrict__ part)
+{
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int64_t l = S.own0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < S.own1;
+         l += (int64_t)gridDim.x * blockDim.x) {
+        if (!S.g.interior(l + S.lbase)) continue;
+        const float al = alpha[l];
+        float cd, co;
+        coef(S, al, cd, co);
+        d[l] += a * p[l];
+        const float ri = r[l] - a * q[l];
+        const float zi = ri / cd;
+        r[l] = ri;
+        z[l] = zi;
+        v[0] += (double)ri / (double)al * (double)zi;
+        v[1] += (double)ri * (double)ri;
+    }
+    block_partials(part, 2, v);
+}
+
+// x64 += d, d = 0 on owned interior cells.
+__global__ void k_slab_x_update(Slab S, double *__restrict__ x, float *__restrict__ d)
+{
+    for (int64_t l = S.own0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < S.own1;
+         l += (int64_t)gridDim.x * blockDim.x) {
+        if (!S.g.interior(l + S.lbase)) continue;
+        x[l] += (double)d[l];
+        d[l] = 0.0f;
+    }
+}
+
+// out[k] = in-order sum over the nblocks partials of value k (one warp per value).
+__global__ void k_slab_finish(const double *__restrict__ part, int nblocks, int nvals, double *__restrict__ out)
+{
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (k >= nvals) return;
+    double s = 0.0;
+    for (int i = lane; i < nblocks; i += 32) s += part[(int64_t)k * nblocks + i];
+    s = warp_sum(s);
+    if (lane == 0) out[k] = s;
+}
+
+int slab_make(int nx, int ny, int nz, int z0, int z1, float dt, float norm, Slab *S)
+{
+    PIRO_ARG(nx >= 3 && ny >= 3 && nz >= 3 && z0 >= 0 && z1 > z0 && z1 <= nz && dt > 0.0f && norm > 0.0f &&
+                 (int64_t)nx * ny * nz < ((int64_t)1 << 31),
+             "piro_slab: bad grid, slab or coefficients");
+    const int64_t sxy = (int64_t)nx * ny;
+    S->g = GridDiv(nx, ny, nz);
+    S->lbase = (int64_t)(z0 - 1) * sxy;
+    S->own0 = sxy;
+    S->own1 = (int64_t)(z1 - z0 + 1) * sxy;
+    S->mdt = -dt;
+    S->vself = (float)(-6.0 / (double)norm);
+    S->vnb = (float)(1.0 / (double)norm);
+    return PIRO_OK;
+}
+
+unsigned slab_grid() { return (unsigned)std::min(kSlabBlocks, sm_count() * 8); }
+
+}  // namespace
+}  // namespace piro
+
+using namespace piro;
+
+extern "C" int piro_slab_workspace(int64_t *doubles)
+{
+    PIRO_ARG(doubles, "piro_slab_workspace: bad arguments");
+    *doubles = 4 * (int64_t)kSlabBlocks;  // partial sums: [value][block]
+    return PIRO_OK;
+}
+
+extern "C" int piro_slab_be_residual(int nx, int ny, int nz, int z0, int z1, float dt, float norm,
+                                     const float *alpha, const float *b, const double *x64, float *r, float *z,
+                                     double *work, double *sums, piro_stream_t stream)
+{
+    Slab S;
+    int rc = slab_make(nx, ny, nz, z0, z1, dt, norm, &S);
+    if (rc) return rc;
+    PIRO_ARG(alpha && b && x64 && r && z && work && sums, "piro_slab_be_residual: null pointer");
+    cudaStream_t st = as_stream(stream);
+    const unsigned grid = slab_grid();
+    k_slab_residual<<<grid, kSlabThreads, 0, st>>>(S, alpha, b, x64, r, z, work);
+    PIRO_CHECK_LAUNCH("k_slab_residual");
+    k_slab_finish<<<1, 32 * 4, 0, st>>>(work, (int)grid, 4, sums);
+    PIRO_CHECK_LAUNCH("k_slab_finish");
+    return PIRO_OK;
+}
+
+extern "C" int piro_slab_cg_spmv(int nx, int ny, int nz, int z0, int z1, float dt, float norm, float beta,
+                                 const float *alpha, const float *z, const float *p_old, float *p_new, float *q,
+                                 double *work, double *sums, piro_stream_t stream)
+{
+    Slab S;
+    int rc = slab_make(nx, ny, nz, z0, z1, dt, norm, &S);
+    if (rc) return rc;
+    PIRO_ARG(alpha && z && p_old && p_new && q && work && sums && p_old != p_new, "piro_slab_cg_spmv: bad pointers");
+    cudaStream_t st = as_stream(stream);
+    const unsigned grid = slab_grid();
+    k_slab_cg_spmv<<<grid, kSlabThreads, 0, st>>>(S, beta, alpha, z, p_old, p_new, q, work);
+    PIRO_CHECK_LAUNCH("k_slab_cg_spmv");
+    k_slab_finish<<<1, 32, 0, st>>>(work, (int)grid, 1, sums);
+    PIRO_CHECK_LAUNCH("k_slab_finish");
+    return PIRO_OK;
+}
+
+extern "C" int piro_slab_cg_update(int nx, int ny, int nz, int z0, int z1, float dt, float norm, float a,
+                                   const float *alpha, const float *p, const float *q, float *d, float *r, float *z,
+                                   double *work, double *sums, piro_stream_t stream)
+{
+    Slab S;
+    int rc = slab_make(nx, ny, nz, z0, z1, dt, norm, &S);
+    if (rc) return rc;
+    PIRO_ARG(alpha && p && q && d && r && z && work && sums, "piro_slab_cg_update: null pointer");
+    cudaStream_t st = as_stream(stream);
+    const unsigned grid = slab_grid();
+    k_slab_cg_update<<<grid, kSlabThreads, 0, st>>>(S, a, alpha, p, q, d, r, z, work);
+    PIRO_CHECK_LAUNCH("k_slab_cg_update");
+    k_slab_finish<<<1, 64, 0, st>>>(work, (int)grid, 2, sums);
+    PIRO_CHECK_LAUNCH("k_slab_finish");
+    return PIRO_OK;
+}
+
+extern "C" int piro_slab_x_update(int nx, int ny, int nz, int z0, int z1, double *x64, float *d, piro_stream_t stream)
+{
+    Slab S;
+    int rc = slab_make(nx, ny, nz, z0, z1, 1.0f, 1.0f, &S);
+    if (rc) return rc;
+    PIRO_ARG(x64 && d, "piro_slab_x_update: null pointer");
+    k_slab_x_update<<<slab_grid(), kSlabThreads, 0, as_stream(stream)>>>(S, x64, d);
+    PIRO_CHECK_LAUNCH("k_slab_x_update");
+    return PIRO_OK;
+}

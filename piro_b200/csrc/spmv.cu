@@ -17,17 +17,25 @@ namespace {
 
 // mode 0: SpMVCSR (out = u + sum), mode 1: SpMVCSR_I1 (out = u - sum).
 template <int kMode>
+// Matrix row `row` is grid row row0 + row (interior test) and reads/writes
+// u[ubase + row] / out[ubase + row]; columns index u directly.  (The whole
+// grid: row0 = ubase = 0; a z-slab with one halo plane below: row0 = first
+// owned row, ubase = nx*ny.)
 struct FeRow {
     GridDiv g;
     float dt;
     const float *__restrict__ u;
     float *__restrict__ out;
+    int64_t row0, ubase;
     float result;
     __device__ __forceinline__ void begin(int64_t) { result = 0.0f; }
     __device__ __forceinline__ void add(int32_t c, float v) { result = add_rn(result, mul_rn(mul_rn(dt, v), __ldg(u + c))); }
     __device__ __forceinline__ void end(int64_t row)
     {
-        if (g.interior(row)) out[row] = kMode == 0 ? add_rn(result, u[row]) : sub_rn(u[row], result);
+        if (g.interior(row0 + row)) {
+            const int64_t k = ubase + row;
+            out[k] = kMode == 0 ? add_rn(result, u[k]) : sub_rn(u[k], result);
+        }
     }
 };
 
@@ -35,9 +43,10 @@ template <int kMode>
 __global__ void __launch_bounds__(kRowThreads) k_csr_step(GridDiv g, int64_t N, const int32_t *__restrict__ rowptr,
                                                           const int32_t *__restrict__ col,
                                                           const float *__restrict__ val, float dt,
-                                                          const float *__restrict__ u, float *__restrict__ out)
+                                                          const float *__restrict__ u, float *__restrict__ out,
+                                                          int64_t row0, int64_t ubase)
 {
-    FeRow<kMode> op{g, dt, u, out, 0.0f};
+    FeRow<kMode> op{g, dt, u, out, row0, ubase, 0.0f};
     csr_for_rows(N, rowptr, col, val, op);
 }
 
@@ -222,7 +231,7 @@ int launch_csr_step(int nx, int ny, int nz, const int32_t *rowptr, const int32_t
     PIRO_ARG(u != out, "csr step: u and out must differ (the reference writes a fresh buffer)");
     const int64_t N = (int64_t)nx * ny * nz;
     k_csr_step<kMode><<<csr_rows_grid(N), kRowThreads, 0, as_stream(stream)>>>(GridDiv(nx, ny, nz), N, rowptr, col,
-                                                                              val, dt, u, out);
+                                                                              val, dt, u, out, 0, 0);
     PIRO_CHECK_LAUNCH("k_csr_step");
     return PIRO_OK;
 }
@@ -236,6 +245,20 @@ extern "C" int piro_csr_fe_step(int nx, int ny, int nz, const int32_t *rowptr, c
                                 float dt, const float *u, float *out, piro_stream_t stream)
 {
     return launch_csr_step<0>(nx, ny, nz, rowptr, col, val, dt, u, out, stream);
+}
+
+extern "C" int piro_csr_fe_step_rows(int nx, int ny, int nz, int64_t row0, int64_t nrows, const int32_t *rowptr,
+                                     const int32_t *col, const float *val, float dt, const float *u, int64_t ubase,
+                                     float *out, piro_stream_t stream)
+{
+    const int64_t N = (int64_t)nx * ny * nz;
+    PIRO_ARG(grid_ok(nx, ny, nz) && rowptr && col && val && u && out && u != out && row0 >= 0 && nrows > 0 &&
+                 row0 + nrows <= N && ubase >= 0,
+             "piro_csr_fe_step_rows: bad arguments");
+    k_csr_step<0><<<csr_rows_grid(nrows), kRowThreads, 0, as_stream(stream)>>>(GridDiv(nx, ny, nz), nrows, rowptr,
+                                                                              col, val, dt, u, out, row0, ubase);
+    PIRO_CHECK_LAUNCH("k_csr_step");
+    return PIRO_OK;
 }
 
 extern "C" int piro_csr_i1(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val,
