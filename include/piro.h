@@ -519,6 +519,26 @@ int piro_solve(piro_ctx *ctx, int64_t *steps_taken);
 int piro_op_export_csr(piro_ctx *ctx, piro_op op, int32_t *rowptr, int32_t *col, float *val, int64_t cap,
                        int64_t *nnz);
 
+/* -- ParaView output (Piro::paraview, src/paraview.cpp:12-137) ------------------
+ *
+ * piro_write_paraview writes <root>/<casename>/mesh/mesh_<ts>.vth and
+ * .../mesh/level/<ts>_level_0.vti (ts zero-padded to 5 digits) with the bytes
+ * PIRO writes: ASCII cell data of every scalar and vector field (constants
+ * skipped; vectors as _x/_y/_z arrays), boundary cells removed, values
+ * formatted as std::ostream formats a float.  The interior cells are gathered
+ * on the device, so only they cross PCIe (the reference copies whole fields
+ * and erases boundary entries one at a time).  [Mesh] index must be 1 per
+ * level: the reference only has data for level data set 0.
+ * piro_set_output sets the root (NULL disables output; [File] restart = 1
+ * clears <root>/<casename> first, as Piro::init); piro_step_solve then writes
+ * every Save steps as scalarMatrix::Solve does (src/process.cpp:236-247).
+ * piro_interior_gather: dst[k*Ni + j] = src[k*N + interior cell j] for ncomp
+ * components (Ni = (nx-2)(ny-2)(nz-2), x fastest). */
+int piro_write_paraview(piro_ctx *c, const char *root, int timestep);
+int piro_set_output(piro_ctx *c, const char *root);
+int piro_interior_gather(int nx, int ny, int nz, int ncomp, const float *src, float *dst, piro_stream_t stream);
+
+
 #ifdef __cplusplus
 }
 #endif

@@ -431,6 +431,27 @@ class Ref:
         q = self.lib.ref_initbc(nx, ny, nz, assets_root.encode(), scalar.encode(), idx, flen, field)
         return idx[:q].copy(), flen, field
 
+    def paraview(self, nx, ny, nz, origin, spacing, out_dir, casename, timestep, fields):
+        """Piro::paraview::writevth (src/paraview.cpp:106-137) on `fields`, a list
+        of (name, type 0/1/2, float32 values): writes the .vth and level-0 .vti
+        under out_dir/casename/mesh/ and returns (vth text, vti text)."""
+        L = self.lib
+        L.ref_paraview.restype = None
+        mesh = os.path.join(out_dir, casename, "mesh")
+        os.makedirs(os.path.join(mesh, "level"), exist_ok=True)
+        names = (C.c_char_p * len(fields))(*[f[0].encode() for f in fields])
+        types = (C.c_int * len(fields))(*[int(f[1]) for f in fields])
+        arrs = [np.ascontiguousarray(f[2], np.float32) for f in fields]
+        vals = (C.c_void_p * len(fields))(*[a.ctypes.data for a in arrs])
+        L.ref_paraview(nx, ny, nz, *[int(v) for v in origin], *[int(v) for v in spacing], out_dir.encode(),
+                       casename.encode(), int(timestep), len(fields), names, types, vals)
+        ts = f"{int(timestep):05d}"
+        with open(os.path.join(mesh, f"mesh_{ts}.vth")) as f:
+            vth = f.read()
+        with open(os.path.join(mesh, "level", f"{ts}_level_0.vti")) as f:
+            vti = f.read()
+        return vth, vti
+
     def initialcondition(self, nx, ny, nz, l, assets_root, ic_name):
         out = np.zeros(3 * n_cells(nx, ny, nz), np.float32)
         n = self.lib.ref_initialcondition(nx, ny, nz, *map(np.float32, l), assets_root.encode(), ic_name.encode(),

@@ -13,6 +13,7 @@
 #include <fileutilities.hpp>
 #include <methods.hpp>
 #include <openclutilities.hpp>
+#include <postprocess.hpp>
 #include <stencils.hpp>
 
 #include <cstdint>
@@ -176,6 +177,46 @@ long long ref_initialcondition(int nx, int ny, int nz, float l0, float l1, float
     std::vector<float> v = Piro::initialcondition(0);
     std::memcpy(out, v.data(), sizeof(float) * v.size());
     return (long long)v.size();
+}
+
+// Piro::paraview::writevth (src/paraview.cpp:106-137) for a one-level mesh:
+// the fields of AMR[0].CD (constants type 0, scalars type 1, vectors type 2,
+// vectors holding 3N values), then the three operator slots preprocess.cpp
+// appends; bc::prepbc() supplies the boundary cells to strip.  Files go under
+// <dir>/<casename>/mesh/ (the directories must exist).
+void ref_paraview(int nx, int ny, int nz, int ox, int oy, int oz, int sx, int sy, int sz, const char *dir,
+                  const char *casename, int timestep, int nfields, const char *const *names, const int *types,
+                  const float *const *values)
+{
+    set_grid(nx, ny, nz);
+    const long long N = (long long)nx * ny * nz;
+    Piro::file_utilities::current_path = std::string(dir);
+    Piro::MeshParams &MP = Piro::MeshParams::getInstance();
+    Piro::SolveParams &SP = Piro::SolveParams::getInstance();
+    SP.setvalue(Piro::SolveParams::CASENAME, std::string(casename));
+    MP.setvalue(Piro::MeshParams::LEVELS, 1);
+    MP.setvalue(Piro::MeshParams::INDEX, std::vector<int>{1});
+    int nvec = 0;
+    Piro::AMR amr;
+    amr.WholeExtent[0] = 0; amr.WholeExtent[1] = nx;
+    amr.WholeExtent[2] = 0; amr.WholeExtent[3] = ny;
+    amr.WholeExtent[4] = 0; amr.WholeExtent[5] = nz;
+    amr.Origin[0] = ox; amr.Origin[1] = oy; amr.Origin[2] = oz;
+    amr.Spacing[0] = sx; amr.Spacing[1] = sy; amr.Spacing[2] = sz;
+    for (int f = 0; f < nfields; ++f) {
+        Piro::CellData cd;
+        cd.type = types[f];
+        cd.Scalars = names[f];
+        const long long cnt = types[f] == 2 ? 3 * N : N;
+        cd.values.assign(values[f], values[f] + cnt);
+        if (types[f] == 2) ++nvec;
+        amr.CD.push_back(cd);
+    }
+    for (int k = 0; k < 3; ++k) amr.CD.push_back(Piro::CellData());
+    MP.setvalue(Piro::MeshParams::VECTORNUM, nvec);
+    MP.setvalue(Piro::MeshParams::AMR, std::vector<Piro::AMR>{amr, Piro::AMR()});
+    Piro::bc::prepbc();
+    Piro::paraview::writevth(timestep);
 }
 
 }  // extern "C"

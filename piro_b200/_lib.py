@@ -98,6 +98,9 @@ SIGNATURES = {
     "piro_pcnet_destroy": (i32, [vp]),
     "piro_be_set_preconditioner": (i32, [vp, i32, vp]),
     "piro_be_pc_stats": (i32, [vp, i32, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]),
+    "piro_write_paraview": (i32, [vp, C.c_char_p, i32]),
+    "piro_set_output": (i32, [vp, C.c_char_p]),
+    "piro_interior_gather": (i32, [i32, i32, i32, i32, vp, vp, vp]),
     "piro_laplacian_nnz_rows": (i32, [i32, i32, i32, i64, i64, pi64]),
     "piro_csr_laplacian_rows": (i32, [i32, i32, i32, i32, f32, i64, i64, i64, vp, vp, vp, vp]),
     "piro_csr_fe_step_rows": (i32, [i32, i32, i32, i64, i64, vp, vp, vp, f32, vp, i64, vp, vp]),

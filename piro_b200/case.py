@@ -70,6 +70,14 @@ class Case:
               "piro_op_export_csr")
         return rp, col, val
 
+    def write_paraview(self, root: str, timestep: int) -> None:
+        """Piro::paraview::writevth: <root>/<casename>/mesh/mesh_<ts>.vth and level/<ts>_level_0.vti."""
+        check(lib().piro_write_paraview(self.h, root.encode(), int(timestep)), "piro_write_paraview")
+
+    def set_output(self, root) -> None:
+        """Write ParaView files every Save steps under root (None: no output)."""
+        check(lib().piro_set_output(self.h, None if root is None else root.encode()), "piro_set_output")
+
     def close(self) -> None:
         if getattr(self, "h", None):
             lib().piro_close(self.h)

@@ -405,3 +405,33 @@ extern "C" int piro_face_lists(int nx, int ny, int nz, uint32_t *idx, piro_strea
     PIRO_CHECK_LAUNCH("k_faces");
     return PIRO_OK;
 }
+
+namespace piro {
+namespace {
+// dst[k*Ni + j] = src[k*N + cell(j)] for the interior cells j (x fastest) of
+// each of ncomp components.
+__global__ void k_interior_gather(int nx, int ny, int nz, int ncomp, const float *__restrict__ src,
+                                  float *__restrict__ dst)
+{
+    const int64_t ix = nx - 2, iy = ny - 2, iz = nz - 2;
+    const int64_t Ni = ix * iy * iz, N = (int64_t)nx * ny * nz;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < Ni * ncomp;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = t / Ni, j = t - k * Ni;
+        const int64_t z = j / (ix * iy), rem = j - z * ix * iy;
+        const int64_t y = rem / ix, x = rem - y * ix;
+        dst[t] = src[k * N + (x + 1) + (y + 1) * nx + (z + 1) * (int64_t)nx * ny];
+    }
+}
+}  // namespace
+}  // namespace piro
+
+extern "C" int piro_interior_gather(int nx, int ny, int nz, int ncomp, const float *src, float *dst,
+                                    piro_stream_t stream)
+{
+    PIRO_ARG(src && dst && grid_ok(nx, ny, nz) && ncomp >= 1, "piro_interior_gather: bad arguments");
+    const int64_t total = (int64_t)(nx - 2) * (ny - 2) * (nz - 2) * ncomp;
+    k_interior_gather<<<grid_for(total, 256, 4), 256, 0, as_stream(stream)>>>(nx, ny, nz, ncomp, src, dst);
+    PIRO_CHECK_LAUNCH("k_interior_gather");
+    return PIRO_OK;
+}

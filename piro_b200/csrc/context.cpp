@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <fstream>
 #include <map>
 #include <sstream>
@@ -162,6 +163,12 @@ struct piro_ctx {
     float *partD = nullptr, *partC = nullptr;
     piro_be_solver *be = nullptr;
     int64_t steps = 0;
+    // ParaView output (Piro::paraview, src/paraview.cpp): [File] casename and
+    // restart, [Mesh] o, s, levels, index; written when an output root is set
+    std::string casename = "case", out_root;
+    int restart = 0, levels = 1;
+    int origin[3] = {0, 0, 0}, spacing[3] = {1, 1, 1};
+    std::vector<int> index{1};
     cudaStream_t stream = nullptr;
     void *work = nullptr;
     size_t work_bytes = 0;
@@ -350,6 +357,19 @@ int open_case(piro_ctx *c, const std::string &case_name)
         PK(need_float(sol, "JLI", "URF", c->jli_urf));
         PK(need_int(sol, "JLI", "max_iter", c->jli_maxiter));
     }
+    // output settings: optional here (the reference throws on a missing key)
+    if (ini_get(I, "File", "casename", s)) c->casename = s;
+    if (ini_get(I, "File", "restart", s)) c->restart = std::atoi(s.c_str());
+    if (ini_get(I, "Mesh", "o", s)) {
+        const std::vector<float> o = parse_list<float>(s);
+        for (int k = 0; k < 3 && k < (int)o.size(); ++k) c->origin[k] = (int)o[k];  // AMR::Origin is int
+    }
+    if (ini_get(I, "Mesh", "s", s)) {
+        const std::vector<float> o = parse_list<float>(s);
+        for (int k = 0; k < 3 && k < (int)o.size(); ++k) c->spacing[k] = (int)o[k];
+    }
+    if (ini_get(I, "Mesh", "levels", s)) c->levels = std::atoi(s.c_str());
+    if (ini_get(I, "Mesh", "index", s)) c->index = parse_list<int>(s);
     PK(need_float(I, "Solve", "Timestep", c->timestep));
     PK(need_float(I, "Solve", "TotalTime", c->totaltime));
     PK(need_int(I, "Solve", "Save", c->save));
@@ -783,9 +803,133 @@ extern "C" int piro_assign(piro_ctx *c, piro_buf lhs, piro_op rhs, piro_buf *out
     return PIRO_OK;
 }
 
+// ---- ParaView output: Piro::paraview::writevth / writevti (src/paraview.cpp:12-137)
+static std::string fmt_g(float v)
+{
+    char b[48];
+    std::snprintf(b, sizeof b, "%g", (double)v);  // std::ostream << float (precision 6)
+    return b;
+}
+
+static void append_values(std::string &out, const float *v, int64_t n)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        if (i) out += ' ';
+        out += fmt_g(v[i]);
+    }
+}
+
+// The .vti of one level: cell data of the scalar and vector fields with the
+// boundary cells removed (bc::prepbc's list), gathered on the device.
+static int vti_text(piro_ctx *c, std::string &out)
+{
+    const int nx = c->nx, ny = c->ny, nz = c->nz;
+    const int64_t Ni = (int64_t)(nx - 2) * (ny - 2) * (nz - 2);
+    auto ext = [&]() {
+        return "0 " + std::to_string(nx - 2) + " 0 " + std::to_string(ny - 2) + " 0 " + std::to_string(nz - 2);
+    };
+    out = "<VTKFile type=\"ImageData\" version=\"1.0\" byte_order=\"LittleEndian\">\n";
+    out += "<ImageData WholeExtent=\"" + ext() + "\" Origin=\"" + std::to_string(c->origin[0]) + " " +
+           std::to_string(c->origin[1]) + " " + std::to_string(c->origin[2]) + "\" Spacing=\"" +
+           std::to_string(c->spacing[0]) + " " + std::to_string(c->spacing[1]) + " " + std::to_string(c->spacing[2]) +
+           "\">\n";
+    out += "<Piece Extent=\"" + ext() + "\">\n";
+    out += "<PointData Scalars=\"ScalarValues\">\n</PointData>\n<CellData>\n";
+    float *d = nullptr;
+    CK(cudaMalloc(&d, sizeof(float) * (size_t)(3 * Ni)));
+    std::vector<float> h((size_t)(3 * Ni));
+    int rc = PIRO_OK;
+    for (const Field &f : c->fields) {
+        if (f.kind == 0 || (f.kind == 2 && c->nvector <= 0)) continue;
+        const int ncomp = f.kind == 2 ? 3 : 1;
+        rc = piro_interior_gather(nx, ny, nz, ncomp, f.d, d, c->stream);
+        if (rc) break;
+        if (cudaMemcpyAsync(h.data(), d, sizeof(float) * (size_t)(ncomp * Ni), cudaMemcpyDeviceToHost, c->stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(c->stream) != cudaSuccess) {
+            rc = fail(PIRO_ERR_CUDA, "paraview: device read failed");
+            break;
+        }
+        static const char *suffix[3] = {"_x", "_y", "_z"};
+        for (int k = 0; k < ncomp; ++k) {
+            out += "<DataArray type=\"Float64\" Name=\"" + f.name + (ncomp == 3 ? suffix[k] : "") +
+                   "\" format=\"ascii\">\n";
+            append_values(out, h.data() + k * Ni, Ni);
+            out += "</DataArray>\n";
+        }
+    }
+    cudaFree(d);
+    if (rc) return rc;
+    out += "</CellData>\n</Piece>\n</ImageData>\n</VTKFile>\n";
+    return PIRO_OK;
+}
+
+static int write_text(const std::string &path, const std::string &text)
+{
+    std::ofstream f(path);
+    if (!f.is_open()) return fail(PIRO_ERR_CONFIG, "paraview: cannot write %s", path);
+    f << text << std::endl;  // file_utilities::writefile appends a newline
+    return f.good() ? PIRO_OK : fail(PIRO_ERR_CONFIG, "paraview: write failed for %s", path);
+}
+
+extern "C" int piro_write_paraview(piro_ctx *c, const char *root, int timestep)
+{
+    if (!c || !root || timestep < 0) {
+        piro::set_error("piro_write_paraview: bad arguments");
+        return PIRO_ERR_ARG;
+    }
+    for (int i = 0; i < c->levels; ++i)
+        if (i >= (int)c->index.size() || c->index[i] != 1)
+            return fail(PIRO_ERR_CONFIG, "paraview: [Mesh] index must be 1 per level (the reference writes "
+                                         "only level data set 0)");
+    const std::string base = std::string(root) + "/" + c->casename + "/mesh";
+    std::error_code ec;
+    std::filesystem::create_directories(base + "/level", ec);
+    if (ec) return fail(PIRO_ERR_CONFIG, "paraview: cannot create %s/level", base);
+    std::string ts = std::to_string(timestep);
+    if (ts.size() < 5) ts = std::string(5 - ts.size(), '0') + ts;
+    std::string vth = "<?xml version=\"1.0\"?>\n";
+    vth += "<VTKFile type=\"vtkOverlappingAMR\" version=\"1.1\" byte_order=\"LittleEndian\" "
+           "header_type=\"UInt32\">\n";
+    vth += "<vtkOverlappingAMR origin=\"0 0 0\" grid_description=\"XYZ\">\n";
+    std::string vti;
+    PK(vti_text(c, vti));
+    for (int i = 0; i < c->levels; ++i) {
+        for (int j = 0; j < c->index[i]; ++j) {
+            vth += "<Block level=\"" + std::to_string(i) + "\" spacing=\"1 1 1\">\n";
+            vth += "<DataSet index=\"0\" amr_box=\"0 " + std::to_string(c->nx - 2) + " 0 " +
+                   std::to_string(c->ny - 2) + " 0 " + std::to_string(c->nz - 2) + "\" file=\"level/" + ts +
+                   "_level_" + std::to_string(j) + ".vti\">\n</DataSet>\n";
+            PK(write_text(base + "/level/" + ts + "_level_" + std::to_string(j) + ".vti", vti));
+        }
+        vth += "</Block>\n";
+    }
+    vth += "</vtkOverlappingAMR>\n</VTKFile>\n";
+    return write_text(base + "/mesh_" + ts + ".vth", vth);
+}
+
+extern "C" int piro_set_output(piro_ctx *c, const char *root)
+{
+    if (!c) {
+        piro::set_error("piro_set_output: null context");
+        return PIRO_ERR_ARG;
+    }
+    if (!root) {
+        c->out_root.clear();
+        return PIRO_OK;
+    }
+    c->out_root = root;
+    // Piro::init (src/init.cpp:10-21): a restart clears the case directory
+    const std::string dir = c->out_root + "/" + c->casename;
+    std::error_code ec;
+    if (c->restart) std::filesystem::remove_all(dir, ec);
+    std::filesystem::create_directories(dir + "/mesh/level", ec);
+    if (ec) return fail(PIRO_ERR_CONFIG, "piro_set_output: cannot create %s/mesh/level", dir);
+    return PIRO_OK;
+}
+
 extern "C" int piro_step_solve(piro_ctx *c, piro_buf eqn, float time)
 {
-    (void)time;
     if (!c || eqn.id != PIRO_EQN_RESULT || c->fields.size() < 2) {
         piro::set_error("piro_step_solve: needs the result of piro_assign and at least two fields");
         return PIRO_ERR_ARG;
@@ -796,6 +940,11 @@ extern "C" int piro_step_solve(piro_ctx *c, piro_buf eqn, float time)
     if (c->q > 0) PK(piro_set_bc(c->q, c->bc_idx, c->memD, c->fields[1].d, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     ++c->steps;
+    // post-processing every Save steps (process.cpp:236-247), when an output root is set
+    if (!c->out_root.empty() && c->save > 0) {
+        const int ts = (int)(time / c->timestep);
+        if ((ts + 1) % c->save == 0) PK(piro_write_paraview(c, c->out_root.c_str(), ts));
+    }
     return PIRO_OK;
 }
 
