@@ -46,6 +46,7 @@ extern "C" {
 #define PIRO_ERR_SCHEME 9       /* TIMESCHEME / SOLVERSCHEME / space scheme unsupported */
 #define PIRO_ERR_NOMEM 10       /* device allocation failed                      */
 #define PIRO_ERR_STATE 11       /* call out of order (e.g. operator not built)  */
+#define PIRO_ERR_ZERO_PIVOT 12  /* elimination without pivoting met a zero pivot */
 
 typedef void *piro_stream_t; /* a cudaStream_t */
 
@@ -151,6 +152,31 @@ int piro_coo_fe_step(int64_t N, int64_t nnz, const int32_t *rows, const int32_t 
  * (kernelsolve::HT::TIMESCHEME_11, src/kernelprocess.cpp:68-91). */
 int piro_ht_spmv(int nx, int ny, int nz, const int64_t *keys, const float *vals, int64_t ts, float dt, int fe,
                  const float *u, float *out, piro_stream_t stream);
+
+/* Scheme 27 (TIMESCHEME 12 + solver 27) on a table built by piro_ht_build
+ * (int64 keys, -1 empty; -2 marks a deleted key).  piro_ht_lu_reference is
+ * PIRO's factorization (src/matrixoperations.cpp:10-104, lu_decompHT.cl) in
+ * place, resident on the device: per pivot row the fill-in (explicit zeros
+ * inserted in the reference's order) and the elimination round, with entries
+ * below 1e-6 deleted -- the multipliers included, so no solve follows, as in
+ * the reference.  Each round's items read the pre-round factor.  Returns
+ * PIRO_ERR_TABLE_FULL when the fill-in does not fit.  N <= 46340 (int32 keys
+ * in the reference).
+ * piro_ht_lu_factor is the same elimination kept exact (zero tests against 0,
+ * nothing deleted) with the multiplier stored in place of a(r, ro): an in-place
+ * LU, L unit lower, for a matrix of bandwidth bw (nx*ny for the 7-point grid;
+ * N if unknown).  It first inserts the whole band as explicit zeros, so the
+ * table must hold the band: piro_ht_lu_table_size gives the band's entry count
+ * and a prime table size for load factor lf.  PIRO_ERR_ARG when a stored entry
+ * lies outside the band; PIRO_ERR_ZERO_PIVOT when a pivot is exactly zero (no
+ * pivoting, as in the reference).  piro_ht_lu_solve then solves L U x = b (b, x device
+ * float[N]) by forward and backward substitution: scheme 27 with a solution,
+ * which the reference does not compute. */
+int piro_ht_lu_reference(int64_t N, int64_t *keys, float *vals, int64_t ts, piro_stream_t stream);
+int piro_ht_lu_table_size(int64_t N, int64_t bw, float lf, int64_t *entries, int64_t *ts);
+int piro_ht_lu_factor(int64_t N, int64_t bw, int64_t *keys, float *vals, int64_t ts, piro_stream_t stream);
+int piro_ht_lu_solve(int64_t N, int64_t bw, const int64_t *keys, const float *vals, int64_t ts, const float *b,
+                     float *x, piro_stream_t stream);
 
 /* Matrix-free 7-point step, the comparison point for CSR (laplacianscalar.cl:1-21
  * extended by alpha and the Euler update): interior cells
@@ -483,6 +509,14 @@ int piro_ctx_query(piro_ctx *ctx, piro_case_info *info);
  * reference's csrscale actually behaves (src/kernelcsrgeam.cpp:224-231).
  * Must be set before the Laplacian is assembled. */
 int piro_set_alpha_mode(piro_ctx *ctx, int mode);
+/* Scheme 27 (TIMESCHEME 12, solver 27, Data 2).  0 (default): backward Euler
+ * solved directly -- A = I - dt*M in a hash table that holds its band
+ * (bandwidth nx*ny), factorized in place on the first step
+ * (piro_ht_lu_factor), then substitution every step.  1: as the reference
+ * runs -- PIRO's factorization of the operator's own table on the first step
+ * (piro_ht_lu_reference) and a zero result field
+ * (src/operatoroverload.cpp:65-81).  Must be set before the first step. */
+int piro_set_lu_mode(piro_ctx *ctx, int mode);
 
 /* process::ddt_r / process::vector / matchscalartovar (src/process.cpp:20-58,
  * 154-166): the handle of the named field (field 0 when no name matches, as

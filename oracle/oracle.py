@@ -526,6 +526,12 @@ class Ref:
                                        np.float32(dt), N)
         return Cc
 
+    def ht_lu(self, N, keys32, vals, TS):
+        """Scheme 27's factorization of the table (matrixoperations.cpp:37-99), in place."""
+        self.lib.ref_ht_lu.restype = None
+        self.lib.ref_ht_lu.argtypes = [C.c_int, _i32p, _f32p, C.c_int]
+        self.lib.ref_ht_lu(N, keys32, vals, TS)
+
     def lu_round(self, keys32, vals, N, rowouter, TS):
         limit = (N - rowouter - 1) * (N - rowouter)
         self.lib.refcl_lu_round(keys32, vals, N, rowouter, TS, limit)

@@ -16,6 +16,8 @@
 #include <postprocess.hpp>
 #include <stencils.hpp>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -217,6 +219,40 @@ void ref_paraview(int nx, int ny, int nz, int ox, int oy, int oz, int sx, int sy
     MP.setvalue(Piro::MeshParams::AMR, std::vector<Piro::AMR>{amr, Piro::AMR()});
     Piro::bc::prepbc();
     Piro::paraview::writevth(timestep);
+}
+
+void refcl_lu_round(int *keys, float *vals, int N, int rowouter, int TS, int limit);
+
+// Scheme 27's factorization (src/matrixoperations.cpp:37-99): per pivot row,
+// the reference's host fill-in with methods::lookup / lookupandset on the
+// table, then one lu_decompHT.cl round (refcl_lu_round, ids descending).  The
+// reference's OpenCL upload/download around each round is an identity here.
+// The table gets one spare slot before it: an item whose own key is absent
+// writes slot -1 in the reference (lu_decompHT.cl:61-64), here that spare.
+void ref_ht_lu(int N, int *keys, float *vals, int TS)
+{
+    std::vector<int> K(TS + 1, -1);
+    std::vector<float> V(TS + 1, 0.0f);
+    std::memcpy(K.data() + 1, keys, sizeof(int) * TS);
+    std::memcpy(V.data() + 1, vals, sizeof(float) * TS);
+    std::vector<int> k(K.begin() + 1, K.end());
+    std::vector<float> v(V.begin() + 1, V.end());
+    for (int ro = 0; ro < N - 1; ++ro) {
+        std::vector<int> cols;
+        for (int co = ro; co < N; co++)
+            if (std::abs(Piro::methods::lookup(ro, co, N, k, v, TS)) > 1E-6) cols.push_back(co);
+        for (int r = ro + 1; r < N; ++r) {
+            if (Piro::methods::lookup(r, ro, N, k, v, TS) == 0.0) continue;
+            for (int col : cols) Piro::methods::lookupandset(r, col, N, 0.0f, k, v, TS);
+        }
+        std::copy(k.begin(), k.end(), K.begin() + 1);
+        std::copy(v.begin(), v.end(), V.begin() + 1);
+        refcl_lu_round(K.data() + 1, V.data() + 1, N, ro, TS, (N - ro - 1) * (N - ro));
+        std::copy(K.begin() + 1, K.end(), k.begin());
+        std::copy(V.begin() + 1, V.end(), v.begin());
+    }
+    std::memcpy(keys, k.data(), sizeof(int) * TS);
+    std::memcpy(vals, v.data(), sizeof(float) * TS);
 }
 
 }  // extern "C"

@@ -61,6 +61,10 @@ SIGNATURES = {
     "piro_coo_spmv": (i32, [i64, i64, vp, vp, vp, f32, vp, vp, vp]),
     "piro_coo_fe_step": (i32, [i64, i64, vp, vp, vp, f32, vp, vp, vp]),
     "piro_ht_spmv": (i32, [i32, i32, i32, vp, vp, i64, f32, i32, vp, vp, vp]),
+    "piro_ht_lu_reference": (i32, [i64, vp, vp, i64, vp]),
+    "piro_ht_lu_table_size": (i32, [i64, i64, f32, pi64, pi64]),
+    "piro_ht_lu_factor": (i32, [i64, i64, vp, vp, i64, vp]),
+    "piro_ht_lu_solve": (i32, [i64, i64, vp, vp, i64, vp, vp, vp]),
     "piro_stencil_fe_step": (i32, [i32, i32, i32, f32, f32, f32, f32, vp, vp, vp, vp]),
     "piro_set_bc": (i32, [i64, vp, vp, vp, vp]),
     "piro_face_count": (i32, [i32, i32, i32, pi64, pi64]),
@@ -122,6 +126,7 @@ SIGNATURES = {
     "piro_close": (None, [vp]),
     "piro_ctx_query": (i32, [vp, C.POINTER(CaseInfo)]),
     "piro_set_alpha_mode": (i32, [vp, i32]),
+    "piro_set_lu_mode": (i32, [vp, i32]),
     "piro_ddt_r": (i32, [vp, C.c_char_p, C.POINTER(Buf)]),
     "piro_vector": (i32, [vp, C.c_char_p, C.POINTER(Buf)]),
     "piro_field": (i32, [vp, C.c_char_p, C.POINTER(Buf)]),

@@ -21,12 +21,14 @@ from ._lib import Buf, CaseInfo, Op, check, lib
 class Case:
     """One PIRO run (piro_ctx): a case .ini and its assets directory."""
 
-    def __init__(self, assets_dir: str, case_name: str, alpha_mode: int = 0):
+    def __init__(self, assets_dir: str, case_name: str, alpha_mode: int = 0, lu_mode: int = 0):
         h = C.c_void_p()
         check(lib().piro_open(assets_dir.encode(), case_name.encode(), C.byref(h)), "piro_open")
         self.h = h
         if alpha_mode:
             check(lib().piro_set_alpha_mode(self.h, alpha_mode), "piro_set_alpha_mode")
+        if lu_mode:
+            check(lib().piro_set_lu_mode(self.h, lu_mode), "piro_set_lu_mode")
 
     @property
     def info(self) -> CaseInfo:

@@ -145,6 +145,7 @@ struct piro_ctx {
     int jli_maxiter = 0;
     float ht_a = 0, ht_b = 0, ht_c = 0, ht_lf = 0.7f;
     int alpha_mode = 0;  // 0 intended (SpMDSM row scale), 1 as the reference runs (alpha dropped)
+    int lu_mode = 0;     // scheme 27: 0 solve by the banded LU, 1 as the reference runs (factor only, zero field)
     std::vector<Field> fields;
     int nconst = 0, nscalar = 0, nvector = 0;
     // boundary
@@ -158,6 +159,11 @@ struct piro_ctx {
     int64_t *ht_keys = nullptr;
     float *ht_vals = nullptr;
     int64_t ht_ts = 0;
+    // scheme 27: factorized once (INIT::RHS_INIT, operatoroverload.cpp:68-81)
+    bool lu_done = false;
+    int64_t *lu_keys = nullptr;
+    float *lu_vals = nullptr;
+    int64_t lu_ts = 0, lu_bw = 0;
     int lap_coeff = -1;
     // equation result (partD) and scratch (partC)
     float *partD = nullptr, *partC = nullptr;
@@ -511,6 +517,8 @@ extern "C" void piro_close(piro_ctx *c)
     cudaFree(c->coo_rows);
     cudaFree(c->ht_keys);
     cudaFree(c->ht_vals);
+    cudaFree(c->lu_keys);
+    cudaFree(c->lu_vals);
     cudaFree(c->bc_idx);
     cudaFree(c->memD);
     cudaFree(c->partD);
@@ -555,6 +563,20 @@ extern "C" int piro_set_alpha_mode(piro_ctx *c, int mode)
         return PIRO_ERR_STATE;
     }
     c->alpha_mode = mode;
+    return PIRO_OK;
+}
+
+extern "C" int piro_set_lu_mode(piro_ctx *c, int mode)
+{
+    if (!c || mode < 0 || mode > 1) {
+        piro::set_error("piro_set_lu_mode: mode must be 0 (solve) or 1 (as run by the reference)");
+        return PIRO_ERR_ARG;
+    }
+    if (c->lu_done) {
+        piro::set_error("piro_set_lu_mode: the LU is already factorized");
+        return PIRO_ERR_STATE;
+    }
+    c->lu_mode = mode;
     return PIRO_OK;
 }
 
@@ -756,6 +778,57 @@ static int be_pcg(piro_ctx *c, const Csr *M, const float *b, float *x)
     return piro_be_solve(c->be, b, x, 1e-8, 20, 20000, &info);
 }
 
+// Scheme 27 on the hash-table operator M (TIMESCHEME 12, solver 27, Data 2).
+// Mode 1: PIRO's factorization of M's own table on the first step
+// (matrix_operations::HT::lu_decomposition), the result field zero, as the
+// reference returns it.  Mode 0: A = I - dt*M in a table that holds its band
+// (bandwidth nx*ny), factorized in place on the first step; every step then
+// solves A x = u by substitution.
+static int lu_step(piro_ctx *c, const float *u, float *x)
+{
+    const int64_t N = c->N;
+    if (c->lu_mode == 1) {
+        if (!c->lu_done) PK(piro_ht_lu_reference(N, c->ht_keys, c->ht_vals, c->ht_ts, c->stream));
+        c->lu_done = true;
+        return PIRO_OK;
+    }
+    if (!c->lu_done) {
+        Csr I, A;
+        PK(alloc_csr(I, N, N));
+        PK(piro_csr_identity(N, I.rp, I.col, I.val, c->stream));
+        size_t wb = 0;
+        PK(piro_scan_workspace(N, &wb));
+        PK(ensure_work(c, wb));
+        CK(cudaMalloc(&A.rp, sizeof(int32_t) * (size_t)(N + 1)));
+        PK(piro_csrgeam2_count(N, I.rp, I.col, c->lap.rp, c->lap.col, A.rp, c->work, c->work_bytes, c->stream));
+        int32_t nnz = 0;
+        CK(cudaMemcpyAsync(&nnz, A.rp + N, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        CK(cudaMalloc(&A.col, sizeof(int32_t) * (size_t)nnz));
+        CK(cudaMalloc(&A.val, sizeof(float) * (size_t)nnz));
+        A.nnz = nnz;
+        PK(piro_csrgeam2_fill(N, I.rp, I.col, I.val, -c->timestep, c->lap.rp, c->lap.col, c->lap.val, A.rp, A.col,
+                              A.val, c->stream));
+        free_csr(I);
+        c->lu_bw = (int64_t)c->nx * c->ny;
+        int64_t entries = 0;
+        int rc = piro_ht_lu_table_size(N, c->lu_bw, c->ht_lf, &entries, &c->lu_ts);
+        if (rc == PIRO_OK) rc = piro_ht_build_workspace(c->lu_ts, &wb);
+        if (rc == PIRO_OK) rc = ensure_work(c, wb);
+        if (rc == PIRO_OK && (cudaMalloc(&c->lu_keys, sizeof(int64_t) * (size_t)c->lu_ts) != cudaSuccess ||
+                              cudaMalloc(&c->lu_vals, sizeof(float) * (size_t)c->lu_ts) != cudaSuccess))
+            rc = fail(PIRO_ERR_CUDA, "scheme 27: no device memory for a %s-slot band table", std::to_string(c->lu_ts));
+        if (rc == PIRO_OK)
+            rc = piro_ht_build(N, A.rp, A.col, A.val, nnz, c->lu_ts, c->lu_keys, c->lu_vals, c->work, c->work_bytes,
+                               c->stream);
+        free_csr(A);
+        if (rc) return rc;
+        PK(piro_ht_lu_factor(N, c->lu_bw, c->lu_keys, c->lu_vals, c->lu_ts, c->stream));
+        c->lu_done = true;
+    }
+    return piro_ht_lu_solve(N, c->lu_bw, c->lu_keys, c->lu_vals, c->lu_ts, u, x, c->stream);
+}
+
 extern "C" int piro_assign(piro_ctx *c, piro_buf lhs, piro_op rhs, piro_buf *out)
 {
     if (!c || !out || lhs.id < 0 || lhs.id >= (int)c->fields.size()) {
@@ -781,6 +854,11 @@ extern "C" int piro_assign(piro_ctx *c, piro_buf lhs, piro_op rhs, piro_buf *out
         } else {
             return fail(PIRO_ERR_DATATYPE, "piro_assign: Data not supported on this path");
         }
+    } else if (c->timescheme == 12 && c->solverscheme == 27) {
+        if (c->datatype != 2) return fail(PIRO_ERR_DATATYPE, "piro_assign: solver 27 needs Data = 2 (hash table)");
+        if (!c->ht_keys || rhs.kind != PIRO_OP_LAPLACIAN)
+            return fail(PIRO_ERR_STATE, "piro_assign: hash table not built");
+        PK(lu_step(c, u, c->partD));
     } else if (c->timescheme == 12) {
         const Csr *M = op_csr(c, rhs);
         if (c->datatype != 0 || !M) return fail(PIRO_ERR_DATATYPE, "piro_assign: backward Euler needs a CSR operator");
@@ -791,7 +869,7 @@ extern "C" int piro_assign(piro_ctx *c, piro_buf lhs, piro_op rhs, piro_buf *out
         } else if (c->solverscheme == 39) {
             PK(be_pcg(c, M, u, c->partD));
         } else {
-            piro::set_error("piro_assign: Solver %d not available for TIMESCHEME 12 (40 JLI, 39 PCG)", c->solverscheme);
+            piro::set_error("piro_assign: Solver %d not available for TIMESCHEME 12 (40 JLI, 39 PCG, 27 LU)", c->solverscheme);
             return PIRO_ERR_SCHEME;
         }
     } else {

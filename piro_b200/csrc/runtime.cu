@@ -50,6 +50,7 @@ extern "C" const char *piro_status_string(int status)
     case PIRO_ERR_SCHEME: return "PIRO_ERR_SCHEME";
     case PIRO_ERR_NOMEM: return "PIRO_ERR_NOMEM";
     case PIRO_ERR_STATE: return "PIRO_ERR_STATE";
+    case PIRO_ERR_ZERO_PIVOT: return "PIRO_ERR_ZERO_PIVOT";
     default: return "PIRO_ERR_UNKNOWN";
     }
 }

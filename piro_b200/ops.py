@@ -121,6 +121,30 @@ def ht_build(N, rowptr, col, val, ts):
     return keys, vals
 
 
+def ht_lu_reference(N, keys, vals, ts):
+    """Scheme 27's factorization of the table, in place (PIRO's algorithm)."""
+    check(lib().piro_ht_lu_reference(N, _p(keys), _p(vals), ts, _stream()), "piro_ht_lu_reference")
+
+
+def ht_lu_table_size(N, bw, lf=0.7):
+    """(band entries, table size) for piro_ht_lu_factor at bandwidth bw."""
+    n, ts = C.c_int64(), C.c_int64()
+    check(lib().piro_ht_lu_table_size(N, bw, lf, C.byref(n), C.byref(ts)), "piro_ht_lu_table_size")
+    return n.value, ts.value
+
+
+def ht_lu_factor(N, bw, keys, vals, ts):
+    """In-place LU of the table (multipliers kept) within bandwidth bw."""
+    check(lib().piro_ht_lu_factor(N, bw, _p(keys), _p(vals), ts, _stream()), "piro_ht_lu_factor")
+
+
+def ht_lu_solve(N, bw, keys, vals, ts, b, x=None):
+    if x is None:
+        x = torch.empty_like(b)
+    check(lib().piro_ht_lu_solve(N, bw, _p(keys), _p(vals), ts, _p(b), _p(x), _stream()), "piro_ht_lu_solve")
+    return x
+
+
 # ----------------------------------------------------------------- steps
 def csr_fe_step(nx, ny, nz, A, dt, u, out):
     check(lib().piro_csr_fe_step(nx, ny, nz, _p(A[0]), _p(A[1]), _p(A[2]), float(dt), _p(u), _p(out), _stream()),

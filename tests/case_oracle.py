@@ -40,7 +40,7 @@ def floats(s):
     return out
 
 
-def run_case(assets, case_name, alpha_mode=0):
+def run_case(assets, case_name, alpha_mode=0, lu_mode=0):
     cfg = read_ini(os.path.join(assets, case_name))
     dist = read_ini(os.path.join(assets, "IC", "distribution.ini"))
     n = [int(v) for v in cfg["Mesh"]["n"].split(" ")]
@@ -110,6 +110,7 @@ def run_case(assets, case_name, alpha_mode=0):
             if data == 0 and alpha_mode == 0:
                 val = O.csr_rowscale(N, rp, val, dev[match("Alpha")])
             op = ("csr", (rp, col, val))
+            csr = (rp, col, val)
             if data == 2:
                 tsz = O.ht_table_size_reference(len(val), N)
                 keys, vals = O.ht_build(N, rp, col, val, tsz)
@@ -128,6 +129,17 @@ def run_case(assets, case_name, alpha_mode=0):
                 part = u + O.spmv_coo(N, op[1], dt, u)
             else:
                 part = u + O.spmv_ht(N, op[1][0], op[1][1], dt, u)
+        elif solver == 27:
+            # lu_mode 1: the reference factorizes and returns a zero field
+            # (operatoroverload.cpp:65-81); 0: FP64 solve of (I - dt*M) x = u
+            part = np.zeros(N, np.float32)
+            if lu_mode == 0:
+                import scipy.sparse as sp
+                import scipy.sparse.linalg as spl
+                I = (np.arange(N + 1, dtype=np.int32), np.arange(N, dtype=np.int32), np.ones(N, np.float32))
+                arp, acol, aval = O.csrgeam2(N, I, np.float32(-dt), csr)
+                A = sp.csr_matrix((aval.astype(np.float64), acol, arp), shape=(N, N))
+                part = spl.spsolve(A.tocsc(), u.astype(np.float64)).astype(np.float32)
         elif solver == 40:
             part, _ = O.be_jli(nx, ny, nz, op[1], dt, u)
         else:  # 39: FP64 solve of (I - dt*M) x = u on the interior

@@ -20,6 +20,7 @@ CASES = [
     ("adv_fe.ini", None),          # advection: vector & gradient (csrgeam), upwind
     ("heat_be_jli.ini", 1e-6),     # BE, the reference's JLI iteration (FP64 residual sums)
     ("heat_be_pcg.ini", 1e-6),     # BE, FP32 PCG in FP64 refinement vs an FP64 solve
+    ("heat_be_lu.ini", 1e-5),      # BE, scheme 27: FP32 banded LU in the hash table vs an FP64 solve
 ]
 
 
@@ -37,6 +38,19 @@ def test_case_solve_matches_oracle(cuda, oracle, name, tol):
         assert f32_bits_equal(got, want), np.abs(got - want).max()
     else:
         np.testing.assert_allclose(got, want, rtol=tol, atol=tol * np.abs(want).max())
+    c.close()
+
+
+def test_scheme27_as_the_reference_runs(cuda, oracle):
+    """lu_mode 1: PIRO's factorization on the first step, a zero result field
+    with the boundary values put back (the 5^3 case of Test/LUDecomp.ini)."""
+    from case_oracle import run_case
+    from piro_b200.case import Case
+    ref = run_case(ASSETS, "heat_lu_ref.ini", lu_mode=1)
+    c = Case(ASSETS, "heat_lu_ref.ini", lu_mode=1)
+    assert c.solve() == ref["steps"] == 3
+    assert f32_bits_equal(c.get("T"), ref["fields"][1])
+    assert c.get("T").max() == 1.0
     c.close()
 
 
