@@ -162,21 +162,23 @@ int piro_ht_spmv(int nx, int ny, int nz, const int64_t *keys, const float *vals,
  * the reference.  Each round's items read the pre-round factor.  Returns
  * PIRO_ERR_TABLE_FULL when the fill-in does not fit.  N <= 46340 (int32 keys
  * in the reference).
- * piro_ht_lu_factor is the same elimination kept exact (zero tests against 0,
- * nothing deleted) with the multiplier stored in place of a(r, ro): an in-place
- * LU, L unit lower, for a matrix of bandwidth bw (nx*ny for the 7-point grid;
- * N if unknown).  It first inserts the whole band as explicit zeros, so the
- * table must hold the band: piro_ht_lu_table_size gives the band's entry count
- * and a prime table size for load factor lf.  PIRO_ERR_ARG when a stored entry
- * lies outside the band; PIRO_ERR_ZERO_PIVOT when a pivot is exactly zero (no
- * pivoting, as in the reference).  piro_ht_lu_solve then solves L U x = b (b, x device
- * float[N]) by forward and backward substitution: scheme 27 with a solution,
- * which the reference does not compute. */
+ * piro_ht_lu_factor / piro_ht_lu_solve give scheme 27 a solution, which the
+ * reference does not compute.  The factor reads the table once and writes
+ * shift*I + scale*M (M the table's matrix) into a dense band of bandwidth bw
+ * (nx*ny for the 7-point grid; row r, column c at band[r*(2bw+1) + c-r+bw]),
+ * then factorizes it in place without pivoting: U on and above the diagonal,
+ * the unit-lower L's multipliers below.  band is a device buffer of
+ * piro_ht_lu_band_bytes bytes (the band, then the solve's scratch).
+ * PIRO_ERR_ARG when a table entry lies outside the band; PIRO_ERR_ZERO_PIVOT
+ * when a pivot is exactly zero.  piro_ht_lu_solve solves L U x = b (b, x
+ * device float[N], distinct) by forward and backward substitution, one
+ * cooperative launch, and synchronizes the stream. */
 int piro_ht_lu_reference(int64_t N, int64_t *keys, float *vals, int64_t ts, piro_stream_t stream);
-int piro_ht_lu_table_size(int64_t N, int64_t bw, float lf, int64_t *entries, int64_t *ts);
-int piro_ht_lu_factor(int64_t N, int64_t bw, int64_t *keys, float *vals, int64_t ts, piro_stream_t stream);
-int piro_ht_lu_solve(int64_t N, int64_t bw, const int64_t *keys, const float *vals, int64_t ts, const float *b,
-                     float *x, piro_stream_t stream);
+int piro_ht_lu_band_bytes(int64_t N, int64_t bw, size_t *bytes);
+int piro_ht_lu_factor(int64_t N, int64_t bw, const int64_t *keys, const float *vals, int64_t ts, float shift,
+                      float scale, void *band, size_t band_bytes, piro_stream_t stream);
+int piro_ht_lu_solve(int64_t N, int64_t bw, void *band, size_t band_bytes, const float *b, float *x,
+                     piro_stream_t stream);
 
 /* Matrix-free 7-point step, the comparison point for CSR (laplacianscalar.cl:1-21
  * extended by alpha and the Euler update): interior cells
@@ -510,9 +512,9 @@ int piro_ctx_query(piro_ctx *ctx, piro_case_info *info);
  * Must be set before the Laplacian is assembled. */
 int piro_set_alpha_mode(piro_ctx *ctx, int mode);
 /* Scheme 27 (TIMESCHEME 12, solver 27, Data 2).  0 (default): backward Euler
- * solved directly -- A = I - dt*M in a hash table that holds its band
- * (bandwidth nx*ny), factorized in place on the first step
- * (piro_ht_lu_factor), then substitution every step.  1: as the reference
+ * solved directly -- A = I - dt*M (M the operator's table) factorized in a
+ * dense band of bandwidth nx*ny on the first step (piro_ht_lu_factor), then
+ * substitution every step (piro_ht_lu_solve).  1: as the reference
  * runs -- PIRO's factorization of the operator's own table on the first step
  * (piro_ht_lu_reference) and a zero result field
  * (src/operatoroverload.cpp:65-81).  Must be set before the first step. */

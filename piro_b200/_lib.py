@@ -62,9 +62,9 @@ SIGNATURES = {
     "piro_coo_fe_step": (i32, [i64, i64, vp, vp, vp, f32, vp, vp, vp]),
     "piro_ht_spmv": (i32, [i32, i32, i32, vp, vp, i64, f32, i32, vp, vp, vp]),
     "piro_ht_lu_reference": (i32, [i64, vp, vp, i64, vp]),
-    "piro_ht_lu_table_size": (i32, [i64, i64, f32, pi64, pi64]),
-    "piro_ht_lu_factor": (i32, [i64, i64, vp, vp, i64, vp]),
-    "piro_ht_lu_solve": (i32, [i64, i64, vp, vp, i64, vp, vp, vp]),
+    "piro_ht_lu_band_bytes": (i32, [i64, i64, C.POINTER(sz)]),
+    "piro_ht_lu_factor": (i32, [i64, i64, vp, vp, i64, f32, f32, vp, sz, vp]),
+    "piro_ht_lu_solve": (i32, [i64, i64, vp, sz, vp, vp, vp]),
     "piro_stencil_fe_step": (i32, [i32, i32, i32, f32, f32, f32, f32, vp, vp, vp, vp]),
     "piro_set_bc": (i32, [i64, vp, vp, vp, vp]),
     "piro_face_count": (i32, [i32, i32, i32, pi64, pi64]),

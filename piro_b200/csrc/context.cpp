@@ -161,9 +161,9 @@ struct piro_ctx {
     int64_t ht_ts = 0;
     // scheme 27: factorized once (INIT::RHS_INIT, operatoroverload.cpp:68-81)
     bool lu_done = false;
-    int64_t *lu_keys = nullptr;
-    float *lu_vals = nullptr;
-    int64_t lu_ts = 0, lu_bw = 0;
+    void *lu_band = nullptr;
+    size_t lu_band_bytes = 0;
+    int64_t lu_bw = 0;
     int lap_coeff = -1;
     // equation result (partD) and scratch (partC)
     float *partD = nullptr, *partC = nullptr;
@@ -517,8 +517,7 @@ extern "C" void piro_close(piro_ctx *c)
     cudaFree(c->coo_rows);
     cudaFree(c->ht_keys);
     cudaFree(c->ht_vals);
-    cudaFree(c->lu_keys);
-    cudaFree(c->lu_vals);
+    cudaFree(c->lu_band);
     cudaFree(c->bc_idx);
     cudaFree(c->memD);
     cudaFree(c->partD);
@@ -781,9 +780,8 @@ static int be_pcg(piro_ctx *c, const Csr *M, const float *b, float *x)
 // Scheme 27 on the hash-table operator M (TIMESCHEME 12, solver 27, Data 2).
 // Mode 1: PIRO's factorization of M's own table on the first step
 // (matrix_operations::HT::lu_decomposition), the result field zero, as the
-// reference returns it.  Mode 0: A = I - dt*M in a table that holds its band
-// (bandwidth nx*ny), factorized in place on the first step; every step then
-// solves A x = u by substitution.
+// reference returns it.  Mode 0: A = I - dt*M factorized in a dense band
+// (bandwidth nx*ny) on the first step; every step then solves A x = u.
 static int lu_step(piro_ctx *c, const float *u, float *x)
 {
     const int64_t N = c->N;
@@ -793,40 +791,19 @@ static int lu_step(piro_ctx *c, const float *u, float *x)
         return PIRO_OK;
     }
     if (!c->lu_done) {
-        Csr I, A;
-        PK(alloc_csr(I, N, N));
-        PK(piro_csr_identity(N, I.rp, I.col, I.val, c->stream));
-        size_t wb = 0;
-        PK(piro_scan_workspace(N, &wb));
-        PK(ensure_work(c, wb));
-        CK(cudaMalloc(&A.rp, sizeof(int32_t) * (size_t)(N + 1)));
-        PK(piro_csrgeam2_count(N, I.rp, I.col, c->lap.rp, c->lap.col, A.rp, c->work, c->work_bytes, c->stream));
-        int32_t nnz = 0;
-        CK(cudaMemcpyAsync(&nnz, A.rp + N, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        CK(cudaMalloc(&A.col, sizeof(int32_t) * (size_t)nnz));
-        CK(cudaMalloc(&A.val, sizeof(float) * (size_t)nnz));
-        A.nnz = nnz;
-        PK(piro_csrgeam2_fill(N, I.rp, I.col, I.val, -c->timestep, c->lap.rp, c->lap.col, c->lap.val, A.rp, A.col,
-                              A.val, c->stream));
-        free_csr(I);
         c->lu_bw = (int64_t)c->nx * c->ny;
-        int64_t entries = 0;
-        int rc = piro_ht_lu_table_size(N, c->lu_bw, c->ht_lf, &entries, &c->lu_ts);
-        if (rc == PIRO_OK) rc = piro_ht_build_workspace(c->lu_ts, &wb);
-        if (rc == PIRO_OK) rc = ensure_work(c, wb);
-        if (rc == PIRO_OK && (cudaMalloc(&c->lu_keys, sizeof(int64_t) * (size_t)c->lu_ts) != cudaSuccess ||
-                              cudaMalloc(&c->lu_vals, sizeof(float) * (size_t)c->lu_ts) != cudaSuccess))
-            rc = fail(PIRO_ERR_CUDA, "scheme 27: no device memory for a %s-slot band table", std::to_string(c->lu_ts));
-        if (rc == PIRO_OK)
-            rc = piro_ht_build(N, A.rp, A.col, A.val, nnz, c->lu_ts, c->lu_keys, c->lu_vals, c->work, c->work_bytes,
-                               c->stream);
-        free_csr(A);
-        if (rc) return rc;
-        PK(piro_ht_lu_factor(N, c->lu_bw, c->lu_keys, c->lu_vals, c->lu_ts, c->stream));
+        PK(piro_ht_lu_band_bytes(N, c->lu_bw, &c->lu_band_bytes));
+        if (cudaMalloc(&c->lu_band, c->lu_band_bytes) != cudaSuccess) {
+            (void)cudaGetLastError();
+            c->lu_band = nullptr;
+            return fail(PIRO_ERR_NOMEM, "scheme 27: no device memory for the %s-byte band",
+                        std::to_string(c->lu_band_bytes));
+        }
+        PK(piro_ht_lu_factor(N, c->lu_bw, c->ht_keys, c->ht_vals, c->ht_ts, 1.0f, -c->timestep, c->lu_band,
+                             c->lu_band_bytes, c->stream));
         c->lu_done = true;
     }
-    return piro_ht_lu_solve(N, c->lu_bw, c->lu_keys, c->lu_vals, c->lu_ts, u, x, c->stream);
+    return piro_ht_lu_solve(N, c->lu_bw, c->lu_band, c->lu_band_bytes, u, x, c->stream);
 }
 
 extern "C" int piro_assign(piro_ctx *c, piro_buf lhs, piro_op rhs, piro_buf *out)

@@ -126,23 +126,24 @@ def ht_lu_reference(N, keys, vals, ts):
     check(lib().piro_ht_lu_reference(N, _p(keys), _p(vals), ts, _stream()), "piro_ht_lu_reference")
 
 
-def ht_lu_table_size(N, bw, lf=0.7):
-    """(band entries, table size) for piro_ht_lu_factor at bandwidth bw."""
-    n, ts = C.c_int64(), C.c_int64()
-    check(lib().piro_ht_lu_table_size(N, bw, lf, C.byref(n), C.byref(ts)), "piro_ht_lu_table_size")
-    return n.value, ts.value
+class HtLu:
+    """Scheme 27 with a solution: shift*I + scale*M (M the table's matrix)
+    factorized in a dense band of bandwidth bw; solve(b) -> x."""
 
+    def __init__(self, N, bw, keys, vals, ts, shift=1.0, scale=1.0):
+        n = C.c_size_t()
+        check(lib().piro_ht_lu_band_bytes(N, bw, C.byref(n)), "piro_ht_lu_band_bytes")
+        self.N, self.bw, self.nbytes = N, bw, n.value
+        self.band = torch.empty(self.nbytes, dtype=torch.uint8, device="cuda")
+        check(lib().piro_ht_lu_factor(N, bw, _p(keys), _p(vals), ts, shift, scale, _p(self.band), self.nbytes,
+                                      _stream()), "piro_ht_lu_factor")
 
-def ht_lu_factor(N, bw, keys, vals, ts):
-    """In-place LU of the table (multipliers kept) within bandwidth bw."""
-    check(lib().piro_ht_lu_factor(N, bw, _p(keys), _p(vals), ts, _stream()), "piro_ht_lu_factor")
-
-
-def ht_lu_solve(N, bw, keys, vals, ts, b, x=None):
-    if x is None:
-        x = torch.empty_like(b)
-    check(lib().piro_ht_lu_solve(N, bw, _p(keys), _p(vals), ts, _p(b), _p(x), _stream()), "piro_ht_lu_solve")
-    return x
+    def solve(self, b, x=None):
+        if x is None:
+            x = torch.empty_like(b)
+        check(lib().piro_ht_lu_solve(self.N, self.bw, _p(self.band), self.nbytes, _p(b), _p(x), _stream()),
+              "piro_ht_lu_solve")
+        return x
 
 
 # ----------------------------------------------------------------- steps

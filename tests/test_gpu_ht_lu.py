@@ -61,29 +61,29 @@ def _fp32_nopivot_berr(Ad, b):
 
 # dt 0.05: well conditioned (cond ~ 10); dt 0.7: PIRO's 10.0 boundary entries
 # make the elements grow ~1e4 during elimination without pivoting
-@pytest.mark.parametrize("n,dt", [((8, 7, 6), 0.05), ((12, 10, 9), 0.05), ((8, 7, 6), 0.7), ((12, 10, 9), 0.7)])
+@pytest.mark.parametrize("n,dt", [((8, 7, 6), 0.05), ((12, 10, 9), 0.05), ((8, 7, 6), 0.7), ((12, 10, 9), 0.7),
+                                  ((40, 3, 3), 0.05), ((3, 3, 40), 0.05)])
 def test_ht_lu_solve(cuda, n, dt):
     import torch
     from piro_b200 import ops
     nx, ny, nz = n
     N = nx * ny * nz
     L = ops.csr_laplacian(nx, ny, nz, 3, 1.0)
-    I = ops.csr_identity(N)
-    A = ops.csrgeam2(N, I, -dt, L)  # I - dt L, all rows
     bw = nx * ny
-    _, ts = ops.ht_lu_table_size(N, bw)
-    keys, vals = ops.ht_build(N, *A, ts)
+    ts = ops.ht_table_size(L[2].numel(), N, 1)
+    keys, vals = ops.ht_build(N, *L, ts)  # the operator's table: the factor scales and shifts it
+    A = ops.csrgeam2(N, ops.csr_identity(N), -dt, L)  # I - dt L, all rows
     Ad = np.zeros((N, N))
     rp, col, val = (t.cpu().numpy() for t in A)
     for r in range(N):
         for k in range(rp[r], rp[r + 1]):
             Ad[r, col[k]] += val[k]
     cond = np.linalg.cond(Ad)
-    ops.ht_lu_factor(N, bw, keys, vals, ts)
+    lu = ops.HtLu(N, bw, keys, vals, ts, 1.0, -dt)
     rng = np.random.default_rng(3)
     for _ in range(2):
         b = rng.random(N).astype(np.float32)
-        x = ops.ht_lu_solve(N, bw, keys, vals, ts, torch.from_numpy(b).cuda()).cpu().numpy().astype(np.float64)
+        x = lu.solve(torch.from_numpy(b).cuda()).cpu().numpy().astype(np.float64)
         ref = np.linalg.solve(Ad, b.astype(np.float64))
         berr = np.abs(Ad @ x - b).max() / (np.abs(Ad).sum(1).max() * np.abs(x).max())
         if dt == 0.05:
@@ -91,6 +91,37 @@ def test_ht_lu_solve(cuda, n, dt):
             assert np.abs(x - ref).max() <= 4 * cond * 6e-8 * np.abs(ref).max()
         else:
             assert berr <= 4 * _fp32_nopivot_berr(Ad, b)
+
+
+def test_ht_lu_factor_matches_elimination(cuda):
+    """The band after the factor: U and the multipliers of an FP32
+    elimination without pivoting in the same operation order, bit for bit."""
+    import torch
+    from piro_b200 import ops
+    nx, ny, nz = 6, 5, 4
+    N, bw, dt = nx * ny * nz, nx * ny, np.float32(0.05)
+    L = ops.csr_laplacian(nx, ny, nz, 3, 1.0)
+    ts = ops.ht_table_size(L[2].numel(), N, 1)
+    keys, vals = ops.ht_build(N, *L, ts)
+    lu = ops.HtLu(N, bw, keys, vals, ts, 1.0, float(-dt))
+    W = 2 * bw + 1
+    band = lu.band[: N * W * 4].view(torch.float32).cpu().numpy().reshape(N, W)
+    rp, col, val = (t.cpu().numpy() for t in L)
+    U = np.zeros((N, N), np.float32)
+    for r in range(N):
+        for k in range(rp[r], rp[r + 1]):
+            U[r, col[k]] = np.float32(-dt) * val[k]
+        U[r, r] = np.float32(1.0) + U[r, r]
+    for k in range(N - 1):
+        f = U[k + 1:, k] / U[k, k]
+        U[k + 1:, k + 1:] -= np.outer(f, U[k, k + 1:]).astype(np.float32)
+        U[k + 1:, k] = f
+    got = np.zeros((N, N), np.float32)
+    for r in range(N):
+        for d in range(-bw, bw + 1):
+            if 0 <= r + d < N:
+                got[r, r + d] = band[r, d + bw]
+    assert np.array_equal(got, U), np.abs(got - U).max()
 
 
 def test_ht_lu_zero_pivot_is_reported(cuda):
@@ -101,11 +132,11 @@ def test_ht_lu_zero_pivot_is_reported(cuda):
     from piro_b200._lib import PiroError
     nx, ny, nz = 8, 7, 6
     N = nx * ny * nz
-    A = ops.csrgeam2(N, ops.csr_identity(N), -0.1, ops.csr_laplacian(nx, ny, nz, 3, 1.0))
-    _, ts = ops.ht_lu_table_size(N, nx * ny)
-    keys, vals = ops.ht_build(N, *A, ts)
+    L = ops.csr_laplacian(nx, ny, nz, 3, 1.0)
+    ts = ops.ht_table_size(L[2].numel(), N, 1)
+    keys, vals = ops.ht_build(N, *L, ts)
     with pytest.raises(PiroError, match="zero pivot at row 0") as e:
-        ops.ht_lu_factor(N, nx * ny, keys, vals, ts)
+        ops.HtLu(N, nx * ny, keys, vals, ts, 1.0, -0.1)
     assert e.value.status == 12  # PIRO_ERR_ZERO_PIVOT
 
 
@@ -114,9 +145,9 @@ def test_ht_lu_entry_outside_band_is_reported(cuda):
     from piro_b200._lib import PiroError
     nx, ny, nz = 6, 5, 4
     N = nx * ny * nz
-    A = ops.csrgeam2(N, ops.csr_identity(N), -0.05, ops.csr_laplacian(nx, ny, nz, 3, 1.0))
-    _, ts = ops.ht_lu_table_size(N, nx)
-    keys, vals = ops.ht_build(N, *A, ts)
+    L = ops.csr_laplacian(nx, ny, nz, 3, 1.0)
+    ts = ops.ht_table_size(L[2].numel(), N, 1)
+    keys, vals = ops.ht_build(N, *L, ts)
     with pytest.raises(PiroError, match="outside the bandwidth") as e:
-        ops.ht_lu_factor(N, nx, keys, vals, ts)  # the z neighbours sit nx*ny away
+        ops.HtLu(N, nx, keys, vals, ts, 1.0, -0.05)  # the z neighbours sit nx*ny away
     assert e.value.status == 1
