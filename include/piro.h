@@ -180,6 +180,17 @@ int piro_ht_lu_factor(int64_t N, int64_t bw, const int64_t *keys, const float *v
 int piro_ht_lu_solve(int64_t N, int64_t bw, void *band, size_t band_bytes, const float *b, float *x,
                      piro_stream_t stream);
 
+/* DENSE format (Data 1).  piro_dense_laplacian: Piro::DENSE::stencils::
+ * laplacian_* (src/stencils.cpp:431-570) into A (N x N row-major floats,
+ * a_bytes >= 4*N*N; zeroed here), values -6/norm and 1/norm in float, uw/dw
+ * assignments in the reference's order.  piro_dense_fe_step:
+ * kernelsolve::DENSE::TIMESCHEME_11 (src/kernelprocess.cpp:42-66,
+ * SpMVDENSE.cl + addVectors.cl): out[r] = u[r] + dt*sum_k A[r][k]*u[k], every
+ * row, the sum in ascending k as the kernel adds it. */
+int piro_dense_laplacian(int nx, int ny, int nz, int scheme, float norm, float *A, size_t a_bytes,
+                         piro_stream_t stream);
+int piro_dense_fe_step(int64_t N, const float *A, float dt, const float *u, float *out, piro_stream_t stream);
+
 /* Matrix-free 7-point step, the comparison point for CSR (laplacianscalar.cl:1-21
  * extended by alpha and the Euler update): interior cells
  * out = u + dt*(alpha*((u[x+1]+u[x-1]-2u)*idx2 + (..y..)*idy2 + (..z..)*idz2)),
@@ -485,6 +496,7 @@ typedef struct piro_op {
 #define PIRO_OP_LAPLACIAN 1
 #define PIRO_OP_GRADIENT 2
 #define PIRO_OP_DOT 3        /* vector & gradient (csrgeam result) */
+#define PIRO_OP_DIV 4        /* div(var1, var2): csrgeam_2 of the divergence matrices */
 #define PIRO_EQN_RESULT (-1) /* piro_buf id of the operator= result (partD) */
 
 typedef struct piro_case_info {
@@ -508,8 +520,9 @@ int piro_open(const char *assets_dir, const char *case_name, piro_ctx **out);
 void piro_close(piro_ctx *ctx);
 int piro_ctx_query(piro_ctx *ctx, piro_case_info *info);
 /* 0 (default): alpha applied as SpMDSM intends; 1: alpha dropped, as the
- * reference's csrscale actually behaves (src/kernelcsrgeam.cpp:224-231).
- * Must be set before the Laplacian is assembled. */
+ * reference's csrscale actually behaves (src/kernelcsrgeam.cpp:224-231), and
+ * likewise div's velocity scaling (SpMSCSR, kernelcsrgeam.cpp:100-130).
+ * Must be set before the operator is assembled. */
 int piro_set_alpha_mode(piro_ctx *ctx, int mode);
 /* Scheme 27 (TIMESCHEME 12, solver 27, Data 2).  0 (default): backward Euler
  * solved directly -- A = I - dt*M (M the operator's table) factorized in a
@@ -532,24 +545,34 @@ int piro_field_download(piro_ctx *ctx, piro_buf f, float *host, int64_t n);
 int piro_field_device_ptr(piro_ctx *ctx, piro_buf f, float **dptr);
 
 /* process::laplacian (src/process.cpp:60-122): assembled on the first call
- * per [Solve] Data (0 CSR, 2 HT, 3 COO; 1 DENSE gives PIRO_ERR_DATATYPE) and
- * cached; for CSR the rows are scaled by the field named `coeff`. */
+ * per [Solve] Data (0 CSR, 1 DENSE (N x N floats), 2 HT, 3 COO) and cached;
+ * for CSR the rows are scaled by the field named `coeff`. */
 int piro_laplacian(piro_ctx *ctx, const char *var, const char *coeff, piro_op *out);
 /* process::gradient (src/process.cpp:124-152): the three CSR matrices. */
 int piro_gradient(piro_ctx *ctx, const char *var, piro_op *out);
 /* operator& (src/operatoroverload.cpp:102-123): csrgeam of a vector field
  * with the gradient, merged once and cached. */
 int piro_dot(piro_ctx *ctx, piro_buf v, piro_op grad, piro_op *out);
+/* process::div (src/process.cpp:168-215): the divergence matrices (the
+ * gradient stencils, operatordivergenceCSR.cpp:21-101) with matrix a's rows
+ * scaled by component a of the vector field var2, merged as csrgeam_2
+ * (kernelcsrgeam.cpp:88-207); CSR only.  Under piro_set_alpha_mode(1) the
+ * rows stay unscaled, as the reference's SpMSCSR launches (int arguments set
+ * with sizeof(cl_mem)) never run. */
+int piro_div(piro_ctx *ctx, const char *var1, const char *var2, piro_op *out);
 /* CLBuffer::operator= (src/operatoroverload.cpp:20-100): one time step of
- * lhs by [Schemes] Time: 11 forward Euler (CSR, HT or COO), 12 backward
- * Euler with Solver 40 (JLI, as written) or 39 (FP32 PCG in FP64
- * refinement to 1e-8).  *out is the new field (partD, PIRO_EQN_RESULT). */
+ * lhs by [Schemes] Time: 11 forward Euler (CSR, DENSE, HT or COO), 12
+ * backward Euler with Solver 40 (JLI, as written, CSR), 39 (FP32 PCG in FP64
+ * refinement to 1e-8, CSR Laplacian) or 27 (HT LU, piro_set_lu_mode).  *out
+ * is the new field (partD, PIRO_EQN_RESULT). */
 int piro_assign(piro_ctx *ctx, piro_buf lhs, piro_op rhs, piro_buf *out);
 /* scalarMatrix::Solve (src/process.cpp:221-236): copy the result into field
  * 1 and apply the Dirichlet face values (setBC). */
 int piro_step_solve(piro_ctx *ctx, piro_buf eqn, float time);
 /* Piro::solve (src/solve.cpp:11-48): while (time < TotalTime) with float
- * time, the equation of [File] simindex (0 heat, 1 advection) per step. */
+ * time, the equation of [File] simindex per step: 0 heat
+ * ddt_r(T) = laplacian(T, Alpha), 1 advection ddt_r(U) = vector(v) &
+ * gradient(U), 2 continuity ddt_r(rho) = div(rho, u). */
 int piro_solve(piro_ctx *ctx, int64_t *steps_taken);
 /* Download an assembled operator in CSR form (nnz only when rowptr is NULL). */
 int piro_op_export_csr(piro_ctx *ctx, piro_op op, int32_t *rowptr, int32_t *col, float *val, int64_t cap,

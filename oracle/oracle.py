@@ -69,6 +69,8 @@ def _load():
         "or_be_jli": (i32, [i64, i32, i32, _i32p, _i32p, _f32p, f32, _f32p, _f32p, _f32p, f32, f32, i32]),
         "or_be_cg_f64": (i32, [i64, i32, i32, i32, _i32p, _i32p, _f32p, _f32p, _f32p, _f64p, f64, i32,
                                C.POINTER(C.c_double)]),
+        "or_dense_laplacian": (None, [i32, i32, i32, i32, f32, _f32p]),
+        "or_fe_dense_step": (None, [i64, _f32p, f32, _f32p, _f32p, _f32p]),
         "or_ic_gaussian": (None, [i32, i32, i32, f32, f32, f32, f32, _f32p, _f32p, _f32p]),
         "or_ic_coulomb": (None, [i32, i32, i32, f32, f32, f32, _f32p, f32, f64, f64, _f32p]),
         "or_ic_uniform_vector": (None, [i64, _f32p, f32, _f32p]),
@@ -135,6 +137,30 @@ def gradient3(nx, ny, nz, scheme, norm):
         nnz = lib().or_gradient(nx, ny, nz, scheme, axis, np.float32(norm), rp, col, val)
         out.append((rp.copy(), col[:nnz].copy(), val[:nnz].copy()))
     return out
+
+
+def dense_laplacian(nx, ny, nz, scheme, norm):
+    """N x N row-major DENSE Laplacian (stencils.cpp:431-570)."""
+    N = n_cells(nx, ny, nz)
+    A = np.empty((N, N), np.float32)
+    lib().or_dense_laplacian(nx, ny, nz, scheme, np.float32(norm), A.reshape(-1))
+    return A
+
+
+def fe_dense(A, dt, B):
+    """One DENSE forward-Euler step (kernelprocess.cpp:42-66): (C, D = B + C)."""
+    N = A.shape[0]
+    C_ = np.zeros(N, np.float32)
+    D = np.zeros(N, np.float32)
+    lib().or_fe_dense_step(N, np.ascontiguousarray(A, np.float32).reshape(-1), np.float32(dt),
+                           np.ascontiguousarray(B, np.float32), C_, D)
+    return C_, D
+
+
+def div3(nx, ny, nz, scheme, norm):
+    """The three divergence matrices (operatordivergenceCSR.cpp:21-101): the
+    gradient stencils (stencils.cpp:995-1003 forward to them) with the same norm."""
+    return gradient3(nx, ny, nz, scheme, norm)
 
 
 HT_A, HT_B, HT_C, HT_LF = 3.3608, -0.5552, -0.0143, 0.7  # assets/Data/hashtable.ini:3-7
@@ -385,7 +411,14 @@ class Ref:
         L.refcl_setbc.argtypes = [_f32p, _f32p, _u32p, C.c_uint]
         L.refcl_laplacianscalar.argtypes = [_f32p, _f32p, f32, f32, f32, C.c_uint, C.c_uint, f32, C.c_uint]
         L.refcl_lu_round.argtypes = [_i32p, _f32p, i32, i32, i32, i32]
-        for n in ("refcl_spmvcsr", "refcl_spmvcsr_i1", "refcl_spmvcoo", "refcl_spmvht", "refcl_add", "refcl_sub",
+        L.ref_div.restype = None
+        L.ref_div.argtypes = [i32, i32, i32, i32, f32, _i32p, _i32p, _f32p, np.ctypeslib.ndpointer(np.int64)]
+        L.ref_dense_laplacian.restype = None
+        L.ref_dense_laplacian.argtypes = [i32, i32, i32, i32, f32, _f32p]
+        L.refcl_csrgeam2_merge.argtypes = [i32, _i32p, _i32p, _f32p, _i32p, _i32p, _f32p, _i32p, _i32p, _f32p,
+                                           _i32p, _i32p, _f32p, _i32p]
+        L.refcl_fe_dense.argtypes = [i32, _f32p, _f32p, _f32p, _f32p, f32]
+        for n in ("refcl_csrgeam2_merge", "refcl_fe_dense", "refcl_spmvcsr", "refcl_spmvcsr_i1", "refcl_spmvcoo", "refcl_spmvht", "refcl_add", "refcl_sub",
                   "refcl_urf", "refcl_csrgeam", "refcl_spmdsm", "refcl_setbc", "refcl_laplacianscalar",
                   "refcl_lu_round"):
             getattr(L, n).restype = None
@@ -525,6 +558,46 @@ class Ref:
         self.lib.refcl_laplacianscalar(np.ascontiguousarray(B, np.float32).copy(), Cc, dx, dy, dz, nx, ny,
                                        np.float32(dt), N)
         return Cc
+
+    def div3(self, nx, ny, nz, scheme, norm):
+        N = n_cells(nx, ny, nz)
+        rp = np.zeros(3 * (N + 1), np.int32)
+        col = np.zeros(6 * N, np.int32)
+        val = np.zeros(6 * N, np.float32)
+        nnz3 = np.zeros(3, np.int64)
+        self.lib.ref_div(nx, ny, nz, scheme, np.float32(norm), rp, col, val, nnz3)
+        out, off = [], 0
+        for a in range(3):
+            k = int(nnz3[a])
+            out.append((rp[a * (N + 1):(a + 1) * (N + 1)].copy(), col[off:off + k].copy(), val[off:off + k].copy()))
+            off += k
+        return out
+
+    def csrgeam2_merge(self, N, A, B, Cm):
+        """kernelmethods::csrgeam_2's merge of three matrices, unscaled."""
+        nnz = len(A[2]) + len(B[2]) + len(Cm[2])
+        count = np.zeros(N, np.int32)
+        rpD = np.zeros(N + 1, np.int32)
+        cD = np.zeros(max(nnz, 1), np.int32)
+        vD = np.zeros(max(nnz, 1), np.float32)
+        self.lib.refcl_csrgeam2_merge(N, A[0], A[1], A[2], B[0], B[1], B[2], Cm[0], Cm[1], Cm[2], rpD, cD, vD,
+                                      count)
+        k = int(rpD[N])
+        return rpD, cD[:k], vD[:k]
+
+    def dense_laplacian(self, nx, ny, nz, scheme, norm):
+        N = n_cells(nx, ny, nz)
+        A = np.zeros((N, N), np.float32)
+        self.lib.ref_dense_laplacian(nx, ny, nz, scheme, np.float32(norm), A.reshape(-1))
+        return A
+
+    def fe_dense(self, A, dt, B):
+        N = A.shape[0]
+        Bc = np.ascontiguousarray(B, np.float32).copy()
+        C_ = np.zeros(N, np.float32)
+        D = np.zeros(N, np.float32)
+        self.lib.refcl_fe_dense(N, np.ascontiguousarray(A, np.float32).reshape(-1), Bc, C_, D, np.float32(dt))
+        return C_, D
 
     def ht_lu(self, N, keys32, vals, TS):
         """Scheme 27's factorization of the table (matrixoperations.cpp:37-99), in place."""

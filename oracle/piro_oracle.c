@@ -342,6 +342,50 @@ void or_csrgeam2_fill(int64_t N, const int32_t *rpA, const int32_t *cA, const fl
 }
 
 /* ------------------------------------------------------------------------ */
+/* DENSE Laplacian (src/stencils.cpp:431-570, from src/operatorlaplacian.cpp:
+ * 65-103): A is N x N row-major, zero except per row l, in this order,
+ * A[l][l] = -6/norm, then for each existing neighbour (x-, x+, y-, y+, z-, z+)
+ * A[l][nb] = 1/norm -- assignments, so where uw/dw replace a neighbour by l
+ * itself the diagonal ends as 1/norm.  No 10.0 rule on this path.  The
+ * constants are int / float: float divisions (stencils.cpp:439,445). */
+void or_dense_laplacian(int nx, int ny, int nz, int scheme, float norm, float *A)
+{
+    const int64_t N = (int64_t)nx * ny * nz;
+    memset(A, 0, sizeof(float) * (size_t)N * (size_t)N);
+    if (scheme < 1 || scheme > 3) return;
+    const float v_self = -6.0f / norm, v_nb = 1.0f / norm;
+#pragma omp parallel for schedule(static)
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                const int64_t l = idx3(x, y, z, nx, ny);
+                float *row = A + l * N;
+                row[l] = v_self;
+                if (x > 0) row[scheme == 2 ? l : idx3(x - 1, y, z, nx, ny)] = v_nb;
+                if (x < nx - 1) row[scheme == 1 ? l : idx3(x + 1, y, z, nx, ny)] = v_nb;
+                if (y > 0) row[scheme == 2 ? l : idx3(x, y - 1, z, nx, ny)] = v_nb;
+                if (y < ny - 1) row[scheme == 1 ? l : idx3(x, y + 1, z, nx, ny)] = v_nb;
+                if (z > 0) row[scheme == 2 ? l : idx3(x, y, z - 1, nx, ny)] = v_nb;
+                if (z < nz - 1) row[scheme == 1 ? l : idx3(x, y, z + 1, nx, ny)] = v_nb;
+            }
+}
+
+/* DENSE forward Euler (src/kernelprocess.cpp:42-66): SpMVDENSE.cl (P = 1)
+ * C[r] = deltat * sum, sum += A[r][k]*B[k] over k ascending, every row; then
+ * addVectors.cl: D = B + C. */
+void or_fe_dense_step(int64_t N, const float *A, float dt, const float *B, float *C, float *D)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t r = 0; r < N; ++r) {
+        float sum = 0.0f;
+        const float *row = A + r * N;
+        for (int64_t k = 0; k < N; ++k) sum += row[k] * B[k];
+        C[r] = dt * sum;
+        D[r] = B[r] + C[r];
+    }
+}
+
+/* ------------------------------------------------------------------------ */
 /* Interior mask used by SpMVCSR.cl:29-32 and SpMVCSR_I1.cl:28-31. */
 static inline int interior_row(int64_t id, uint32_t nx, uint32_t ny, uint32_t size)
 {

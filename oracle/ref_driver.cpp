@@ -99,6 +99,55 @@ void ref_gradient(int nx, int ny, int nz, int scheme, float norm, int *rp, int *
     }
 }
 
+// The three divergence matrices as Piro::CSR::div builds them
+// (operatordivergenceCSR.cpp:21-101: div_*_x/y/z, one rowpointers vector,
+// norm = 2*(l0/(n0-2))).  Same layout as ref_gradient.
+void ref_div(int nx, int ny, int nz, int scheme, float norm, int *rp, int *col, float *val, long long *nnz3)
+{
+    set_grid(nx, ny, nz);
+    std::vector<uint> n{(uint)nx, (uint)ny, (uint)nz};
+    const int N = nx * ny * nz;
+    Piro::CellData cd;
+    cd.rowpointers.assign(N + 1, 0);
+    size_t off = 0;
+    for (int axis = 0; axis < 3; ++axis) {
+        cd.columns.clear();
+        cd.values.clear();
+        if (axis == 0) {
+            if (scheme == 3) Piro::CSR::stencils::div_cd_x(cd, n, norm);
+            else if (scheme == 2) Piro::CSR::stencils::div_dw_x(cd, n, norm);
+            else if (scheme == 1) Piro::CSR::stencils::div_uw_x(cd, n, norm);
+        } else if (axis == 1) {
+            if (scheme == 3) Piro::CSR::stencils::div_cd_y(cd, n, norm);
+            else if (scheme == 2) Piro::CSR::stencils::div_dw_y(cd, n, norm);
+            else if (scheme == 1) Piro::CSR::stencils::div_uw_y(cd, n, norm);
+        } else {
+            if (scheme == 3) Piro::CSR::stencils::div_cd_z(cd, n, norm);
+            else if (scheme == 2) Piro::CSR::stencils::div_dw_z(cd, n, norm);
+            else if (scheme == 1) Piro::CSR::stencils::div_uw_z(cd, n, norm);
+        }
+        std::memcpy(rp + axis * (N + 1), cd.rowpointers.data(), sizeof(int) * (N + 1));
+        std::memcpy(col + off, cd.columns.data(), sizeof(int) * cd.columns.size());
+        std::memcpy(val + off, cd.values.data(), sizeof(float) * cd.values.size());
+        nnz3[axis] = (long long)cd.values.size();
+        off += cd.values.size();
+    }
+}
+
+// Piro::DENSE::stencils::laplacian_* (stencils.cpp:431-570) into A[N*N].
+void ref_dense_laplacian(int nx, int ny, int nz, int scheme, float norm, float *A)
+{
+    set_grid(nx, ny, nz);
+    std::vector<uint> n{(uint)nx, (uint)ny, (uint)nz};
+    const size_t N = (size_t)nx * ny * nz;
+    Piro::CellData cd;
+    cd.matrix.resize(N * N);  // operatorlaplacian.cpp:79
+    if (scheme == 3) Piro::DENSE::stencils::laplacian_cd(cd, n, norm);
+    else if (scheme == 2) Piro::DENSE::stencils::laplacian_dw(cd, n, norm);
+    else if (scheme == 1) Piro::DENSE::stencils::laplacian_uw(cd, n, norm);
+    std::memcpy(A, cd.matrix.data(), sizeof(float) * N * N);
+}
+
 // Piro::methods::sethash on an int32 table (methods.cpp:74-118), fed in the
 // row-major order of operatorlaplacian.cpp:190-203.  keys/vals hold TS.
 int ref_ht_insert_all(int N, const int *rowptr, const int *col, const float *val, int TS, int *keys, float *vals)

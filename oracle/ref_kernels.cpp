@@ -17,8 +17,8 @@
 #include <cstdio>
 
 namespace clshim {
-thread_local size_t g_gid = 0;
-inline size_t get_global_id(int) { return g_gid; }
+thread_local size_t g_gid = 0, g_gid1 = 0;
+inline size_t get_global_id(int d) { return d == 0 ? g_gid : g_gid1; }
 inline int min(int a, int b) { return a < b ? a : b; }
 inline float fabs(float a) { return std::fabs(a); }
 }  // namespace clshim
@@ -63,6 +63,12 @@ _Pragma("GCC diagnostic pop") }
 CL_UNIT(k_g3, "csrgeam_3.cl")
 #include "csrgeam_3.cl"
 _Pragma("GCC diagnostic pop") }
+CL_UNIT(k_g2, "csrgeam_2.cl")
+#include "csrgeam_2.cl"
+_Pragma("GCC diagnostic pop") }
+CL_UNIT(k_dense, "SpMVDENSE.cl")
+#include "SpMVDENSE.cl"
+_Pragma("GCC diagnostic pop") }
 CL_UNIT(k_spmdsm, "SpMDSM.cl")
 #include "SpMDSM.cl"
 _Pragma("GCC diagnostic pop") }
@@ -81,6 +87,14 @@ _Pragma("GCC diagnostic pop") }
         clshim::g_gid = gid_;                                    \
         call;                                                    \
     }
+
+#define NDRANGE2(n0, n1, call)                                   \
+    for (size_t g1_ = 0; g1_ < (size_t)(n1); ++g1_)              \
+        for (size_t g0_ = 0; g0_ < (size_t)(n0); ++g0_) {        \
+            clshim::g_gid = g0_;                                 \
+            clshim::g_gid1 = g1_;                                \
+            call;                                                \
+        }
 
 extern "C" {
 
@@ -126,6 +140,27 @@ void refcl_csrgeam(int N, const int *rpA, const int *cA, const float *vA, const 
     for (int i = 0; i < N; ++i) rpD[i + 1] = count[i];  // clEnqueueCopyBuffer, :53
     for (int row = 0; row < N; ++row) NDRANGE(N, k_ps::prefixsum(count, rpD, N, row));
     NDRANGE(N, k_g3::csrgeam_3(vA, cA, rpA, vB, cB, rpB, vC, cC, rpC, vD, cD, rpD, count, v, N));
+}
+
+// kernelmethods::csrgeam_2's merge (kernelcsrgeam.cpp:142-203): the same
+// count and scan as csrgeam, then csrgeam_2.cl (no vector scaling).
+void refcl_csrgeam2_merge(int N, const int *rpA, const int *cA, const float *vA, const int *rpB, const int *cB,
+                          const float *vB, const int *rpC, const int *cC, const float *vC, int *rpD, int *cD,
+                          float *vD, int *count)
+{
+    NDRANGE(N, k_g1::csrgeam_1(cA, rpA, cB, rpB, cC, rpC, count, N));
+    rpD[0] = 0;
+    for (int i = 0; i < N; ++i) rpD[i + 1] = count[i];
+    for (int row = 0; row < N; ++row) NDRANGE(N, k_ps::prefixsum(count, rpD, N, row));
+    NDRANGE(N, k_g2::csrgeam_2(vA, cA, rpA, vB, cB, rpB, vC, cC, rpC, vD, cD, rpD, count, N));
+}
+
+// kernelsolve::DENSE::TIMESCHEME_11 (kernelprocess.cpp:42-66): SpMVDENSE over
+// the (N, N) range with P = 1 (only id(0) = 0 does work), then addVectors.
+void refcl_fe_dense(int N, const float *A, float *B, float *C, float *D, float dt)
+{
+    NDRANGE2(N, N, k_dense::SpMVDENSE(A, B, C, (uint)N, (uint)N, 1u, dt));
+    NDRANGE(N, k_add::addVectors(D, B, C, (unsigned)N));
 }
 
 void refcl_spmdsm(int nnz, int M, float *val, const int *col, const int *rp, const float *diag, int ind)

@@ -61,6 +61,8 @@ SIGNATURES = {
     "piro_coo_spmv": (i32, [i64, i64, vp, vp, vp, f32, vp, vp, vp]),
     "piro_coo_fe_step": (i32, [i64, i64, vp, vp, vp, f32, vp, vp, vp]),
     "piro_ht_spmv": (i32, [i32, i32, i32, vp, vp, i64, f32, i32, vp, vp, vp]),
+    "piro_dense_laplacian": (i32, [i32, i32, i32, i32, f32, vp, sz, vp]),
+    "piro_dense_fe_step": (i32, [i64, vp, f32, vp, vp, vp]),
     "piro_ht_lu_reference": (i32, [i64, vp, vp, i64, vp]),
     "piro_ht_lu_band_bytes": (i32, [i64, i64, C.POINTER(sz)]),
     "piro_ht_lu_factor": (i32, [i64, i64, vp, vp, i64, f32, f32, vp, sz, vp]),
@@ -136,6 +138,7 @@ SIGNATURES = {
     "piro_laplacian": (i32, [vp, C.c_char_p, C.c_char_p, C.POINTER(Op)]),
     "piro_gradient": (i32, [vp, C.c_char_p, C.POINTER(Op)]),
     "piro_dot": (i32, [vp, Buf, Op, C.POINTER(Op)]),
+    "piro_div": (i32, [vp, C.c_char_p, C.c_char_p, C.POINTER(Op)]),
     "piro_assign": (i32, [vp, Buf, Op, C.POINTER(Buf)]),
     "piro_step_solve": (i32, [vp, Buf, f32]),
     "piro_solve": (i32, [vp, C.POINTER(C.c_int64)]),

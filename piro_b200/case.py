@@ -142,6 +142,11 @@ class process:
         check(lib().piro_gradient(self.case.h, var.encode(), C.byref(o)), "piro_gradient")
         return Operator(self.case, o)
 
+    def div(self, var1: str, var2: str) -> Operator:
+        o = Op()
+        check(lib().piro_div(self.case.h, var1.encode(), var2.encode(), C.byref(o)), "piro_div")
+        return Operator(self.case, o)
+
 
 class scalarMatrix:
     """Piro::scalarMatrix: Solve copies the result into field 1 and applies setBC."""

@@ -153,8 +153,9 @@ struct piro_ctx {
     uint32_t *bc_idx = nullptr;
     float *memD = nullptr;
     // operators (cached on first use, like the INIT flags of preprocess.hpp:105-122)
-    bool lap_init = false, grad_init = false, dot_init = false;
-    Csr lap, grad[3], dot, be_A;
+    bool lap_init = false, grad_init = false, dot_init = false, div_init = false;
+    Csr lap, grad[3], dot, divm, be_A;
+    float *dense = nullptr;  // DENSE Laplacian, N x N row-major (Data 1)
     int32_t *coo_rows = nullptr;
     int64_t *ht_keys = nullptr;
     float *ht_vals = nullptr;
@@ -513,7 +514,9 @@ extern "C" void piro_close(piro_ctx *c)
     free_csr(c->lap);
     for (Csr &g : c->grad) free_csr(g);
     free_csr(c->dot);
+    free_csr(c->divm);
     free_csr(c->be_A);
+    cudaFree(c->dense);
     cudaFree(c->coo_rows);
     cudaFree(c->ht_keys);
     cudaFree(c->ht_vals);
@@ -637,8 +640,19 @@ extern "C" int piro_laplacian(piro_ctx *c, const char *var, const char *coeff, p
     const int64_t N = c->N;
     const int coef = match_field(c, coeff);
     if (c->datatype == 1) {
-        piro::set_error("piro_laplacian: DENSE (Data = 1) is not on this path");
-        return PIRO_ERR_DATATYPE;
+        // Piro::DENSE::laplacian (operatorlaplacian.cpp:65-103): N x N, alpha never applied
+        const size_t bytes = sizeof(float) * (size_t)N * (size_t)N;
+        if (cudaMalloc(&c->dense, bytes) != cudaSuccess) {
+            (void)cudaGetLastError();
+            c->dense = nullptr;
+            return fail(PIRO_ERR_NOMEM, "piro_laplacian: no device memory for the %s-byte DENSE matrix",
+                        std::to_string(bytes));
+        }
+        PK(piro_dense_laplacian(c->nx, c->ny, c->nz, c->spacescheme, lap_norm(c), c->dense, bytes, c->stream));
+        c->lap_coeff = coef;
+        c->lap_init = true;
+        CK(cudaStreamSynchronize(c->stream));
+        return PIRO_OK;
     }
     if (c->datatype != 0 && c->datatype != 2 && c->datatype != 3) {
         piro::set_error("piro_laplacian: invalid Data %d", c->datatype);
@@ -729,10 +743,64 @@ extern "C" int piro_dot(piro_ctx *c, piro_buf v, piro_op grad, piro_op *out)
     return PIRO_OK;
 }
 
+// process::div (src/process.cpp:168-215): Piro::CSR::div's three matrices
+// (operatordivergenceCSR.cpp:21-101; the div_* stencils forward to the
+// gradient ones, stencils.cpp:995-1003, with the same norm) merged by
+// csrgeam_2 (kernelcsrgeam.cpp:88-207) after SpMSCSR scales matrix a's rows
+// by component a of var2.  That merge is csrgeam3 with var2 as the vector.
+// alpha_mode 1 keeps the reference's literal behaviour: its SpMSCSR launches
+// set their int arguments with sizeof(cl_mem) (kernelcsrgeam.cpp:103-129) and
+// never run, so the gradients are merged unscaled.  CSR only (the reference
+// exits otherwise).
+extern "C" int piro_div(piro_ctx *c, const char *var1, const char *var2, piro_op *out)
+{
+    (void)var1;
+    if (!c || !var2 || !out) {
+        piro::set_error("piro_div: null argument");
+        return PIRO_ERR_ARG;
+    }
+    out->kind = PIRO_OP_DIV;
+    if (c->div_init) return PIRO_OK;  // DIV_INIT
+    if (c->datatype != 0) {
+        piro::set_error("piro_div: only CSR (Data = 0), as in process.cpp:181-213");
+        return PIRO_ERR_DATATYPE;
+    }
+    piro_op g;
+    PK(piro_gradient(c, var1, &g));
+    const Field &f = c->fields[(size_t)match_field(c, var2)];
+    if (f.n < 3 * c->N) {
+        piro::set_error("piro_div: field '%s' is not a vector field", f.name.c_str());
+        return PIRO_ERR_ARG;
+    }
+    const float *v = f.d;
+    float *ones = nullptr;
+    if (c->alpha_mode == 1) {
+        CK(cudaMalloc(&ones, sizeof(float) * 3 * (size_t)c->N));
+        CK(cudaMemsetAsync(ones, 0, sizeof(float) * 3 * (size_t)c->N, c->stream));
+        PK(piro_vec_op_scalar(0, 3 * c->N, 1.0f, ones, ones, c->stream));
+        v = ones;
+    }
+    const int64_t nnz = c->grad[0].nnz + c->grad[1].nnz + c->grad[2].nnz;
+    size_t wb = 0;
+    int rc = piro_scan_workspace(c->N, &wb);
+    if (rc == PIRO_OK) rc = ensure_work(c, wb);
+    if (rc == PIRO_OK) rc = alloc_csr(c->divm, c->N, nnz);
+    if (rc == PIRO_OK)
+        rc = piro_csrgeam3(c->N, c->grad[0].rp, c->grad[0].col, c->grad[0].val, c->grad[1].rp, c->grad[1].col,
+                           c->grad[1].val, c->grad[2].rp, c->grad[2].col, c->grad[2].val, v, c->divm.rp,
+                           c->divm.col, c->divm.val, c->work, c->work_bytes, c->stream);
+    if (rc == PIRO_OK && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = PIRO_ERR_CUDA;
+    cudaFree(ones);
+    if (rc) return rc;
+    c->div_init = true;
+    return PIRO_OK;
+}
+
 static const Csr *op_csr(const piro_ctx *c, piro_op op)
 {
-    if (op.kind == PIRO_OP_LAPLACIAN && c->lap_init) return &c->lap;
+    if (op.kind == PIRO_OP_LAPLACIAN && c->lap_init && c->datatype != 1) return &c->lap;
     if (op.kind == PIRO_OP_DOT && c->dot_init) return &c->dot;
+    if (op.kind == PIRO_OP_DIV && c->div_init) return &c->divm;
     return nullptr;
 }
 
@@ -822,6 +890,10 @@ extern "C" int piro_assign(piro_ctx *c, piro_buf lhs, piro_op rhs, piro_buf *out
             const Csr *M = op_csr(c, rhs);
             if (!M) return fail(PIRO_ERR_STATE, "piro_assign: operator not assembled");
             PK(piro_csr_fe_step(c->nx, c->ny, c->nz, M->rp, M->col, M->val, dt, u, c->partD, c->stream));
+        } else if (c->datatype == 1) {
+            if (!c->dense || rhs.kind != PIRO_OP_LAPLACIAN)
+                return fail(PIRO_ERR_STATE, "piro_assign: DENSE operator not assembled");
+            PK(piro_dense_fe_step(N, c->dense, dt, u, c->partD, c->stream));
         } else if (c->datatype == 2) {
             if (!c->ht_keys) return fail(PIRO_ERR_STATE, "piro_assign: hash table not built");
             PK(piro_ht_spmv(c->nx, c->ny, c->nz, c->ht_keys, c->ht_vals, c->ht_ts, dt, 1, u, c->partD, c->stream));
@@ -844,6 +916,8 @@ extern "C" int piro_assign(piro_ctx *c, piro_buf lhs, piro_op rhs, piro_buf *out
             PK(piro_be_jli(c->nx, c->ny, c->nz, M->rp, M->col, M->val, dt, u, c->partD, c->partC, c->jli_tol,
                            c->jli_urf, c->jli_maxiter, &iters, c->stream));
         } else if (c->solverscheme == 39) {
+            if (rhs.kind != PIRO_OP_LAPLACIAN)
+                return fail(PIRO_ERR_SCHEME, "piro_assign: solver 39 (PCG) needs the symmetric Laplacian");
             PK(be_pcg(c, M, u, c->partD));
         } else {
             piro::set_error("piro_assign: Solver %d not available for TIMESCHEME 12 (40 JLI, 39 PCG, 27 LU)", c->solverscheme);
@@ -1025,8 +1099,11 @@ extern "C" int piro_solve(piro_ctx *c, int64_t *steps_taken)
             PK(piro_vector(c, "v", &v));
             PK(piro_gradient(c, "U", &g));
             PK(piro_dot(c, v, g, &op));
+        } else if (c->simindex == 2) {
+            PK(piro_ddt_r(c, "rho", &lhs));
+            PK(piro_div(c, "rho", "u", &op));
         } else {
-            piro::set_error("piro_solve: simindex %d not on this path (0 heat, 1 advection)", c->simindex);
+            piro::set_error("piro_solve: simindex %d invalid (0 heat, 1 advection, 2 continuity)", c->simindex);
             return PIRO_ERR_SCHEME;
         }
         PK(piro_assign(c, lhs, op, &res));

@@ -126,6 +126,22 @@ def ht_lu_reference(N, keys, vals, ts):
     check(lib().piro_ht_lu_reference(N, _p(keys), _p(vals), ts, _stream()), "piro_ht_lu_reference")
 
 
+def dense_laplacian(nx, ny, nz, scheme, norm):
+    """N x N DENSE Laplacian on the device (row-major float32)."""
+    N = nx * ny * nz
+    A = torch.empty((N, N), dtype=torch.float32, device="cuda")
+    check(lib().piro_dense_laplacian(nx, ny, nz, scheme, norm, _p(A), A.numel() * 4, _stream()),
+          "piro_dense_laplacian")
+    return A
+
+
+def dense_fe_step(A, dt, u, out=None):
+    if out is None:
+        out = torch.empty_like(u)
+    check(lib().piro_dense_fe_step(u.numel(), _p(A), dt, _p(u), _p(out), _stream()), "piro_dense_fe_step")
+    return out
+
+
 class HtLu:
     """Scheme 27 with a solution: shift*I + scale*M (M the table's matrix)
     factorized in a dense band of bandwidth bw; solve(b) -> x."""

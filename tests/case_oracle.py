@@ -101,7 +101,9 @@ def run_case(assets, case_name, alpha_mode=0, lu_mode=0):
 
     norm = O.laplacian_norm(l[0], nx)
     op = None
-    if sim == 0:
+    if sim == 0 and data == 1:
+        op = ("dense", O.dense_laplacian(nx, ny, nz, ss, norm))
+    elif sim == 0:
         if data == 3:
             rows, col, val = O.laplacian(nx, ny, nz, ss, norm, "coo")
             op = ("coo", (rows, col, val))
@@ -115,16 +117,22 @@ def run_case(assets, case_name, alpha_mode=0, lu_mode=0):
                 tsz = O.ht_table_size_reference(len(val), N)
                 keys, vals = O.ht_build(N, rp, col, val, tsz)
                 op = ("ht", (keys, vals))
-    else:
+    elif sim == 1:
         G = O.gradient3(nx, ny, nz, ss, O.gradient_norm(l[0], nx))
         op = ("csr", O.csrgeam3(N, *G, dev[match("v")]))
-    lhs = match("T" if sim == 0 else "U")
+    else:  # continuity: div(rho, u), the divergence matrices row-scaled by u (or not: alpha_mode 1)
+        G = O.div3(nx, ny, nz, ss, O.gradient_norm(l[0], nx))
+        vel = dev[match("u")] if alpha_mode == 0 else np.ones(3 * N, np.float32)
+        op = ("csr", O.csrgeam3(N, *G, vel))
+    lhs = match({0: "T", 1: "U", 2: "rho"}[sim])
     steps = O.step_count(total, dt)
     for _ in range(steps):
         u = dev[lhs]
         if ts == 11:
             if op[0] == "csr":
                 part = O.spmv_csr_fe(nx, ny, nz, op[1], dt, u, np.zeros(N, np.float32))
+            elif op[0] == "dense":
+                part = O.fe_dense(op[1], dt, u)[1]
             elif op[0] == "coo":
                 part = u + O.spmv_coo(N, op[1], dt, u)
             else:

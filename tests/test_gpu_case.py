@@ -21,6 +21,8 @@ CASES = [
     ("heat_be_jli.ini", 1e-6),     # BE, the reference's JLI iteration (FP64 residual sums)
     ("heat_be_pcg.ini", 1e-6),     # BE, FP32 PCG in FP64 refinement vs an FP64 solve
     ("heat_be_lu.ini", 1e-5),      # BE, scheme 27: FP32 banded LU in the hash table vs an FP64 solve
+    ("heat_fe_dense.ini", None),   # FE, DENSE (N x N), downwind: SpMVDENSE's sequential sums
+    ("cont_fe.ini", None),         # continuity: div(rho, u), central
 ]
 
 
