@@ -198,6 +198,93 @@ def config_sections(torch, peak):
     return out
 
 
+def next_rows_section(torch, ops, peak):
+    """DENSE forward Euler at 34^3 (N = 39,304: a 6.2 GB matrix, HBM stream)
+    and scheme 27: the banded LU (factor once, solve per step) at 34^3, and
+    PIRO's own factorization on the Test/LUDecomp.ini shape (5^3 with ghosts,
+    central, l = 5) on the device and by the reference's code on the host."""
+    out = {}
+    n = 34
+    N = n ** 3
+    A = ops.dense_laplacian(n, n, n, 3, 1.0)
+    u = torch.rand(N, device="cuda")
+    x = torch.empty_like(u)
+    for _ in range(3):
+        ops.dense_fe_step(A, 0.01, u, x)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(10):
+        ops.dense_fe_step(A, 0.01, u, x)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 10
+    byt = 4 * N * N + 8 * N
+    out["dense_fe_34"] = {"kernel": "k_dense_fe_bulk", "N": N, "ms": round(ms, 4), "bytes": byt,
+                          "gbs": round(byt / ms / 1e6, 1), "frac": round(byt / ms / 1e6 / peak, 4),
+                          "note": "A (4 N^2 bytes) read once per step, larger than L2"}
+    del A
+    torch.cuda.empty_cache()
+
+    L = ops.csr_laplacian(n, n, n, 3, 1.0)
+    ts = ops.ht_table_size(L[2].numel(), N, 1)
+    keys, vals = ops.ht_build(N, *L, ts)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lu = ops.HtLu(N, n * n, keys, vals, ts, 1.0, -0.05)
+    torch.cuda.synchronize()
+    f_ms = (time.perf_counter() - t0) * 1e3
+    b = torch.rand(N, device="cuda")
+    lu.solve(b, x)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        lu.solve(b, x)
+    s_ms = (time.perf_counter() - t0) * 1e3 / 5
+    out["scheme27_band_34"] = {"N": N, "bandwidth": n * n, "band_bytes": lu.nbytes, "factor_ms": round(f_ms, 2),
+                               "solve_ms": round(s_ms, 3), "matrix": "I - 0.05 L (central, h = 1)"}
+    del lu, keys, vals, L
+    torch.cuda.empty_cache()
+
+    # PIRO's factorization, LUDecomp.ini shape: n = 3 3 3 (+2), l = 5, reference table size
+    nx = 5
+    Nl = nx ** 3
+    norm = float(np.float32(float(np.float32(5.0) / np.float32(nx - 2)) ** 2))  # operatorlaplacian.cpp:33
+    L = ops.csr_laplacian(nx, nx, nx, 3, norm)
+    ts = ops.ht_table_size(L[2].numel(), Nl, 0)
+    keys, vals = ops.ht_build(Nl, *L, ts)
+    k0, v0 = keys.clone(), vals.clone()
+    ops.ht_lu_reference(Nl, keys, vals, ts)
+    reps = 5
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        keys.copy_(k0)
+        vals.copy_(v0)
+        ops.ht_lu_reference(Nl, keys, vals, ts)
+    torch.cuda.synchronize()
+    g_ms = (time.perf_counter() - t0) * 1e3 / reps
+    ref_ms = None
+    try:  # CPU baseline of this row: PIRO's own code (oracle/_ref), when it was built
+        from oracle import oracle as O
+        R = O.Ref()
+        kh = k0.cpu().numpy().astype(np.int32)
+        vh = v0.cpu().numpy()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            k, v = kh.copy(), vh.copy()
+            R.ht_lu(Nl, k, v, ts)
+        ref_ms = (time.perf_counter() - t0) * 1e3 / reps
+        same = bool(np.array_equal(k.astype(np.int64), keys.cpu().numpy()))
+    except (FileNotFoundError, OSError):
+        same = None
+    out["scheme27_reference_5"] = {"N": Nl, "table_slots": ts, "device_ms": round(g_ms, 3),
+                                   "reference_host_ms": None if ref_ms is None else round(ref_ms, 3),
+                                   "same_table": same,
+                                   "note": "reference: PIRO's fill-in and lu_decompHT.cl compiled for the host, "
+                                           "without its per-round full-table transfers"}
+    return out
+
+
 def learned_section(torch, ops, cfg, A, alpha, plain_ms, plain_iters, steps, tflops_peak):
     """Configuration 4: the backward-Euler step with the learned preconditioner
     (the network trained on the device on seeds 100-199 by
@@ -453,6 +540,7 @@ def run_piro(args):
     learned = (learned_section(torch, ops, cfg, A, alpha, ms_step, main["iters"], min(args.steps, 40), tf_peak)
                if rank == 0 else None)
     batched = batched_section(torch, ops, peak) if rank == 0 else None
+    next_rows = next_rows_section(torch, ops, peak) if rank == 0 else None
 
     cpu = None
     fp64 = None
@@ -505,6 +593,7 @@ def run_piro(args):
         "configs": configs,
         "learned": learned,
         "batched": batched,
+        "next_rows": next_rows,
         "fp64_check": fp64,
         "cpu_baseline": cpu,
     }

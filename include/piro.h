@@ -190,6 +190,9 @@ int piro_ht_lu_solve(int64_t N, int64_t bw, void *band, size_t band_bytes, const
 int piro_dense_laplacian(int nx, int ny, int nz, int scheme, float norm, float *A, size_t a_bytes,
                          piro_stream_t stream);
 int piro_dense_fe_step(int64_t N, const float *A, float dt, const float *u, float *out, piro_stream_t stream);
+/* Synchronizes the stream; PIRO_ERR_CUDA if a DENSE step's stage wait (a
+ * bounded wait on the bulk copies, never expected to run out) gave up. */
+int piro_dense_check(piro_stream_t stream);
 
 /* Matrix-free 7-point step, the comparison point for CSR (laplacianscalar.cl:1-21
  * extended by alpha and the Euler update): interior cells

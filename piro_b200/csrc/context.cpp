@@ -894,6 +894,7 @@ extern "C" int piro_assign(piro_ctx *c, piro_buf lhs, piro_op rhs, piro_buf *out
             if (!c->dense || rhs.kind != PIRO_OP_LAPLACIAN)
                 return fail(PIRO_ERR_STATE, "piro_assign: DENSE operator not assembled");
             PK(piro_dense_fe_step(N, c->dense, dt, u, c->partD, c->stream));
+            PK(piro_dense_check(c->stream));
         } else if (c->datatype == 2) {
             if (!c->ht_keys) return fail(PIRO_ERR_STATE, "piro_assign: hash table not built");
             PK(piro_ht_spmv(c->nx, c->ny, c->nz, c->ht_keys, c->ht_vals, c->ht_ts, dt, 1, u, c->partD, c->stream));

@@ -10,20 +10,22 @@
 // kernelsolve::DENSE::TIMESCHEME_11 (src/kernelprocess.cpp:42-66) runs
 // SpMVDENSE.cl -- C[r] = dt * sum, sum += A[r][k]*u[k] for k ascending, every
 // row -- then addVectors.cl, D = u + C.  The step reads N^2 floats: an HBM
-// stream.  Each block takes 32 rows; warps 1-7 stream the next 32 x 256 tile
-// of A (and the matching 256 entries of u) into shared memory while warp 0,
-// one lane per row, adds the current tile in ascending column order, so every
-// row's sum is the reference's sequential FP32 sum (multiply, then add: no
-// fused multiply-add).  Padding past N adds +0, which leaves the sum as it is
-// (a sum that starts at +0 never becomes -0).
+// stream.  One thread per row keeps the reference's sequential FP32 sum
+// (multiply, then add: no fused multiply-add).  A block of 256 rows streams
+// its rows through shared memory 32 columns at a time, three stages deep, with
+// cp.async (any N: 4-byte copies, no alignment needed; zero-filled past N), so
+// that ~100 KB per block are in flight; each warp copies whole 128-byte row
+// segments.  Padding adds +0, which leaves the sum as it is (a sum that starts
+// at +0 never becomes -0).
 #include "common.cuh"
 
 namespace piro {
 namespace {
 
-constexpr int kDenseRows = 32, kDenseCols = 256, kDenseThreads = 256;
-constexpr int kTileStride = kDenseCols + 1;  // conflict-free per-lane row reads
-constexpr size_t kDenseSmem = sizeof(float) * (2 * kDenseRows * kTileStride + 2 * kDenseCols);
+constexpr int kDenseRows = 256, kDenseCols = 32, kDenseStages = 3, kDenseThreads = kDenseRows;
+constexpr int kTileStride = kDenseCols + 1;  // conflict-free per-thread row reads
+constexpr int kStageFloats = kDenseRows * kTileStride + kDenseCols;
+constexpr size_t kDenseSmem = sizeof(float) * kDenseStages * kStageFloats;
 
 __global__ void k_dense_laplacian(int nx, int ny, int nz, int scheme, float vs, float vn, float *__restrict__ A)
 {
@@ -42,46 +44,179 @@ __global__ void k_dense_laplacian(int nx, int ny, int nz, int scheme, float vs, 
     }
 }
 
-__device__ __forceinline__ void dense_load_tile(int64_t N, const float *__restrict__ A, const float *__restrict__ u,
-                                                int64_t R0, int64_t k0, float *__restrict__ sa, float *__restrict__ su)
+__device__ __forceinline__ void cp_async4(float *dst, const float *src, bool valid)
 {
-    const int t = threadIdx.x - 32, nt = kDenseThreads - 32;
-    for (int e = t; e < kDenseRows * kDenseCols; e += nt) {
-        const int r = e / kDenseCols, c = e % kDenseCols;
-        const int64_t gr = R0 + r, gc = k0 + c;
-        sa[r * kTileStride + c] = (gr < N && gc < N) ? __ldcs(A + gr * N + gc) : 0.0f;
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+
+// Stage tile t (columns 32t .. 32t+31 of the block's rows, and u there).
+__device__ __forceinline__ void dense_issue(int64_t N, const float *__restrict__ A, const float *__restrict__ u,
+                                            int64_t R0, int64_t t, float *stage)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t c = t * kDenseCols + lane;
+    const bool cok = c < N;
+    for (int r = warp; r < kDenseRows; r += kDenseThreads / 32) {
+        const int64_t row = R0 + r;
+        const bool ok = cok && row < N;
+        cp_async4(stage + r * kTileStride + lane, ok ? A + row * N + c : A, ok);
     }
-    for (int c = t; c < kDenseCols; c += nt) su[c] = k0 + c < N ? __ldg(u + k0 + c) : 0.0f;
+    if (warp == 0) cp_async4(stage + kDenseRows * kTileStride + lane, cok ? u + c : u, cok);
+}
+
+// The stream when N % 4 == 0 and A, u are 16-byte aligned: per item, 32 rows
+// x BC columns, each row segment (contiguous) one cp.async.bulk into a padded
+// row (float4 reads conflict-free), completion on an mbarrier.  One warp per
+// CTA, lane = row, persistent over row blocks; the (row block, column tile)
+// items stream through S stages without a bubble at row-block boundaries.
+// Measured on B200 (tail-free N): two stages and many CTAs per SM stream
+// best -- 128 columns x 6 CTAs/SM 6.7 TB/s, 256 columns x 3 CTAs/SM
+// 6.1 TB/s -- since each CTA's sequential row sums, not the copies, set its
+// pace; the host picks the shape whose last round of row blocks wastes
+// least.  Every wait is bounded.
+constexpr int kBR = 32;
+constexpr long long kBSpin = 1ll << 22;
+
+template <int BC, int S>
+constexpr size_t bulk_smem() { return sizeof(float) * S * (kBR * (BC + 4) + BC); }
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool bar_try_wait(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity)
+{
+    for (long long i = 0; i < kBSpin; ++i)
+        if (bar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+template <int BC, int S>
+__global__ void __launch_bounds__(32) k_dense_fe_bulk(int64_t N, const float *__restrict__ A, float dt,
+                                                      const float *__restrict__ u, float *__restrict__ out, int *err)
+{
+    constexpr int RS = BC + 4, SF = kBR * RS + BC;
+    extern __shared__ __align__(128) float smb[];
+    __shared__ __align__(8) uint64_t bars[S];
+    const int lane = threadIdx.x;
+    const int64_t nrb = cdiv(N, kBR), ntile = cdiv(N, BC);
+    const int64_t my_rb = nrb > (int64_t)blockIdx.x ? cdiv(nrb - blockIdx.x, gridDim.x) : 0;
+    const int64_t items = my_rb * ntile;
+    if (lane == 0) {
+        for (int s = 0; s < S; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[s])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    auto issue = [&](int64_t i) {
+        const int s = (int)(i % S);
+        const int64_t t = i % ntile, rb = blockIdx.x + (i / ntile) * gridDim.x;
+        const int64_t R0 = rb * kBR, k0 = t * BC;
+        const int nrows = (int)(N - R0 < kBR ? N - R0 : kBR);
+        const uint32_t bytes = (uint32_t)(4 * (N - k0 < BC ? N - k0 : BC));
+        float *stage = smb + s * SF;
+        const uint32_t bar = smem_addr(&bars[s]);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // this lane's reads of the stage first
+        __syncwarp();
+        if (lane == 0)
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                         "r"(bytes * (uint32_t)(nrows + 1))
+                         : "memory");
+        __syncwarp();
+        if (lane < nrows)
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_addr(stage + lane * RS)),
+                "l"(A + (R0 + lane) * N + k0), "r"(bytes), "r"(bar)
+                : "memory");
+        if (lane == 31)
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_addr(stage + kBR * RS)),
+                "l"(u + k0), "r"(bytes), "r"(bar)
+                : "memory");
+    };
+    int64_t issued = 0;
+    for (; issued < S && issued < items; ++issued) issue(issued);
+    float sum = 0.0f;
+    int64_t i = 0;
+    bool ok = true;
+    for (; i < items; ++i) {
+        const int s = (int)(i % S);
+        if (!bar_wait(smem_addr(&bars[s]), (uint32_t)((i / S) & 1))) {
+            ok = false;
+            break;
+        }
+        const int64_t t = i % ntile, rb = blockIdx.x + (i / ntile) * gridDim.x;
+        const int64_t R0 = rb * kBR, k0 = t * BC;
+        const int ncols = (int)(N - k0 < BC ? N - k0 : BC);
+        const float *stage = smb + s * SF;
+        if (R0 + lane < N) {
+            const float4 *a = reinterpret_cast<const float4 *>(stage + lane * RS);
+            const float4 *uu = reinterpret_cast<const float4 *>(stage + kBR * RS);
+#pragma unroll 8
+            for (int c = 0; c < ncols / 4; ++c) {
+                const float4 av = a[c], uv = uu[c];
+                sum = __fadd_rn(sum, __fmul_rn(av.x, uv.x));
+                sum = __fadd_rn(sum, __fmul_rn(av.y, uv.y));
+                sum = __fadd_rn(sum, __fmul_rn(av.z, uv.z));
+                sum = __fadd_rn(sum, __fmul_rn(av.w, uv.w));
+            }
+        }
+        if (t == ntile - 1) {
+            const int64_t r = R0 + lane;
+            if (r < N) out[r] = __fadd_rn(u[r], __fmul_rn(dt, sum));
+            sum = 0.0f;
+        }
+        __syncwarp();
+        if (issued < items) issue(issued++);
+    }
+    if (!ok) {
+        if (lane == 0) atomicExch(err, 1);
+        for (; i < issued; ++i) (void)bar_wait(smem_addr(&bars[i % S]), (uint32_t)((i / S) & 1));
+    }
 }
 
 __global__ void __launch_bounds__(kDenseThreads) k_dense_fe(int64_t N, const float *__restrict__ A, float dt,
                                                             const float *__restrict__ u, float *__restrict__ out)
 {
     extern __shared__ float sm[];
-    float *sa0 = sm, *sa1 = sm + kDenseRows * kTileStride;
-    float *su0 = sm + 2 * kDenseRows * kTileStride, *su1 = su0 + kDenseCols;
     const int64_t R0 = (int64_t)blockIdx.x * kDenseRows;
     const int64_t ntile = cdiv(N, kDenseCols);
-    if (threadIdx.x >= 32) dense_load_tile(N, A, u, R0, 0, sa0, su0);
-    __syncthreads();
+    for (int s = 0; s < kDenseStages - 1; ++s) {
+        if (s < ntile) dense_issue(N, A, u, R0, s, sm + s * kStageFloats);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
     float sum = 0.0f;
     for (int64_t t = 0; t < ntile; ++t) {
-        const bool odd = t & 1;
-        if (threadIdx.x >= 32) {
-            if (t + 1 < ntile) dense_load_tile(N, A, u, R0, (t + 1) * kDenseCols, odd ? sa0 : sa1, odd ? su0 : su1);
-        } else {
-            const float *a = (odd ? sa1 : sa0) + threadIdx.x * kTileStride;
-            const float *uu = odd ? su1 : su0;
-#pragma unroll 16
-            for (int c = 0; c < kDenseCols; ++c) sum = __fadd_rn(sum, __fmul_rn(a[c], uu[c]));
-        }
+        const int64_t tn = t + kDenseStages - 1;
+        if (tn < ntile) dense_issue(N, A, u, R0, tn, sm + (int)(tn % kDenseStages) * kStageFloats);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kDenseStages - 1) : "memory");
         __syncthreads();
+        const float *st = sm + (int)(t % kDenseStages) * kStageFloats;
+        const float *a = st + threadIdx.x * kTileStride, *uu = st + kDenseRows * kTileStride;
+#pragma unroll
+        for (int c = 0; c < kDenseCols; ++c) sum = __fadd_rn(sum, __fmul_rn(a[c], uu[c]));
+        __syncthreads();  // the stage is refilled by the next iteration's issue
     }
-    if (threadIdx.x < 32) {
-        const int64_t r = R0 + threadIdx.x;
-        if (r < N) out[r] = __fadd_rn(u[r], __fmul_rn(dt, sum));
-    }
+    const int64_t r = R0 + threadIdx.x;
+    if (r < N) out[r] = __fadd_rn(u[r], __fmul_rn(dt, sum));
 }
+
+int *dense_err_flag[64] = {nullptr};  // per device: a bulk-stage wait timed out
 
 }  // namespace
 }  // namespace piro
@@ -108,13 +243,62 @@ extern "C" int piro_dense_fe_step(int64_t N, const float *A, float dt, const flo
     PIRO_ARG(N >= 1 && A && u && out && u != out, "piro_dense_fe_step: bad arguments");
     PIRO_ARG(cdiv(N, kDenseRows) < 2147483647, "piro_dense_fe_step: N too large");
     static bool attr_set[64] = {false};
+    int *(&err_flag)[64] = dense_err_flag;
     int dev = 0;
     PIRO_CUDA(cudaGetDevice(&dev));
-    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    PIRO_ARG(dev >= 0 && dev < 64, "piro_dense_fe_step: device index");
+    static int occ_a[64], occ_b[64];
+    if (!attr_set[dev]) {
         PIRO_CUDA(cudaFuncSetAttribute(k_dense_fe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDenseSmem));
+        PIRO_CUDA(cudaFuncSetAttribute(k_dense_fe_bulk<256, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)bulk_smem<256, 2>()));
+        PIRO_CUDA(cudaFuncSetAttribute(k_dense_fe_bulk<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)bulk_smem<128, 2>()));
+        PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a[dev], k_dense_fe_bulk<256, 2>, 32,
+                                                                bulk_smem<256, 2>()));
+        PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b[dev], k_dense_fe_bulk<128, 2>, 32,
+                                                                bulk_smem<128, 2>()));
+        PIRO_CUDA(cudaMalloc(&err_flag[dev], sizeof(int)));
+        PIRO_CUDA(cudaMemset(err_flag[dev], 0, sizeof(int)));
         attr_set[dev] = true;
     }
-    k_dense_fe<<<(unsigned)cdiv(N, kDenseRows), kDenseThreads, kDenseSmem, as_stream(stream)>>>(N, A, dt, u, out);
+    cudaStream_t st = as_stream(stream);
+    const bool bulk = N % 4 == 0 && ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(u)) & 15) == 0;
+    if (bulk && occ_a[dev] >= 1 && occ_b[dev] >= 1) {
+        // time ~ rounds of row blocks x (CTAs per SM / measured stream rate):
+        // 256 columns at up to 3 CTAs/SM ~6.1 TB/s, 128 columns at up to 6 ~6.7 TB/s
+        const int64_t nrb = cdiv(N, kBR), sms = sm_count();
+        const int ga = occ_a[dev] < 3 ? occ_a[dev] : 3, gb = occ_b[dev] < 6 ? occ_b[dev] : 6;
+        const double ta = (double)cdiv(nrb, ga * sms) * ga / 6.1, tb = (double)cdiv(nrb, gb * sms) * gb / 6.7;
+        if (ta <= tb) {
+            const int64_t grid = nrb < ga * sms ? nrb : ga * sms;
+            k_dense_fe_bulk<256, 2><<<(unsigned)grid, 32, bulk_smem<256, 2>(), st>>>(N, A, dt, u, out, err_flag[dev]);
+        } else {
+            const int64_t grid = nrb < gb * sms ? nrb : gb * sms;
+            k_dense_fe_bulk<128, 2><<<(unsigned)grid, 32, bulk_smem<128, 2>(), st>>>(N, A, dt, u, out, err_flag[dev]);
+        }
+        PIRO_CHECK_LAUNCH("k_dense_fe_bulk");
+        return PIRO_OK;
+    }
+    k_dense_fe<<<(unsigned)cdiv(N, kDenseRows), kDenseThreads, kDenseSmem, st>>>(N, A, dt, u, out);
     PIRO_CHECK_LAUNCH("k_dense_fe");
+    return PIRO_OK;
+}
+
+extern "C" int piro_dense_check(piro_stream_t stream)
+{
+    int dev = 0;
+    PIRO_CUDA(cudaGetDevice(&dev));
+    PIRO_ARG(dev >= 0 && dev < 64, "piro_dense_check: device index");
+    if (!dense_err_flag[dev]) return PIRO_OK;
+    int h = 0;
+    cudaStream_t st = as_stream(stream);
+    PIRO_CUDA(cudaMemcpyAsync(&h, dense_err_flag[dev], sizeof(int), cudaMemcpyDeviceToHost, st));
+    PIRO_CUDA(cudaStreamSynchronize(st));
+    if (h) {
+        PIRO_CUDA(cudaMemsetAsync(dense_err_flag[dev], 0, sizeof(int), st));
+        set_error("piro_dense_fe_step: a stage wait timed out");
+        return PIRO_ERR_CUDA;
+    }
     return PIRO_OK;
 }

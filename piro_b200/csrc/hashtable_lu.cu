@@ -21,6 +21,10 @@
 // that factorization on the device with no per-round table round trips (the
 // reference uploads and downloads the whole table each round).  The fill-in
 // is one device thread, because slot placement depends on the insertion order.
+// When the table fits in shared memory (up to ~18 K slots, which covers the
+// grids the reference runs this scheme on), the whole factorization is one
+// block with the table in shared memory; otherwise it is a gather, fill-in and
+// elimination launch per round on the table in HBM.
 //
 // piro_ht_lu_factor / piro_ht_lu_solve make scheme 27 return a solution.  The
 // table is the input format only: one pass over its slots scatters
@@ -64,6 +68,22 @@ __device__ __forceinline__ float ht_find(int64_t key, const int64_t *__restrict_
     }
     *slot = -1;
     return 0.0f;
+}
+
+// Where methods::lookupandset would put key now: -1 if present; the first
+// deleted slot on the probe path, else the empty slot that ends it; -2 if
+// the table has neither.
+__device__ __forceinline__ int64_t ht_candidate(int64_t key, const int64_t *keys, int64_t ts)
+{
+    int64_t h = key % ts, first_deleted = -1;
+    for (int64_t a = 0; a <= ts; ++a) {
+        const int64_t k = keys[h];
+        if (k == key) return -1;
+        if (k == kEmpty) return first_deleted != -1 ? first_deleted : h;
+        if (k == kDeleted && first_deleted == -1) first_deleted = h;
+        h = h + 1 == ts ? 0 : h + 1;
+    }
+    return first_deleted != -1 ? first_deleted : -2;
 }
 
 // methods::lookupandset with value 0: insert the key if absent.  false if the
@@ -146,6 +166,110 @@ __global__ void k_lu_round(int64_t N, int64_t ro, int64_t *keys, float *vals, in
         if ((double)fabsf(val) < 1e-6) keys[hk] = kDeleted;
     }
 }
+
+// The whole factorization in one block, the table in shared memory (when
+// keys, values and the round's gathers fit): the same gather, fill-in and
+// elimination per round, separated by __syncthreads instead of launches, and
+// every probe served by shared memory instead of a dependent L2 load.
+__global__ void __launch_bounds__(1024) k_lu_reference_smem(int64_t N, int64_t *__restrict__ keys_g,
+                                                            float *__restrict__ vals_g, int64_t ts, int *err)
+{
+    extern __shared__ __align__(16) unsigned char lu_smem[];
+    int64_t *keys = reinterpret_cast<int64_t *>(lu_smem);
+    float *vals = reinterpret_cast<float *>(keys + ts);
+    float *prow = vals + ts;
+    float *fac = prow + N;
+    int32_t *cols = reinterpret_cast<int32_t *>(fac + N);
+    __shared__ int s_err, s_nc;
+    __shared__ int32_t s_cand[1024];
+    for (int64_t s = threadIdx.x; s < ts; s += blockDim.x) {
+        keys[s] = keys_g[s];
+        vals[s] = vals_g[s];
+    }
+    if (threadIdx.x == 0) s_err = 0;
+    __syncthreads();
+    for (int64_t ro = 0; ro < N - 1; ++ro) {
+        const int64_t ncol = N - ro, nrow = ncol - 1;
+        for (int64_t t = threadIdx.x; t < ncol + nrow; t += blockDim.x) {
+            int64_t sl;
+            if (t < ncol)
+                prow[t] = ht_find(ro * N + ro + t, keys, vals, ts, &sl);
+            else
+                fac[t - ncol] = ht_find((ro + 1 + t - ncol) * N + ro, keys, vals, ts, &sl);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int nc = 0;
+            for (int64_t co = ro; co < N; ++co)
+                if ((double)fabsf(prow[co - ro]) > 1e-6) cols[nc++] = (int32_t)co;
+            s_nc = nc;
+        }
+        __syncthreads();
+        // Fill-in, in the reference's order (rows, then columns), by chunks of
+        // blockDim pairs: every thread walks its key's probe path at once
+        // (present, or the slot lookupandset would take now); then thread 0
+        // places the absent keys in order.  A slot taken by an earlier key of
+        // the chunk moves the placement on to the next deleted or empty slot,
+        // which is where the sequential walk would stop.
+        const int64_t npairs = nrow * s_nc;
+        for (int64_t base = 0; base < npairs && !s_err; base += blockDim.x) {
+            const int64_t p = base + threadIdx.x;
+            int32_t cand = -1;
+            if (p < npairs && fac[p / s_nc] != 0.0f)
+                cand = (int32_t)ht_candidate((ro + 1 + p / s_nc) * N + cols[p % s_nc], keys, ts);
+            s_cand[threadIdx.x] = cand;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                const int64_t m = npairs - base < blockDim.x ? npairs - base : blockDim.x;
+                for (int64_t q = 0; q < m && !s_err; ++q) {
+                    const int32_t c0 = s_cand[q];
+                    if (c0 == -1) continue;
+                    if (c0 == -2) {
+                        s_err = 1;
+                        break;
+                    }
+                    int64_t h = c0, a = 0;
+                    while (keys[h] >= 0 && a < ts) {
+                        h = h + 1 == ts ? 0 : h + 1;
+                        ++a;
+                    }
+                    if (a == ts) {
+                        s_err = 1;
+                        break;
+                    }
+                    const int64_t pq = base + q;
+                    keys[h] = (ro + 1 + pq / s_nc) * N + cols[pq % s_nc];
+                    vals[h] = 0.0f;
+                }
+            }
+            __syncthreads();
+        }
+        if (s_err) break;
+        const float piv = prow[0];
+        if (piv != 0.0f) {
+            for (int64_t t = threadIdx.x; t < nrow * ncol; t += blockDim.x) {
+                const int64_t i = t / ncol, j = t % ncol;
+                const float factor = fac[i];
+                if (factor == 0.0f) continue;
+                int64_t hk;
+                float val = ht_find((ro + 1 + i) * N + ro + j, keys, vals, ts, &hk);
+                if (hk < 0) continue;
+                val = __fsub_rn(val, __fmul_rn(__fdiv_rn(factor, piv), prow[j]));
+                vals[hk] = val;
+                if ((double)fabsf(val) < 1e-6) keys[hk] = kDeleted;
+            }
+        }
+        __syncthreads();
+    }
+    for (int64_t s = threadIdx.x; s < ts; s += blockDim.x) {
+        keys_g[s] = keys[s];
+        vals_g[s] = vals[s];
+    }
+    if (threadIdx.x == 0 && s_err) *err = 1;
+}
+
+size_t lu_reference_smem_bytes(int64_t N, int64_t ts) { return (size_t)ts * 12 + (size_t)N * 12; }
+constexpr size_t kLuSmemMax = 220 * 1024;
 
 // ---------------------------------------------------------------- banded LU and substitution
 
@@ -419,7 +543,16 @@ extern "C" int piro_ht_lu_reference(int64_t N, int64_t *keys, float *vals, int64
     if (e == cudaSuccess) e = cudaMalloc(&cols, sizeof(int32_t) * (size_t)N);
     if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), st);
     float *fac = prow + N;
-    for (int64_t ro = 0; ro < N - 1 && e == cudaSuccess; ++ro) {
+    const size_t smem = lu_reference_smem_bytes(N, ts);
+    const bool one_block = smem <= kLuSmemMax;
+    if (e == cudaSuccess && one_block) {
+        e = cudaFuncSetAttribute(k_lu_reference_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) {
+            k_lu_reference_smem<<<1, 1024, smem, st>>>(N, keys, vals, ts, err);
+            e = cudaGetLastError();
+        }
+    }
+    for (int64_t ro = 0; !one_block && ro < N - 1 && e == cudaSuccess; ++ro) {
         const int64_t ncol = N - ro, nrow = ncol - 1;
         k_lu_gather<<<grid_for(ncol + nrow, 256, 4), 256, 0, st>>>(N, ro, ncol, nrow, keys, vals, ts, prow, fac);
         k_lu_fill<<<1, 1, 0, st>>>(N, ro, keys, vals, ts, prow, fac, cols, err);

@@ -142,6 +142,10 @@ def dense_fe_step(A, dt, u, out=None):
     return out
 
 
+def dense_check():
+    check(lib().piro_dense_check(_stream()), "piro_dense_check")
+
+
 class HtLu:
     """Scheme 27 with a solution: shift*I + scale*M (M the table's matrix)
     factorized in a dense band of bandwidth bw; solve(b) -> x."""

@@ -26,7 +26,11 @@ def test_dense_laplacian_and_step_match_reference(cuda, s):
     assert f32_bits_equal(out.cpu().numpy(), g[f"dense_D_s{s}"])
 
 
-@pytest.mark.parametrize("n", [(7, 5, 3), (20, 18, 16), (33, 9, 11)])
+# N % 4 == 0 takes the bulk-copy path (120 rows in the fixture test, 5760 and
+# 4352 here: the 256-column shape; 14240 = 445 row blocks of 32, where one
+# round of 6 CTAs/SM beats two rounds of 3 on 148 SMs: the 128-column shape);
+# 105 and 3267 the 4-byte cp.async path
+@pytest.mark.parametrize("n", [(7, 5, 3), (20, 18, 16), (33, 9, 11), (17, 16, 16), (89, 20, 8)])
 def test_dense_step_matches_oracle(cuda, oracle, n):
     """Ragged sizes (N not a multiple of the 32-row or 256-column tiles) and a
     larger matrix (N = 5760, 133 MB)."""
@@ -39,6 +43,7 @@ def test_dense_step_matches_oracle(cuda, oracle, n):
     assert f32_bits_equal(A.cpu().numpy(), Ah)
     u = np.random.default_rng(5).standard_normal(nx * ny * nz).astype(np.float32)
     out = ops.dense_fe_step(A, 0.013, torch.from_numpy(u).cuda())
+    ops.dense_check()
     assert f32_bits_equal(out.cpu().numpy(), oracle.fe_dense(Ah, 0.013, u)[1])
 
 

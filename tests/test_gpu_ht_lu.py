@@ -11,13 +11,13 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-@pytest.mark.parametrize("n", [(6, 5, 4), (5, 5, 5), (7, 6, 5)])
-def test_ht_lu_matches_reference(cuda, n):
+@pytest.mark.parametrize("n,suffix", [((6, 5, 4), ""), ((5, 5, 5), ""), ((7, 6, 5), ""), ((6, 5, 4), "_ts30011")])
+def test_ht_lu_matches_reference(cuda, n, suffix):
     import torch
     from piro_b200 import ops
     g = np.load(os.path.join(HERE, "golden", "ht_lu.npz"))
     nx, ny, nz = n
-    tag = f"{nx}x{ny}x{nz}"
+    tag = f"{nx}x{ny}x{nz}{suffix}"
     N, ts = nx * ny * nz, int(g[f"ts_{tag}"])
     A = ops.csr_laplacian(nx, ny, nz, 3, 1.0)
     keys, vals = ops.ht_build(N, *A, ts)
