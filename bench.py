@@ -644,7 +644,9 @@ def run_reference(args):
 def run_profile_case(args):
     """Small fixed cases for ncu captures (no timing, no JSON): `be` solves the
     128^3 backward-Euler step twice, `spmv` runs each 256^3 forward-Euler
-    kernel four times."""
+    kernel four times, `dense` three DENSE steps at N = 12,288 (a 604 MB
+    matrix), `learned` two learned-preconditioner solves of the 128^3 step,
+    `batched` two steps of a 64-member batch."""
     import torch
 
     from piro_b200 import ops
@@ -661,6 +663,35 @@ def run_profile_case(args):
             info = s.solve(b, x, rtol=1e-8)
         print("be", s.inner_operator, info.inner_iterations, info.rel_residual)
         s.close()
+    elif args.profile == "dense":
+        A = ops.dense_laplacian(32, 24, 16, 3, 1.0)
+        u = torch.rand(32 * 24 * 16, device="cuda")
+        x = torch.empty_like(u)
+        for _ in range(3):
+            ops.dense_fe_step(A, 0.01, u, x)
+        ops.dense_check()
+        print("dense ok")
+    elif args.profile == "learned":
+        cfg = W.heat_be_128()
+        nx, ny, nz = cfg["n"]
+        A, alpha = be_problem(torch, ops, cfg)
+        net = ops.PCNet(seed=0)
+        net.set_params(np.load(os.path.join(ROOT, "piro_b200", "data", "pcnet_be128.npy")))
+        s = ops.BESolver(nx, ny, nz, A, alpha, stencil=(float(cfg["dt"]), 1.0))
+        s.set_preconditioner(net)
+        b = torch.from_numpy(cfg["u0"]).cuda()
+        x = torch.empty_like(b)
+        for _ in range(2):
+            info = s.solve(b, x, rtol=1e-8)
+        print("learned", info.inner_iterations, info.rel_residual)
+        s.close()
+        net.close()
+    elif args.profile == "batched":
+        cfg = W.batched(count=64)
+        B = ops.Batch(cfg["n"], cfg["alpha"], cfg["dt"], cfg["scheme"])
+        B.set_fields(W.pack_batch(cfg["fields"], B.offsets, B.total))
+        B.step(2)
+        print("batched ok")
     else:
         cfg = W.spmv_256()
         nx, ny, nz = cfg["n"]
@@ -683,7 +714,8 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="piro", choices=["piro", "reference"])
-    ap.add_argument("--profile", choices=["be", "spmv"], help="run a small fixed case for ncu, print no JSON")
+    ap.add_argument("--profile", choices=["be", "spmv", "dense", "learned", "batched"],
+                    help="run a small fixed case for ncu, print no JSON")
     args = ap.parse_args()
     if args.profile:
         run_profile_case(args)
