@@ -39,6 +39,20 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def profiled_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from its committed ncu summary
+    (profiles/<kernel>_128.md, line `traffic_bytes_per_launch: N`), or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_128.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def load_tflops_peak():
     """Dense BF16 TFLOP/s (burst: the network applies are short kernels)."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -585,7 +599,10 @@ def run_piro(args):
         "roofline": {"kernel": k_name, "bound": "hbm", "achieved": round(achieved, 1),
                      "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "peak_kind": peak_kind, "bytes_per_launch": bytes_spmv,
-                     "avg_launch_ms": avg_spmv_ms, "launches": main["spmv_launches"], "traffic": None},
+                     "avg_launch_ms": avg_spmv_ms, "launches": main["spmv_launches"],
+                     "traffic": profiled_traffic(k_name),
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture of the same "
+                                       "kernel on the same 128^3 step (profiles/k_be_persistent_128.md)"},
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms/step", "h2d_bytes_per_step": 4 * N, "d2h_bytes_per_step": 4 * N},
         "gpu_launches": launches,
         "clocks": ck,
