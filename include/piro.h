@@ -152,6 +152,15 @@ int piro_coo_fe_step(int64_t N, int64_t nnz, const int32_t *rows, const int32_t 
  * (kernelsolve::HT::TIMESCHEME_11, src/kernelprocess.cpp:68-91). */
 int piro_ht_spmv(int nx, int ny, int nz, const int64_t *keys, const float *vals, int64_t ts, float dt, int fe,
                  const float *u, float *out, piro_stream_t stream);
+/* The same step with the rows taken in the order of their keys' home slot
+ * (i*N + i) mod ts, as piro_ht_row_order gives it (int32 order[N], computed
+ * once per table; workspace piro_ht_row_order_workspace bytes): the table is
+ * then read as a window moving through it, not at random.  Same results bit
+ * for bit (each row's sum is computed the same way). */
+int piro_ht_row_order_workspace(int64_t N, int64_t ts, size_t *bytes);
+int piro_ht_row_order(int64_t N, int64_t ts, int32_t *order, void *work, size_t work_bytes, piro_stream_t stream);
+int piro_ht_spmv_ordered(int nx, int ny, int nz, const int64_t *keys, const float *vals, int64_t ts, float dt, int fe,
+                         const int32_t *order, const float *u, float *out, piro_stream_t stream);
 
 /* Scheme 27 (TIMESCHEME 12 + solver 27) on a table built by piro_ht_build
  * (int64 keys, -1 empty; -2 marks a deleted key).  piro_ht_lu_reference is

@@ -13,6 +13,11 @@
 #include <algorithm>
 
 namespace piro {
+int scan_rowptr_inplace(int64_t N, int32_t *rowptr, void *work, size_t work_bytes, cudaStream_t s);
+size_t scan_workspace_bytes(int64_t N);
+}  // namespace piro
+
+namespace piro {
 namespace {
 
 // mode 0: SpMVCSR (out = u + sum), mode 1: SpMVCSR_I1 (out = u - sum).
@@ -96,11 +101,11 @@ __global__ void k_scale_add(int64_t n, float dt, const float *acc, const float *
     }
 }
 
-// HT lookup with linear probing (SpMVHT.cl:1-20); bounded by ts probes.
-__device__ __forceinline__ float ht_get(int64_t key, const int64_t *__restrict__ keys, const float *__restrict__ vals,
-                                        int64_t ts)
+// HT lookup with linear probing (SpMVHT.cl:1-20) from slot h on; bounded by
+// ts probes.
+__device__ __forceinline__ float ht_get_from(int64_t key, int64_t h, const int64_t *__restrict__ keys,
+                                             const float *__restrict__ vals, int64_t ts)
 {
-    int64_t h = key % ts;
     for (int64_t a = 0; a < ts; ++a) {
         const int64_t k = __ldg(keys + h);
         if (k == key) return __ldg(vals + h);
@@ -110,35 +115,81 @@ __device__ __forceinline__ float ht_get(int64_t key, const int64_t *__restrict__
     return 0.0f;
 }
 
+// Row i of the 7-point matrix (row order[j] of thread j when ordered): the
+// candidate columns c = i + off, off in
+// {-nx*ny, -nx, -1, 0, 1, nx, nx*ny}, in ascending order; absent keys give 0,
+// adding 0*u exactly as the reference's loop over the row does.  The keys
+// i*N + c have home slots (i*N + i + off) mod ts: one 64-bit modulo per row,
+// then small offsets (|off| < ts, since ts > nnz > N).  The seven first probes
+// are issued together, then the seven value loads; only a collision (a first
+// probe holding another key) walks on.
+template <bool kOrdered>
 __global__ void k_ht_spmv(int nx, int ny, int nz, int64_t N, const int64_t *__restrict__ keys,
-                          const float *__restrict__ vals, int64_t ts, float dt, int fe, const float *__restrict__ u,
-                          float *__restrict__ out)
+                          const float *__restrict__ vals, int64_t ts, float dt, int fe,
+                          const int32_t *__restrict__ order, const float *__restrict__ u, float *__restrict__ out)
 {
     const int64_t sxy = (int64_t)nx * ny;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < N; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = kOrdered ? (int64_t)__ldg(order + j) : j;
         const int z = (int)(i / sxy);
         const int64_t rem = i - (int64_t)z * sxy;
         const int y = (int)(rem / nx);
         const int x = (int)(rem - (int64_t)y * nx);
-        // candidate columns in ascending order
-        int64_t cand[7];
-        int n = 0;
-        if (z > 0) cand[n++] = i - sxy;
-        if (y > 0) cand[n++] = i - nx;
-        if (x > 0) cand[n++] = i - 1;
-        cand[n++] = i;
-        if (x < nx - 1) cand[n++] = i + 1;
-        if (y < ny - 1) cand[n++] = i + nx;
-        if (z < nz - 1) cand[n++] = i + sxy;
-        float sum = 0.0f;
-        for (int t = 0; t < n; ++t) {
-            // absent keys give 0, adding 0*u exactly as the reference's full column loop does
-            const float h = ht_get(i * N + cand[t], keys, vals, ts);
-            sum = __fadd_rn(sum, __fmul_rn(h, __ldg(u + cand[t])));
+        // the seven directions in ascending column order, each present or not
+        const int64_t off[7] = {-sxy, -(int64_t)nx, -1, 0, 1, (int64_t)nx, sxy};
+        const bool ok[7] = {z > 0, y > 0, x > 0, true, x < nx - 1, y < ny - 1, z < nz - 1};
+        const int64_t kd = i * N + i, base = kd % ts;
+        int64_t h[7], k[7];
+#pragma unroll
+        for (int t = 0; t < 7; ++t) {
+            if (ok[t]) {
+                int64_t hh = base + off[t];
+                hh += hh < 0 ? ts : 0;
+                hh -= hh >= ts ? ts : 0;
+                h[t] = hh;
+                k[t] = __ldg(keys + hh);
+            }
         }
+        float v[7];
+#pragma unroll
+        for (int t = 0; t < 7; ++t) {
+            if (ok[t]) {
+                const int64_t key = kd + off[t];
+                if (k[t] == key)
+                    v[t] = __ldg(vals + h[t]);
+                else if (k[t] == -1)
+                    v[t] = 0.0f;
+                else
+                    v[t] = ht_get_from(key, h[t] + 1 == ts ? 0 : h[t] + 1, keys, vals, ts);
+            }
+        }
+        float sum = 0.0f;
+#pragma unroll
+        for (int t = 0; t < 7; ++t)
+            if (ok[t]) sum = __fadd_rn(sum, __fmul_rn(v[t], __ldg(u + i + off[t])));
         const float c = __fmul_rn(dt, sum);
         out[i] = fe ? __fadd_rn(u[i], c) : c;
     }
+}
+
+// Rows by home slot: rows whose keys sit close in the table run close in
+// time, so that the table is read as a moving window of about +-nx*ny slots
+// (resident in L2) instead of at random.  Counting sort on buckets of
+// kOrderBucket slots of the home slot (i*N + i) mod ts; the order inside a
+// bucket is whatever the atomics give (each row's result does not depend on
+// it).
+constexpr int kOrderShift = 7;  // 128-slot buckets
+
+__global__ void k_order_count(int64_t N, int64_t ts, int32_t *__restrict__ cnt)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(cnt + 1 + (((i * N + i) % ts) >> kOrderShift), 1);
+}
+
+__global__ void k_order_scatter(int64_t N, int64_t ts, int32_t *__restrict__ cursor, int32_t *__restrict__ order)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        order[atomicAdd(cursor + (((i * N + i) % ts) >> kOrderShift), 1)] = (int32_t)i;
 }
 
 // Matrix-free 7-point update: one (x, y) column per thread over a run of
@@ -301,7 +352,52 @@ extern "C" int piro_ht_spmv(int nx, int ny, int nz, const int64_t *keys, const f
 {
     PIRO_ARG(grid_ok(nx, ny, nz) && keys && vals && ts > 0 && u && out && u != out, "piro_ht_spmv: bad arguments");
     const int64_t N = (int64_t)nx * ny * nz;
-    k_ht_spmv<<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(nx, ny, nz, N, keys, vals, ts, dt, fe, u, out);
+    k_ht_spmv<false><<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(nx, ny, nz, N, keys, vals, ts, dt, fe, nullptr,
+                                                                         u, out);
+    PIRO_CHECK_LAUNCH("k_ht_spmv");
+    return PIRO_OK;
+}
+
+extern "C" int piro_ht_row_order_workspace(int64_t N, int64_t ts, size_t *bytes)
+{
+    PIRO_ARG(bytes && N > 0 && ts > 0, "piro_ht_row_order_workspace: bad arguments");
+    const int64_t nbk = (ts >> kOrderShift) + 1;
+    *bytes = sizeof(int32_t) * (size_t)(nbk + 1) + 256 + scan_workspace_bytes(nbk);
+    return PIRO_OK;
+}
+
+extern "C" int piro_ht_row_order(int64_t N, int64_t ts, int32_t *order, void *work, size_t work_bytes,
+                                 piro_stream_t stream)
+{
+    PIRO_ARG(N > 0 && N < INT32_MAX && ts > 0 && order && work, "piro_ht_row_order: bad arguments");
+    PIRO_ARG(N <= INT64_MAX / (N + 1), "piro_ht_row_order: row*N+col overflows int64");
+    size_t need = 0;
+    piro_ht_row_order_workspace(N, ts, &need);
+    PIRO_ARG(work_bytes >= need, "piro_ht_row_order: workspace too small");
+    const int64_t nbk = (ts >> kOrderShift) + 1;
+    cudaStream_t s = as_stream(stream);
+    int32_t *cnt = static_cast<int32_t *>(work);  // [nbk + 1]: cnt[0] = 0, bucket counts after it
+    void *scan_work = static_cast<char *>(work) + (sizeof(int32_t) * (size_t)(nbk + 1) + 255) / 256 * 256;
+    PIRO_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * (size_t)(nbk + 1), s));
+    k_order_count<<<grid_for(N, 256, 8), 256, 0, s>>>(N, ts, cnt);
+    PIRO_CHECK_LAUNCH("k_order_count");
+    const int rc = scan_rowptr_inplace(nbk, cnt, scan_work, scan_workspace_bytes(nbk), s);
+    if (rc) return rc;
+    // cnt[b] is now the first position of bucket b: use it as the cursor
+    k_order_scatter<<<grid_for(N, 256, 8), 256, 0, s>>>(N, ts, cnt, order);
+    PIRO_CHECK_LAUNCH("k_order_scatter");
+    return PIRO_OK;
+}
+
+extern "C" int piro_ht_spmv_ordered(int nx, int ny, int nz, const int64_t *keys, const float *vals, int64_t ts,
+                                    float dt, int fe, const int32_t *order, const float *u, float *out,
+                                    piro_stream_t stream)
+{
+    PIRO_ARG(grid_ok(nx, ny, nz) && keys && vals && ts > 0 && order && u && out && u != out,
+             "piro_ht_spmv_ordered: bad arguments");
+    const int64_t N = (int64_t)nx * ny * nz;
+    k_ht_spmv<true><<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(nx, ny, nz, N, keys, vals, ts, dt, fe, order,
+                                                                        u, out);
     PIRO_CHECK_LAUNCH("k_ht_spmv");
     return PIRO_OK;
 }

@@ -192,6 +192,22 @@ def ht_spmv(nx, ny, nz, keys, vals, dt, u, out, fe=False):
     return out
 
 
+def ht_row_order(N, ts):
+    """Rows by the home slot of their keys (for ht_spmv(order=...))."""
+    n = C.c_size_t()
+    check(lib().piro_ht_row_order_workspace(N, ts, C.byref(n)), "piro_ht_row_order_workspace")
+    work = torch.empty(n.value, dtype=torch.uint8, device="cuda")
+    order = torch.empty(N, dtype=i32, device="cuda")
+    check(lib().piro_ht_row_order(N, ts, _p(order), _p(work), n.value, _stream()), "piro_ht_row_order")
+    return order
+
+
+def ht_spmv_ordered(nx, ny, nz, keys, vals, dt, order, u, out, fe=False):
+    check(lib().piro_ht_spmv_ordered(nx, ny, nz, _p(keys), _p(vals), keys.numel(), float(dt), int(fe), _p(order),
+                                     _p(u), _p(out), _stream()), "piro_ht_spmv_ordered")
+    return out
+
+
 def stencil_fe_step(nx, ny, nz, dt, u, out, alpha=None, idx2=1.0, idy2=1.0, idz2=1.0):
     check(lib().piro_stencil_fe_step(nx, ny, nz, idx2, idy2, idz2, float(dt), _p(alpha), _p(u), _p(out), _stream()),
           "piro_stencil_fe_step")

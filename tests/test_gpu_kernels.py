@@ -109,6 +109,11 @@ def test_step_kernels_vs_golden(cuda, golden_grids):
             hv = dev(torch, g[f"ht_vals_{t}"])
             ops.ht_spmv(nx, ny, nz, keys, hv, 0.01, u, out)
             assert f32_bits_equal(h(out), g[f"spmvht_{t}"])
+            order = ops.ht_row_order(N, keys.numel())
+            assert np.array_equal(np.sort(h(order)), np.arange(N))  # a permutation of the rows
+            out2 = torch.full_like(out, float("nan"))
+            ops.ht_spmv_ordered(nx, ny, nz, keys, hv, 0.01, order, u, out2)
+            assert f32_bits_equal(h(out2), g[f"spmvht_{t}"])
             val = A[2].clone()
             ops.csr_rowscale(A[0], val, dev(torch, g[f"in_alpha_{t}"]))
             assert f32_bits_equal(h(val), g[f"spmdsm_{t}"])
@@ -231,6 +236,13 @@ def test_fe_steps_match_oracle(cuda, oracle, n):
     out = torch.empty_like(u)
     for _ in range(3):
         ops.ht_spmv(nx, ny, nz, keys, vals, dt, u, out, fe=True)
+        ops.set_bc(idx, bc, out)
+        u, out = out, u
+    assert f32_bits_equal(h(u), ref_ht)
+    order = ops.ht_row_order(N, ts)
+    u = dev(torch, u0)
+    for _ in range(3):
+        ops.ht_spmv_ordered(nx, ny, nz, keys, vals, dt, order, u, out, fe=True)
         ops.set_bc(idx, bc, out)
         u, out = out, u
     assert f32_bits_equal(h(u), ref_ht)
