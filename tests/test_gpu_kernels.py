@@ -258,7 +258,8 @@ def test_fe_steps_match_oracle(cuda, oracle, n):
     np.testing.assert_allclose(h(u), ref_coo, rtol=1e-5, atol=1e-6)
 
 
-@pytest.mark.parametrize("n", [(48, 40, 36), (33, 9, 17), (3, 3, 3), (70, 12, 5)])
+# nx % 4 == 0 takes the float4 path (48, 64, 4, 8); the others the z-march
+@pytest.mark.parametrize("n", [(48, 40, 36), (33, 9, 17), (3, 3, 3), (70, 12, 5), (64, 8, 5), (4, 4, 4), (8, 3, 3)])
 def test_stencil_matches_oracle(cuda, oracle, n):
     import torch
     from piro_b200 import ops
