@@ -144,6 +144,16 @@ int piro_coo_spmv(int64_t N, int64_t nnz, const int32_t *rows, const int32_t *co
  * out = u + dt*M*u on every row. */
 int piro_coo_fe_step(int64_t N, int64_t nnz, const int32_t *rows, const int32_t *cols, const float *vals, float dt,
                      const float *u, float *out, piro_stream_t stream);
+/* COO with a row index, built once per operator: rowstart[r] = the first
+ * entry of row r in the row-sorted arrays (int32[N+1]; PIRO_ERR_ARG if rows
+ * are not sorted ascending or out of range; workspace >= 4 bytes; the call
+ * synchronizes).  piro_coo_step_indexed then computes out = dt*(A u), or
+ * u + dt*(A u) with fe = 1, on every row, each row's products summed in
+ * storage order: the CSR row loop over cols/vals, without reading rows. */
+int piro_coo_row_index(int64_t N, int64_t nnz, const int32_t *rows, int32_t *rowstart, void *work, size_t work_bytes,
+                       piro_stream_t stream);
+int piro_coo_step_indexed(int64_t N, const int32_t *rowstart, const int32_t *cols, const float *vals, float dt, int fe,
+                          const float *u, float *out, piro_stream_t stream);
 
 /* SpMVHT.cl:22-40 semantics: out[r] = dt * sum over present keys (r, c) of
  * H(r,c)*u[c] in ascending c, found by linear-probe lookups of the 7-point

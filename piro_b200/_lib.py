@@ -60,6 +60,8 @@ SIGNATURES = {
     "piro_csr_i1": (i32, [i32, i32, i32, vp, vp, vp, f32, vp, vp, vp]),
     "piro_coo_spmv": (i32, [i64, i64, vp, vp, vp, f32, vp, vp, vp]),
     "piro_coo_fe_step": (i32, [i64, i64, vp, vp, vp, f32, vp, vp, vp]),
+    "piro_coo_row_index": (i32, [i64, i64, vp, vp, vp, sz, vp]),
+    "piro_coo_step_indexed": (i32, [i64, vp, vp, vp, f32, i32, vp, vp, vp]),
     "piro_ht_spmv": (i32, [i32, i32, i32, vp, vp, i64, f32, i32, vp, vp, vp]),
     "piro_ht_row_order_workspace": (i32, [i64, i64, C.POINTER(sz)]),
     "piro_ht_row_order": (i32, [i64, i64, vp, vp, sz, vp]),

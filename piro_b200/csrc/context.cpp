@@ -157,6 +157,7 @@ struct piro_ctx {
     Csr lap, grad[3], dot, divm, be_A;
     float *dense = nullptr;  // DENSE Laplacian, N x N row-major (Data 1)
     int32_t *coo_rows = nullptr;
+    int32_t *coo_rowstart = nullptr;  // first entry of each row (piro_coo_row_index)
     int64_t *ht_keys = nullptr;
     float *ht_vals = nullptr;
     int64_t ht_ts = 0;
@@ -519,6 +520,7 @@ extern "C" void piro_close(piro_ctx *c)
     free_csr(c->be_A);
     cudaFree(c->dense);
     cudaFree(c->coo_rows);
+    cudaFree(c->coo_rowstart);
     cudaFree(c->ht_keys);
     cudaFree(c->ht_vals);
     cudaFree(c->ht_order);
@@ -668,6 +670,9 @@ extern "C" int piro_laplacian(piro_ctx *c, const char *var, const char *coeff, p
         CK(cudaMalloc(&c->coo_rows, sizeof(int32_t) * (size_t)nnz));
         PK(piro_coo_laplacian(c->nx, c->ny, c->nz, c->spacescheme, norm, c->coo_rows, c->lap.col, c->lap.val,
                               c->stream));
+        CK(cudaMalloc(&c->coo_rowstart, sizeof(int32_t) * (size_t)(N + 1)));
+        PK(ensure_work(c, 256));
+        PK(piro_coo_row_index(N, nnz, c->coo_rows, c->coo_rowstart, c->work, c->work_bytes, c->stream));
     } else {
         PK(alloc_csr(c->lap, N, nnz));
         PK(piro_csr_laplacian(c->nx, c->ny, c->nz, c->spacescheme, norm, c->lap.rp, c->lap.col, c->lap.val, c->stream));
@@ -907,7 +912,7 @@ extern "C" int piro_assign(piro_ctx *c, piro_buf lhs, piro_op rhs, piro_buf *out
                                     c->partD, c->stream));
         } else if (c->datatype == 3) {
             if (!c->coo_rows) return fail(PIRO_ERR_STATE, "piro_assign: COO operator not assembled");
-            PK(piro_coo_fe_step(N, c->lap.nnz, c->coo_rows, c->lap.col, c->lap.val, dt, u, c->partD, c->stream));
+            PK(piro_coo_step_indexed(N, c->coo_rowstart, c->lap.col, c->lap.val, dt, 1, u, c->partD, c->stream));
         } else {
             return fail(PIRO_ERR_DATATYPE, "piro_assign: Data not supported on this path");
         }

@@ -55,6 +55,50 @@ __global__ void __launch_bounds__(kRowThreads) k_csr_step(GridDiv g, int64_t N, 
     csr_for_rows(N, rowptr, col, val, op);
 }
 
+// COO with a row index: rowstart[r] = the first entry of row r in the
+// row-sorted entry arrays (rowstart[N] = nnz), built once per operator; then
+// the step is the CSR row loop over cols/vals (each row's entries summed in
+// storage order), out = dt*sum or u + dt*sum on every row (SpMVCOO then
+// addVectors).  err: rows not sorted, or out of range.
+__global__ void k_coo_rowstart(int64_t N, int64_t nnz, const int32_t *__restrict__ rows, int32_t *__restrict__ rowstart,
+                               int *err)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r1 = rows[k], r0 = k > 0 ? rows[k - 1] : -1;
+        if (r1 < r0 || r1 < 0 || r1 >= N) {
+            atomicExch(err, 1);
+            continue;
+        }
+        for (int64_t r = r0 + 1; r <= r1; ++r) rowstart[r] = (int32_t)k;
+        if (k == nnz - 1)
+            for (int64_t r = r1 + 1; r <= N; ++r) rowstart[r] = (int32_t)nnz;
+    }
+}
+
+struct CooRow {
+    float dt;
+    const float *__restrict__ u;
+    float *__restrict__ out;
+    int fe;
+    float acc;
+    __device__ __forceinline__ void begin(int64_t) { acc = 0.0f; }
+    __device__ __forceinline__ void add(int32_t c, float v) { acc = __fadd_rn(acc, __fmul_rn(v, __ldg(u + c))); }
+    __device__ __forceinline__ void end(int64_t row)
+    {
+        const float c = __fmul_rn(dt, acc);
+        out[row] = fe ? __fadd_rn(__ldg(u + row), c) : c;
+    }
+};
+
+__global__ void __launch_bounds__(kRowThreads) k_coo_rows(int64_t N, const int32_t *__restrict__ rowstart,
+                                                          const int32_t *__restrict__ cols,
+                                                          const float *__restrict__ vals, float dt, int fe,
+                                                          const float *__restrict__ u, float *__restrict__ out)
+{
+    CooRow op{dt, u, out, fe, 0.0f};
+    csr_for_rows(N, rowstart, cols, vals, op);
+}
+
 // COO: each warp takes 32 consecutive entries per pass; a segmented inclusive
 // scan over equal row ids gives each row's partial sum in the segment's last
 // lane.  Rows wholly inside the warp's span are stored; rows cut by the span
@@ -394,6 +438,37 @@ extern "C" int piro_coo_fe_step(int64_t N, int64_t nnz, const int32_t *rows, con
                                 float dt, const float *u, float *out, piro_stream_t stream)
 {
     return coo_common(N, nnz, rows, cols, vals, dt, u, out, true, stream);
+}
+
+extern "C" int piro_coo_row_index(int64_t N, int64_t nnz, const int32_t *rows, int32_t *rowstart, void *work,
+                                  size_t work_bytes, piro_stream_t stream)
+{
+    PIRO_ARG(N > 0 && N < INT32_MAX && nnz >= 0 && nnz < INT32_MAX && rowstart && (nnz == 0 || rows),
+             "piro_coo_row_index: bad arguments");
+    PIRO_ARG(work && work_bytes >= sizeof(int), "piro_coo_row_index: workspace too small");
+    cudaStream_t s = as_stream(stream);
+    if (nnz == 0) {
+        PIRO_CUDA(cudaMemsetAsync(rowstart, 0, sizeof(int32_t) * (size_t)(N + 1), s));
+        return PIRO_OK;
+    }
+    int *err = static_cast<int *>(work);
+    PIRO_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    k_coo_rowstart<<<grid_for(nnz, 256, 8), 256, 0, s>>>(N, nnz, rows, rowstart, err);
+    PIRO_CHECK_LAUNCH("k_coo_rowstart");
+    int h = 0;
+    PIRO_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PIRO_CUDA(cudaStreamSynchronize(s));
+    PIRO_ARG(!h, "piro_coo_row_index: rows not sorted ascending, or out of range");
+    return PIRO_OK;
+}
+
+extern "C" int piro_coo_step_indexed(int64_t N, const int32_t *rowstart, const int32_t *cols, const float *vals,
+                                     float dt, int fe, const float *u, float *out, piro_stream_t stream)
+{
+    PIRO_ARG(N > 0 && rowstart && cols && vals && u && out && u != out, "piro_coo_step_indexed: bad arguments");
+    k_coo_rows<<<csr_rows_grid(N), kRowThreads, 0, as_stream(stream)>>>(N, rowstart, cols, vals, dt, fe, u, out);
+    PIRO_CHECK_LAUNCH("k_coo_rows");
+    return PIRO_OK;
 }
 
 extern "C" int piro_ht_spmv(int nx, int ny, int nz, const int64_t *keys, const float *vals, int64_t ts, float dt, int fe,

@@ -192,6 +192,21 @@ def ht_spmv(nx, ny, nz, keys, vals, dt, u, out, fe=False):
     return out
 
 
+def coo_row_index(N, rows):
+    """rowstart[N+1] of a row-sorted COO (built once per operator)."""
+    rowstart = torch.empty(N + 1, dtype=i32, device="cuda")
+    work = torch.empty(256, dtype=torch.uint8, device="cuda")
+    check(lib().piro_coo_row_index(N, rows.numel(), _p(rows), _p(rowstart), _p(work), 256, _stream()),
+          "piro_coo_row_index")
+    return rowstart
+
+
+def coo_step_indexed(N, rowstart, cols, vals, dt, u, out, fe=False):
+    check(lib().piro_coo_step_indexed(N, _p(rowstart), _p(cols), _p(vals), float(dt), int(fe), _p(u), _p(out),
+                                      _stream()), "piro_coo_step_indexed")
+    return out
+
+
 def ht_row_order(N, ts):
     """Rows by the home slot of their keys (for ht_spmv(order=...))."""
     n = C.c_size_t()

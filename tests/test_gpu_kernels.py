@@ -105,6 +105,10 @@ def test_step_kernels_vs_golden(cuda, golden_grids):
             out = torch.empty(N, dtype=torch.float32, device="cuda")
             ops.coo_spmv(N, coo, 0.01, u, out)
             np.testing.assert_allclose(h(out), g[f"spmvcoo_{t}"], rtol=1e-5, atol=1e-6)
+            rowstart = ops.coo_row_index(N, coo[0])
+            assert np.array_equal(h(rowstart), g[f"csr_rowptr_{t}"])  # the row index is the CSR row pointer
+            ops.coo_step_indexed(N, rowstart, coo[1], coo[2], 0.01, u, out)
+            np.testing.assert_allclose(h(out), g[f"spmvcoo_{t}"], rtol=1e-5, atol=1e-6)
             keys = dev(torch, g[f"ht_keys_{t}"].astype(np.int64))
             hv = dev(torch, g[f"ht_vals_{t}"])
             ops.ht_spmv(nx, ny, nz, keys, hv, 0.01, u, out)
@@ -256,6 +260,16 @@ def test_fe_steps_match_oracle(cuda, oracle, n):
         ops.set_bc(idx, bc, out)
         u, out = out, u
     np.testing.assert_allclose(h(u), ref_coo, rtol=1e-5, atol=1e-6)
+    rowstart = ops.coo_row_index(N, coo_s[0])
+    u = dev(torch, u0)
+    for _ in range(3):
+        ops.coo_step_indexed(N, rowstart, coo_s[1], coo_s[2], dt, u, out, fe=True)
+        ops.set_bc(idx, bc, out)
+        u, out = out, u
+    np.testing.assert_allclose(h(u), ref_coo, rtol=1e-5, atol=1e-6)
+    bad = coo_s[0].flip(0).contiguous()
+    with pytest.raises(Exception, match="not sorted"):
+        ops.coo_row_index(N, bad)
 
 
 # nx % 4 == 0 takes the float4 path (48, 64, 4, 8); the others the z-march
