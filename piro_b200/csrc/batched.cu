@@ -131,6 +131,23 @@ __device__ __forceinline__ double block_sum(double v, double *s_warp)
     return t;  // thread 0
 }
 
+// kN block sums in one shared-memory round (thread 0 holds the totals).
+template <int kN>
+__device__ __forceinline__ void block_sums(double (&v)[kN], double *s_red)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int t = 0; t < kN; ++t) v[t] = warp_sum(v[t]);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int t = 0; t < kN; ++t) s_red[t * 32 + w] = v[t];
+    __syncthreads();
+    if (w == 0)
+#pragma unroll
+        for (int t = 0; t < kN; ++t) v[t] = warp_sum(lane < nw ? s_red[t * 32 + lane] : 0.0);
+}
+
 // In-order (lane-strided, then butterfly) sum of `count` partials of stride 4
 // starting at p; every lane gets the result.
 __device__ __forceinline__ double warp_partial_sum(const double *p, int count)
@@ -150,6 +167,7 @@ __device__ __forceinline__ float a_apply32(const BMember &m, const float *v, int
 __global__ void __launch_bounds__(kThreads) k_batch_step(BArgs A)
 {
     __shared__ double s_warp[32];
+    __shared__ double s_red[4 * 32];
     __shared__ int s_ok;
     const int nwarps_grid = (int)(gridDim.x * (blockDim.x >> 5));
     const int gwarp = (int)(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5));
@@ -259,14 +277,19 @@ __global__ void __launch_bounds__(kThreads) k_batch_step(BArgs A)
             } else {
                 continue;
             }
-            const double t0 = block_sum(v0, s_warp), t1 = block_sum(v1, s_warp), t2 = block_sum(v2, s_warp),
-                         t3 = block_sum(v3, s_warp);
-            if (threadIdx.x == 0) {
-                double *pp = A.partials + 4 * (int64_t)t;
-                pp[0] = t0;
-                pp[1] = t1;
-                pp[2] = t2;
-                pp[3] = t3;
+            if (s.mode == kResid) {
+                double v[4] = {v0, v1, v2, v3};
+                block_sums<4>(v, s_red);
+                if (threadIdx.x == 0) {
+                    double *pp = A.partials + 4 * (int64_t)t;
+                    pp[0] = v[0];
+                    pp[1] = v[1];
+                    pp[2] = v[2];
+                    pp[3] = v[3];
+                }
+            } else {
+                const double t0 = block_sum(v0, s_warp);  // CG: <p, q> only
+                if (threadIdx.x == 0) A.partials[4 * (int64_t)t] = t0;
             }
         }
         if (!grid_sync(A.bar, A.spin_limit, &s_ok)) return;
@@ -341,24 +364,44 @@ __global__ void __launch_bounds__(kThreads) k_batch_step(BArgs A)
                     if (s.mode == kFinish) A.out[m.off + i] = (float)xn;
                 }
             } else if (s.mode == kCg) {
+                // Boundary cells carry p = q = r = 0 (V1 and RESID write them so):
+                // the update leaves them at zero and they add nothing to the sums,
+                // so every cell is updated without a test, float4 groups where the
+                // tile is 16-byte aligned (members start 64-cell aligned, tiles
+                // are multiples of 64 cells), scalars for the tail.
                 const float a = (float)s.a;
                 const float *pn = ((s.it & 1) ? A.p0 : A.p1) + m.off;
                 const float *qq = A.q + m.off;
                 float *rr = A.r + m.off, *dd = A.d + m.off;
                 double v0 = 0.0, v1 = 0.0;
-                for (int64_t i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
-                    if (!m.g.interior(i)) continue;
+                const int64_t g0 = s0 >> 2, g1 = s1 >> 2;  // s0 % 4 == 0
+                for (int64_t gi = g0 + threadIdx.x; gi < g1; gi += blockDim.x) {
+                    const float4 p4 = reinterpret_cast<const float4 *>(pn)[gi];
+                    const float4 q4 = reinterpret_cast<const float4 *>(qq)[gi];
+                    float4 d4 = reinterpret_cast<float4 *>(dd)[gi];
+                    float4 r4 = reinterpret_cast<float4 *>(rr)[gi];
+                    d4.x += a * p4.x; d4.y += a * p4.y; d4.z += a * p4.z; d4.w += a * p4.w;
+                    r4.x = r4.x - a * q4.x; r4.y = r4.y - a * q4.y; r4.z = r4.z - a * q4.z; r4.w = r4.w - a * q4.w;
+                    reinterpret_cast<float4 *>(dd)[gi] = d4;
+                    reinterpret_cast<float4 *>(rr)[gi] = r4;
+                    v0 += (double)r4.x * (double)(r4.x * m.dinv) + (double)r4.y * (double)(r4.y * m.dinv) +
+                          (double)r4.z * (double)(r4.z * m.dinv) + (double)r4.w * (double)(r4.w * m.dinv);
+                    v1 += (double)r4.x * (double)r4.x + (double)r4.y * (double)r4.y + (double)r4.z * (double)r4.z +
+                          (double)r4.w * (double)r4.w;
+                }
+                for (int64_t i = (g1 << 2) + threadIdx.x; i < s1; i += blockDim.x) {
                     dd[i] += a * pn[i];
                     const float ri = rr[i] - a * qq[i];
                     rr[i] = ri;
                     v0 += (double)ri * (double)(ri * m.dinv);
                     v1 += (double)ri * (double)ri;
                 }
-                const double t0 = block_sum(v0, s_warp), t1 = block_sum(v1, s_warp);
+                double v[2] = {v0, v1};
+                block_sums<2>(v, s_red);
                 if (threadIdx.x == 0) {
                     double *pp = A.partials + 4 * (int64_t)t;
-                    pp[0] = t0;
-                    pp[1] = t1;
+                    pp[0] = v[0];
+                    pp[1] = v[1];
                 }
             }
         }
