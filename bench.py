@@ -228,6 +228,40 @@ def config_sections(torch, peak):
     return out
 
 
+def assembly_section(torch, ops, peak):
+    """Assembly of the CSR Laplacian (central): on the device at 32^3 and
+    256^3, and PIRO's own host assembly (CSR::stencils::laplacian_cd, with
+    its std::find over the whole column array per boundary row) at 32^3,
+    the largest size where it is tractable (it is O(nnz * boundary rows))."""
+    out = {}
+    for n in (32, 256):
+        N = n ** 3
+        for _ in range(2):
+            A = ops.csr_laplacian(n, n, n, 3, 1.0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            A = ops.csr_laplacian(n, n, n, 3, 1.0)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 5
+        nnz = A[2].numel()
+        byt = 4 * (N + 1) + 8 * nnz
+        out[f"csr_laplacian_{n}"] = {"ms": round(ms, 4), "nnz": nnz, "bytes_written": byt,
+                                     "gbs": round(byt / ms / 1e6, 1), "frac": round(byt / ms / 1e6 / peak, 4)}
+        del A
+    try:  # PIRO's own host code (oracle/_ref), when it was built
+        from oracle import oracle as O
+        R = O.Ref()
+        t0 = time.perf_counter()
+        R.laplacian(32, 32, 32, 3, np.float32(1.0))
+        out["reference_host_32_ms"] = round((time.perf_counter() - t0) * 1e3, 1)
+    except (FileNotFoundError, OSError):
+        out["reference_host_32_ms"] = None
+    return out
+
+
 def next_rows_section(torch, ops, peak):
     """DENSE forward Euler at 34^3 (N = 39,304: a 6.2 GB matrix, HBM stream)
     and scheme 27: the banded LU (factor once, solve per step) at 34^3, and
@@ -571,6 +605,7 @@ def run_piro(args):
                if rank == 0 else None)
     batched = batched_section(torch, ops, peak) if rank == 0 else None
     next_rows = next_rows_section(torch, ops, peak) if rank == 0 else None
+    assembly = assembly_section(torch, ops, peak) if rank == 0 else None
 
     cpu = None
     fp64 = None
@@ -581,9 +616,16 @@ def run_piro(args):
         t0 = time.perf_counter()
         u64, cg_its, rel = O.be_cg_f64(nx, ny, nz, Ah, al, cfg["u0"], rtol=1e-8)
         cpu_ms = (time.perf_counter() - t0) * 1e3
-        cpu = {"value": cpu_ms, "unit": "ms/step", "cores": O.num_threads(), "kind": "port",
+        nthr = O.num_threads()
+        O.set_threads(1)
+        t0 = time.perf_counter()
+        O.be_cg_f64(nx, ny, nz, Ah, al, cfg["u0"], rtol=1e-8)
+        cpu1_ms = (time.perf_counter() - t0) * 1e3
+        O.set_threads(nthr)
+        cpu = {"value": cpu_ms, "unit": "ms/step", "cores": nthr, "kind": "port",
                "sample": f"1 backward-Euler step of the 128^3 config, FP64 Jacobi-PCG to 1e-8 ({cg_its} iterations), "
-                         "OpenMP over all host threads"}
+                         "OpenMP over all host threads",
+               "one_thread": {"value": round(cpu1_ms, 1), "unit": "ms/step", "cores": 1}}
         # per-step error of the device result against an FP64-only solve
         solver.solve(u0, x, rtol=1e-8)
         u64b, _, _ = O.be_cg_f64(nx, ny, nz, Ah, al, cfg["u0"], rtol=1e-13)
@@ -627,6 +669,7 @@ def run_piro(args):
         "learned": learned,
         "batched": batched,
         "next_rows": next_rows,
+        "assembly": assembly,
         "fp64_check": fp64,
         "cpu_baseline": cpu,
     }

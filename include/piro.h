@@ -89,6 +89,13 @@ int piro_gradient_nnz(int nx, int ny, int nz, int axis, int64_t *nnz);
  * CSR::gradient (src/operatorgradient.cpp:13-117, norm = 2*(l0/(n0-2)), :25). */
 int piro_csr_gradient(int nx, int ny, int nz, int space_scheme, int axis, float norm, int32_t *rowptr,
                       int32_t *col, float *val, piro_stream_t stream);
+/* Rows row0 .. row0+nrows-1 of one axis's gradient matrix with columns
+ * shifted down by col_shift (col_shift <= row0 - nx*ny when row0 > 0): the
+ * rows a z-slab owns, with its local column numbering; the entries of each
+ * row exactly as piro_csr_gradient gives them. */
+int piro_gradient_nnz_rows(int nx, int ny, int nz, int axis, int64_t row0, int64_t nrows, int64_t *nnz);
+int piro_csr_gradient_rows(int nx, int ny, int nz, int space_scheme, int axis, float norm, int64_t row0, int64_t nrows,
+                           int64_t col_shift, int32_t *rowptr, int32_t *col, float *val, piro_stream_t stream);
 
 /* val[k] *= s[row(k)]: the row scale diag(s)*M that kernelmethods::csrscale
  * (src/kernelcsrgeam.cpp:208-234) intends through SpMDSM.cl:20-31. */

@@ -52,6 +52,8 @@ SIGNATURES = {
     "piro_coo_laplacian": (i32, [i32, i32, i32, i32, f32, vp, vp, vp, vp]),
     "piro_gradient_nnz": (i32, [i32, i32, i32, i32, pi64]),
     "piro_csr_gradient": (i32, [i32, i32, i32, i32, i32, f32, vp, vp, vp, vp]),
+    "piro_gradient_nnz_rows": (i32, [i32, i32, i32, i32, i64, i64, pi64]),
+    "piro_csr_gradient_rows": (i32, [i32, i32, i32, i32, i32, f32, i64, i64, i64, vp, vp, vp, vp]),
     "piro_csr_rowscale": (i32, [i64, vp, vp, vp, vp]),
     "piro_ht_table_size": (i32, [i64, i64, i32, f32, f32, f32, f32, pi64]),
     "piro_ht_build_workspace": (i32, [i64, psz]),

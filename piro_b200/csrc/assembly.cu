@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, 
 
 // Gradient prefix: number of entries of rows before i for `axis`
 // (each row has [a > 0] + [a < n_a - 1] entries).
-__device__ __forceinline__ int64_t grad_prefix(int64_t i, int x, int y, int z, int axis, const Grid &g)
+__host__ __device__ __forceinline__ int64_t grad_prefix(int64_t i, int x, int y, int z, int axis, const Grid &g)
 {
     int64_t c0, c1;  // rows before i with a == 0, with a == n_a - 1
     if (axis == 0) {
@@ -171,30 +171,48 @@ __device__ __forceinline__ int64_t grad_prefix(int64_t i, int x, int y, int z, i
     return 2 * i - c0 - c1;
 }
 
-__global__ void __launch_bounds__(kRowsPerBlock) k_gradient(Grid g, int64_t N, int scheme, int axis, float vm, float vp,
+// Rows row0 .. row0+n-1 of one axis's matrix into local arrays: entry
+// positions relative to row row0's first entry, columns shifted down by
+// col_shift (the whole matrix: row0 = col_shift = 0, n = N).
+__global__ void __launch_bounds__(kRowsPerBlock) k_gradient(Grid g, int64_t n, int scheme, int axis, float vm, float vp,
                                                             int32_t *__restrict__ rowptr, int32_t *__restrict__ col,
-                                                            float *__restrict__ val)
+                                                            float *__restrict__ val, int64_t row0, int64_t p0,
+                                                            int64_t col_shift)
 {
     const int64_t e = axis == 0 ? 1 : axis == 1 ? g.nx : g.sxy;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = row0 + j;
         int x, y, z;
         coords(i, g, x, y, z);
         const int a = axis == 0 ? x : axis == 1 ? y : z;
         const int na = axis == 0 ? g.nx : axis == 1 ? g.ny : g.nz;
-        int64_t p = grad_prefix(i, x, y, z, axis, g);
+        int64_t p = grad_prefix(i, x, y, z, axis, g) - p0;
         if (a > 0) {
-            col[p] = (int32_t)(scheme == 2 ? i : i - e);
+            col[p] = (int32_t)((scheme == 2 ? i : i - e) - col_shift);
             val[p] = vm;
             ++p;
         }
         if (a < na - 1) {
-            col[p] = (int32_t)(scheme == 1 ? i : i + e);
+            col[p] = (int32_t)((scheme == 1 ? i : i + e) - col_shift);
             val[p] = vp;
             ++p;
         }
-        rowptr[i + 1] = (int32_t)p;
-        if (i == 0) rowptr[0] = 0;
+        rowptr[j + 1] = (int32_t)p;
+        if (j == 0) rowptr[0] = 0;
     }
+}
+
+// grad_prefix at a row index on the host (row == N: every entry)
+int64_t grad_prefix_host(int64_t i, int axis, const Grid &g, int64_t N)
+{
+    if (i >= N) {
+        const int64_t na = axis == 0 ? g.nx : axis == 1 ? g.ny : g.nz;
+        return 2 * N - 2 * (N / na);
+    }
+    const int z = (int)(i / g.sxy);
+    const int64_t rem = i - (int64_t)z * g.sxy;
+    const int y = (int)(rem / g.nx);
+    return grad_prefix(i, (int)(rem - (int64_t)y * g.nx), y, z, axis, g);
 }
 
 __global__ void k_rowscale(int64_t nrows, const int32_t *__restrict__ rowptr, float *__restrict__ val,
@@ -360,7 +378,40 @@ extern "C" int piro_csr_gradient(int nx, int ny, int nz, int space_scheme, int a
     const int64_t N = (int64_t)nx * ny * nz;
     // -1/norm and 1/norm are float divisions (int operand promoted), stencils.cpp:17,24.
     const float vm = -1 / norm, vp = 1 / norm;
-    k_gradient<<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(g, N, space_scheme, axis, vm, vp, rowptr, col, val);
+    k_gradient<<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(g, N, space_scheme, axis, vm, vp, rowptr, col, val,
+                                                                   0, 0, 0);
+    PIRO_CHECK_LAUNCH("k_gradient");
+    return PIRO_OK;
+}
+
+extern "C" int piro_gradient_nnz_rows(int nx, int ny, int nz, int axis, int64_t row0, int64_t nrows, int64_t *nnz)
+{
+    const int64_t N = (int64_t)nx * ny * nz;
+    PIRO_ARG(nnz && grid_ok(nx, ny, nz) && axis >= 0 && axis <= 2 && row0 >= 0 && nrows >= 0 && row0 + nrows <= N,
+             "piro_gradient_nnz_rows: bad arguments");
+    const Grid g{nx, ny, nz, (int64_t)nx * ny};
+    *nnz = grad_prefix_host(row0 + nrows, axis, g, N) - grad_prefix_host(row0, axis, g, N);
+    return PIRO_OK;
+}
+
+extern "C" int piro_csr_gradient_rows(int nx, int ny, int nz, int space_scheme, int axis, float norm, int64_t row0,
+                                      int64_t nrows, int64_t col_shift, int32_t *rowptr, int32_t *col, float *val,
+                                      piro_stream_t stream)
+{
+    const int64_t N = (int64_t)nx * ny * nz;
+    // columns of rows >= row0 reach down to row0 - nx*ny at most: local columns stay >= 0
+    PIRO_ARG(grid_ok(nx, ny, nz) && axis >= 0 && axis <= 2 && rowptr && col && val && row0 >= 0 && nrows > 0 &&
+                 row0 + nrows <= N && col_shift <= row0 - (row0 > 0 ? (int64_t)nx * ny : 0),
+             "piro_csr_gradient_rows: bad arguments");
+    if (space_scheme < 1 || space_scheme > 3) {
+        piro::set_error("piro_csr_gradient_rows: space scheme %d not in {1,2,3}", space_scheme);
+        return PIRO_ERR_SCHEME;
+    }
+    Grid g{nx, ny, nz, (int64_t)nx * ny};
+    const float vm = -1 / norm, vp = 1 / norm;
+    const int64_t p0 = grad_prefix_host(row0, axis, g, N);
+    k_gradient<<<grid_for(nrows, 256, 8), 256, 0, as_stream(stream)>>>(g, nrows, space_scheme, axis, vm, vp, rowptr,
+                                                                       col, val, row0, p0, col_shift);
     PIRO_CHECK_LAUNCH("k_gradient");
     return PIRO_OK;
 }

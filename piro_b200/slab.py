@@ -11,6 +11,11 @@ never read by an owned interior row.
   (piro_csr_laplacian_rows, columns local) stepped as SpMVCSR.cl after a halo
   exchange of u: a sharded forward-Euler step equals the single-grid step bit
   for bit.
+- SlabAdvection: ddt_r(U) = vector(v) & gradient(U) on the slab: the owned
+  rows of the three gradient matrices (piro_csr_gradient_rows, columns
+  local) merged with the owned part of v by csrgeam (a row-local merge, so no
+  shard needs another's row offsets), then stepped like SlabFE: bit for bit
+  the single-grid advection step.
 - SlabBE: the single-grid backward-Euler method -- FP32 Jacobi-PCG inside FP64
   iterative refinement on A = I - dt*diag(alpha)*L (central scheme) -- with a
   matrix-free operator on the slab: per CG iteration one halo exchange of z
@@ -147,6 +152,22 @@ class CudaBackend:
         from . import ops
         ops.csr_rowscale(A[0], A[2], s)
 
+    def gradient_rows(self, nx, ny, nz, scheme, axis, norm, row0, nrows, col_shift):
+        t, L = self.torch, self.lib()
+        nnz = C.c_int64()
+        self.check(L.piro_gradient_nnz_rows(nx, ny, nz, axis, row0, nrows, C.byref(nnz)), "piro_gradient_nnz_rows")
+        rp = t.empty(nrows + 1, dtype=t.int32, device="cuda")
+        col = t.empty(nnz.value, dtype=t.int32, device="cuda")
+        val = t.empty(nnz.value, dtype=t.float32, device="cuda")
+        self.check(L.piro_csr_gradient_rows(nx, ny, nz, scheme, axis, float(norm), row0, nrows, col_shift,
+                                            self._p(rp), self._p(col), self._p(val), self._stream()),
+                   "piro_csr_gradient_rows")
+        return rp, col, val
+
+    def geam3(self, nrows, G, v_owned):
+        from . import ops
+        return ops.csrgeam3(nrows, *G, v_owned)
+
     def fe_rows(self, nx, ny, nz, row0, nrows, A, dt, u, ubase, out):
         self.check(self.lib().piro_csr_fe_step_rows(nx, ny, nz, row0, nrows, self._p(A[0]), self._p(A[1]),
                                                     self._p(A[2]), float(dt), self._p(u), ubase, self._p(out),
@@ -203,6 +224,22 @@ class SlabFE:
         """out = u + dt*A u on the owned interior rows (u's halo planes are exchanged first)."""
         self.comm.halo(u, self.plane)
         self.b.fe_rows(self.nx, self.ny, self.nz, self.row0, self.nrows, self.A, dt, u, self.plane, out)
+
+
+class SlabAdvection(SlabFE):
+    """Advection (simindex 1, TIMESCHEME 11, CSR) on this rank's slab:
+    vector(v) & gradient(U) over the owned rows.  v_owned is the owned part
+    of the SoA vector field: three blocks of (z1-z0)*nx*ny values."""
+
+    def __init__(self, backend, comm, nx, ny, nz, z0, z1, scheme, gnorm, v_owned):
+        self.b, self.comm = backend, comm
+        self.nx, self.ny, self.nz, self.z0, self.z1 = nx, ny, nz, z0, z1
+        self.plane = nx * ny
+        self.row0 = z0 * self.plane
+        self.nrows = (z1 - z0) * self.plane
+        shift = (z0 - 1) * self.plane
+        G = [backend.gradient_rows(nx, ny, nz, scheme, a, gnorm, self.row0, self.nrows, shift) for a in range(3)]
+        self.A = backend.geam3(self.nrows, G, v_owned)
 
 
 class SlabBE:

@@ -31,6 +31,17 @@ class NumpyBackend:
         return (torch.from_numpy((rp[row0:row0 + nrows + 1] - rp[row0]).astype(np.int32)),
                 torch.from_numpy((col[a:b] - col_shift).astype(np.int32)), torch.from_numpy(val[a:b].copy()))
 
+    def gradient_rows(self, nx, ny, nz, scheme, axis, norm, row0, nrows, col_shift):
+        rp, col, val = O.gradient3(nx, ny, nz, scheme, np.float32(norm))[axis]
+        a, b = int(rp[row0]), int(rp[row0 + nrows])
+        return (torch.from_numpy((rp[row0:row0 + nrows + 1] - rp[row0]).astype(np.int32)),
+                torch.from_numpy((col[a:b] - col_shift).astype(np.int32)), torch.from_numpy(val[a:b].copy()))
+
+    def geam3(self, nrows, G, v_owned):
+        Gn = [tuple(t.numpy() for t in g) for g in G]
+        rp, col, val = O.csrgeam3(nrows, *Gn, v_owned.numpy())
+        return torch.from_numpy(rp), torch.from_numpy(col), torch.from_numpy(val)
+
     def rowscale(self, A, s):
         rp, val = A[0].numpy(), A[2].numpy()
         A[2].copy_(torch.from_numpy(O.csr_rowscale(len(rp) - 1, rp, val, s.numpy())))

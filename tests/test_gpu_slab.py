@@ -76,6 +76,41 @@ def test_slab_fe_bitexact(cuda, world, scheme):
     assert np.array_equal(got[inter], ref[inter])
 
 
+@pytest.mark.parametrize("world,scheme", [(2, 1), (3, 3)])
+def test_slab_advection_bitexact(cuda, world, scheme):
+    import torch
+    from piro_b200 import ops, slab
+    nx, ny, nz = 20, 17, 23
+    N, plane = nx * ny * nz, nx * ny
+    rng = np.random.default_rng(2)
+    u = rng.random(N).astype(np.float32)
+    vel = rng.standard_normal(3 * N).astype(np.float32)
+    G = [ops.csr_gradient(nx, ny, nz, scheme, a, 2.0) for a in range(3)]
+    A = ops.csrgeam3(N, *G, torch.from_numpy(vel).cuda())
+    ref = torch.zeros(N, device="cuda")
+    ops.csr_fe_step(nx, ny, nz, A, 0.01, torch.from_numpy(u).cuda(), ref)
+    ref = ref.cpu().numpy()
+    parts = slab.split_planes(nz, world)
+
+    def fn(r, comm):
+        z0, z1 = parts[r]
+        be = slab.CudaBackend()
+        v_own = np.concatenate([vel[c * N + z0 * plane:c * N + z1 * plane] for c in range(3)])
+        ad = slab.SlabAdvection(be, comm, nx, ny, nz, z0, z1, scheme, 2.0, torch.from_numpy(v_own).cuda())
+        ul = torch.from_numpy(_local(u, z0, z1, plane)).cuda()
+        o = torch.zeros_like(ul)
+        ad.step(ul, o, 0.01)
+        torch.cuda.synchronize()
+        return o.cpu().numpy()[plane:(z1 - z0 + 1) * plane]
+
+    got = np.concatenate(_run_ranks(world, fn))
+    idx = np.arange(N)
+    z, rem = np.divmod(idx, plane)
+    y, x = np.divmod(rem, nx)
+    inter = (x > 0) & (x < nx - 1) & (y > 0) & (y < ny - 1) & (z > 0) & (z < nz - 1)
+    assert np.array_equal(got[inter], ref[inter])
+
+
 @pytest.mark.parametrize("world", [2, 3])
 def test_slab_be_matches_single_grid(cuda, world):
     import torch
