@@ -202,9 +202,9 @@ def config_sections(torch, peak):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     out["heat_fe_32"] = {"steps": c["steps"], "ms_total": round(ms, 4), "us_per_step": round(1e3 * ms / c["steps"], 2),
-                         "note": "graph replays of two steps each (memset + SpMVCSR-order step + setBC per step), "
-                                 "captured once; 32^3 = 2.3 MB per step is launch-bound and L2-resident by size "
-                                 "(no flush between the graph's steps)"}
+                         "note": "graph replays of two steps each, one fused kernel per step (zero-filled result, "
+                                 "SpMVCSR-order update, setBC), captured once; 32^3 = 2.3 MB per step is "
+                                 "launch-bound and L2-resident by size (no flush between the graph's steps)"}
     c = W.advection(256)
     nx, ny, nz = c["n"]
     N = nx * ny * nz
@@ -223,7 +223,7 @@ def config_sections(torch, peak):
     byt = 8 * nnz + 4 * (N + 1) + 8 * N
     out["advection_256"] = {"steps": steps, "ms_per_step": round(ms, 4), "nnz": nnz, "gbs": round(byt / ms / 1e6, 1),
                             "frac": round(byt / ms / 1e6 / peak, 4),
-                            "note": "per step: memset + SpMVCSR-order step + setBC; bytes counted for the step kernel"}
+                            "note": "per step: one fused kernel (zero-filled result, SpMVCSR-order update, setBC)"}
     del run
     torch.cuda.empty_cache()
     return out

@@ -134,6 +134,14 @@ int piro_ht_build(int64_t N, const int32_t *rowptr, const int32_t *col, const fl
  * no fused multiply-add; boundary rows of out are not written. */
 int piro_csr_fe_step(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val, float dt,
                      const float *u, float *out, piro_stream_t stream);
+/* One whole forward-Euler step of Solve(): a zero-filled result, the
+ * SpMVCSR update of the interior rows, and setBC of the face cells from bc
+ * (bc::opencl_setBC; NULL: no [BC], faces stay 0), in one pass.  Face cells
+ * are the cells with exactly one coordinate on the boundary, which is the
+ * union of bc::initbc's six lists; edges and corners are 0.  Same result bit
+ * for bit as memset + piro_csr_fe_step + piro_set_bc. */
+int piro_csr_fe_step_bc(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val, float dt,
+                        const float *u, const float *bc, float *out, piro_stream_t stream);
 
 /* SpMVCSR_I1.cl:12-36 (backward-Euler residual form): interior rows get
  * out[r] = u[r] - sum_k (dt*val[k])*u[col[k]]; boundary rows untouched. */

@@ -59,6 +59,7 @@ SIGNATURES = {
     "piro_ht_build_workspace": (i32, [i64, psz]),
     "piro_ht_build": (i32, [i64, vp, vp, vp, i64, i64, vp, vp, vp, sz, vp]),
     "piro_csr_fe_step": (i32, [i32, i32, i32, vp, vp, vp, f32, vp, vp, vp]),
+    "piro_csr_fe_step_bc": (i32, [i32, i32, i32, vp, vp, vp, f32, vp, vp, vp, vp]),
     "piro_csr_i1": (i32, [i32, i32, i32, vp, vp, vp, f32, vp, vp, vp]),
     "piro_coo_spmv": (i32, [i64, i64, vp, vp, vp, f32, vp, vp, vp]),
     "piro_coo_fe_step": (i32, [i64, i64, vp, vp, vp, f32, vp, vp, vp]),

@@ -32,13 +32,23 @@ struct FeRow {
     const float *__restrict__ u;
     float *__restrict__ out;
     int64_t row0, ubase;
+    const float *__restrict__ bc;  // kMode 2: the saved face values (may be NULL)
     float result;
     __device__ __forceinline__ void begin(int64_t) { result = 0.0f; }
     __device__ __forceinline__ void add(int32_t c, float v) { result = add_rn(result, mul_rn(mul_rn(dt, v), __ldg(u + c))); }
     __device__ __forceinline__ void end(int64_t row)
     {
-        if (g.interior(row0 + row)) {
-            const int64_t k = ubase + row;
+        const int64_t k = ubase + row;
+        if (kMode == 2) {
+            // the whole next field: interior rows the step, face cells (one
+            // coordinate on the boundary: exactly bc::initbc's face lists) their
+            // saved value, edges and corners 0 -- zero-filled partD, SpMVCSR,
+            // then setBC, in one pass
+            int x, y, z;
+            g.coords((uint32_t)(row0 + row), x, y, z);
+            const int ex = (x == 0 || x == g.nx - 1) + (y == 0 || y == g.ny - 1) + (z == 0 || z == g.nz - 1);
+            out[k] = ex == 0 ? add_rn(result, u[k]) : (ex == 1 && bc) ? bc[k] : 0.0f;
+        } else if (g.interior(row0 + row)) {
             out[k] = kMode == 0 ? add_rn(result, u[k]) : sub_rn(u[k], result);
         }
     }
@@ -51,7 +61,17 @@ __global__ void __launch_bounds__(kRowThreads) k_csr_step(GridDiv g, int64_t N, 
                                                           const float *__restrict__ u, float *__restrict__ out,
                                                           int64_t row0, int64_t ubase)
 {
-    FeRow<kMode> op{g, dt, u, out, row0, ubase, 0.0f};
+    FeRow<kMode> op{g, dt, u, out, row0, ubase, nullptr, 0.0f};
+    csr_for_rows(N, rowptr, col, val, op);
+}
+
+__global__ void __launch_bounds__(kRowThreads) k_csr_step_bc(GridDiv g, int64_t N, const int32_t *__restrict__ rowptr,
+                                                             const int32_t *__restrict__ col,
+                                                             const float *__restrict__ val, float dt,
+                                                             const float *__restrict__ u, const float *__restrict__ bc,
+                                                             float *__restrict__ out)
+{
+    FeRow<2> op{g, dt, u, out, 0, 0, bc, 0.0f};
     csr_for_rows(N, rowptr, col, val, op);
 }
 
@@ -438,6 +458,18 @@ extern "C" int piro_coo_fe_step(int64_t N, int64_t nnz, const int32_t *rows, con
                                 float dt, const float *u, float *out, piro_stream_t stream)
 {
     return coo_common(N, nnz, rows, cols, vals, dt, u, out, true, stream);
+}
+
+extern "C" int piro_csr_fe_step_bc(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val,
+                                   float dt, const float *u, const float *bc, float *out, piro_stream_t stream)
+{
+    PIRO_ARG(grid_ok(nx, ny, nz) && rowptr && col && val && u && out && u != out && bc != out,
+             "piro_csr_fe_step_bc: bad arguments");
+    const int64_t N = (int64_t)nx * ny * nz;
+    k_csr_step_bc<<<csr_rows_grid(N), kRowThreads, 0, as_stream(stream)>>>(GridDiv(nx, ny, nz), N, rowptr, col, val,
+                                                                            dt, u, bc, out);
+    PIRO_CHECK_LAUNCH("k_csr_step_bc");
+    return PIRO_OK;
 }
 
 extern "C" int piro_coo_row_index(int64_t N, int64_t nnz, const int32_t *rows, int32_t *rowstart, void *work,

@@ -1,7 +1,7 @@
 """Forward-Euler time loops (TIMESCHEME 11) on the device, one Solve() per
-step as src/solve.cpp:18-46 runs them: a zero-filled result buffer, the fused
-SpMV + update kernel over the interior (SpMVCSR.cl), then setBC restoring the
-face values saved at start-up.  The per-step launches can be captured once in
+step as src/solve.cpp:18-46 runs them: a zero-filled result buffer, the
+SpMV + update over the interior (SpMVCSR.cl), then setBC restoring the face
+values saved at start-up -- all three in one kernel (piro_csr_fe_step_bc).  The per-step launches can be captured once in
 a CUDA graph and replayed (graph=True), which removes the host from the loop
 for small grids where a step is a few microseconds."""
 from __future__ import annotations
@@ -17,9 +17,8 @@ class _Loop:
         self.memD = u0.clone()  # face values at start-up (bc.cpp:31-32)
 
     def _step(self, u: torch.Tensor, out: torch.Tensor) -> None:
-        out.zero_()
-        ops.csr_fe_step(self.nx, self.ny, self.nz, self.A, self.dt, u, out)
-        ops.set_bc(self.bc_idx, self.memD, out)
+        # zero-filled result, SpMVCSR update, setBC of the faces: one kernel
+        ops.csr_fe_step_bc(self.nx, self.ny, self.nz, self.A, self.dt, u, self.memD, out)
 
     def capture(self, u0: torch.Tensor):
         """Set up the boundary values and capture two steps in a CUDA graph

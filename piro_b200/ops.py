@@ -207,6 +207,13 @@ def coo_step_indexed(N, rowstart, cols, vals, dt, u, out, fe=False):
     return out
 
 
+def csr_fe_step_bc(nx, ny, nz, A, dt, u, bc, out):
+    """memset + SpMVCSR step + setBC from bc (None: faces 0) in one kernel."""
+    check(lib().piro_csr_fe_step_bc(nx, ny, nz, _p(A[0]), _p(A[1]), _p(A[2]), float(dt), _p(u), _p(bc), _p(out),
+                                    _stream()), "piro_csr_fe_step_bc")
+    return out
+
+
 def ht_row_order(N, ts):
     """Rows by the home slot of their keys (for ht_spmv(order=...))."""
     n = C.c_size_t()

@@ -315,3 +315,29 @@ def test_vector_ops_and_dot(cuda, oracle):
         got = ops.dot_f64(dev(torch, x), dev(torch, y)) if n else 0.0
         want = float(np.dot(x.astype(np.float64), y.astype(np.float64)))
         assert abs(got - want) <= 1e-12 * max(1.0, np.abs(x.astype(np.float64) * y).sum())
+
+
+@pytest.mark.parametrize("n", [(12, 10, 9), (3, 3, 3), (33, 17, 5)])
+def test_fused_fe_step_with_bc(cuda, n):
+    """piro_csr_fe_step_bc = zero-filled result + SpMVCSR step + setBC, bit for bit."""
+    import torch
+    from piro_b200 import ops
+    nx, ny, nz = n
+    N = nx * ny * nz
+    rng = np.random.default_rng(4)
+    u = torch.from_numpy(rng.random(N, dtype=np.float32)).cuda()
+    memD = torch.from_numpy(rng.random(N, dtype=np.float32)).cuda()
+    A = ops.csr_laplacian(nx, ny, nz, 3, 1.0)
+    ops.csr_rowscale(A[0], A[2], torch.from_numpy(np.exp(rng.standard_normal(N)).astype(np.float32)).cuda())
+    idx, _ = ops.face_lists(nx, ny, nz)
+    ref = torch.zeros(N, device="cuda")
+    ops.csr_fe_step(nx, ny, nz, A, 0.013, u, ref)
+    ops.set_bc(idx, memD, ref)
+    got = torch.full((N,), float("nan"), device="cuda")
+    ops.csr_fe_step_bc(nx, ny, nz, A, 0.013, u, memD, got)
+    assert f32_bits_equal(h(got), h(ref))
+    ref = torch.zeros(N, device="cuda")
+    ops.csr_fe_step(nx, ny, nz, A, 0.013, u, ref)
+    got.fill_(float("nan"))
+    ops.csr_fe_step_bc(nx, ny, nz, A, 0.013, u, None, got)  # no [BC]: faces stay 0
+    assert f32_bits_equal(h(got), h(ref))
