@@ -735,8 +735,8 @@ def run_reference(args):
 
 def run_profile_case(args):
     """Small fixed cases for ncu captures (no timing, no JSON): `be` solves the
-    128^3 backward-Euler step twice, `spmv` runs each 256^3 forward-Euler
-    kernel four times, `dense` three DENSE steps at N = 12,288 (a 604 MB
+    128^3 backward-Euler step twice, `spmv` runs the 256^3 forward-Euler
+    kernels (CSR, matrix-free, fused CSR + setBC, indexed COO, ordered HT), `dense` three DENSE steps at N = 12,288 (a 604 MB
     matrix), `learned` two learned-preconditioner solves of the 128^3 step,
     `batched` two steps of a 64-member batch."""
     import torch
@@ -796,6 +796,20 @@ def run_profile_case(args):
             ops.csr_fe_step(nx, ny, nz, A, 0.01, u, out)
         for _ in range(4):
             ops.stencil_fe_step(nx, ny, nz, 0.01, u, out, alpha=alpha)
+        for _ in range(2):
+            ops.csr_fe_step_bc(nx, ny, nz, A, 0.01, u, u, out)
+        N = nx * ny * nz
+        rows = torch.repeat_interleave(torch.arange(N, device="cuda", dtype=torch.int32),
+                                       (A[0][1:] - A[0][:-1]).to(torch.int64))
+        rowstart = ops.coo_row_index(N, rows)
+        for _ in range(2):
+            ops.coo_step_indexed(N, rowstart, A[1], A[2], 0.01, u, out, fe=True)
+        del rows, rowstart
+        ts = ops.ht_table_size(A[2].numel(), N, 1)
+        keys, vals = ops.ht_build(N, *A, ts)
+        order = ops.ht_row_order(N, ts)
+        for _ in range(2):
+            ops.ht_spmv_ordered(nx, ny, nz, keys, vals, 0.01, order, u, out, fe=True)
         torch.cuda.synchronize()
         print("spmv ok")
 
