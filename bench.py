@@ -614,13 +614,16 @@ def run_piro(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
 
-    spmv = spmv_section(torch, ops, steps=20, warmup=3, peak=peak) if rank == 0 else None
-    configs = config_sections(torch, peak) if rank == 0 else None
+    # the per-configuration sections run on a single-GPU run only: under
+    # torchrun the other ranks would wait for them at the closing barrier
+    solo = world == 1
+    spmv = spmv_section(torch, ops, steps=20, warmup=3, peak=peak) if solo else None
+    configs = config_sections(torch, peak) if solo else None
     learned = (learned_section(torch, ops, cfg, A, alpha, ms_step, main["iters"], min(args.steps, 40), tf_peak,
-                               l2_flush) if rank == 0 else None)
-    batched = batched_section(torch, ops, peak) if rank == 0 else None
-    next_rows = next_rows_section(torch, ops, peak) if rank == 0 else None
-    assembly = assembly_section(torch, ops, peak) if rank == 0 else None
+                               l2_flush) if solo else None)
+    batched = batched_section(torch, ops, peak) if solo else None
+    next_rows = next_rows_section(torch, ops, peak) if solo else None
+    assembly = assembly_section(torch, ops, peak) if solo else None
 
     cpu = None
     fp64 = None
