@@ -5,6 +5,8 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <atomic>
+#include <mutex>
 #include <string>
 
 #include "piro.h"
@@ -28,6 +30,30 @@ inline unsigned grid_for(int64_t n, int64_t per_block, int blocks_per_sm = 8)
     int64_t cap = (int64_t)sm_count() * blocks_per_sm * 16;
     if (want < 1) want = 1;
     return (unsigned)(want < cap ? want : cap);
+}
+
+// One-time setup per (call site, device): kernel attributes, occupancy
+// figures, small device buffers.  Safe when several host threads drive the
+// library; a setup that fails is tried again on the next call.
+constexpr int kMaxDevices = 64;
+struct DeviceOnce {
+    std::mutex mu;
+    std::atomic<bool> done[kMaxDevices] = {};
+};
+
+template <typename F>
+int device_once(DeviceOnce &once, int dev, F &&init)
+{
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("device index %d out of range", dev);
+        return PIRO_ERR_CUDA;
+    }
+    if (once.done[dev].load(std::memory_order_acquire)) return PIRO_OK;
+    std::lock_guard<std::mutex> lock(once.mu);
+    if (once.done[dev].load(std::memory_order_relaxed)) return PIRO_OK;
+    const int rc = init();
+    if (rc == PIRO_OK) once.done[dev].store(true, std::memory_order_release);
+    return rc;
 }
 
 }  // namespace piro

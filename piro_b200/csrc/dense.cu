@@ -216,7 +216,35 @@ __global__ void __launch_bounds__(kDenseThreads) k_dense_fe(int64_t N, const flo
     if (r < N) out[r] = __fadd_rn(u[r], __fmul_rn(dt, sum));
 }
 
-int *dense_err_flag[64] = {nullptr};  // per device: a bulk-stage wait timed out
+// Per-device setup of the FE step: occupancy of the two bulk shapes and the
+// flag a bulk-stage wait sets when it times out.
+struct DenseDevice {
+    int occ_a = 0, occ_b = 0;
+    int *err_flag = nullptr;
+};
+DenseDevice dense_dev[kMaxDevices];
+DeviceOnce dense_once;
+
+int dense_setup(int dev)
+{
+    return device_once(dense_once, dev, [dev]() -> int {
+        DenseDevice &d = dense_dev[dev];
+        PIRO_CUDA(cudaFuncSetAttribute(k_dense_fe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDenseSmem));
+        PIRO_CUDA(cudaFuncSetAttribute(k_dense_fe_bulk<256, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)bulk_smem<256, 2>()));
+        PIRO_CUDA(cudaFuncSetAttribute(k_dense_fe_bulk<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)bulk_smem<128, 2>()));
+        PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_a, k_dense_fe_bulk<256, 2>, 32,
+                                                                bulk_smem<256, 2>()));
+        PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.occ_b, k_dense_fe_bulk<128, 2>, 32,
+                                                                bulk_smem<128, 2>()));
+        if (!d.err_flag) {
+            PIRO_CUDA(cudaMalloc(&d.err_flag, sizeof(int)));
+            PIRO_CUDA(cudaMemset(d.err_flag, 0, sizeof(int)));
+        }
+        return PIRO_OK;
+    });
+}
 
 }  // namespace
 }  // namespace piro
@@ -242,40 +270,25 @@ extern "C" int piro_dense_fe_step(int64_t N, const float *A, float dt, const flo
 {
     PIRO_ARG(N >= 1 && A && u && out && u != out, "piro_dense_fe_step: bad arguments");
     PIRO_ARG(cdiv(N, kDenseRows) < 2147483647, "piro_dense_fe_step: N too large");
-    static bool attr_set[64] = {false};
-    int *(&err_flag)[64] = dense_err_flag;
     int dev = 0;
     PIRO_CUDA(cudaGetDevice(&dev));
-    PIRO_ARG(dev >= 0 && dev < 64, "piro_dense_fe_step: device index");
-    static int occ_a[64], occ_b[64];
-    if (!attr_set[dev]) {
-        PIRO_CUDA(cudaFuncSetAttribute(k_dense_fe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDenseSmem));
-        PIRO_CUDA(cudaFuncSetAttribute(k_dense_fe_bulk<256, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)bulk_smem<256, 2>()));
-        PIRO_CUDA(cudaFuncSetAttribute(k_dense_fe_bulk<128, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)bulk_smem<128, 2>()));
-        PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a[dev], k_dense_fe_bulk<256, 2>, 32,
-                                                                bulk_smem<256, 2>()));
-        PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b[dev], k_dense_fe_bulk<128, 2>, 32,
-                                                                bulk_smem<128, 2>()));
-        PIRO_CUDA(cudaMalloc(&err_flag[dev], sizeof(int)));
-        PIRO_CUDA(cudaMemset(err_flag[dev], 0, sizeof(int)));
-        attr_set[dev] = true;
-    }
+    const int rc = dense_setup(dev);
+    if (rc != PIRO_OK) return rc;
+    const DenseDevice &d = dense_dev[dev];
     cudaStream_t st = as_stream(stream);
     const bool bulk = N % 4 == 0 && ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(u)) & 15) == 0;
-    if (bulk && occ_a[dev] >= 1 && occ_b[dev] >= 1) {
+    if (bulk && d.occ_a >= 1 && d.occ_b >= 1) {
         // time ~ rounds of row blocks x (CTAs per SM / measured stream rate):
         // 256 columns at up to 3 CTAs/SM ~6.1 TB/s, 128 columns at up to 6 ~6.7 TB/s
         const int64_t nrb = cdiv(N, kBR), sms = sm_count();
-        const int ga = occ_a[dev] < 3 ? occ_a[dev] : 3, gb = occ_b[dev] < 6 ? occ_b[dev] : 6;
+        const int ga = d.occ_a < 3 ? d.occ_a : 3, gb = d.occ_b < 6 ? d.occ_b : 6;
         const double ta = (double)cdiv(nrb, ga * sms) * ga / 6.1, tb = (double)cdiv(nrb, gb * sms) * gb / 6.7;
         if (ta <= tb) {
             const int64_t grid = nrb < ga * sms ? nrb : ga * sms;
-            k_dense_fe_bulk<256, 2><<<(unsigned)grid, 32, bulk_smem<256, 2>(), st>>>(N, A, dt, u, out, err_flag[dev]);
+            k_dense_fe_bulk<256, 2><<<(unsigned)grid, 32, bulk_smem<256, 2>(), st>>>(N, A, dt, u, out, d.err_flag);
         } else {
             const int64_t grid = nrb < gb * sms ? nrb : gb * sms;
-            k_dense_fe_bulk<128, 2><<<(unsigned)grid, 32, bulk_smem<128, 2>(), st>>>(N, A, dt, u, out, err_flag[dev]);
+            k_dense_fe_bulk<128, 2><<<(unsigned)grid, 32, bulk_smem<128, 2>(), st>>>(N, A, dt, u, out, d.err_flag);
         }
         PIRO_CHECK_LAUNCH("k_dense_fe_bulk");
         return PIRO_OK;
@@ -289,14 +302,15 @@ extern "C" int piro_dense_check(piro_stream_t stream)
 {
     int dev = 0;
     PIRO_CUDA(cudaGetDevice(&dev));
-    PIRO_ARG(dev >= 0 && dev < 64, "piro_dense_check: device index");
-    if (!dense_err_flag[dev]) return PIRO_OK;
+    PIRO_ARG(dev >= 0 && dev < kMaxDevices, "piro_dense_check: device index");
+    if (!dense_once.done[dev].load(std::memory_order_acquire)) return PIRO_OK;  // no FE step ran here
+    int *flag = dense_dev[dev].err_flag;
     int h = 0;
     cudaStream_t st = as_stream(stream);
-    PIRO_CUDA(cudaMemcpyAsync(&h, dense_err_flag[dev], sizeof(int), cudaMemcpyDeviceToHost, st));
+    PIRO_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
     PIRO_CUDA(cudaStreamSynchronize(st));
     if (h) {
-        PIRO_CUDA(cudaMemsetAsync(dense_err_flag[dev], 0, sizeof(int), st));
+        PIRO_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));
         set_error("piro_dense_fe_step: a stage wait timed out");
         return PIRO_ERR_CUDA;
     }

@@ -633,11 +633,11 @@ extern "C" int piro_ht_lu_solve(int64_t N, int64_t bw, void *band, size_t band_b
     PIRO_ARG(band && b && x && b != x && band_layout(N, bw, &W, &nf) == PIRO_OK, "piro_ht_lu_solve: bad arguments");
     PIRO_ARG(band_bytes >= scratch_offset(nf) + kScratchBytes, "piro_ht_lu_solve: band buffer too small");
     cudaStream_t st = as_stream(stream);
-    static int grid[64] = {0};
+    static int grid[kMaxDevices] = {0};
+    static DeviceOnce once;
     int dev = 0;
     PIRO_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return PIRO_ERR_CUDA;
-    if (!grid[dev]) {
+    const int rc = device_once(once, dev, [dev]() -> int {
         int per_sm = 0;
         PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_band_solve, kSolveThreads, 0));
         const int g = sm_count();  // at most one CTA per SM
@@ -646,7 +646,9 @@ extern "C" int piro_ht_lu_solve(int64_t N, int64_t bw, void *band, size_t band_b
             return PIRO_ERR_CUDA;
         }
         grid[dev] = g < 2 ? 2 : (g > kMaxCta ? kMaxCta : g);
-    }
+        return PIRO_OK;
+    });
+    if (rc != PIRO_OK) return rc;
     char *scratch = static_cast<char *>(band) + scratch_offset(nf);
     SolveArgs A;
     A.N = N;

@@ -658,14 +658,17 @@ template <int kEpi>
 static int conv_tc(const bf16 *in, bf16 *out, float *zout, const bf16 *wpk, const GridDiv &g, int64_t N, int batch,
                    const double *rr, double n_int, const int *skip, int *err, cudaStream_t st)
 {
-    static bool attr = false;
-    if (!attr) {
+    static DeviceOnce once;
+    int dev = 0;
+    PIRO_CUDA(cudaGetDevice(&dev));
+    int rc = device_once(once, dev, []() -> int {
         PIRO_CUDA(cudaFuncSetAttribute(tc::k_conv16_tc<kEpi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        tc::kSmemBytes));
-        attr = true;
-    }
+        return PIRO_OK;
+    });
+    if (rc != PIRO_OK) return rc;
     CUtensorMap map;
-    int rc = encode_rows_map(&map, in, N * batch);
+    rc = encode_rows_map(&map, in, N * batch);
     if (rc) return rc;
     const int64_t nxy = (int64_t)g.nx * g.ny;
     const int ncol = (int)cdiv(nxy, tc::kRows);
@@ -708,12 +711,15 @@ static int launch_bwd_w(piro_pcnet *n, const GridDiv &g, int64_t N, int batch, c
                         float *grad_w, cudaStream_t st)
 {
     const size_t smem = sizeof(float) * (9 * (kWChunk + 2) * CI + kWChunk * CO);
-    static bool attr = false;
-    if (!attr) {
+    static DeviceOnce once;
+    int dev = 0;
+    PIRO_CUDA(cudaGetDevice(&dev));
+    const int rc = device_once(once, dev, [smem]() -> int {
         PIRO_CUDA(cudaFuncSetAttribute(k_conv_bwd_w<CI, CO, GT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
-        attr = true;
-    }
+        return PIRO_OK;
+    });
+    if (rc != PIRO_OK) return rc;
     const int nblocks = kRedBlocks;
     constexpr int P = kTaps * CI * CO;
     k_conv_bwd_w<CI, CO, GT><<<nblocks, 256, smem, st>>>(g, N, batch, x, gy, n->partials);
