@@ -628,7 +628,6 @@ __global__ void k_pc_feature(GridDiv g, int64_t N, const float *__restrict__ alp
 // B200: 0.869 vs 0.924 ms per 128^3 step; 1024 x 1: 0.924).
 constexpr int kPT = 512;
 constexpr int kPMaxBlocks = 2048;
-constexpr int kPSlots = 8;
 
 struct PArgs {
     GridDiv g;
@@ -646,7 +645,12 @@ struct PArgs {
     int max_outer, max_inner;
     long long spin_limit;
     int vec_a, vec_b;  // float4 paths usable (alignment and divisibility checked on the host)
+    int64_t own_cells;  // resident variant: cells per block (a multiple of 4), else 0
 };
+
+// Dynamic shared memory the resident variant may use per block: two blocks of
+// 512 threads per SM within the 228 KB of a B200 SM.
+constexpr int kResSmemMax = 110 * 1024;
 
 // Loads of data written earlier in the same launch by other blocks: ordinary
 // (L1-cacheable, never the read-only .nc path) loads, ordered after the grid
@@ -659,30 +663,29 @@ __device__ __forceinline__ T ld_(const T *p)
 }
 
 // Grid barrier with a bounded wait: false if the wait ran out or another block
-// reported an error (every block then leaves the kernel).
-__device__ __forceinline__ bool grid_barrier(DevState *st, long long spin_limit, int *s_ok)
+// reported an error (every block then leaves the kernel).  The arrival count
+// only grows within a launch (it is zeroed before the launch): barrier k waits
+// for k * gridDim arrivals, so no block resets the counter and the last block
+// releases the others by its arrival alone.  Measured on B200 at 296 blocks:
+// 3.4 us per barrier and all-sum, against 4.2 us when the last block resets
+// the counter and then bumps a generation word that the others poll.
+__device__ __forceinline__ bool grid_barrier(DevState *st, unsigned &target, long long spin_limit, int *s_ok)
 {
     __syncthreads();
+    target += gridDim.x;
     if (threadIdx.x == 0) {
-        volatile unsigned *vgen = &st->bar_gen;
-        volatile int *verr = &st->bar_err;
-        const unsigned g = *vgen;
         __threadfence();
-        const unsigned arrived = atomicAdd(&st->bar_count, 1u) + 1u;
+        atomicAdd(&st->bar_count, 1u);
+        volatile unsigned *vcount = &st->bar_count;
+        volatile int *verr = &st->bar_err;
         int ok = 1;
-        if (arrived == gridDim.x) {
-            atomicExch(&st->bar_count, 0u);
-            __threadfence();
-            atomicAdd(&st->bar_gen, 1u);
-        } else {
-            long long spins = 0;
-            while (*vgen == g) {
-                if (*verr || ++spins > spin_limit) {
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(32);
+        long long spins = 0;
+        while ((int)(*vcount - target) < 0) {
+            if (*verr || ++spins > spin_limit) {
+                ok = 0;
+                break;
             }
+            __nanosleep(32);
         }
         if (*verr) ok = 0;
         if (!ok) atomicExch(&st->bar_err, 1);
@@ -759,19 +762,32 @@ __device__ __forceinline__ void all_sums(const double *partials, int first, doub
     __syncthreads();
 }
 
+// Where a block keeps r, d and q: the global arrays (indexed by cell), or, in
+// the resident variant, shared memory holding the block's own contiguous
+// cells [c0, c0 + own_cells) (indexed by cell - c0).  No phase reads r, d or q
+// at a neighbour, so only z and p have to go through global memory.
+template <bool kRes>
+struct Own {
+    float *r, *d, *q;
+    int64_t c0;
+    __device__ __forceinline__ int64_t c(int64_t i) const { return kRes ? i - c0 : i; }
+    __device__ __forceinline__ int64_t g(int64_t v) const { return kRes ? v - (c0 >> 2) : v; }
+};
+
 // Phase A on groups of 4 x-adjacent cells (nx % 4 == 0: a group never spans
 // two x-lines, and every row offset keeps 16-byte alignment).  Per group:
 // 11 float4 loads + 4 scalar halo loads instead of 60 scalar loads.
-__device__ __forceinline__ double cg_phase_a_vec(const PArgs &P, const float *pold, float *pnew, float fb, int64_t v0,
-                                                 int64_t dv)
+template <bool kRes>
+__device__ __forceinline__ double cg_phase_a_vec(const PArgs &P, const Own<kRes> &O, const float *pold, float *pnew,
+                                                 float fb, int64_t v0, int64_t v1, int64_t dv)
 {
     const GridDiv &g = P.g;
-    const int64_t nv = P.N >> 2, rx = g.nx >> 2, rxy = ((int64_t)g.nx * g.ny) >> 2;
+    const int64_t rx = g.nx >> 2, rxy = ((int64_t)g.nx * g.ny) >> 2;
     const float4 *Z = reinterpret_cast<const float4 *>(P.z);
     const float4 *Po = reinterpret_cast<const float4 *>(pold);
     const float4 *Al = reinterpret_cast<const float4 *>(P.alpha);
     double pq = 0.0;
-    for (int64_t v = v0; v < nv; v += dv) {
+    for (int64_t v = v0; v < v1; v += dv) {
         const int64_t i = v << 2;
         int x0, y, z;
         g.coords((uint32_t)i, x0, y, z);
@@ -805,7 +821,7 @@ __device__ __forceinline__ double cg_phase_a_vec(const PArgs &P, const float *po
             }
         }
         reinterpret_cast<float4 *>(pnew)[v] = make_float4(pn[0], pn[1], pn[2], pn[3]);
-        reinterpret_cast<float4 *>(P.q)[v] = make_float4(qv[0], qv[1], qv[2], qv[3]);
+        reinterpret_cast<float4 *>(O.q)[O.g(v)] = make_float4(qv[0], qv[1], qv[2], qv[3]);
     }
     return pq;
 }
@@ -813,22 +829,25 @@ __device__ __forceinline__ double cg_phase_a_vec(const PArgs &P, const float *po
 // Phase B on float4 groups (N % 4 == 0).  Boundary lanes carry p = q = r = 0
 // and dinv = 0, so the update leaves them at zero without a branch; only the
 // dot products are masked.
-__device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const float *pnew, float fa, int64_t v0, int64_t dv,
-                                               double &rzn, double &rr)
+template <bool kRes>
+__device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const Own<kRes> &O, const float *pnew, float fa,
+                                               int64_t v0, int64_t v1, int64_t dv, double &rzn, double &rr)
 {
-    const int64_t nv = P.N >> 2;
-    for (int64_t v = v0; v < nv; v += dv) {
+    float4 *D = reinterpret_cast<float4 *>(O.d), *R = reinterpret_cast<float4 *>(O.r);
+    const float4 *Q = reinterpret_cast<const float4 *>(O.q);
+    for (int64_t v = v0; v < v1; v += dv) {
+        const int64_t o = O.g(v);
         const float4 di = __ldg(reinterpret_cast<const float4 *>(P.dinv) + v);
         const float4 al = __ldg(reinterpret_cast<const float4 *>(P.alpha) + v);
         const float4 pp = ld_(reinterpret_cast<const float4 *>(pnew) + v);
-        const float4 qq = ld_(reinterpret_cast<const float4 *>(P.q) + v);
-        float4 dd = ld_(reinterpret_cast<const float4 *>(P.d) + v);
-        float4 r4 = ld_(reinterpret_cast<const float4 *>(P.r) + v);
+        const float4 qq = Q[o];
+        float4 dd = D[o];
+        float4 r4 = R[o];
         dd.x += fa * pp.x; dd.y += fa * pp.y; dd.z += fa * pp.z; dd.w += fa * pp.w;
         r4.x -= fa * qq.x; r4.y -= fa * qq.y; r4.z -= fa * qq.z; r4.w -= fa * qq.w;
         const float4 z4 = make_float4(r4.x * di.x, r4.y * di.y, r4.z * di.z, r4.w * di.w);
-        reinterpret_cast<float4 *>(P.d)[v] = dd;
-        reinterpret_cast<float4 *>(P.r)[v] = r4;
+        D[o] = dd;
+        R[o] = r4;
         reinterpret_cast<float4 *>(P.z)[v] = z4;
         if (di.x != 0.0f) { rzn += (double)r4.x / (double)al.x * (double)z4.x; rr += (double)r4.x * (double)r4.x; }
         if (di.y != 0.0f) { rzn += (double)r4.y / (double)al.y * (double)z4.y; rr += (double)r4.y * (double)r4.y; }
@@ -837,6 +856,12 @@ __device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const float *pnew
     }
 }
 
+// kRes: the resident variant (P.own_cells > 0, float4 paths only): each block
+// works on its own contiguous cells and keeps their r, d and q in dynamic
+// shared memory (3 * own_cells floats), so phase B streams 16 instead of 36
+// bytes per cell through L2 and phase A stores no q.  Otherwise the grid
+// strides over all cells and r, d, q live in global memory.
+template <bool kRes>
 __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
 {
     __shared__ double s_warp[32];
@@ -844,17 +869,44 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
     __shared__ double s_b;
     __shared__ double s_bn[4];
     __shared__ int s_ok;
+    extern __shared__ float4 s_own[];
     const GridDiv g = P.g;
     const int64_t N = P.N;
     const int64_t sxy = (int64_t)g.nx * g.ny;
-    const int64_t i0 = (int64_t)blockIdx.x * kPT + threadIdx.x, di = (int64_t)gridDim.x * kPT;
+    // cells [c_beg, c_end) step c_step and float4 groups [v_beg, v_end) step c_step of this thread
+    int64_t c_beg, c_end, c_step, v_beg, v_end;
+    Own<kRes> O;
+    if (kRes) {
+        const int64_t c0 = (int64_t)blockIdx.x * P.own_cells, c1 = c0 + P.own_cells < N ? c0 + P.own_cells : N;
+        const int64_t G = P.own_cells >> 2;
+        c_beg = c0 + threadIdx.x;
+        c_end = c1;
+        c_step = kPT;
+        v_beg = (c0 >> 2) + threadIdx.x;
+        v_end = c1 >> 2;
+        O.r = reinterpret_cast<float *>(s_own);
+        O.d = reinterpret_cast<float *>(s_own + G);
+        O.q = reinterpret_cast<float *>(s_own + 2 * G);
+        O.c0 = c0;
+    } else {
+        c_beg = (int64_t)blockIdx.x * kPT + threadIdx.x;
+        c_end = N;
+        c_step = (int64_t)gridDim.x * kPT;
+        v_beg = c_beg;
+        v_end = N >> 2;
+        O.r = P.r;
+        O.d = P.d;
+        O.q = P.q;
+        O.c0 = 0;
+    }
     auto inter = [&](int64_t i) {
         int x, y, z;
         g.coords((uint32_t)i, x, y, z);
         return x > 0 && x < g.nx - 1 && y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1;
     };
+    unsigned bar_target = 0;
     // P0: x = b on the interior (0 on the boundary), beff = b_I - A_IB b_B, d = p = 0
-    for (int64_t i = i0; i < N; i += di) {
+    for (int64_t i = c_beg; i < c_end; i += c_step) {
         if (inter(i)) {
             const float bi = P.b[i];
             double be = (double)bi;
@@ -865,17 +917,21 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
             P.x64[i] = 0.0;
             P.beff[i] = 0.0;
         }
-        P.d[i] = 0.0f;
+        O.d[O.c(i)] = 0.0f;
+        if (kRes) {  // the global r, q hold zeros on boundary cells from creation; shared memory does not
+            O.r[O.c(i)] = 0.0f;
+            O.q[O.c(i)] = 0.0f;
+        }
         P.p0[i] = 0.0f;
         P.p1[i] = 0.0f;
     }
     int status = PIRO_ERR_NOT_CONVERGED, outer = 0, inner_total = 0;
     double rel = INFINITY, prev_rel = INFINITY;
-    bool ok = grid_barrier(P.st, P.spin_limit, &s_ok);
+    bool ok = grid_barrier(P.st, bar_target, P.spin_limit, &s_ok);
     for (int sweep = 0; ok; ++sweep) {
         // R: r = beff - A_II x in FP64, z = r / A_rr
         double rr64 = 0.0, bb = 0.0, rz = 0.0, rr32 = 0.0;
-        for (int64_t i = i0; i < N; i += di) {
+        for (int64_t i = c_beg; i < c_end; i += c_step) {
             if (!inter(i)) continue;
             const float a = __ldg(P.alpha + i);
             const double cd = (double)__fadd_rn(1.0f, __fmul_rn(P.mdt, __fmul_rn(a, P.vself)));
@@ -886,7 +942,7 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
             const double ri = ld_(P.beff + i) - (cd * ld_(P.x64 + i) + co * nb);
             const float rf = (float)ri;
             const float zf = rf * __ldg(P.dinv + i);
-            P.r[i] = rf;
+            O.r[O.c(i)] = rf;
             P.z[i] = zf;
             const double bi = (double)P.b[i];
             rr64 += ri * ri;
@@ -896,7 +952,7 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
         }
         double rsum[4] = {rr64, bb, rz, rr32};
         put_partials<4>(P.partials, 0, rsum, s_red);
-        if (!(ok = grid_barrier(P.st, P.spin_limit, &s_ok))) break;
+        if (!(ok = grid_barrier(P.st, bar_target, P.spin_limit, &s_ok))) break;
         double rt[4];
         all_sums<4>(P.partials, 0, rt, s_red, s_bn);
         const double t_rr64 = rt[0], t_bb = rt[1];
@@ -922,9 +978,9 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
             const float fb = (float)beta;
             double pq = 0.0;
             if (P.vec_a) {
-                pq = cg_phase_a_vec(P, pold, pnew, fb, i0, di);
+                pq = cg_phase_a_vec<kRes>(P, O, pold, pnew, fb, v_beg, v_end, c_step);
             } else {
-                for (int64_t i = i0; i < N; i += di) {
+                for (int64_t i = c_beg; i < c_end; i += c_step) {
                     if (!inter(i)) continue;
                     const float a = __ldg(P.alpha + i);
                     const float cur = ld_(P.z + i) + fb * ld_(pold + i);
@@ -938,12 +994,12 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
                     const float co = __fmul_rn(P.mdt, __fmul_rn(a, P.vnb));
                     const float qv = cd * cur + co * (((xm + xp) + (ym + yp)) + (zm + zp));
                     pnew[i] = cur;
-                    P.q[i] = qv;
+                    O.q[O.c(i)] = qv;
                     pq += (double)cur * (double)qv / (double)a;
                 }
             }
             put_partial(P.partials, 4, pq, s_warp);
-            if (!(ok = grid_barrier(P.st, P.spin_limit, &s_ok))) break;
+            if (!(ok = grid_barrier(P.st, bar_target, P.spin_limit, &s_ok))) break;
             const double t_pq = all_sum(P.partials, 4, s_warp, &s_b);
             const double alpha_k = t_rz / t_pq;
             if (!isfinite(alpha_k) || t_pq <= 0.0) { broken = true; break; }
@@ -951,22 +1007,22 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
             // B: d += a p, r -= a q, z = r / A_rr
             double bsum[2] = {0.0, 0.0};
             if (P.vec_b) {
-                cg_phase_b_vec(P, pnew, fa, i0, di, bsum[0], bsum[1]);
+                cg_phase_b_vec<kRes>(P, O, pnew, fa, v_beg, v_end, c_step, bsum[0], bsum[1]);
             } else {
-                for (int64_t i = i0; i < N; i += di) {
+                for (int64_t i = c_beg; i < c_end; i += c_step) {
                     const float dv = __ldg(P.dinv + i);
                     if (dv == 0.0f) continue;
-                    P.d[i] += fa * pnew[i];
-                    const float ri = P.r[i] - fa * P.q[i];
+                    O.d[O.c(i)] += fa * pnew[i];
+                    const float ri = O.r[O.c(i)] - fa * O.q[O.c(i)];
                     const float zi = ri * dv;
-                    P.r[i] = ri;
+                    O.r[O.c(i)] = ri;
                     P.z[i] = zi;
                     bsum[0] += (double)ri / (double)__ldg(P.alpha + i) * (double)zi;
                     bsum[1] += (double)ri * (double)ri;
                 }
             }
             put_partials<2>(P.partials, 5, bsum, s_red);
-            if (!(ok = grid_barrier(P.st, P.spin_limit, &s_ok))) break;
+            if (!(ok = grid_barrier(P.st, bar_target, P.spin_limit, &s_ok))) break;
             double bt[2];
             all_sums<2>(P.partials, 5, bt, s_red, s_bn);
             const double t_rzn = bt[0], t_rr = bt[1];
@@ -982,17 +1038,17 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
         if (!ok) break;
         if (broken) { status = PIRO_STATUS_STALLED; break; }
         // X: x += d, d = 0
-        for (int64_t i = i0; i < N; i += di) {
-            const float dv = P.d[i];
+        for (int64_t i = c_beg; i < c_end; i += c_step) {
+            const float dv = O.d[O.c(i)];
             if (dv != 0.0f) {
                 P.x64[i] += (double)dv;
-                P.d[i] = 0.0f;
+                O.d[O.c(i)] = 0.0f;
             }
         }
-        if (!(ok = grid_barrier(P.st, P.spin_limit, &s_ok))) break;
+        if (!(ok = grid_barrier(P.st, bar_target, P.spin_limit, &s_ok))) break;
     }
     // output: interior from x, boundary from b
-    for (int64_t i = i0; i < N; i += di) P.xout[i] = inter(i) ? (float)P.x64[i] : P.b[i];
+    for (int64_t i = c_beg; i < c_end; i += c_step) P.xout[i] = inter(i) ? (float)P.x64[i] : P.b[i];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         P.st->p_status = ok ? status : PIRO_ERR_CUDA;
         P.st->p_outer = outer;
@@ -1100,6 +1156,8 @@ struct piro_be_solver {
     int32_t *ib_ptr, *ib_col;
     float *ib_val;
     double *beff;
+    int64_t res_cells;  // resident variant: cells per block, 0 if it does not fit
+    size_t res_smem;
     cudaEvent_t pev0, pev1;
     double persist_ms;
     long long persist_launches;
@@ -1267,7 +1325,7 @@ static int be_setup_persistent(piro_be_solver *s)
     int dev = 0, coop = 0, per_sm = 0;
     PIRO_CUDA(cudaGetDevice(&dev));
     PIRO_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-    PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_be_persistent, kPT, 0));
+    PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_be_persistent<false>, kPT, 0));
     if (!coop || per_sm < 1) return PIRO_OK;
     const int64_t N = s->N;
     const GridDiv g(s->nx, s->ny, s->nz);
@@ -1299,6 +1357,27 @@ static int be_setup_persistent(piro_be_solver *s)
     if (grid > need) grid = need;
     s->grid_p = (unsigned)grid;
     s->persist = 1;
+    // resident variant: every block's r, d, q in shared memory, if they fit
+    // with the same grid still co-resident
+    s->res_cells = 0;
+    s->res_smem = 0;
+    const int64_t groups = cdiv(N >> 2, grid);
+    const size_t smem = (size_t)3 * groups * sizeof(float4);
+    if (N % 4 == 0 && s->nx % 4 == 0 && smem <= (size_t)kResSmemMax) {
+        static DeviceOnce once;
+        int rc2 = device_once(once, dev, []() -> int {
+            PIRO_CUDA(cudaFuncSetAttribute(k_be_persistent<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kResSmemMax));
+            return PIRO_OK;
+        });
+        if (rc2) return rc2;
+        int per_sm_res = 0;
+        PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_res, k_be_persistent<true>, kPT, smem));
+        if ((int64_t)per_sm_res * nsm >= grid) {
+            s->res_cells = 4 * groups;
+            s->res_smem = smem;
+        }
+    }
     return PIRO_OK;
 }
 
@@ -1552,10 +1631,17 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
         const bool al16 = ((reinterpret_cast<uintptr_t>(s->alpha) | reinterpret_cast<uintptr_t>(s->dinv)) & 15) == 0;
         P.vec_b = (N % 4 == 0) && al16;
         P.vec_a = P.vec_b && (s->nx % 4 == 0);
+        const bool res = s->res_cells > 0 && P.vec_a;
+        P.own_cells = res ? s->res_cells : 0;
         void *args[] = {&P};
         PIRO_CUDA(cudaMemsetAsync(s->st, 0, sizeof(DevState), st));
         PIRO_CUDA(cudaEventRecord(s->pev0, st));
-        PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_be_persistent, dim3(s->grid_p), dim3(kPT), args, 0, st));
+        if (res)
+            PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_be_persistent<true>, dim3(s->grid_p), dim3(kPT), args,
+                                                  s->res_smem, st));
+        else
+            PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_be_persistent<false>, dim3(s->grid_p), dim3(kPT),
+                                                  args, 0, st));
         PIRO_CUDA(cudaEventRecord(s->pev1, st));
         s->kernel_launches += 1;
         PIRO_CUDA(cudaMemcpyAsync(s->h_st, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, st));
