@@ -235,6 +235,13 @@ int piro_dense_check(piro_stream_t stream);
 int piro_stencil_fe_step(int nx, int ny, int nz, float idx2, float idy2, float idz2, float dt, const float *alpha,
                          const float *u, float *out, piro_stream_t stream);
 
+/* Synchronizes the stream; PIRO_ERR_CUDA if a matrix-free step staged through
+ * TMA (16 <= nx <= 256, nx a divisor of 2048 and a multiple of 4, 16-byte
+ * aligned buffers) had a stage wait -- a bounded wait on its tile copies,
+ * never expected to run out -- give up.  No reference counterpart (the
+ * reference's laplacianscalar.cl is never launched). */
+int piro_stencil_check(piro_stream_t stream);
+
 /* setBC.cl (launched by bc::opencl_setBC, src/bc.cpp:38-65): dst[idx[i]] = src[idx[i]]. */
 int piro_set_bc(int64_t q, const uint32_t *idx, const float *src, float *dst, piro_stream_t stream);
 

@@ -72,6 +72,7 @@ SIGNATURES = {
     "piro_dense_laplacian": (i32, [i32, i32, i32, i32, f32, vp, sz, vp]),
     "piro_dense_fe_step": (i32, [i64, vp, f32, vp, vp, vp]),
     "piro_dense_check": (i32, [vp]),
+    "piro_stencil_check": (i32, [vp]),
     "piro_ht_lu_reference": (i32, [i64, vp, vp, i64, vp]),
     "piro_ht_lu_band_bytes": (i32, [i64, i64, C.POINTER(sz)]),
     "piro_ht_lu_factor": (i32, [i64, i64, vp, vp, i64, f32, f32, vp, sz, vp]),

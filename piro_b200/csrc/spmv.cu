@@ -7,6 +7,9 @@
 // CSR kernels are HBM-bound (8 bytes per nonzero + 12 per row) and share the
 // row loop of csr_tile.cuh: one row per thread in storage order -- the
 // reference's summation order -- so results are bit-exact with SpMVCSR.cl.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "common.cuh"
 #include "csr_tile.cuh"
 
@@ -400,6 +403,241 @@ int launch_csr_step(int nx, int ny, int nz, const int32_t *rowptr, const int32_t
     return PIRO_OK;
 }
 
+
+// The matrix-free update with TMA tile staging, for 16 <= nx <= 256 with
+// nx % 4 == 0 and 2048 % nx == 0.  A CTA of 512 threads owns TY = 2048 / nx
+// full x-rows and marches a run of z planes.  Per plane, thread 0 issues one
+// 3-D TMA load of u's rows y0-1 .. y0+TY (the y halo; coordinates outside the
+// grid arrive as zeros and feed only boundary cells, which copy u) and one of
+// alpha's TY rows, into a ring of kTmaStages stages completed on mbarriers.
+// Planes z-1, z, z+1 are then read from shared memory, so u crosses HBM about
+// once (plus two halo planes per run; the y halo rows are L2 hits, since the
+// CTAs of neighbouring row blocks run together).  Each thread updates 4
+// x-adjacent cells of one row (x neighbours by warp shuffle) and stores them
+// as one float4.  The TMA x coordinate is always 0, so every copy starts on
+// a 16-byte boundary.  Every wait is bounded: a timed-out wait sets *err, and
+// thread 0 waits (bounded) for the CTA's copies in flight before leaving.
+constexpr int kTmaThreads = 512, kTmaStages = 6;
+constexpr long long kTmaSpin = 1ll << 22;
+
+struct StencilTma {
+    int nx, ny, nz, ty, zchunk, has_alpha;
+    float idx2, idy2, idz2, dt;
+    float *out;
+    int *err;
+};
+
+__device__ __forceinline__ uint32_t st_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool st_bar_wait(uint32_t bar, uint32_t parity)
+{
+    for (long long i = 0; i < kTmaSpin; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(kTmaThreads, 2) k_stencil_tma(const __grid_constant__ CUtensorMap umap,
+                                                                 const __grid_constant__ CUtensorMap amap,
+                                                                 StencilTma a)
+{
+    extern __shared__ __align__(128) float sm[];
+    __shared__ __align__(8) uint64_t bars[kTmaStages];
+    const int nx = a.nx, TY = a.ty, tid = threadIdx.x;
+    const int y0 = blockIdx.x * TY;
+    const int z0 = blockIdx.y * a.zchunk, z1 = z0 + a.zchunk < a.nz ? z0 + a.zchunk : a.nz;
+    const int ufl = (TY + 2) * nx, sfl = ufl + (a.has_alpha ? TY * nx : 0);
+    const int nload = z1 - z0 + 2;  // planes z0-1 .. z1
+    if (tid == 0) {
+        for (int s = 0; s < kTmaStages; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(st_smem(&bars[s])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    auto issue = [&](int k) {  // thread 0: plane z0 - 1 + k into stage k % kTmaStages
+        const int s = k % kTmaStages, zz = z0 - 1 + k;
+        const bool with_a = a.has_alpha && zz >= z0 && zz < z1;
+        const uint32_t bar = st_smem(&bars[s]);
+        const uint32_t bytes = (uint32_t)(4 * ufl) + (with_a ? (uint32_t)(4 * TY * nx) : 0u);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+            "[%2];" ::"r"(st_smem(sm + s * sfl)),
+            "l"(reinterpret_cast<uint64_t>(&umap)), "r"(bar), "r"(0), "r"(y0 - 1), "r"(zz)
+            : "memory");
+        if (with_a)
+            asm volatile(
+                "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
+                "%5}], [%2];" ::"r"(st_smem(sm + s * sfl + ufl)),
+                "l"(reinterpret_cast<uint64_t>(&amap)), "r"(bar), "r"(0), "r"(y0), "r"(zz)
+                : "memory");
+    };
+    int next = nload < kTmaStages ? nload : kTmaStages;  // loads issued (same count in every thread)
+    if (tid == 0)
+        for (int k = 0; k < next; ++k) issue(k);
+    const int gpr = nx >> 2;                       // float4 groups per row
+    const int r = tid / gpr, x0 = (tid - r * gpr) << 2;
+    const int y = y0 + r, lane = tid & 31;
+    const bool row_ok = r < TY && y < a.ny;
+    const int64_t sxy = (int64_t)nx * a.ny;
+    int waited = 0;
+    bool ok = true;
+    for (int k = 1; k + 1 < nload; ++k) {  // plane z = z0 - 1 + k from stages k-1, k, k+1
+        bool mine = true;
+        while (mine && waited <= k + 1) {
+            mine = st_bar_wait(st_smem(&bars[waited % kTmaStages]), (uint32_t)((waited / kTmaStages) & 1));
+            waited += mine;
+        }
+        if (!__syncthreads_and(mine)) {
+            ok = false;
+            break;
+        }
+        // every thread is done with plane k - 1, so stage (k - 2) % S is free
+        if (k >= 2 && next < nload) {
+            if (tid == 0) issue(next);
+            ++next;
+        }
+        const int z = z0 - 1 + k;
+        const float *cen = sm + (k % kTmaStages) * sfl, *bel = sm + ((k - 1) % kTmaStages) * sfl,
+                    *abv = sm + ((k + 1) % kTmaStages) * sfl;
+        const int o = (r + 1) * nx + x0;
+        float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (row_ok) c = *reinterpret_cast<const float4 *>(cen + o);
+        // x neighbours: lane - 1's last and lane + 1's first cell (same row when they are needed)
+        float xl = __shfl_up_sync(0xffffffffu, c.w, 1), xr = __shfl_down_sync(0xffffffffu, c.x, 1);
+        if (row_ok) {
+            if (lane == 0 && x0 > 0) xl = cen[o - 1];
+            if (lane == 31 && x0 + 4 < nx) xr = cen[o + 4];
+            float4 res = c;
+            if (y > 0 && y < a.ny - 1 && z > 0 && z < a.nz - 1) {
+                const float4 ym = *reinterpret_cast<const float4 *>(cen + o - nx);
+                const float4 yp = *reinterpret_cast<const float4 *>(cen + o + nx);
+                const float4 zm = *reinterpret_cast<const float4 *>(bel + o);
+                const float4 zp = *reinterpret_cast<const float4 *>(abv + o);
+                const float4 al = a.has_alpha ? *reinterpret_cast<const float4 *>(cen + ufl + r * nx + x0)
+                                              : make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+                const float cs[6] = {xl, c.x, c.y, c.z, c.w, xr};
+                const float ymv[4] = {ym.x, ym.y, ym.z, ym.w}, ypv[4] = {yp.x, yp.y, yp.z, yp.w};
+                const float zmv[4] = {zm.x, zm.y, zm.z, zm.w}, zpv[4] = {zp.x, zp.y, zp.z, zp.w};
+                const float av[4] = {al.x, al.y, al.z, al.w};
+                float rv[4];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    const int x = x0 + t;
+                    rv[t] = (x > 0 && x < nx - 1) ? st_update(cs[t + 1], cs[t], cs[t + 2], ymv[t], ypv[t], zmv[t],
+                                                              zpv[t], av[t], a.idx2, a.idy2, a.idz2, a.dt)
+                                                  : cs[t + 1];
+                }
+                res = make_float4(rv[0], rv[1], rv[2], rv[3]);
+            }
+            __stcs(reinterpret_cast<float4 *>(a.out + (int64_t)z * sxy + (int64_t)y * nx + x0), res);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // this thread's reads before the next refill
+    }
+    if (!ok && tid == 0) {
+        atomicExch(a.err, 1);
+        for (; waited < next; ++waited)
+            (void)st_bar_wait(st_smem(&bars[waited % kTmaStages]), (uint32_t)((waited / kTmaStages) & 1));
+    }
+}
+
+// Per device: the flag a timed-out stage wait of k_stencil_tma sets, and the
+// CTAs of it resident per SM.
+struct StencilTmaDevice {
+    int *err_flag = nullptr;
+    int per_sm = 0;
+};
+StencilTmaDevice stencil_tma_dev[kMaxDevices];
+DeviceOnce stencil_tma_once;
+
+size_t stencil_tma_smem(int nx) { return sizeof(float) * kTmaStages * (size_t)((2 * (2048 / nx) + 2) * nx); }
+
+bool stencil_tma_fits(int nx, int ny, int nz, const float *alpha, const float *u, const float *out)
+{
+    const uintptr_t al = reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(out) |
+                         reinterpret_cast<uintptr_t>(alpha);
+    return nx >= 16 && nx <= 256 && nx % 4 == 0 && 2048 % nx == 0 && (al & 15) == 0 &&
+           (int64_t)nx * ny * nz < ((int64_t)1 << 31);
+}
+
+int encode_plane_map(CUtensorMap *m, const float *base, int nx, int ny, int nz, int rows)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            set_error("cuTensorMapEncodeTiled is not available");
+            return PIRO_ERR_CUDA;
+        }
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+    const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * ny * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)nx, (cuuint32_t)rows, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims, strides, box,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return PIRO_ERR_CUDA;
+    }
+    return PIRO_OK;
+}
+
+int stencil_tma_setup(int dev)
+{
+    return device_once(stencil_tma_once, dev, [dev]() -> int {
+        StencilTmaDevice &d = stencil_tma_dev[dev];
+        // the largest stage ring (nx = 256) sets the attribute for every nx
+        PIRO_CUDA(cudaFuncSetAttribute(k_stencil_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)stencil_tma_smem(256)));
+        PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.per_sm, k_stencil_tma, kTmaThreads,
+                                                                stencil_tma_smem(256)));
+        if (!d.err_flag) {
+            PIRO_CUDA(cudaMalloc(&d.err_flag, sizeof(int)));
+            PIRO_CUDA(cudaMemset(d.err_flag, 0, sizeof(int)));
+        }
+        return PIRO_OK;
+    });
+}
+
+int stencil_tma_step(int nx, int ny, int nz, float idx2, float idy2, float idz2, float dt, const float *alpha,
+                     const float *u, float *out, cudaStream_t st)
+{
+    int dev = 0;
+    PIRO_CUDA(cudaGetDevice(&dev));
+    int rc = stencil_tma_setup(dev);
+    if (rc != PIRO_OK) return rc;
+    const StencilTmaDevice &d = stencil_tma_dev[dev];
+    const int TY = 2048 / nx;
+    const int ytiles = (int)cdiv(ny, TY);
+    // one wave: about (resident CTAs) / (row blocks) z runs per row block
+    const int wave = (d.per_sm > 0 ? d.per_sm : 1) * sm_count();
+    int runs = wave / ytiles;
+    runs = runs < 1 ? 1 : (runs > nz ? nz : runs);
+    const int zchunk = (int)cdiv(nz, runs);
+    runs = (int)cdiv(nz, zchunk);
+    CUtensorMap umap, amap;
+    rc = encode_plane_map(&umap, u, nx, ny, nz, TY + 2);
+    if (!rc) rc = encode_plane_map(&amap, alpha ? alpha : u, nx, ny, nz, TY);
+    if (rc) return rc;
+    StencilTma a{nx, ny, nz, TY, zchunk, alpha ? 1 : 0, idx2, idy2, idz2, dt, out, d.err_flag};
+    k_stencil_tma<<<dim3((unsigned)ytiles, (unsigned)runs), kTmaThreads, stencil_tma_smem(nx), st>>>(umap, amap, a);
+    PIRO_CHECK_LAUNCH("k_stencil_tma");
+    return PIRO_OK;
+}
+
 }  // namespace
 }  // namespace piro
 
@@ -563,6 +801,8 @@ extern "C" int piro_stencil_fe_step(int nx, int ny, int nz, float idx2, float id
 {
     PIRO_ARG(grid_ok(nx, ny, nz) && u && out && u != out, "piro_stencil_fe_step: bad arguments");
     const int64_t N = (int64_t)nx * ny * nz;
+    if (stencil_tma_fits(nx, ny, nz, alpha, u, out))
+        return stencil_tma_step(nx, ny, nz, idx2, idy2, idz2, dt, alpha, u, out, as_stream(stream));
     const uintptr_t al = reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(out) |
                          reinterpret_cast<uintptr_t>(alpha);
     if (nx % 4 == 0 && N < ((int64_t)1 << 32) && (al & 15) == 0) {
@@ -575,6 +815,25 @@ extern "C" int piro_stencil_fe_step(int nx, int ny, int nz, float idx2, float id
     const dim3 grid((unsigned)cdiv(nx, kStX), (unsigned)cdiv(ny, kStY), (unsigned)cdiv(nz, kStZ));
     k_stencil<<<grid, block, 0, as_stream(stream)>>>(nx, ny, nz, idx2, idy2, idz2, dt, alpha, u, out);
     PIRO_CHECK_LAUNCH("k_stencil");
+    return PIRO_OK;
+}
+
+extern "C" int piro_stencil_check(piro_stream_t stream)
+{
+    int dev = 0;
+    PIRO_CUDA(cudaGetDevice(&dev));
+    PIRO_ARG(dev >= 0 && dev < kMaxDevices, "piro_stencil_check: device index");
+    if (!stencil_tma_once.done[dev].load(std::memory_order_acquire)) return PIRO_OK;  // no staged step ran here
+    int *flag = stencil_tma_dev[dev].err_flag;
+    int h = 0;
+    cudaStream_t st = as_stream(stream);
+    PIRO_CUDA(cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PIRO_CUDA(cudaStreamSynchronize(st));
+    if (h) {
+        PIRO_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));
+        set_error("piro_stencil_fe_step: a stage wait timed out");
+        return PIRO_ERR_CUDA;
+    }
     return PIRO_OK;
 }
 

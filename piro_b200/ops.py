@@ -236,6 +236,11 @@ def stencil_fe_step(nx, ny, nz, dt, u, out, alpha=None, idx2=1.0, idy2=1.0, idz2
     return out
 
 
+def stencil_check():
+    """Raise if a TMA-staged matrix-free step gave up on a stage wait."""
+    check(lib().piro_stencil_check(_stream()), "piro_stencil_check")
+
+
 def set_bc(idx, src, dst):
     check(lib().piro_set_bc(idx.numel(), _p(idx), _p(src), _p(dst), _stream()), "piro_set_bc")
     return dst

@@ -272,8 +272,11 @@ def test_fe_steps_match_oracle(cuda, oracle, n):
         ops.coo_row_index(N, bad)
 
 
-# nx % 4 == 0 takes the float4 path (48, 64, 4, 8); the others the z-march
-@pytest.mark.parametrize("n", [(48, 40, 36), (33, 9, 17), (3, 3, 3), (70, 12, 5), (64, 8, 5), (4, 4, 4), (8, 3, 3)])
+# nx in {16, 32, 64, 128, 256} takes the TMA-staged path (partial row blocks,
+# one-plane z runs); other nx % 4 == 0 the float4 path (48, 4, 8); the rest
+# the z-march
+@pytest.mark.parametrize("n", [(48, 40, 36), (33, 9, 17), (3, 3, 3), (70, 12, 5), (64, 8, 5), (4, 4, 4), (8, 3, 3),
+                               (16, 130, 6), (32, 70, 11), (128, 19, 33), (256, 10, 3), (64, 64, 64)])
 def test_stencil_matches_oracle(cuda, oracle, n):
     import torch
     from piro_b200 import ops
@@ -289,6 +292,7 @@ def test_stencil_matches_oracle(cuda, oracle, n):
     ref = oracle.stencil_fe(nx, ny, nz, 0.01, u)
     ops.stencil_fe_step(nx, ny, nz, 0.01, dev(torch, u), out)
     assert f32_bits_equal(h(out), ref)
+    ops.stencil_check()
 
 
 def test_vector_ops_and_dot(cuda, oracle):
