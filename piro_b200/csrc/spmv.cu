@@ -405,19 +405,23 @@ int launch_csr_step(int nx, int ny, int nz, const int32_t *rowptr, const int32_t
 
 
 // The matrix-free update with TMA tile staging, for 16 <= nx <= 256 with
-// nx % 4 == 0 and 2048 % nx == 0.  A CTA of 512 threads owns TY = 2048 / nx
-// full x-rows and marches a run of z planes.  Per plane, thread 0 issues one
-// 3-D TMA load of u's rows y0-1 .. y0+TY (the y halo; coordinates outside the
-// grid arrive as zeros and feed only boundary cells, which copy u) and one of
-// alpha's TY rows, into a ring of kTmaStages stages completed on mbarriers.
-// Planes z-1, z, z+1 are then read from shared memory, so u crosses HBM about
+// nx % 4 == 0 and 2048 % nx == 0.  A CTA owns TY = 2048 / nx full x-rows and
+// marches a run of z planes.  One producer warp (its lane 0) issues, per
+// plane, one 3-D TMA load of u's rows y0-1 .. y0+TY (the y halo; coordinates
+// outside the grid arrive as zeros and feed only boundary cells, which copy u)
+// and one of alpha's TY rows, into a ring of kTmaStages stages: "full"
+// mbarriers complete on the copies' bytes, "empty" mbarriers on the arrival
+// of all 16 consumer warps, so a stage is refilled as soon as the last warp
+// has read it and no warp ever waits for another at a CTA barrier.  Consumer
+// warps read planes z-1, z, z+1 from shared memory, so u crosses HBM about
 // once (plus two halo planes per run; the y halo rows are L2 hits, since the
-// CTAs of neighbouring row blocks run together).  Each thread updates 4
-// x-adjacent cells of one row (x neighbours by warp shuffle) and stores them
-// as one float4.  The TMA x coordinate is always 0, so every copy starts on
-// a 16-byte boundary.  Every wait is bounded: a timed-out wait sets *err, and
-// thread 0 waits (bounded) for the CTA's copies in flight before leaving.
-constexpr int kTmaThreads = 512, kTmaStages = 6;
+// CTAs of neighbouring row blocks run together).  Each consumer thread
+// updates 4 x-adjacent cells of one row (x neighbours by warp shuffle) and
+// stores them as one float4.  The TMA x coordinate is always 0, so every copy
+// starts on a 16-byte boundary.  Every wait is bounded: a timed-out wait sets
+// *err; the producer then waits (bounded) for its copies in flight, so none
+// lands after the CTA has left.
+constexpr int kTmaThreads = 512, kTmaStages = 6, kTmaWarps = kTmaThreads / 32;
 constexpr long long kTmaSpin = 1ll << 22;
 
 struct StencilTma {
@@ -445,65 +449,77 @@ __device__ __forceinline__ bool st_bar_wait(uint32_t bar, uint32_t parity)
     return false;
 }
 
-__global__ void __launch_bounds__(kTmaThreads, 2) k_stencil_tma(const __grid_constant__ CUtensorMap umap,
-                                                                 const __grid_constant__ CUtensorMap amap,
-                                                                 StencilTma a)
+__global__ void __launch_bounds__(kTmaThreads + 32, 2) k_stencil_tma(const __grid_constant__ CUtensorMap umap,
+                                                                      const __grid_constant__ CUtensorMap amap,
+                                                                      StencilTma a)
 {
     extern __shared__ __align__(128) float sm[];
-    __shared__ __align__(8) uint64_t bars[kTmaStages];
+    __shared__ __align__(8) uint64_t full[kTmaStages], empty[kTmaStages];
     const int nx = a.nx, TY = a.ty, tid = threadIdx.x;
     const int y0 = blockIdx.x * TY;
     const int z0 = blockIdx.y * a.zchunk, z1 = z0 + a.zchunk < a.nz ? z0 + a.zchunk : a.nz;
     const int ufl = (TY + 2) * nx, sfl = ufl + (a.has_alpha ? TY * nx : 0);
-    const int nload = z1 - z0 + 2;  // planes z0-1 .. z1
+    const int nload = z1 - z0 + 2;  // planes z0-1 .. z1; load k lives in stage k % kTmaStages
     if (tid == 0) {
-        for (int s = 0; s < kTmaStages; ++s)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(st_smem(&bars[s])) : "memory");
+        for (int s = 0; s < kTmaStages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(st_smem(&full[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(st_smem(&empty[s])), "r"(kTmaWarps)
+                         : "memory");
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    auto issue = [&](int k) {  // thread 0: plane z0 - 1 + k into stage k % kTmaStages
-        const int s = k % kTmaStages, zz = z0 - 1 + k;
-        const bool with_a = a.has_alpha && zz >= z0 && zz < z1;
-        const uint32_t bar = st_smem(&bars[s]);
-        const uint32_t bytes = (uint32_t)(4 * ufl) + (with_a ? (uint32_t)(4 * TY * nx) : 0u);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-        asm volatile(
-            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
-            "[%2];" ::"r"(st_smem(sm + s * sfl)),
-            "l"(reinterpret_cast<uint64_t>(&umap)), "r"(bar), "r"(0), "r"(y0 - 1), "r"(zz)
-            : "memory");
-        if (with_a)
+    if (tid >= kTmaThreads) {  // producer warp
+        if (tid != kTmaThreads) return;
+        int L = 0;
+        bool ok = true;
+        for (; L < nload; ++L) {
+            const int s = L % kTmaStages, zz = z0 - 1 + L;
+            // the stage's previous load (L - S) is released once every consumer warp has read it
+            if (L >= kTmaStages && !st_bar_wait(st_smem(&empty[s]), (uint32_t)((L / kTmaStages - 1) & 1))) {
+                ok = false;
+                break;
+            }
+            const bool with_a = a.has_alpha && zz >= z0 && zz < z1;
+            const uint32_t bar = st_smem(&full[s]);
+            const uint32_t bytes = (uint32_t)(4 * ufl) + (with_a ? (uint32_t)(4 * TY * nx) : 0u);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                         : "memory");
             asm volatile(
                 "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
-                "%5}], [%2];" ::"r"(st_smem(sm + s * sfl + ufl)),
-                "l"(reinterpret_cast<uint64_t>(&amap)), "r"(bar), "r"(0), "r"(y0), "r"(zz)
+                "%5}], [%2];" ::"r"(st_smem(sm + s * sfl)),
+                "l"(reinterpret_cast<uint64_t>(&umap)), "r"(bar), "r"(0), "r"(y0 - 1), "r"(zz)
                 : "memory");
-    };
-    int next = nload < kTmaStages ? nload : kTmaStages;  // loads issued (same count in every thread)
-    if (tid == 0)
-        for (int k = 0; k < next; ++k) issue(k);
-    const int gpr = nx >> 2;                       // float4 groups per row
+            if (with_a)
+                asm volatile(
+                    "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+                    "%4, %5}], [%2];" ::"r"(st_smem(sm + s * sfl + ufl)),
+                    "l"(reinterpret_cast<uint64_t>(&amap)), "r"(bar), "r"(0), "r"(y0), "r"(zz)
+                    : "memory");
+        }
+        if (!ok) {
+            atomicExch(a.err, 1);
+            // each stage's latest load is the only one that can still be in flight
+            for (int j = L - kTmaStages < 0 ? 0 : L - kTmaStages; j < L; ++j)
+                (void)st_bar_wait(st_smem(&full[j % kTmaStages]), (uint32_t)((j / kTmaStages) & 1));
+        }
+        return;
+    }
+    const int gpr = nx >> 2;  // float4 groups per row
     const int r = tid / gpr, x0 = (tid - r * gpr) << 2;
     const int y = y0 + r, lane = tid & 31;
     const bool row_ok = r < TY && y < a.ny;
     const int64_t sxy = (int64_t)nx * a.ny;
     int waited = 0;
-    bool ok = true;
-    for (int k = 1; k + 1 < nload; ++k) {  // plane z = z0 - 1 + k from stages k-1, k, k+1
-        bool mine = true;
-        while (mine && waited <= k + 1) {
-            mine = st_bar_wait(st_smem(&bars[waited % kTmaStages]), (uint32_t)((waited / kTmaStages) & 1));
-            waited += mine;
+    for (int k = 1; k + 1 < nload; ++k) {  // plane z = z0 - 1 + k from loads k-1, k, k+1
+        bool ok = true;
+        while (ok && waited <= k + 1) {
+            ok = st_bar_wait(st_smem(&full[waited % kTmaStages]), (uint32_t)((waited / kTmaStages) & 1));
+            waited += ok;
         }
-        if (!__syncthreads_and(mine)) {
-            ok = false;
+        if (!__all_sync(0xffffffffu, ok)) {  // the whole warp leaves together (the shuffles below take all lanes)
+            if (lane == 0) atomicExch(a.err, 1);
             break;
-        }
-        // every thread is done with plane k - 1, so stage (k - 2) % S is free
-        if (k >= 2 && next < nload) {
-            if (tid == 0) issue(next);
-            ++next;
         }
         const int z = z0 - 1 + k;
         const float *cen = sm + (k % kTmaStages) * sfl, *bel = sm + ((k - 1) % kTmaStages) * sfl,
@@ -540,12 +556,12 @@ __global__ void __launch_bounds__(kTmaThreads, 2) k_stencil_tma(const __grid_con
             }
             __stcs(reinterpret_cast<float4 *>(a.out + (int64_t)z * sxy + (int64_t)y * nx + x0), res);
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // this thread's reads before the next refill
-    }
-    if (!ok && tid == 0) {
-        atomicExch(a.err, 1);
-        for (; waited < next; ++waited)
-            (void)st_bar_wait(st_smem(&bars[waited % kTmaStages]), (uint32_t)((waited / kTmaStages) & 1));
+        // load k - 1 is read for the last time here: this warp releases its stage
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0)
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(st_smem(&empty[(k - 1) % kTmaStages]))
+                         : "memory");
     }
 }
 
@@ -602,7 +618,7 @@ int stencil_tma_setup(int dev)
         // the largest stage ring (nx = 256) sets the attribute for every nx
         PIRO_CUDA(cudaFuncSetAttribute(k_stencil_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)stencil_tma_smem(256)));
-        PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.per_sm, k_stencil_tma, kTmaThreads,
+        PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.per_sm, k_stencil_tma, kTmaThreads + 32,
                                                                 stencil_tma_smem(256)));
         if (!d.err_flag) {
             PIRO_CUDA(cudaMalloc(&d.err_flag, sizeof(int)));
@@ -633,7 +649,8 @@ int stencil_tma_step(int nx, int ny, int nz, float idx2, float idy2, float idz2,
     if (!rc) rc = encode_plane_map(&amap, alpha ? alpha : u, nx, ny, nz, TY);
     if (rc) return rc;
     StencilTma a{nx, ny, nz, TY, zchunk, alpha ? 1 : 0, idx2, idy2, idz2, dt, out, d.err_flag};
-    k_stencil_tma<<<dim3((unsigned)ytiles, (unsigned)runs), kTmaThreads, stencil_tma_smem(nx), st>>>(umap, amap, a);
+    k_stencil_tma<<<dim3((unsigned)ytiles, (unsigned)runs), kTmaThreads + 32, stencil_tma_smem(nx), st>>>(umap, amap,
+                                                                                                        a);
     PIRO_CHECK_LAUNCH("k_stencil_tma");
     return PIRO_OK;
 }
