@@ -339,7 +339,10 @@ void free_csr(Csr &m)
     m = Csr();
 }
 
-int open_case(piro_ctx *c, const std::string &case_name)
+// The host half of opening a case: the .ini files, the fields' initial
+// values.  No CUDA call, so a malformed case reports PIRO_ERR_CONFIG on any
+// machine.
+int parse_case(piro_ctx *c, const std::string &case_name)
 {
     if (!read_ini(c->assets + "/" + case_name, c->cfg))
         return fail(PIRO_ERR_CONFIG, "cannot read case file %s/%s", c->assets, case_name);
@@ -435,6 +438,13 @@ int open_case(piro_ctx *c, const std::string &case_name)
         if ((int64_t)f.host.size() < 3 * N) f.host.resize((size_t)(3 * N), 0.0f);  // the reference reads past the end
         c->fields.push_back(f);
     }
+    return PIRO_OK;
+}
+
+// The device half: upload, boundary conditions, work buffers.
+int load_case(piro_ctx *c)
+{
+    const int64_t N = (int64_t)c->nx * c->ny * c->nz;
     // upload the initial values (before setbc, as clCreateBuffer copies them first)
     for (Field &f : c->fields) {
         CK(cudaMalloc(&f.d, sizeof(float) * (size_t)f.n));
@@ -494,12 +504,12 @@ extern "C" int piro_open(const char *assets_dir, const char *case_name, piro_ctx
     *out = nullptr;
     piro_ctx *c = new piro_ctx();
     c->assets = assets_dir;
-    int rc = PIRO_OK;
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    int rc = parse_case(c, case_name);
+    if (!rc && cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         piro::set_error("piro_open: cannot create a stream");
         rc = PIRO_ERR_CUDA;
     }
-    if (!rc) rc = open_case(c, case_name);
+    if (!rc) rc = load_case(c);
     if (rc) {
         piro_close(c);
         return rc;
