@@ -71,3 +71,24 @@ def test_valid_case_without_a_gpu_fails_loudly(tmp_path):
     assets, name = case_dir(tmp_path)
     e = open_error(assets, name)
     assert "PIRO_ERR_CUDA" in str(e), str(e)
+
+
+REF_DIR = os.environ.get("PIRO_REF_DIR", "/root/reference")
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF_DIR, "Test")), reason="the reference tree is not present")
+@pytest.mark.parametrize("name", ["HeatEq.ini", "AdvEq.ini", "LUDecomp.ini"])
+def test_reference_cases_parse(tmp_path, name):
+    """PIRO's own example cases (Test/*.ini, run by maketest.sh from a copy of
+    dependencies/assets with the case file placed beside setup.ini) get
+    through the front end: with no GPU the first failure is the first CUDA
+    call, never the parser."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present: the case would open")
+    assets = tmp_path / "assets"
+    shutil.copytree(os.path.join(REF_DIR, "dependencies", "assets"), assets,
+                    ignore=shutil.ignore_patterns("kernels"))
+    shutil.copy(os.path.join(REF_DIR, "Test", name), assets / name)
+    e = open_error(str(assets), name)
+    assert "PIRO_ERR_CUDA" in str(e), str(e)
