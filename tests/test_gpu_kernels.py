@@ -260,13 +260,15 @@ def test_fe_steps_match_oracle(cuda, oracle, n):
         ops.set_bc(idx, bc, out)
         u, out = out, u
     np.testing.assert_allclose(h(u), ref_coo, rtol=1e-5, atol=1e-6)
+    # the row-indexed step adds each row's products in entry order, as
+    # SpMVCOO.cl does, then dt * sum and u + that (addVectors.cl): bit-exact
     rowstart = ops.coo_row_index(N, coo_s[0])
     u = dev(torch, u0)
     for _ in range(3):
         ops.coo_step_indexed(N, rowstart, coo_s[1], coo_s[2], dt, u, out, fe=True)
         ops.set_bc(idx, bc, out)
         u, out = out, u
-    np.testing.assert_allclose(h(u), ref_coo, rtol=1e-5, atol=1e-6)
+    assert f32_bits_equal(h(u), ref_coo)
     bad = coo_s[0].flip(0).contiguous()
     with pytest.raises(Exception, match="not sorted"):
         ops.coo_row_index(N, bad)
