@@ -39,18 +39,27 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(kernel):
-    """DRAM bytes per launch of `kernel` from its committed ncu summary
-    (profiles/<kernel>_128.md, line `traffic_bytes_per_launch: N`), or None."""
+def profiled_metrics(kernel):
+    """The figures of `kernel`'s committed ncu summary (profiles/<kernel>_128.md):
+    `traffic_bytes_per_launch: N` and every `metric [unit] = value` line, as
+    {name: float}.  Empty when the summary is absent."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_128.md")
+    out = {}
     try:
         with open(path) as f:
             for line in f:
+                line = line.strip()
                 if line.startswith("traffic_bytes_per_launch:"):
-                    return int(line.split(":")[1])
+                    out["traffic_bytes_per_launch"] = float(line.split(":")[1])
+                elif " = " in line and "[" in line:
+                    name, val = line.split(" = ", 1)
+                    try:
+                        out[name.split(" [")[0].strip()] = float(val.replace(",", ""))
+                    except ValueError:
+                        pass
     except OSError:
         pass
-    return None
+    return out
 
 
 def load_tflops_peak():
@@ -107,6 +116,20 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ problem
+WORKLOAD = ("heat backward Euler 128^3, smoothed log-normal alpha (sigma 1.5, filter 8, seed 2), "
+            "dt = 50x explicit limit, Jacobi-PCG to a 1e-8 FP64 relative residual")
+
+
+def bench_config(cfg, world):
+    """The `config` both arms print (identical, so the two lines describe the
+    same problem): the workload, its grid and the nonzeros of A = I - dt
+    diag(alpha) L (the Laplacian's pattern: 7N - 2(nx ny + ny nz + nx nz))."""
+    nx, ny, nz = cfg["n"]
+    N = nx * ny * nz
+    return {"workload": WORKLOAD, "grid": [nx, ny, nz], "nnz_A": 7 * N - 2 * (nx * ny + ny * nz + nx * nz),
+            "steps_in_trajectory": cfg["steps"], "parallelism": f"replicas x{world}"}
+
+
 def be_problem(torch, ops, cfg):
     nx, ny, nz = cfg["n"]
     N = nx * ny * nz
@@ -177,7 +200,63 @@ def spmv_section(torch, ops, steps, warmup, peak):
     del rowstart
     del A, coo, rows
     torch.cuda.empty_cache()
+    res["cpu_baseline"] = spmv_cpu_baseline(peak)
     return res
+
+
+def spmv_cpu_baseline(peak):
+    """PIRO's own SpMV kernels (SpMVCSR.cl, SpMVCOO.cl, SpMVHT.cl compiled
+    for the host by oracle/Makefile, the NDRange run as an OpenMP loop): CSR
+    at 256^3 on all host threads and on one; COO and HT at 32^3 only, since
+    as written they cost O(N nnz) and O(N^2) per step.  None when the
+    reference build is absent."""
+    from oracle import oracle as O
+    from piro_b200 import workloads as W
+    try:
+        R = O.Ref()
+    except (FileNotFoundError, OSError):
+        return None
+    out = {"kind": "reference", "source": "PIRO's .cl kernels compiled for the host (oracle/_ref)"}
+    cfg = W.spmv_256()
+    nx, ny, nz = cfg["n"]
+    N = nx * ny * nz
+    L = O.laplacian(nx, ny, nz, 3, np.float32(1.0))
+    A = (L[0], L[1], O.csr_rowscale(N, L[0], L[2], cfg["alpha"]))
+    nnz = len(A[2])
+    byt = 8 * nnz + 4 * (N + 1) + 8 * N
+    nthr = O.num_threads()
+    for th, reps in ((nthr, 3), (1, 1)):
+        O.set_threads(th)
+        R.spmv_par("csr", nx, ny, nz, A, 0.01, cfg["u"])
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            R.spmv_par("csr", nx, ny, nz, A, 0.01, cfg["u"])
+        ms = (time.perf_counter() - t0) * 1e3 / reps
+        out[f"csr_256_{'all' if th == nthr else 'one'}_threads"] = {
+            "ms": round(ms, 2), "cores": th, "gbs": round(byt / ms / 1e6, 1), "bytes": byt,
+            "sample": f"SpMVCSR.cl at 256^3 ({N} rows, {nnz} nonzeros), mean of {reps}"}
+    O.set_threads(nthr)
+    del A, L
+    n = 32
+    N = n ** 3
+    u = np.random.default_rng(1).random(N).astype(np.float32)
+    L = O.laplacian(n, n, n, 3, np.float32(1.0))
+    rows = np.repeat(np.arange(N, dtype=np.int32), np.diff(L[0]))
+    t0 = time.perf_counter()
+    R.spmv_par("coo", n, n, n, (rows, L[1], L[2]), 0.01, u)
+    ms = (time.perf_counter() - t0) * 1e3
+    out["coo_32_all_threads"] = {"ms": round(ms, 1), "cores": nthr,
+                                 "sample": f"SpMVCOO.cl at 32^3 ({N} rows, {len(L[2])} nonzeros; every row scans all "
+                                           "nonzeros), one step"}
+    ts = O.ht_table_size_build(len(L[2]))
+    keys, vals = O.ht_build(N, *L, ts)
+    t0 = time.perf_counter()
+    R.spmv_par("ht", n, n, n, (keys.astype(np.int32), vals), 0.01, u)
+    ms = (time.perf_counter() - t0) * 1e3
+    out["ht_32_all_threads"] = {"ms": round(ms, 1), "cores": nthr,
+                                "sample": f"SpMVHT.cl at 32^3 ({N} rows, {ts}-slot table; every row looks up all N "
+                                          "columns), one step"}
+    return out
 
 
 def config_sections(torch, peak):
@@ -488,6 +567,27 @@ def batched_section(torch, ops, peak, steps=4):
 
 
 # ------------------------------------------------------------------ arms
+def fp64_trajectory_check(torch, O, solver, cfg, Ah, x):
+    """The configuration's 20 steps from u0 on the device and by the oracle in
+    FP64 only; per step the device's FP64 relative residual and the max error
+    of its field against the FP64 trajectory (absolute and relative to max |u|)."""
+    nx, ny, nz = cfg["n"]
+    u = torch.from_numpy(cfg["u0"]).cuda()
+    u64 = cfg["u0"].astype(np.float64)
+    per = []
+    for k in range(cfg["steps"]):
+        info = solver.solve(u, x, rtol=1e-8)
+        u64, _, rel64 = O.be_cg_f64(nx, ny, nz, Ah, cfg["alpha"], u64, rtol=1e-13)
+        got = x.cpu().numpy().astype(np.float64)
+        err = float(np.abs(got - u64).max())
+        per.append({"step": k + 1, "rel_residual": info.rel_residual, "inner_iterations": info.inner_iterations,
+                    "max_abs_err": err, "max_rel_err": err / float(np.abs(u64).max())})
+        u, x = x, u
+    return {"steps": per, "worst_rel_err": max(p["max_rel_err"] for p in per),
+            "worst_rel_residual": max(p["rel_residual"] for p in per),
+            "reference": "oracle FP64 Jacobi-PCG to 1e-13 per step (oracle/piro_oracle.c or_be_cg_f64d)"}
+
+
 def run_piro(args):
     import torch
     import torch.distributed as dist
@@ -569,20 +669,46 @@ def run_piro(args):
     ms_step = main["ms"]
     ck = main["clocks"]
     x = torch.empty_like(u0)
-    # roofline of the dominant kernel: the CG operator q = A p, p = z + beta*p_old
-    if inner_op == "stencil-persistent":
-        # one cooperative launch per step; bytes counted from its sweeps and iterations
-        k_name = "k_be_persistent"
-        bytes_spmv = main["pbytes"] / max(1, main["spmv_launches"])
-    elif inner_op == "stencil":
-        k_name, bytes_spmv = "k_cg_spmv_mf", 20 * N  # z, p_old, alpha read; p, q written
-    else:
-        k_name, bytes_spmv = "k_cg_spmv", 8 * nnzA + 4 * (N + 1) + 20 * N
+    # roofline of the dominant kernel (the one persistent launch per step):
+    # what binds it is latency -- L2 round trips of the neighbour reads and
+    # the grid barriers of each CG iteration -- not HBM (its data stay in L2
+    # and shared memory between phases).  achieved/frac: DRAM bytes per launch
+    # (the committed ncu capture of the same 128^3 launch) / event-timed
+    # duration against the copy peak; binding: the L2-throughput and
+    # issue-slot fractions of that capture; effective: the CG bytes of the
+    # CSR formulation (8 nnz + 4(N+1) + 60 N per iteration, 8 nnz + 4(N+1) +
+    # 24 N per FP64 residual) over the same time.
+    k_name = "k_be_persistent" if inner_op == "stencil-persistent" else (
+        "k_cg_spmv_mf" if inner_op == "stencil" else "k_cg_spmv")
     avg_spmv_ms = main["spmv_ms"] / max(1, main["spmv_launches"])
-    achieved = bytes_spmv / avg_spmv_ms / 1e6
+    prof = profiled_metrics(k_name)
+    traffic = prof.get("traffic_bytes_per_launch")
+    dram_gbs = traffic / avg_spmv_ms / 1e6 if traffic else None
+    eff_bytes = (main["iters"] * (8 * nnzA + 4 * (N + 1) + 60 * N) +
+                 (main["outers"] + 1) * (8 * nnzA + 4 * (N + 1) + 24 * N))
     csr_bytes = 8 * nnzA + 4 * (N + 1) + 20 * N
     csr_avg = csr["spmv_ms"] / max(1, csr["spmv_launches"])
     launches = main["launches"]
+    roofline = {
+        "kernel": k_name, "bound": "latency",
+        "achieved": None if dram_gbs is None else round(dram_gbs, 1), "peak": peak, "unit": "GB/s",
+        "frac": None if dram_gbs is None else round(dram_gbs / peak, 4), "peak_kind": peak_kind,
+        "traffic": traffic, "avg_launch_ms": avg_spmv_ms, "launches": main["spmv_launches"],
+        "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch, ncu capture of the same "
+                          "128^3 launch (profiles/k_be_persistent_128.md)",
+        "binding": {"l2_throughput_frac": (prof["lts__throughput.avg.pct_of_peak_sustained_elapsed"] / 100
+                                           if "lts__throughput.avg.pct_of_peak_sustained_elapsed" in prof else None),
+                    "issue_active_frac": (prof["smsp__issue_active.avg.pct_of_peak_sustained_active"] / 100
+                                          if "smsp__issue_active.avg.pct_of_peak_sustained_active" in prof else None),
+                    "us_per_cg_iteration": round(1e3 * avg_spmv_ms / max(main["iters"], 1e-9), 2),
+                    "note": "latency bound: L2 round trips of neighbour reads and two grid all-reduces per CG "
+                            "iteration; DRAM moves only the step's first touch of its data"},
+        "effective": {"bytes_per_launch": eff_bytes, "gbs": round(eff_bytes / avg_spmv_ms / 1e6, 1),
+                      "frac_of_hbm_peak": round(eff_bytes / avg_spmv_ms / 1e6 / peak, 4),
+                      "note": "algorithmic bytes of the CSR formulation (per CG iteration 8 nnz + 4(N+1) + 60 N, "
+                              "per FP64 residual 8 nnz + 4(N+1) + 24 N); this kernel is matrix-free and serves "
+                              "them from L2 and shared memory, so the figure exceeds the HBM peak"},
+    }
 
     # end to end through host buffers: every step copies u_n from pinned host
     # memory to the device, solves, and copies u_{n+1} back; the caller then
@@ -641,14 +767,14 @@ def run_piro(args):
         cpu1_ms = (time.perf_counter() - t0) * 1e3
         O.set_threads(nthr)
         cpu = {"value": cpu_ms, "unit": "ms/step", "cores": nthr, "kind": "port",
-               "sample": f"1 backward-Euler step of the 128^3 config, FP64 Jacobi-PCG to 1e-8 ({cg_its} iterations), "
-                         "OpenMP over all host threads",
-               "one_thread": {"value": round(cpu1_ms, 1), "unit": "ms/step", "cores": 1}}
-        # per-step error of the device result against an FP64-only solve
-        solver.solve(u0, x, rtol=1e-8)
-        u64b, _, _ = O.be_cg_f64(nx, ny, nz, Ah, al, cfg["u0"], rtol=1e-13)
-        err = float(np.abs(x.cpu().numpy().astype(np.float64) - u64b).max())
-        fp64 = {"step": 1, "max_abs_err_vs_fp64": err, "max_u": float(np.abs(u64b).max())}
+               "sample": f"1 backward-Euler step of the 128^3 config by the oracle's FP64 Jacobi-PCG to 1e-8 "
+                         f"({cg_its} iterations), OpenMP over all host threads; a port, no PIRO code runs here "
+                         "(PIRO's JLI iteration diverges at this dt)",
+               "one_thread": {"value": round(cpu1_ms, 1), "unit": "ms/step", "cores": 1},
+               "spmv": spmv.pop("cpu_baseline", None) if spmv else None}
+        # per-step error of the device trajectory against an FP64-only one
+        # (each step solved to 1e-13 from the previous FP64 solution)
+        fp64 = fp64_trajectory_check(torch, O, solver, cfg, Ah, x)
 
     solver.close()
     solver_csr.close()
@@ -661,25 +787,16 @@ def run_piro(args):
         "metric": METRIC, "value": round(ms_step, 4), "unit": "ms/step", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 Krylov + f64 refinement", "data": "synthetic (seeded numpy)",
-        "config": {"workload": "heat backward Euler 128^3, smoothed log-normal alpha (sigma 1.5, filter 8, seed 2), "
-                               "dt = 50x explicit limit, Jacobi-PCG FP32 + FP64 refinement to 1e-8",
-                   "grid": [nx, ny, nz], "nnz_A": nnzA, "preconditioner": "jacobi",
-                   "inner_operator": inner_op,
-                   "l2": "L2 flushed (a 252 MB write) before every timed step, outside the step's own CUDA-event "
-                         "pair; value and e2e are sums of per-step event times",
-                   "parallelism": f"replicas x{world}"},
-        "solver": {"inner_operator": inner_op, "inner_iterations_mean": main["iters"],
+        "config": bench_config(cfg, world),
+        "timing": "L2 flushed (a 252 MB write) before every timed step, outside the step's own CUDA-event pair; "
+                  "value and e2e are sums of per-step event times",
+        "solver": {"inner_operator": inner_op, "preconditioner": "jacobi",
+                   "inner_iterations_mean": main["iters"],
                    "outer_sweeps_mean": main["outers"], "worst_rel_residual": main["worst"],
                    "csr_inner_operator": {"ms_per_step": round(csr["ms"], 4), "inner_iterations_mean": csr["iters"],
                                           "worst_rel_residual": csr["worst"], "k_cg_spmv_avg_ms": csr_avg,
                                           "k_cg_spmv_gbs": round(csr_bytes / csr_avg / 1e6, 1)}},
-        "roofline": {"kernel": k_name, "bound": "hbm", "achieved": round(achieved, 1),
-                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "peak_kind": peak_kind, "bytes_per_launch": bytes_spmv,
-                     "avg_launch_ms": avg_spmv_ms, "launches": main["spmv_launches"],
-                     "traffic": profiled_traffic(k_name),
-                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture of the same "
-                                       "kernel on the same 128^3 step (profiles/k_be_persistent_128.md)"},
+        "roofline": roofline,
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms/step", "h2d_bytes_per_step": 4 * N, "d2h_bytes_per_step": 4 * N},
         "gpu_launches": launches,
         "clocks": ck,
@@ -726,11 +843,11 @@ def run_reference(args):
         "metric": METRIC, "value": round(v, 3), "unit": "ms/step", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded numpy)", "impl": "reference",
-        "config": {"workload": "heat backward Euler 128^3, smoothed log-normal alpha (sigma 1.5, filter 8, seed 2), "
-                               "dt = 50x explicit limit, to 1e-8 FP64 relative residual"},
+        "config": bench_config(cfg, int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": round(v, 3), "unit": "ms/step", "cores": O.num_threads(), "kind": "port",
-                         "sample": "each step one full backward-Euler solve (FP64 Jacobi-PCG, OpenMP); PIRO's own "
-                                   "JLI iteration diverges at this dt"},
+                         "sample": "each step one full backward-Euler solve by the oracle's FP64 Jacobi-PCG "
+                                   "(OpenMP, all host threads); a port of the method, no PIRO code runs in this "
+                                   "arm, because PIRO's own JLI iteration diverges at this dt"},
         "e2e": {"value": round(v, 3), "unit": "ms/step", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

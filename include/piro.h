@@ -55,6 +55,16 @@ const char *piro_last_error(void);
 /* Version string of the library build. */
 const char *piro_version(void);
 
+/* Polls that a bounded device wait makes before it gives up (the grid
+ * barriers of piro_be_solve's persistent kernel and of piro_batch_step, the
+ * stage waits of piro_stencil_fe_step's staged kernel).  A wait that runs out
+ * sets an error flag, every block leaves the kernel, and the call (or
+ * piro_stencil_check) returns PIRO_ERR_CUDA; the CUDA context stays usable.
+ * Negative restores the built-in bound (about 2 s of polling).  Process-wide,
+ * read at each launch.  No counterpart in the reference, which never waits
+ * on the device (it blocks on clFinish).  For tests of the failure path. */
+int piro_set_wait_limit(long long polls);
+
 /* ========================================================================
  * 1. Kernel entry points (device pointers; asynchronous on `stream`)
  * ======================================================================== */
@@ -287,7 +297,11 @@ int piro_csrgeam3(int64_t N, const int32_t *rpA, const int32_t *cA, const float 
  * calls whose GPU work overlaps (other streams or threads on the same device)
  * race and must be serialised by the caller.  The first call on each device
  * looks up the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before starting any stream capture. */
+ * current; under CUDA's lazy module loading that first call is also where the
+ * driver loads the array onto the device.  Make one small call per device at
+ * start-up, before fixing the device-memory budget and before starting any
+ * stream capture; later calls allocate nothing.  Arguments are checked before
+ * any device work. */
 int piro_csrgeam3_noalloc(int64_t N, const int32_t *rpA, const int32_t *cA, const float *vA, const int32_t *rpB,
                           const int32_t *cB, const float *vB, const int32_t *rpC, const int32_t *cC, const float *vC,
                           const float *v, int32_t *rpD, int32_t *cD, float *vD, piro_stream_t stream);
@@ -353,7 +367,10 @@ int piro_be_create_stencil(int nx, int ny, int nz, const int32_t *rowptr, const 
 /* Inner operator in use: 0 CSR SpMV (graph-launched CG), 1 matrix-free
  * 7-point stencil (graph-launched CG), 2 matrix-free stencil with the whole
  * solve in one persistent cooperative launch (FP64 refinement and CG phases
- * separated by a grid barrier whose waits are bounded). */
+ * separated by a grid barrier whose waits are bounded), 3 the same launch
+ * with each block's r, d, q resident in shared memory.  The environment
+ * variable PIRO_BE_PERSISTENT, read at creation, forces kind <= 1 ("0") or
+ * keeps kind 2 instead of 3 ("g"). */
 int piro_be_inner_operator(piro_be_solver *s, int *kind);
 /* Algorithmic bytes moved by the persistent launches counted in
  * piro_be_kernel_stats (since its last reset). */

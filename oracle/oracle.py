@@ -26,9 +26,10 @@ _f64p = np.ctypeslib.ndpointer(np.float64, flags="C")
 
 
 def build(with_ref: bool = False) -> None:
-    """Compile the oracle (and, when the reference tree is present, _ref)."""
+    """Compile the oracle (and _ref, when PIRO_REF_DIR names the PIRO tree)."""
     subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
-    if with_ref and os.path.isdir(os.environ.get("PIRO_REF_DIR", "/root/reference")):
+    ref = os.environ.get("PIRO_REF_DIR", "")
+    if with_ref and ref and os.path.isdir(ref):
         subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref"])
 
 
@@ -69,6 +70,8 @@ def _load():
         "or_be_jli": (i32, [i64, i32, i32, _i32p, _i32p, _f32p, f32, _f32p, _f32p, _f32p, f32, f32, i32]),
         "or_be_cg_f64": (i32, [i64, i32, i32, i32, _i32p, _i32p, _f32p, _f32p, _f32p, _f64p, f64, i32,
                                C.POINTER(C.c_double)]),
+        "or_be_cg_f64d": (i32, [i64, i32, i32, i32, _i32p, _i32p, _f32p, _f32p, _f64p, _f64p, f64, i32,
+                                C.POINTER(C.c_double)]),
         "or_dense_laplacian": (None, [i32, i32, i32, i32, f32, _f32p]),
         "or_fe_dense_step": (None, [i64, _f32p, f32, _f32p, _f32p, _f32p]),
         "or_ic_gaussian": (None, [i32, i32, i32, f32, f32, f32, f32, _f32p, _f32p, _f32p]),
@@ -338,13 +341,19 @@ def be_jli(nx, ny, nz, A, dt, b, tol=1e-5, urf=1.0, maxiter=1000):
 
 def be_cg_f64(nx, ny, nz, A, alpha, b, rtol=1e-12, maxiter=100000):
     """FP64 Jacobi-PCG solve of the backward-Euler system (interior rows,
-    boundary held at b).  Returns (u float64, iterations, final relative
-    residual)."""
+    boundary held at b).  A float64 b is used as is (a step of an FP64-only
+    trajectory); any other b as float32.  Returns (u float64, iterations,
+    final relative residual)."""
     N = n_cells(nx, ny, nz)
     u = np.zeros(N, np.float64)
     rel = C.c_double(0.0)
-    it = lib().or_be_cg_f64(N, nx, ny, nz, A[0], A[1], A[2], np.ascontiguousarray(alpha, np.float32),
-                            np.ascontiguousarray(b, np.float32), u, rtol, maxiter, C.byref(rel))
+    al = np.ascontiguousarray(alpha, np.float32)
+    if isinstance(b, np.ndarray) and b.dtype == np.float64:
+        it = lib().or_be_cg_f64d(N, nx, ny, nz, A[0], A[1], A[2], al, np.ascontiguousarray(b), u, rtol, maxiter,
+                                 C.byref(rel))
+    else:
+        it = lib().or_be_cg_f64(N, nx, ny, nz, A[0], A[1], A[2], al, np.ascontiguousarray(b, np.float32), u, rtol,
+                                maxiter, C.byref(rel))
     return u, it, rel.value
 
 
@@ -402,6 +411,9 @@ class Ref:
         L.refcl_spmvcsr_i1.argtypes = [i32, _f32p, _i32p, _i32p, f32, _f32p, _f32p, C.c_uint, C.c_uint, C.c_uint]
         L.refcl_spmvcoo.argtypes = [i32, i32, _f32p, _i32p, _i32p, f32, _f32p, _f32p, C.c_uint, C.c_uint, C.c_uint]
         L.refcl_spmvht.argtypes = [_i32p, _f32p, _f32p, _f32p, i32, i32, f32]
+        L.refcl_spmvcsr_par.argtypes = L.refcl_spmvcsr.argtypes
+        L.refcl_spmvcoo_par.argtypes = L.refcl_spmvcoo.argtypes
+        L.refcl_spmvht_par.argtypes = L.refcl_spmvht.argtypes
         L.refcl_add.argtypes = [_f32p, _f32p, _f32p, C.c_uint]
         L.refcl_sub.argtypes = [_f32p, _f32p, _f32p, C.c_uint]
         L.refcl_urf.argtypes = [_f32p, _f32p, f32, C.c_uint]
@@ -418,7 +430,8 @@ class Ref:
         L.refcl_csrgeam2_merge.argtypes = [i32, _i32p, _i32p, _f32p, _i32p, _i32p, _f32p, _i32p, _i32p, _f32p,
                                            _i32p, _i32p, _f32p, _i32p]
         L.refcl_fe_dense.argtypes = [i32, _f32p, _f32p, _f32p, _f32p, f32]
-        for n in ("refcl_csrgeam2_merge", "refcl_fe_dense", "refcl_spmvcsr", "refcl_spmvcsr_i1", "refcl_spmvcoo", "refcl_spmvht", "refcl_add", "refcl_sub",
+        for n in ("refcl_csrgeam2_merge", "refcl_fe_dense", "refcl_spmvcsr", "refcl_spmvcsr_i1", "refcl_spmvcoo", "refcl_spmvht",
+                  "refcl_spmvcsr_par", "refcl_spmvcoo_par", "refcl_spmvht_par", "refcl_add", "refcl_sub",
                   "refcl_urf", "refcl_csrgeam", "refcl_spmdsm", "refcl_setbc", "refcl_laplacianscalar",
                   "refcl_lu_round"):
             getattr(L, n).restype = None
@@ -515,6 +528,23 @@ class Ref:
     def spmvht(self, N, keys32, vals, dt, B):
         Cc = np.zeros(N, np.float32)
         self.lib.refcl_spmvht(keys32, vals, np.ascontiguousarray(B, np.float32), Cc, N, len(keys32), np.float32(dt))
+        return Cc
+
+    def spmv_par(self, kind, nx, ny, nz, op, dt, B, C_in=None):
+        """One SpMVCSR / SpMVCOO / SpMVHT NDRange over the OpenMP threads
+        (set_threads picks the count): the CPU baseline of the SpMV steps.
+        op: CSR (rowptr, col, val), COO (rows, col, val), HT (keys32, vals)."""
+        N = n_cells(nx, ny, nz)
+        Bc = np.ascontiguousarray(B, np.float32)
+        if kind == "csr":
+            Cc = np.zeros(N, np.float32) if C_in is None else C_in.copy()
+            self.lib.refcl_spmvcsr_par(N, op[2], op[1], op[0], np.float32(dt), Bc, Cc, nx, ny, N)
+        elif kind == "coo":
+            Cc = np.zeros(N, np.float32)
+            self.lib.refcl_spmvcoo_par(N, len(op[2]), op[2], op[1], op[0], np.float32(dt), Bc, Cc, nx, ny, N)
+        else:
+            Cc = np.zeros(N, np.float32)
+            self.lib.refcl_spmvht_par(op[0], op[1], Bc, Cc, N, len(op[0]), np.float32(dt))
         return Cc
 
     def csrgeam(self, N, A, B, Cm, v):

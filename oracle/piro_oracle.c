@@ -665,8 +665,24 @@ static double dot_f64(int64_t n, const double *a, const double *b)
     return s;
 }
 
+int or_be_cg_f64d(int64_t N, int nx, int ny, int nz, const int32_t *rp, const int32_t *col, const float *val,
+                  const float *alpha, const double *b, double *u, double rtol, int maxiter, double *final_rel);
+
+/* b in float32 (a field as the solvers receive it). */
 int or_be_cg_f64(int64_t N, int nx, int ny, int nz, const int32_t *rp, const int32_t *col, const float *val,
                  const float *alpha, const float *b, double *u, double rtol, int maxiter, double *final_rel)
+{
+    double *bd = (double *)malloc((size_t)N * sizeof(double));
+    for (int64_t i = 0; i < N; ++i) bd[i] = (double)b[i];
+    const int it = or_be_cg_f64d(N, nx, ny, nz, rp, col, val, alpha, bd, u, rtol, maxiter, final_rel);
+    free(bd);
+    return it;
+}
+
+/* b in float64: the step of an FP64-only trajectory (the previous step's
+ * FP64 solution as the right-hand side). */
+int or_be_cg_f64d(int64_t N, int nx, int ny, int nz, const int32_t *rp, const int32_t *col, const float *val,
+                  const float *alpha, const double *b, double *u, double rtol, int maxiter, double *final_rel)
 {
     uint8_t *interior = (uint8_t *)malloc((size_t)N);
     double *r = (double *)calloc((size_t)N, sizeof(double));
@@ -693,7 +709,7 @@ int or_be_cg_f64(int64_t N, int nx, int ny, int nz, const int32_t *rp, const int
     double bnorm2 = 0.0;
     for (int64_t i = 0; i < N; ++i)
         if (interior[i]) {
-            bb[i] = (double)b[i];
+            bb[i] = b[i];
             bnorm2 += bb[i] * bb[i];
             r[i] = bb[i] - q[i];
         }

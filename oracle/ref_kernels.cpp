@@ -88,6 +88,16 @@ _Pragma("GCC diagnostic pop") }
         call;                                                    \
     }
 
+// The same NDRange over the host's OpenMP threads, for kernels whose
+// work-items write only their own row (the CPU baseline of the SpMV steps):
+// each thread sets its own get_global_id (g_gid is thread-local).
+#define NDRANGE_OMP(n, call)                                     \
+    _Pragma("omp parallel for schedule(static)")                 \
+    for (long gid_ = 0; gid_ < (long)(n); ++gid_) {              \
+        clshim::g_gid = (size_t)gid_;                            \
+        call;                                                    \
+    }
+
 #define NDRANGE2(n0, n1, call)                                   \
     for (size_t g1_ = 0; g1_ < (size_t)(n1); ++g1_)              \
         for (size_t g0_ = 0; g0_ < (size_t)(n0); ++g0_) {        \
@@ -120,6 +130,25 @@ void refcl_spmvcoo(int M, int nnz, const float *val, const int *col, const int *
 void refcl_spmvht(int *keys, float *vals, const float *B, float *C, int N, int TS, float dt)
 {
     NDRANGE(N, k_spmvht::SpMVHT(keys, vals, B, C, N, TS, dt));
+}
+
+// The three SpMV kernels over all OpenMP threads (omp_set_num_threads picks
+// the count): every work-item reads the shared inputs and writes C[gid] only.
+void refcl_spmvcsr_par(int M, const float *val, const int *col, const int *rp, float dt, float *B, float *C,
+                       unsigned nx, unsigned ny, unsigned size)
+{
+    NDRANGE_OMP(M, k_spmvcsr::SpMVCSR(M, M, 1, val, col, rp, dt, B, C, nx, ny, size));
+}
+
+void refcl_spmvcoo_par(int M, int nnz, const float *val, const int *col, const int *rows, float dt, float *B,
+                       float *C, unsigned nx, unsigned ny, unsigned size)
+{
+    NDRANGE_OMP(M, k_spmvcoo::SpMVCOO(M, M, nnz, val, col, rows, dt, B, C, nx, ny, size));
+}
+
+void refcl_spmvht_par(int *keys, float *vals, const float *B, float *C, int N, int TS, float dt)
+{
+    NDRANGE_OMP(N, k_spmvht::SpMVHT(keys, vals, B, C, N, TS, dt));
 }
 
 void refcl_add(float *A, const float *B, const float *C, unsigned n) { NDRANGE(n, k_add::addVectors(A, B, C, n)); }

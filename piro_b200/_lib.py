@@ -47,6 +47,7 @@ SIGNATURES = {
     "piro_status_string": (C.c_char_p, [i32]),
     "piro_last_error": (C.c_char_p, []),
     "piro_version": (C.c_char_p, []),
+    "piro_set_wait_limit": (i32, [C.c_longlong]),
     "piro_laplacian_nnz": (i32, [i32, i32, i32, pi64]),
     "piro_csr_laplacian": (i32, [i32, i32, i32, i32, f32, vp, vp, vp, vp]),
     "piro_coo_laplacian": (i32, [i32, i32, i32, i32, f32, vp, vp, vp, vp]),

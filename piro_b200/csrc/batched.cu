@@ -479,6 +479,7 @@ struct piro_batch {
     cudaStream_t own = nullptr;      // non-blocking stream for graph capture
     cudaGraphExec_t pair = nullptr;  // two steps (f[0] -> f[1] -> f[0]) as one graph
     double pair_rtol = 0.0;
+    long long pair_spin = -1;  // the wait limit the pair graph was captured with
     double step_ms = 0.0;
     long long steps = 0;
     double rtol = 1e-8;
@@ -689,8 +690,10 @@ static int batch_launch(piro_batch *s, const float *u, float *out, cudaStream_t 
     A.max_sweeps = 20;
     A.max_inner = 20000;
     A.max_rounds = 40000;
-    A.spin_limit = 1ll << 22;  // ~2 s of polling per barrier wait
+    A.spin_limit = wait_limit(1ll << 22);  // ~2 s of polling per barrier wait
     void *args[] = {&A};
+    // a launch whose barrier wait gave up leaves count, gen and err behind
+    PIRO_CUDA(cudaMemsetAsync(s->bar, 0, sizeof(BarrierState), st));
     PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_batch_step, dim3(s->grid), dim3(kThreads), args, 0, st));
     return PIRO_OK;
 }
@@ -700,7 +703,7 @@ static int batch_launch(piro_batch *s, const float *u, float *out, cudaStream_t 
 // tolerance changes.
 static int batch_pair_graph(piro_batch *s)
 {
-    if (s->pair && s->pair_rtol == s->rtol) return PIRO_OK;
+    if (s->pair && s->pair_rtol == s->rtol && s->pair_spin == wait_limit(1ll << 22)) return PIRO_OK;
     batch_drop_graph(s);
     if (!s->own) PIRO_CUDA(cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking));
     PIRO_CUDA(cudaStreamBeginCapture(s->own, cudaStreamCaptureModeThreadLocal));
@@ -722,6 +725,7 @@ static int batch_pair_graph(piro_batch *s)
         return PIRO_ERR_CUDA;
     }
     s->pair_rtol = s->rtol;
+    s->pair_spin = wait_limit(1ll << 22);
     return PIRO_OK;
 }
 

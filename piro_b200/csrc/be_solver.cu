@@ -1320,7 +1320,7 @@ size_t scan_workspace_bytes(int64_t N);
 
 // Extract A's interior-boundary coupling and size the cooperative grid.  On
 // any failure the solver keeps the multi-kernel path (persist = 0).
-static int be_setup_persistent(piro_be_solver *s)
+static int be_setup_persistent(piro_be_solver *s, bool allow_resident)
 {
     int dev = 0, coop = 0, per_sm = 0;
     PIRO_CUDA(cudaGetDevice(&dev));
@@ -1363,7 +1363,7 @@ static int be_setup_persistent(piro_be_solver *s)
     s->res_smem = 0;
     const int64_t groups = cdiv(N >> 2, grid);
     const size_t smem = (size_t)3 * groups * sizeof(float4);
-    if (N % 4 == 0 && s->nx % 4 == 0 && smem <= (size_t)kResSmemMax) {
+    if (allow_resident && N % 4 == 0 && s->nx % 4 == 0 && smem <= (size_t)kResSmemMax) {
         static DeviceOnce once;
         int rc2 = device_once(once, dev, []() -> int {
             PIRO_CUDA(cudaFuncSetAttribute(k_be_persistent<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1474,9 +1474,11 @@ static int be_create(int nx, int ny, int nz, const int32_t *rowptr, const int32_
         }
         s->op_mf = h_ok ? 1 : 0;
     }
-    const char *env = getenv("PIRO_BE_PERSISTENT");  // "0" keeps the graph-launched CG (testing, tuning)
+    // "0" keeps the graph-launched CG; "g" the persistent kernel without the
+    // shared-memory residency of r, d, q (testing, tuning)
+    const char *env = getenv("PIRO_BE_PERSISTENT");
     if (s->op_mf && !(env && env[0] == '0')) {
-        int rc = be_setup_persistent(s);
+        int rc = be_setup_persistent(s, !(env && env[0] == 'g'));
         if (rc) {
             be_free(s);
             return rc;
@@ -1574,6 +1576,10 @@ extern "C" int piro_be_inner_operator(piro_be_solver *s, int *kind)
 {
     PIRO_ARG(s && kind, "piro_be_inner_operator: bad arguments");
     *kind = s->op_mf ? (s->persist ? 2 : 1) : 0;
+    if (*kind == 2) {  // the resident variant, when its float4 paths are usable at solve time
+        const bool al16 = ((reinterpret_cast<uintptr_t>(s->alpha) | reinterpret_cast<uintptr_t>(s->dinv)) & 15) == 0;
+        if (s->res_cells > 0 && al16 && s->N % 4 == 0 && s->nx % 4 == 0) *kind = 3;
+    }
     return PIRO_OK;
 }
 
@@ -1627,7 +1633,7 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
         P.inner_floor = s->inner_floor;
         P.max_outer = max_outer;
         P.max_inner = max_inner;
-        P.spin_limit = 1ll << 22;  // ~2 s of polling: a stuck barrier ends with an error, not a hang
+        P.spin_limit = wait_limit(1ll << 22);  // ~2 s of polling: a stuck barrier ends with an error, not a hang
         const bool al16 = ((reinterpret_cast<uintptr_t>(s->alpha) | reinterpret_cast<uintptr_t>(s->dinv)) & 15) == 0;
         P.vec_b = (N % 4 == 0) && al16;
         P.vec_a = P.vec_b && (s->nx % 4 == 0);

@@ -21,6 +21,10 @@ inline cudaStream_t as_stream(piro_stream_t s) { return reinterpret_cast<cudaStr
 // B200: 148 SMs; launch grids are sized against the device's SM count.
 int sm_count();
 
+// The poll count of the bounded device waits that piro_set_wait_limit sets,
+// or `builtin` when none is set.
+long long wait_limit(long long builtin);
+
 __host__ __device__ inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 // Grid size for a grid-stride loop over n items with `per_block` items per block.

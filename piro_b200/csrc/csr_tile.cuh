@@ -34,6 +34,58 @@ __device__ __forceinline__ void csr_for_rows(int64_t N, const int32_t *__restric
     }
 }
 
+// Row-per-thread or row-per-warp, chosen per row by its length.  A warp
+// owns 32 consecutive rows per pass; each row of at most kWarpRowMin entries
+// is summed by its own thread as above, and each longer row by the whole
+// warp: lanes load 32 consecutive entries at once (coalesced) and form their
+// terms, then every lane adds the 32 terms in storage order through a
+// shuffle chain, so the sum is still the reference's sequential one, bit for
+// bit; the row's own lane writes the result.  Stencil rows (<= 7 entries)
+// never take the warp path; wide rows (merged or dense-like operators) stop
+// serialising a warp on its longest row and stop reading one line per entry.
+// The functor sees each row as
+//   s = op.accum(s, op.term(col, val)) for every entry in storage order from
+//   s = 0, then op.finish(row, s).
+constexpr int kWarpRowMin = 32;
+
+template <class RowOp>
+__device__ __forceinline__ void csr_for_rows_adaptive(int64_t N, const int32_t *__restrict__ rowptr,
+                                                      const int32_t *__restrict__ col,
+                                                      const float *__restrict__ val, RowOp &op)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < N; base += stride) {
+        const int64_t row = base + lane;
+        const bool valid = row < N;
+        int32_t k0 = 0, k1 = 0;
+        if (valid) {
+            k0 = rowptr[row];
+            k1 = rowptr[row + 1];
+        }
+        const bool wide = valid && k1 - k0 > kWarpRowMin;
+        if (valid && !wide) {
+            float s = 0.0f;
+            for (int32_t q = k0; q < k1; ++q) s = RowOp::accum(s, op.term(col[q], val[q]));
+            op.finish(row, s);
+        }
+        unsigned m = __ballot_sync(0xffffffffu, wide);
+        while (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            const int32_t a = __shfl_sync(0xffffffffu, k0, j), b = __shfl_sync(0xffffffffu, k1, j);
+            float s = 0.0f;
+            for (int32_t c = a; c < b; c += 32) {
+                const int32_t q = c + lane;
+                const float t = q < b ? op.term(col[q], val[q]) : 0.0f;
+                const int cnt = b - c < 32 ? b - c : 32;
+                for (int i = 0; i < cnt; ++i) s = RowOp::accum(s, __shfl_sync(0xffffffffu, t, i));
+            }
+            if (lane == j) op.finish(row, s);
+        }
+    }
+}
+
 inline unsigned csr_rows_grid(int64_t N)
 {
     const int64_t want = cdiv(N, kRowThreads);

@@ -19,8 +19,12 @@
 //
 // Host code cannot use the array's name as a device address (it names a
 // host-side stand-in).  The first call on each device, with that device
-// current, looks the address up once with cudaGetSymbolAddress and caches it;
-// that first call should be made before the caller starts any stream capture.
+// current, looks the address up once with cudaGetSymbolAddress and caches it.
+// Under CUDA's lazy module loading (the default), that lookup is also where
+// the driver loads this file's module onto the device and so reserves the
+// array and its code: a caller that fixes its device-memory budget at
+// start-up makes one small call per device then, before the budget is fixed
+// and before it starts any stream capture.  Later calls touch no allocator.
 #include <mutex>
 
 #include "common.cuh"
@@ -79,6 +83,10 @@ extern "C" int piro_csrgeam3_noalloc(int64_t N, const int32_t *rpA, const int32_
     if (piro::scan_workspace_bytes(N) > kNoAllocBytes) {
         piro::set_error("piro_csrgeam3_noalloc: scan needs %zu bytes, scratch holds %zu",
                         piro::scan_workspace_bytes(N), kNoAllocBytes);
+        return PIRO_ERR_ARG;
+    }
+    if (!(rpA && cA && vA && rpB && cB && vB && rpC && cC && vC && v && rpD && cD && vD)) {
+        piro::set_error("piro_csrgeam3_noalloc: a null pointer argument");
         return PIRO_ERR_ARG;
     }
     void *scratch = nullptr;

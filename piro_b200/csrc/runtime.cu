@@ -7,6 +7,16 @@ namespace piro {
 
 static thread_local char g_err[512] = "";
 
+// Polls a bounded device wait makes before it gives up; negative: each
+// kernel's built-in bound (about 2 s of polling).
+static std::atomic<long long> g_wait_limit{-1};
+
+long long wait_limit(long long builtin)
+{
+    const long long v = g_wait_limit.load(std::memory_order_relaxed);
+    return v < 0 ? builtin : v;
+}
+
 void set_error(const char *fmt, ...)
 {
     va_list ap;
@@ -32,6 +42,12 @@ int sm_count()
 }  // namespace piro
 
 extern "C" const char *piro_last_error(void) { return piro::g_err; }
+
+extern "C" int piro_set_wait_limit(long long polls)
+{
+    piro::g_wait_limit.store(polls < 0 ? -1 : polls, std::memory_order_relaxed);
+    return PIRO_OK;
+}
 
 extern "C" const char *piro_version(void) { return "piro_b200 0.1 (sm_100a)"; }
 

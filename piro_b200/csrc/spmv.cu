@@ -37,8 +37,14 @@ struct FeRow {
     int64_t row0, ubase;
     const float *__restrict__ bc;  // kMode 2: the saved face values (may be NULL)
     float result;
-    __device__ __forceinline__ void begin(int64_t) { result = 0.0f; }
-    __device__ __forceinline__ void add(int32_t c, float v) { result = add_rn(result, mul_rn(mul_rn(dt, v), __ldg(u + c))); }
+    // SpMVCSR.cl's `result += deltat * A[k] * B[col]`, left to right
+    __device__ __forceinline__ float term(int32_t c, float v) const { return mul_rn(mul_rn(dt, v), __ldg(u + c)); }
+    static __device__ __forceinline__ float accum(float s, float t) { return add_rn(s, t); }
+    __device__ __forceinline__ void finish(int64_t row, float s)
+    {
+        result = s;
+        end(row);
+    }
     __device__ __forceinline__ void end(int64_t row)
     {
         const int64_t k = ubase + row;
@@ -65,7 +71,7 @@ __global__ void __launch_bounds__(kRowThreads) k_csr_step(GridDiv g, int64_t N, 
                                                           int64_t row0, int64_t ubase)
 {
     FeRow<kMode> op{g, dt, u, out, row0, ubase, nullptr, 0.0f};
-    csr_for_rows(N, rowptr, col, val, op);
+    csr_for_rows_adaptive(N, rowptr, col, val, op);
 }
 
 __global__ void __launch_bounds__(kRowThreads) k_csr_step_bc(GridDiv g, int64_t N, const int32_t *__restrict__ rowptr,
@@ -75,7 +81,7 @@ __global__ void __launch_bounds__(kRowThreads) k_csr_step_bc(GridDiv g, int64_t 
                                                              float *__restrict__ out)
 {
     FeRow<2> op{g, dt, u, out, 0, 0, bc, 0.0f};
-    csr_for_rows(N, rowptr, col, val, op);
+    csr_for_rows_adaptive(N, rowptr, col, val, op);
 }
 
 // COO with a row index: rowstart[r] = the first entry of row r in the
@@ -104,11 +110,12 @@ struct CooRow {
     float *__restrict__ out;
     int fe;
     float acc;
-    __device__ __forceinline__ void begin(int64_t) { acc = 0.0f; }
-    __device__ __forceinline__ void add(int32_t c, float v) { acc = __fadd_rn(acc, __fmul_rn(v, __ldg(u + c))); }
-    __device__ __forceinline__ void end(int64_t row)
+    // SpMVCOO.cl's `result += values[k] * B[cols[k]]` over the row's entries
+    __device__ __forceinline__ float term(int32_t c, float v) const { return __fmul_rn(v, __ldg(u + c)); }
+    static __device__ __forceinline__ float accum(float s, float t) { return __fadd_rn(s, t); }
+    __device__ __forceinline__ void finish(int64_t row, float s)
     {
-        const float c = __fmul_rn(dt, acc);
+        const float c = __fmul_rn(dt, s);
         out[row] = fe ? __fadd_rn(__ldg(u + row), c) : c;
     }
 };
@@ -119,7 +126,7 @@ __global__ void __launch_bounds__(kRowThreads) k_coo_rows(int64_t N, const int32
                                                           const float *__restrict__ u, float *__restrict__ out)
 {
     CooRow op{dt, u, out, fe, 0.0f};
-    csr_for_rows(N, rowstart, cols, vals, op);
+    csr_for_rows_adaptive(N, rowstart, cols, vals, op);
 }
 
 // COO: each warp takes 32 consecutive entries per pass; a segmented inclusive
@@ -127,17 +134,32 @@ __global__ void __launch_bounds__(kRowThreads) k_coo_rows(int64_t N, const int32
 // lane.  Rows wholly inside the warp's span are stored; rows cut by the span
 // edges are atomically added (at most two contributions for rows of <= 32
 // entries, so the result does not depend on their order).  acc must be zero.
-__global__ void k_coo_segsum(int64_t nnz, const int32_t *__restrict__ rows, const int32_t *__restrict__ cols,
-                             const float *__restrict__ vals, const float *__restrict__ u, float *__restrict__ acc)
+// The segments are only whole rows when the row ids ascend, and SpMVCOO.cl
+// (which scans every entry for each row) matches no row outside [0, N): an
+// entry whose row or column lies outside [0, N) adds nothing (bit 1 of *err),
+// and a row id below its predecessor's sets bit 2 of *err, so the host turns
+// both into an error instead of a wrong sum or an out-of-range access.
+__global__ void k_coo_segsum(int64_t N, int64_t nnz, const int32_t *__restrict__ rows,
+                             const int32_t *__restrict__ cols, const float *__restrict__ vals,
+                             const float *__restrict__ u, float *__restrict__ acc, int *__restrict__ err)
 {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    int bad = 0;
     for (int64_t base = warp * 32; base < nnz; base += nwarps * 32) {
         const int64_t k = base + lane;
-        const bool valid = k < nnz;
-        int r = valid ? __ldcs(rows + k) : -1;
-        float p = valid ? __fmul_rn(__ldcs(vals + k), __ldg(u + __ldcs(cols + k))) : 0.0f;
+        const bool in_span = k < nnz;
+        const int rraw = in_span ? __ldcs(rows + k) : INT32_MAX;
+        const int craw = in_span ? __ldcs(cols + k) : 0;
+        const bool valid = in_span && rraw >= 0 && rraw < N && craw >= 0 && craw < N;
+        if (in_span && !valid) bad |= 1;
+        // ascending row ids: compare with the previous entry (lane 0 reads it)
+        int rprev = __shfl_up_sync(0xffffffffu, rraw, 1);
+        if (lane == 0) rprev = k > 0 && in_span ? __ldg(rows + (k - 1)) : INT32_MIN;
+        if (in_span && rraw < rprev) bad |= 2;
+        int r = valid ? rraw : -1;
+        float p = valid ? __fmul_rn(__ldcs(vals + k), __ldg(u + craw)) : 0.0f;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const float q = __shfl_up_sync(0xffffffffu, p, o);
@@ -156,6 +178,7 @@ __global__ void k_coo_segsum(int64_t nnz, const int32_t *__restrict__ rows, cons
             else acc[r] = p;
         }
     }
+    if (bad) atomicOr(err, bad);
 }
 
 // out = dt*acc (SpMVCOO's C[row] = deltat*result) or u + dt*acc.
@@ -418,9 +441,11 @@ int launch_csr_step(int nx, int ny, int nz, const int32_t *rowptr, const int32_t
 // CTAs of neighbouring row blocks run together).  Each consumer thread
 // updates 4 x-adjacent cells of one row (x neighbours by warp shuffle) and
 // stores them as one float4.  The TMA x coordinate is always 0, so every copy
-// starts on a 16-byte boundary.  Every wait is bounded: a timed-out wait sets
-// *err; the producer then waits (bounded) for its copies in flight, so none
-// lands after the CTA has left.
+// starts on a 16-byte boundary.  Every wait is bounded (a.spin polls,
+// piro_set_wait_limit): a timed-out wait sets *err and its warp leaves.
+// Before the producer leaves -- at the end of the run, or on a timeout -- it
+// waits for each stage's latest copy with its own full bound (kTmaSpin), so no
+// copy lands after the CTA has left, however early the consumers gave up.
 constexpr int kTmaThreads = 512, kTmaStages = 6, kTmaWarps = kTmaThreads / 32;
 constexpr long long kTmaSpin = 1ll << 22;
 
@@ -429,13 +454,14 @@ struct StencilTma {
     float idx2, idy2, idz2, dt;
     float *out;
     int *err;
+    long long spin;  // polls per stage wait
 };
 
 __device__ __forceinline__ uint32_t st_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ bool st_bar_wait(uint32_t bar, uint32_t parity)
+__device__ __forceinline__ bool st_bar_wait(uint32_t bar, uint32_t parity, long long limit)
 {
-    for (long long i = 0; i < kTmaSpin; ++i) {
+    for (long long i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -476,7 +502,7 @@ __global__ void __launch_bounds__(kTmaThreads + 32, 2) k_stencil_tma(const __gri
         for (; L < nload; ++L) {
             const int s = L % kTmaStages, zz = z0 - 1 + L;
             // the stage's previous load (L - S) is released once every consumer warp has read it
-            if (L >= kTmaStages && !st_bar_wait(st_smem(&empty[s]), (uint32_t)((L / kTmaStages - 1) & 1))) {
+            if (L >= kTmaStages && !st_bar_wait(st_smem(&empty[s]), (uint32_t)((L / kTmaStages - 1) & 1), a.spin)) {
                 ok = false;
                 break;
             }
@@ -497,12 +523,10 @@ __global__ void __launch_bounds__(kTmaThreads + 32, 2) k_stencil_tma(const __gri
                     "l"(reinterpret_cast<uint64_t>(&amap)), "r"(bar), "r"(0), "r"(y0), "r"(zz)
                     : "memory");
         }
-        if (!ok) {
-            atomicExch(a.err, 1);
-            // each stage's latest load is the only one that can still be in flight
-            for (int j = L - kTmaStages < 0 ? 0 : L - kTmaStages; j < L; ++j)
-                (void)st_bar_wait(st_smem(&full[j % kTmaStages]), (uint32_t)((j / kTmaStages) & 1));
-        }
+        if (!ok) atomicExch(a.err, 1);
+        // each stage's latest load is the only one that can still be in flight
+        for (int j = L - kTmaStages < 0 ? 0 : L - kTmaStages; j < L; ++j)
+            (void)st_bar_wait(st_smem(&full[j % kTmaStages]), (uint32_t)((j / kTmaStages) & 1), kTmaSpin);
         return;
     }
     const int gpr = nx >> 2;  // float4 groups per row
@@ -514,7 +538,7 @@ __global__ void __launch_bounds__(kTmaThreads + 32, 2) k_stencil_tma(const __gri
     for (int k = 1; k + 1 < nload; ++k) {  // plane z = z0 - 1 + k from loads k-1, k, k+1
         bool ok = true;
         while (ok && waited <= k + 1) {
-            ok = st_bar_wait(st_smem(&full[waited % kTmaStages]), (uint32_t)((waited / kTmaStages) & 1));
+            ok = st_bar_wait(st_smem(&full[waited % kTmaStages]), (uint32_t)((waited / kTmaStages) & 1), a.spin);
             waited += ok;
         }
         if (!__all_sync(0xffffffffu, ok)) {  // the whole warp leaves together (the shuffles below take all lanes)
@@ -586,16 +610,19 @@ bool stencil_tma_fits(int nx, int ny, int nz, const float *alpha, const float *u
 
 int encode_plane_map(CUtensorMap *m, const float *base, int nx, int ny, int nz, int rows)
 {
+    // the driver entry point, resolved once for all host threads
+    static std::once_flag resolved;
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
+    std::call_once(resolved, []() {
         void *fn = nullptr;
         cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess || !fn) {
-            set_error("cuTensorMapEncodeTiled is not available");
-            return PIRO_ERR_CUDA;
-        }
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess && fn)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    if (!encode) {
+        set_error("cuTensorMapEncodeTiled is not available");
+        return PIRO_ERR_CUDA;
     }
     const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
     const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * ny * 4};
@@ -648,7 +675,7 @@ int stencil_tma_step(int nx, int ny, int nz, float idx2, float idy2, float idz2,
     rc = encode_plane_map(&umap, u, nx, ny, nz, TY + 2);
     if (!rc) rc = encode_plane_map(&amap, alpha ? alpha : u, nx, ny, nz, TY);
     if (rc) return rc;
-    StencilTma a{nx, ny, nz, TY, zchunk, alpha ? 1 : 0, idx2, idy2, idz2, dt, out, d.err_flag};
+    StencilTma a{nx, ny, nz, TY, zchunk, alpha ? 1 : 0, idx2, idy2, idz2, dt, out, d.err_flag, wait_limit(kTmaSpin)};
     k_stencil_tma<<<dim3((unsigned)ytiles, (unsigned)runs), kTmaThreads + 32, stencil_tma_smem(nx), st>>>(umap, amap,
                                                                                                         a);
     PIRO_CHECK_LAUNCH("k_stencil_tma");
@@ -686,20 +713,41 @@ extern "C" int piro_csr_i1(int nx, int ny, int nz, const int32_t *rowptr, const 
     return launch_csr_step<1>(nx, ny, nz, rowptr, col, val, dt, u, out, stream);
 }
 
+// Per device: the input-check flags of k_coo_segsum.
+static int *coo_err_dev[kMaxDevices] = {};
+static DeviceOnce coo_err_once;
+
 static int coo_common(int64_t N, int64_t nnz, const int32_t *rows, const int32_t *cols, const float *vals, float dt,
                       const float *u, float *out, bool fe, piro_stream_t stream)
 {
-    PIRO_ARG(N > 0 && nnz >= 0 && rows && cols && vals && u && out, "coo spmv: bad arguments");
+    PIRO_ARG(N > 0 && N < INT32_MAX && nnz >= 0 && (nnz == 0 || (rows && cols && vals)) && u && out,
+             "coo spmv: bad arguments");
     PIRO_ARG(u != out, "coo spmv: u and out must differ");
     cudaStream_t s = as_stream(stream);
+    int dev = 0;
+    PIRO_CUDA(cudaGetDevice(&dev));
+    int rc = device_once(coo_err_once, dev, [dev]() -> int {
+        if (!coo_err_dev[dev]) PIRO_CUDA(cudaMalloc(&coo_err_dev[dev], sizeof(int)));
+        return PIRO_OK;
+    });
+    if (rc != PIRO_OK) return rc;
+    int *err = coo_err_dev[dev];
     // out doubles as the accumulator: zero it, sum into it, then scale in place.
     PIRO_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * N, s));
     if (nnz > 0) {
-        k_coo_segsum<<<grid_for(nnz, 256, 8), 256, 0, s>>>(nnz, rows, cols, vals, u, out);
+        PIRO_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+        k_coo_segsum<<<grid_for(nnz, 256, 8), 256, 0, s>>>(N, nnz, rows, cols, vals, u, out, err);
         PIRO_CHECK_LAUNCH("k_coo_segsum");
     }
     k_scale_add<<<grid_for(N, 256, 8), 256, 0, s>>>(N, dt, out, fe ? u : nullptr, out);
     PIRO_CHECK_LAUNCH("k_scale_add");
+    if (nnz > 0) {
+        int h = 0;
+        PIRO_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        PIRO_CUDA(cudaStreamSynchronize(s));
+        PIRO_ARG(!(h & 1), "coo spmv: a row or column id outside [0, N)");
+        PIRO_ARG(!(h & 2), "coo spmv: row ids not sorted ascending (use piro_coo_row_index for its check)");
+    }
     return PIRO_OK;
 }
 

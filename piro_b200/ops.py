@@ -348,7 +348,14 @@ class BESolver:
     def inner_operator(self):
         k = C.c_int()
         check(lib().piro_be_inner_operator(self.h, C.byref(k)), "piro_be_inner_operator")
-        return ["csr", "stencil", "stencil-persistent"][k.value]
+        return ["csr", "stencil", "stencil-persistent", "stencil-persistent"][k.value]
+
+    @property
+    def persistent_variant(self):
+        """'resident' (r, d, q in shared memory), 'global', or None (no persistent kernel)."""
+        k = C.c_int()
+        check(lib().piro_be_inner_operator(self.h, C.byref(k)), "piro_be_inner_operator")
+        return {2: "global", 3: "resident"}.get(k.value)
 
     def persistent_bytes(self):
         v = C.c_double()

@@ -1,8 +1,8 @@
 """Generate the golden fixtures in tests/golden/ from PIRO's own code.
 
-Run in a container that has the reference tree (default /root/reference):
+Run where the PIRO source tree is present, named by PIRO_REF_DIR:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    PIRO_REF_DIR=<PIRO tree> make -C oracle ref && python tests/golden/make_golden.py
 
 Every array stored here is produced by the reference itself -- its host
 stencil/hash/boundary routines and its .cl kernels compiled for the CPU

@@ -6,6 +6,7 @@ on any machine, GPU or not.  Mirrors the reference's preprocess
 an invalid one."""
 from __future__ import annotations
 
+import json
 import os
 import shutil
 
@@ -73,22 +74,21 @@ def test_valid_case_without_a_gpu_fails_loudly(tmp_path):
     assert "PIRO_ERR_CUDA" in str(e), str(e)
 
 
-REF_DIR = os.environ.get("PIRO_REF_DIR", "/root/reference")
-
-
-@pytest.mark.skipif(not os.path.isdir(os.path.join(REF_DIR, "Test")), reason="the reference tree is not present")
 @pytest.mark.parametrize("name", ["HeatEq.ini", "AdvEq.ini", "LUDecomp.ini"])
 def test_reference_cases_parse(tmp_path, name):
     """PIRO's own example cases (Test/*.ini, run by maketest.sh from a copy of
-    dependencies/assets with the case file placed beside setup.ini) get
-    through the front end: with no GPU the first failure is the first CUDA
-    call, never the parser."""
+    dependencies/assets with the case file placed beside setup.ini; rebuilt
+    here from tests/golden/reference_cases.json) get through the front end:
+    with no GPU the first failure is the first CUDA call, never the parser."""
     import torch
+    from test_gpu_reference_cases import write_ini
     if torch.cuda.is_available():
         pytest.skip("a GPU is present: the case would open")
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_cases.json")) as f:
+        d = json.load(f)
     assets = tmp_path / "assets"
-    shutil.copytree(os.path.join(REF_DIR, "dependencies", "assets"), assets,
-                    ignore=shutil.ignore_patterns("kernels"))
-    shutil.copy(os.path.join(REF_DIR, "Test", name), assets / name)
+    for rel, sections in d["assets"].items():
+        write_ini(os.path.join(assets, *rel.split("/")), sections)
+    write_ini(os.path.join(assets, name), d["cases"][name])
     e = open_error(str(assets), name)
     assert "PIRO_ERR_CUDA" in str(e), str(e)

@@ -123,6 +123,76 @@ def test_step_kernels_vs_golden(cuda, golden_grids):
             assert f32_bits_equal(h(val), g[f"spmdsm_{t}"])
 
 
+def test_coo_bad_rows_are_errors(cuda, golden_grids):
+    """Both COO entry points turn a row id outside [0, N) and row ids that do
+    not ascend into PIRO_ERR_ARG (SpMVCOO.cl matches no row outside [0, N);
+    the warp-segmented sum is only whole rows when the ids ascend), and the
+    library stays usable: the next call with good input matches the fixture."""
+    import torch
+    from piro_b200 import ops
+    from piro_b200._lib import PiroError
+    (nx, ny, nz), g = golden_grids[0]
+    N = nx * ny * nz
+    t = "s3_h1"
+    rows, col, val = (g[f"coo_{k}_{t}"] for k in ("rows", "col", "val"))
+    u = dev(torch, g[f"in_u_{t}"])
+    out = torch.empty(N, dtype=torch.float32, device="cuda")
+    bad_range = rows.copy()
+    bad_range[len(rows) // 2] = N  # one entry's row past the last row
+    bad_order = rows.copy()
+    k = int(np.argmax(np.diff(rows) > 0))  # first row change: swap the ids around it
+    bad_order[k], bad_order[k + 1] = bad_order[k + 1], bad_order[k]
+    for bad in (bad_range, bad_order):
+        coo = (dev(torch, bad), dev(torch, col), dev(torch, val))
+        for fe in (False, True):
+            with pytest.raises(PiroError) as e:
+                ops.coo_spmv(N, coo, 0.01, u, out, fe=fe)
+            assert e.value.status == 1  # PIRO_ERR_ARG
+        with pytest.raises(PiroError) as e:
+            ops.coo_row_index(N, coo[0])
+        assert e.value.status == 1
+    neg = rows.copy()
+    neg[0] = -1
+    with pytest.raises(PiroError):
+        ops.coo_spmv(N, (dev(torch, neg), dev(torch, col), dev(torch, val)), 0.01, u, out)
+    coo = (dev(torch, rows), dev(torch, col), dev(torch, val))
+    ops.coo_spmv(N, coo, 0.01, u, out)
+    np.testing.assert_allclose(h(out), g[f"spmvcoo_{t}"], rtol=1e-5, atol=1e-6)
+
+
+def test_csr_and_coo_steps_on_wide_rows_bitexact(cuda, oracle):
+    """Rows longer than 32 entries are summed by their whole warp (coalesced
+    entry loads, terms added in storage order through a shuffle chain), the
+    rest one row per thread: the result must equal SpMVCSR.cl's / SpMVCOO.cl's
+    sequential sums bit for bit whatever the mix of lengths in a warp."""
+    import torch
+    from piro_b200 import ops
+    nx, ny, nz = 18, 16, 14
+    N = nx * ny * nz
+    rng = np.random.default_rng(21)
+    lengths = rng.choice([0, 1, 3, 7, 31, 32, 33, 64, 100, 257, 1000], size=N,
+                         p=[.05, .05, .1, .3, .05, .05, .1, .1, .1, .07, .03]).astype(np.int64)
+    lengths[5] = 5000  # one very long row
+    rp = np.zeros(N + 1, np.int64)
+    rp[1:] = np.cumsum(lengths)
+    nnz = int(rp[-1])
+    col = rng.integers(0, N, size=nnz).astype(np.int32)  # unsorted, with repeats
+    val = rng.standard_normal(nnz).astype(np.float32)
+    A = (rp.astype(np.int32), col, val)
+    u = rng.standard_normal(N).astype(np.float32)
+    c0 = rng.standard_normal(N).astype(np.float32)
+    dt = np.float32(0.013)
+    want = oracle.spmv_csr_fe(nx, ny, nz, A, dt, u, c0)
+    Ad = tuple(dev(torch, a) for a in A)
+    out = dev(torch, c0)
+    ops.csr_fe_step(nx, ny, nz, Ad, dt, dev(torch, u), out)
+    assert f32_bits_equal(h(out), want)
+    rows = np.repeat(np.arange(N, dtype=np.int32), lengths)
+    want_coo = oracle.spmv_coo(N, (rows, col, val), dt, u)
+    ops.coo_step_indexed(N, Ad[0], Ad[1], Ad[2], dt, dev(torch, u), out)
+    assert f32_bits_equal(h(out), want_coo)
+
+
 def test_csrgeam3_vs_golden(cuda, golden_grids):
     import torch
     from piro_b200 import ops
