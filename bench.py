@@ -489,6 +489,54 @@ def learned_section(torch, ops, cfg, A, alpha, plain_ms, plain_iters, steps, tfl
     }
 
 
+def training_section(torch, ops, tflops_peak, steps=30, batch=16, crop=32):
+    """Training throughput of the learned preconditioner's network: one step =
+    forward, masked-MSE loss, backward and Adam on `batch` crops of crop^3
+    interior cells (+ a ghost layer), the batch the training recipe uses
+    (piro_b200/learned.py: 10 000 pairs of 32^3 crops, batches of 16).  Both
+    engines: every convolution on tcgen05 (forward, data and weight
+    gradients), and the CUDA-core kernels.  Inputs are seeded random crops
+    (the kernels' cost does not depend on the values)."""
+    m = crop + 2
+    N = m ** 3
+    rng = np.random.default_rng(5)
+    r = torch.from_numpy(rng.standard_normal(batch * N).astype(np.float32)).cuda()
+    f = torch.from_numpy((0.5 * rng.standard_normal(batch * N)).astype(np.float32)).cuda()
+    t = torch.from_numpy((0.1 * rng.standard_normal(batch * N)).astype(np.float32)).cuda()
+    mk = torch.from_numpy((rng.random(batch * N) > 0.3).astype(np.float32)).cuda()
+    n_int = batch * crop ** 3
+    # multiply-adds of one step: forward 30 240 N, data gradients of layers 2-4
+    # (16x16, 16x16, 1x16 per tap) and weight gradients of all four layers
+    fwd = 2 * 27 * (2 * 16 + 16 * 16 + 16 * 16 + 16) * n_int
+    bwd_data = 2 * 27 * (16 * 16 + 16 * 16 + 16) * n_int
+    bwd_w = fwd
+    flops = fwd + bwd_data + bwd_w
+    out = {"batch": batch, "crop": crop, "cells_per_step": batch * N, "flop_per_step": flops}
+    for name, tc in (("tensor_cores", True), ("cuda_cores", False)):
+        net = ops.PCNet(seed=0)
+        net.set_engine(tc)
+        for _ in range(3):
+            net.loss_grad(m, m, m, r, f, t, mk, batch=batch, want_loss=False)
+            net.adam_step(1e-4)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            net.loss_grad(m, m, m, r, f, t, mk, batch=batch, want_loss=False)
+            net.adam_step(1e-4)
+        e1.record()
+        loss, _ = net.loss_grad(m, m, m, r, f, t, mk, batch=batch)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[name] = {"ms_per_step": round(ms, 3), "pairs_per_s": round(batch / ms * 1e3, 1),
+                     "tflops": round(flops / ms / 1e9, 1), "frac_of_bf16_peak": round(flops / ms / 1e9 / tflops_peak, 4),
+                     "loss_finite": bool(np.isfinite(loss))}
+        net.close()
+    out["speedup_tensor_vs_cuda_cores"] = round(out["cuda_cores"]["ms_per_step"] / out["tensor_cores"]["ms_per_step"], 2)
+    out["epoch_10k_pairs_s"] = round(10000 / out["tensor_cores"]["pairs_per_s"], 2)
+    return out
+
+
 def batched_section(torch, ops, peak, steps=4):
     """Configuration 5: 512 independent heat problems (cube sides 16..96,
     alpha log-uniform [1e-3, 1e-1], forward or backward Euler, seed 3) in one
@@ -747,6 +795,7 @@ def run_piro(args):
     configs = config_sections(torch, peak) if solo else None
     learned = (learned_section(torch, ops, cfg, A, alpha, ms_step, main["iters"], min(args.steps, 40), tf_peak,
                                l2_flush) if solo else None)
+    training = training_section(torch, ops, tf_peak) if solo else None
     batched = batched_section(torch, ops, peak) if solo else None
     next_rows = next_rows_section(torch, ops, peak) if solo else None
     assembly = assembly_section(torch, ops, peak) if solo else None
@@ -803,6 +852,7 @@ def run_piro(args):
         "spmv_256": spmv,
         "configs": configs,
         "learned": learned,
+        "training": training,
         "batched": batched,
         "next_rows": next_rows,
         "assembly": assembly,
@@ -858,7 +908,8 @@ def run_profile_case(args):
     128^3 backward-Euler step twice, `spmv` runs the 256^3 forward-Euler
     kernels (CSR, matrix-free, fused CSR + setBC, indexed COO, ordered HT), `dense` three DENSE steps at N = 12,288 (a 604 MB
     matrix), `learned` two learned-preconditioner solves of the 128^3 step,
-    `batched` two steps of a 64-member batch."""
+    `batched` two steps of a 64-member batch, `train` four training steps of
+    the network on 8 crops of 34^3 cells."""
     import torch
 
     from piro_b200 import ops
@@ -897,6 +948,19 @@ def run_profile_case(args):
             info = s.solve(b, x, rtol=1e-8)
         print("learned", info.inner_iterations, info.rel_residual)
         s.close()
+        net.close()
+    elif args.profile == "train":
+        m, batch = 34, 8
+        N = m ** 3
+        rng = np.random.default_rng(5)
+        r, f, t = (torch.from_numpy(rng.standard_normal(batch * N).astype(np.float32)).cuda() for _ in range(3))
+        mk = torch.ones(batch * N, device="cuda")
+        net = ops.PCNet(seed=0)
+        for _ in range(3):
+            net.loss_grad(m, m, m, r, f, t, mk, batch=batch, want_loss=False)
+            net.adam_step(1e-4)
+        loss, _ = net.loss_grad(m, m, m, r, f, t, mk, batch=batch)
+        print("train", loss)
         net.close()
     elif args.profile == "batched":
         cfg = W.batched(count=64)
@@ -940,7 +1004,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="piro", choices=["piro", "reference"])
-    ap.add_argument("--profile", choices=["be", "spmv", "dense", "learned", "batched"],
+    ap.add_argument("--profile", choices=["be", "spmv", "dense", "learned", "batched", "train"],
                     help="run a small fixed case for ncu, print no JSON")
     args = ap.parse_args()
     if args.profile:

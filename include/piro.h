@@ -207,22 +207,27 @@ int piro_ht_spmv_ordered(int nx, int ny, int nz, const int64_t *keys, const floa
  * PIRO_ERR_TABLE_FULL when the fill-in does not fit.  N <= 46340 (int32 keys
  * in the reference).
  * piro_ht_lu_factor / piro_ht_lu_solve give scheme 27 a solution, which the
- * reference does not compute.  The factor reads the table once and writes
- * shift*I + scale*M (M the table's matrix) into a dense band of bandwidth bw
- * (nx*ny for the 7-point grid; row r, column c at band[r*(2bw+1) + c-r+bw]),
- * then factorizes it in place without pivoting: U on and above the diagonal,
- * the unit-lower L's multipliers below.  band is a device buffer of
- * piro_ht_lu_band_bytes bytes (the band, then the solve's scratch).
- * PIRO_ERR_ARG when a table entry lies outside the band; PIRO_ERR_ZERO_PIVOT
- * when a pivot is exactly zero.  piro_ht_lu_solve solves L U x = b (b, x
- * device float[N], distinct) by forward and backward substitution, one
- * cooperative launch, and synchronizes the stream. */
+ * reference does not compute (its lu_decompHT.cl eliminates in FP32 without
+ * pivoting and never substitutes).  The factor reads the table once and
+ * writes shift*I + scale*M (M the table's matrix) in FP64 into a band of
+ * bandwidth bw (nx*ny for the 7-point grid), then factorizes it by Gaussian
+ * elimination with partial pivoting in FP64, as LAPACK's banded LU (dgbtrf):
+ * P A = L U with U's upper bandwidth 2bw, the first row of largest magnitude
+ * chosen on a tie.  band is a device buffer of piro_ht_lu_band_bytes bytes
+ * (band, multipliers, pivots and the solve's workspace).  PIRO_ERR_ARG when a
+ * table entry lies outside the band; PIRO_ERR_ZERO_PIVOT when a column has no
+ * nonzero at or below the diagonal (a singular matrix).  piro_ht_lu_solve
+ * solves A x = b (b, x device float[N]) in FP64 -- the row exchanges and
+ * Gauss transforms, then back substitution -- and rounds x to FP32.
+ * piro_ht_lu_pivots copies the pivot rows (0-based, LAPACK's ipiv - 1) to the
+ * host. */
 int piro_ht_lu_reference(int64_t N, int64_t *keys, float *vals, int64_t ts, piro_stream_t stream);
 int piro_ht_lu_band_bytes(int64_t N, int64_t bw, size_t *bytes);
 int piro_ht_lu_factor(int64_t N, int64_t bw, const int64_t *keys, const float *vals, int64_t ts, float shift,
                       float scale, void *band, size_t band_bytes, piro_stream_t stream);
 int piro_ht_lu_solve(int64_t N, int64_t bw, void *band, size_t band_bytes, const float *b, float *x,
                      piro_stream_t stream);
+int piro_ht_lu_pivots(int64_t N, int64_t bw, const void *band, size_t band_bytes, int32_t *piv_host);
 
 /* DENSE format (Data 1).  piro_dense_laplacian: Piro::DENSE::stencils::
  * laplacian_* (src/stencils.cpp:431-570) into A (N x N row-major floats,
@@ -425,11 +430,14 @@ int piro_pcnet_loss_grad(piro_pcnet *n, int batch, int nx, int ny, int nz, const
                          const float *target, const float *mask, double *loss, float *grad, piro_stream_t stream);
 /* Adam (beta1 0.9, beta2 0.999, eps 1e-8) with the last computed gradient. */
 int piro_pcnet_adam_step(piro_pcnet *n, float lr, piro_stream_t stream);
-/* Engine of the inference forward pass (default: tensor cores) of piro_pcnet_forward and the solver's
- * preconditioner apply): CUDA-core kernels, or all four layers as tcgen05
+/* Engine of the network's kernels (default: tensor cores), for the
+ * inference forward pass (piro_pcnet_forward and the solver's preconditioner
+ * apply) and for training (piro_pcnet_loss_grad): CUDA-core kernels, or every
+ * convolution on tcgen05 -- the forward passes and the data gradients as
  * implicit GEMMs (TMA-staged BF16 operands with the channels padded to 16,
- * FP32 accumulation in tensor memory).  Training always uses the CUDA-core
- * kernels. */
+ * FP32 accumulation in tensor memory), the weight gradients as GEMMs over the
+ * cells with MN-major operands; in training the loss gradient enters the last
+ * layer in BF16. */
 #define PIRO_PCNET_CUDA_CORES 0
 #define PIRO_PCNET_TENSOR_CORES 1
 int piro_pcnet_set_engine(piro_pcnet *n, int engine);

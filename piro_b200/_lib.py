@@ -78,6 +78,7 @@ SIGNATURES = {
     "piro_ht_lu_band_bytes": (i32, [i64, i64, C.POINTER(sz)]),
     "piro_ht_lu_factor": (i32, [i64, i64, vp, vp, i64, f32, f32, vp, sz, vp]),
     "piro_ht_lu_solve": (i32, [i64, i64, vp, sz, vp, vp, vp]),
+    "piro_ht_lu_pivots": (i32, [i64, i64, vp, sz, vp]),
     "piro_stencil_fe_step": (i32, [i32, i32, i32, f32, f32, f32, f32, vp, vp, vp, vp]),
     "piro_set_bc": (i32, [i64, vp, vp, vp, vp]),
     "piro_face_count": (i32, [i32, i32, i32, pi64, pi64]),

@@ -66,12 +66,14 @@ struct Args {
     int64_t N, nxy;
     int ncol, zchunk;
     const bf16 *wpk;   // packed weights of this layer
-    bf16 *out;         // output activations (epilogue 0)
+    bf16 *out;         // output activations (epilogues 0, 2) or gradient (epilogue 3)
     float *zout;       // FP32 output channel 0 (epilogue 1)
     const double *rr;  // epilogue 1: output scale sqrt(rr[b] / n_int) (NULL: 1)
     double n_int;
     const int *skip;   // launch returns at once when set (may be NULL)
     int *err;          // raised on a timed-out wait
+    bf16 *yout;        // epilogue 2: the pre-activation bf16(acc)
+    const bf16 *yprev; // epilogue 3: the previous layer's pre-activation
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -110,6 +112,15 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int *er
     }
     atomicExch(err, 1);
     return false;
+}
+
+// Wait for a phase that is certain to complete (copies or MMAs this CTA
+// issued itself), with its own bound so that a role which gave up on a
+// partner still leaves nothing in flight behind it.
+__device__ __forceinline__ void mbar_drain(uint32_t bar, uint32_t parity)
+{
+    for (long long i = 0; i < kSpin; ++i)
+        if (mbar_try_wait(bar, parity)) return;
 }
 
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0, int c1, int c2)
@@ -173,8 +184,21 @@ __device__ __forceinline__ float gelu_tc(float x)
     return 0.5f * x * (1.0f + t);
 }
 
+// GELU'(x) of the tanh form above: 0.5 (1 + t) + 0.5 x (1 - t^2) c (1 + 3 a x^2).
+__device__ __forceinline__ float gelu_d_tc(float x)
+{
+    float t;
+    const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * 0.7978845608028654f * (1.0f + 0.134145f * x * x);
+}
+
 // kEpi 0: GELU, 16 BF16 channels out (hidden layers); 1: output channel 0 in
-// FP32 times the batch member's scale (the last layer, N padded to 16).
+// FP32 times the batch member's scale (the last layer, N padded to 16);
+// 2 (training forward): the pre-activation y = bf16(acc) to yout and GELU(y)
+// to out; 3 (data gradient, run with the transposed, tap-reversed weights):
+// out = bf16(acc * GELU'(yprev)), the gradient with respect to the previous
+// layer's pre-activation.  Every epilogue writes zeros on non-interior cells.
 template <int kEpi>
 __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant__ CUtensorMap xmap, Args a)
 {
@@ -189,6 +213,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
     auto empty = [&](int i) { return bar_s + 8u * (kSlots + i); };
     auto accf = [&](int b) { return bar_s + 8u * (2 * kSlots + b); };
     auto acce = [&](int b) { return bar_s + 8u * (2 * kSlots + 2 + b); };
+    const uint32_t drain_s = bar_s + 8u * (2 * kSlots + 4);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t boff = (int64_t)blockIdx.y * a.N;  // batch member: rows b*N ..
@@ -212,6 +237,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
             mbar_init(accf(b), 1);
             mbar_init(acce(b), 4);
         }
+        mbar_init(drain_s, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -230,7 +256,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
         if (warp == 4) {
             if (lane == 0) {
                 // producer: planes zb-1 .. ze, three line blocks each
-                for (int p = 0; p < P + 2; ++p) {
+                int p = 0;
+                for (; p < P + 2; ++p) {
                     const int slot = p % kSlots;
                     if (p >= kSlots && !mbar_wait(empty(slot), ((p / kSlots) - 1) & 1, a.err)) break;
                     const int64_t L = zb - 1 + p;
@@ -241,6 +268,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
                                     0);
                     }
                 }
+                // no copy may land after the CTA has left, whatever the other
+                // roles did: wait for each slot's latest load
+                for (int q = p - kSlots < 0 ? 0 : p - kSlots; q < p; ++q) mbar_drain(full(q % kSlots), (q / kSlots) & 1);
             }
         } else if (warp == 5) {
             if (lane == 0) {
@@ -273,6 +303,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
                     mma_commit(accf(buf));
                     mma_commit(empty(j % kSlots));  // plane z-1 is read by no later tile
                 }
+                // every MMA issued here has completed before TMEM is released
+                mma_commit(drain_s);
+                mbar_drain(drain_s, 0);
             }
         } else {
             // epilogue: warp w holds tile rows 32w .. 32w+31
@@ -292,8 +325,27 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
                         if (a.rr) sc = (float)sqrt(a.rr[blockIdx.y] / a.n_int);
                         a.zout[boff + c] = a.g.interior(c) ? __uint_as_float(v[0]) * sc : 0.0f;
                     }
+                } else if (kEpi == 3) {
+                    if (c < a.N) {
+                        uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                        if (a.g.interior(c)) {
+                            const uint4 *yp = reinterpret_cast<const uint4 *>(a.yprev + (boff + c) * 16);
+                            const uint4 u0 = yp[0], u1 = yp[1];
+                            const uint32_t yw[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+#pragma unroll
+                            for (int k = 0; k < 8; ++k) {
+                                const float2 y = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&yw[k]));
+                                const __nv_bfloat162 h = __floats2bfloat162_rn(__uint_as_float(v[2 * k]) * gelu_d_tc(y.x),
+                                                                               __uint_as_float(v[2 * k + 1]) * gelu_d_tc(y.y));
+                                w[k] = *reinterpret_cast<const uint32_t *>(&h);
+                            }
+                        }
+                        uint4 *o = reinterpret_cast<uint4 *>(a.out + (boff + c) * 16);
+                        o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                        o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                    }
                 } else if (c < a.N) {
-                    uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                    uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0}, yw[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                     if (a.g.interior(c)) {
 #pragma unroll
                         for (int k = 0; k < 8; ++k) {
@@ -301,11 +353,20 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
                             const float y1 = __bfloat162float(__float2bfloat16_rn(__uint_as_float(v[2 * k + 1])));
                             const __nv_bfloat162 h = __floats2bfloat162_rn(gelu_tc(y0), gelu_tc(y1));
                             w[k] = *reinterpret_cast<const uint32_t *>(&h);
+                            if (kEpi == 2) {
+                                const __nv_bfloat162 hy = __floats2bfloat162_rn(y0, y1);
+                                yw[k] = *reinterpret_cast<const uint32_t *>(&hy);
+                            }
                         }
                     }
                     uint4 *o = reinterpret_cast<uint4 *>(a.out + (boff + c) * 16);
                     o[0] = make_uint4(w[0], w[1], w[2], w[3]);
                     o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                    if (kEpi == 2) {
+                        uint4 *oy = reinterpret_cast<uint4 *>(a.yout + (boff + c) * 16);
+                        oy[0] = make_uint4(yw[0], yw[1], yw[2], yw[3]);
+                        oy[1] = make_uint4(yw[4], yw[5], yw[6], yw[7]);
+                    }
                 }
             }
         }

@@ -28,29 +28,21 @@
 //
 // piro_ht_lu_factor / piro_ht_lu_solve make scheme 27 return a solution.  The
 // table is the input format only: one pass over its slots scatters
-// shift*I + scale*M into a dense band (row r, column c at
-// band[r*(2bw+1) + c - r + bw]; bw = nx*ny for the 7-point grid in natural
-// order).  Elimination without pivoting fills in nothing outside the band,
-// and in the band no lookup probes a cluster: keys r*N + c of one row are
-// contiguous, so at load 0.7 the rows' runs of slots merge and a table lookup
-// walks thousands of slots.  The LU runs in place in the band, one launch per
-// pivot row over the (bw x bw) block below and right of it; the multipliers
-// of a column are stored by the next launch, which no longer reads that
-// column.  The substitution is one cooperative launch: per block of 32 rows,
-// the worker CTAs form the partial sums of the NEXT block over the solved
-// part of its band while CTA 0 finishes the current block (its sums, the
-// contribution of the block just solved, and the 32x32 triangle in one warp);
-// one grid barrier per block, every wait bounded.
+// shift*I + scale*M in FP64 into a band (bandwidth bw = nx*ny for the 7-point
+// grid in natural order).  The table stays out of the elimination: keys
+// r*N + c of one row are contiguous, so at load 0.7 the rows' runs of slots
+// merge and a table lookup walks thousands of slots.  The factorization is
+// Gaussian elimination with partial pivoting in FP64 (LAPACK's banded LU,
+// dgbtrf): per pivot row one launch chooses the pivot, exchanges the two
+// rows and forms the multipliers, a second applies the rank-1 update to the
+// (bw x 2bw) block below and right of it.  The solve (one block, FP64)
+// replays the exchanges and Gauss transforms on b and back-substitutes.
 #include "common.cuh"
 
 namespace piro {
 namespace {
 
 constexpr int64_t kEmpty = -1, kDeleted = -2;
-constexpr int kTri = 32;          // rows per substitution block
-constexpr int kSolveThreads = 256;
-constexpr int kMaxCta = 1024;     // partial-sum slots per buffer
-constexpr long long kSpinLimit = 1ll << 22;  // a stuck barrier ends with an error, not a hang
 
 // methods::lookup / lu_decompHT.cl lookup: value and slot of key, or 0 and -1.
 __device__ __forceinline__ float ht_find(int64_t key, const int64_t *__restrict__ keys, const float *__restrict__ vals,
@@ -271,18 +263,32 @@ __global__ void __launch_bounds__(1024) k_lu_reference_smem(int64_t N, int64_t *
 size_t lu_reference_smem_bytes(int64_t N, int64_t ts) { return (size_t)ts * 12 + (size_t)N * 12; }
 constexpr size_t kLuSmemMax = 220 * 1024;
 
-// ---------------------------------------------------------------- banded LU and substitution
+// ---------------------------------------------------------------- banded LU with partial pivoting (FP64)
+//
+// A = shift*I + scale*M in FP64, bandwidths kl = ku = bw.  Row r of the band
+// holds columns r - bw .. r + 2bw (W = 3bw + 1 doubles, column c at
+// band[r*W + c - r + bw]): row interchanges can move entries up to 2bw right
+// of the diagonal into U, as in LAPACK's banded LU (dgbtrf).  Pivot row ro,
+// one launch: piv[ro] = the row p in [ro, ro+bw] with the largest |a(p, ro)|
+// (the first such row on a tie), rows ro and p exchanged over columns ro ..
+// ro+2bw, and the multipliers l(i) = a(ro+i, ro) / a(ro, ro) written to
+// Lc[ro*bw + i - 1].  A second launch subtracts l(i) * a(ro, c) from
+// a(ro+i, c) for c in (ro, ro+2bw].  The multipliers stay with the row
+// positions of their step (earlier columns are never exchanged), so the
+// solve applies, step by step, the exchange and then the Gauss transform to
+// b, and back-substitutes with U.  A column without a nonzero in its band is
+// a singular matrix (PIRO_ERR_ZERO_PIVOT).
 
-__global__ void k_band_diag(int64_t N, int64_t W, int64_t bw, float shift, float *__restrict__ band)
+__global__ void k_lup_diag(int64_t N, int64_t W, int64_t bw, double shift, double *__restrict__ band)
 {
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < N; r += (int64_t)gridDim.x * blockDim.x)
         band[r * W + bw] = shift;
 }
 
-// band(r, c) = shift*[r == c] + scale*M(r, c) for every key in the table.
-__global__ void k_band_scatter(int64_t N, int64_t bw, int64_t W, const int64_t *__restrict__ keys,
-                               const float *__restrict__ vals, int64_t ts, float shift, float scale,
-                               float *__restrict__ band, int *err)
+// band(r, c) = shift*[r == c] + scale*M(r, c) in FP64 for every key in the table.
+__global__ void k_lup_scatter(int64_t N, int64_t bw, int64_t W, const int64_t *__restrict__ keys,
+                              const float *__restrict__ vals, int64_t ts, double shift, double scale,
+                              double *__restrict__ band, int *err)
 {
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < ts; s += (int64_t)gridDim.x * blockDim.x) {
         const int64_t k = keys[s];
@@ -292,239 +298,173 @@ __global__ void k_band_scatter(int64_t N, int64_t bw, int64_t W, const int64_t *
             atomicCAS(err, 0, 2);
             continue;
         }
-        const float v = __fmul_rn(scale, vals[s]);
-        band[r * W + d + bw] = d == 0 ? __fadd_rn(shift, v) : v;
+        const double v = scale * (double)vals[s];
+        band[r * W + d + bw] = d == 0 ? shift + v : v;
     }
 }
 
-// Pivot row ro: a(r, c) -= (a(r, ro)/a(ro, ro)) * a(ro, c) for r, c in
-// (ro, ro+span]; block (x, y) takes row ro+1+y, columns kRoundCols*x ..; and
-// the multipliers of column ro-1 divided in place (no item of this round
-// reads that column).
-constexpr int kRoundThreads = 256, kRoundCols = 1024;
+constexpr int kPivThreads = 1024;
 
-__global__ void __launch_bounds__(kRoundThreads) k_band_round(int64_t N, int64_t bw, int64_t W,
-                                                              float *__restrict__ band, int64_t ro, int *err)
+// Pivot search, row exchange and multipliers of pivot row ro (one block).
+__global__ void __launch_bounds__(kPivThreads) k_lup_pivot(int64_t N, int64_t bw, int64_t W,
+                                                           double *__restrict__ band, double *__restrict__ Lc,
+                                                           int32_t *__restrict__ piv, int64_t ro, int *err)
 {
-    const float piv = band[ro * W + bw];
-    if (piv == 0.0f) {
-        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && atomicCAS(err, 0, 3) == 0) err[1] = (int)ro;
-        return;
-    }
+    __shared__ double s_v[32];
+    __shared__ int64_t s_i[32];
+    __shared__ int64_t s_p;
+    if (*((volatile int *)err)) return;  // an earlier pivot was zero
     const int64_t span = N - 1 - ro < bw ? N - 1 - ro : bw;
-    if (ro > 0 && blockIdx.x == 0) {
-        const int64_t pspan = N - ro < bw ? N - ro : bw;
-        const float pp = band[(ro - 1) * W + bw];
-        for (int64_t t = (int64_t)blockIdx.y * blockDim.x + threadIdx.x; t < pspan; t += (int64_t)gridDim.y * blockDim.x) {
-            float *m = band + (ro + t) * W + (bw - 1 - t);  // a(ro+t, ro-1)
-            *m = __fdiv_rn(*m, pp);
+    // largest |a(ro+t, ro)|, the smallest t on a tie
+    double best = -1.0;
+    int64_t bi = 0;
+    for (int64_t t = threadIdx.x; t <= span; t += blockDim.x) {
+        const double v = fabs(band[(ro + t) * W + bw - t]);
+        if (v > best) {
+            best = v;
+            bi = t;
         }
     }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_down_sync(0xffffffffu, best, o);
+        const int64_t oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ov > best || (ov == best && oi < bi)) {
+            best = ov;
+            bi = oi;
+        }
+    }
+    if (lane == 0) {
+        s_v[warp] = best;
+        s_i[warp] = bi;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        best = lane < (int)(blockDim.x >> 5) ? s_v[lane] : -1.0;
+        bi = lane < (int)(blockDim.x >> 5) ? s_i[lane] : 0;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_down_sync(0xffffffffu, best, o);
+            const int64_t oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) {
+                best = ov;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            s_p = best > 0.0 ? bi : -1;
+            piv[ro] = (int32_t)(ro + (best > 0.0 ? bi : 0));
+            if (best <= 0.0 && atomicCAS(err, 0, 3) == 0) err[1] = (int)ro;
+        }
+    }
+    __syncthreads();
+    const int64_t p = s_p;
+    if (p < 0) return;
+    // exchange rows ro and ro+p over columns ro .. ro+2bw
+    const int64_t cend = N - 1 - ro < 2 * bw ? N - 1 - ro : 2 * bw;
+    if (p > 0)
+        for (int64_t j = threadIdx.x; j <= cend; j += blockDim.x) {
+            double *a = band + ro * W + bw + j;             // a(ro, ro+j)
+            double *b = band + (ro + p) * W + bw - p + j;   // a(ro+p, ro+j)
+            const double t = *a;
+            *a = *b;
+            *b = t;
+        }
+    __syncthreads();
+    const double pv = band[ro * W + bw];
+    for (int64_t t = 1 + threadIdx.x; t <= span; t += blockDim.x) {
+        double *m = band + (ro + t) * W + bw - t;  // a(ro+t, ro)
+        const double l = *m / pv;
+        *m = l;
+        Lc[ro * bw + t - 1] = l;
+    }
+}
+
+// a(ro+i, ro+j) -= l(i) * a(ro, ro+j), i in 1..span, j in 1..2bw: block y
+// takes row ro+1+y, its threads the columns.
+constexpr int kUpdThreads = 256;
+
+__global__ void __launch_bounds__(kUpdThreads) k_lup_update(int64_t N, int64_t bw, int64_t W,
+                                                            double *__restrict__ band, int64_t ro,
+                                                            const int *__restrict__ err)
+{
+    if (*((volatile const int *)err)) return;
     const int64_t i = (int64_t)blockIdx.y + 1;
-    if (i > span) return;
-    const float f = band[(ro + i) * W + bw - i];  // a(ro+i, ro)
-    if (f == 0.0f) return;
-    const float m = __fdiv_rn(f, piv);
-    const float *u = band + ro * W + bw;          // u[j] = a(ro, ro+j)
-    float *a = band + (ro + i) * W + (bw - i);    // a[j] = a(ro+i, ro+j)
-    const int64_t j0 = (int64_t)blockIdx.x * kRoundCols + 1;
-    const int64_t j1 = j0 + kRoundCols <= span + 1 ? j0 + kRoundCols : span + 1;
-#pragma unroll 4
-    for (int64_t j = j0 + threadIdx.x; j < j1; j += kRoundThreads) a[j] = __fsub_rn(a[j], __fmul_rn(m, u[j]));
+    const double l = band[(ro + i) * W + bw - i];
+    if (l == 0.0) return;
+    const int64_t cend = N - 1 - ro < 2 * bw ? N - 1 - ro : 2 * bw;
+    const double *u = band + ro * W + bw;          // u[j] = a(ro, ro+j)
+    double *a = band + (ro + i) * W + bw - i;      // a[j] = a(ro+i, ro+j)
+    for (int64_t j = 1 + (int64_t)blockIdx.x * kUpdThreads + threadIdx.x; j <= cend; j += (int64_t)gridDim.x * kUpdThreads)
+        a[j] = fma(-l, u[j], a[j]);
 }
 
-struct BarState {
-    unsigned count, gen;
-    int err, pad;
-};
-
-__device__ __forceinline__ bool grid_barrier(BarState *st, int *s_ok)
+// Solve with the factor (one block): y = b in FP64; per step ro the row
+// exchange and the Gauss transform y[ro+t] -= l(t) y[ro]; then x from U,
+// row by row from the last (each row a block-wide dot product over its at
+// most 2bw entries right of the diagonal); x demoted to FP32.
+__global__ void __launch_bounds__(kPivThreads) k_lup_solve(int64_t N, int64_t bw, int64_t W,
+                                                           const double *__restrict__ band,
+                                                           const double *__restrict__ Lc,
+                                                           const int32_t *__restrict__ piv, const float *__restrict__ b,
+                                                           double *__restrict__ y, float *__restrict__ x)
 {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned *vgen = &st->gen;
-        volatile int *verr = &st->err;
-        const unsigned g = *vgen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(&st->count, 1u) + 1u;
-        int ok = 1;
-        if (arrived == gridDim.x) {
-            atomicExch(&st->count, 0u);
-            __threadfence();
-            atomicAdd(&st->gen, 1u);
-        } else {
-            long long spins = 0;
-            while (*vgen == g) {
-                if (*verr || ++spins > kSpinLimit) {
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(32);
-            }
-        }
-        if (*verr) ok = 0;
-        if (!ok) atomicExch(&st->err, 1);
-        __threadfence();
-        *s_ok = ok;
-    }
-    __syncthreads();
-    return *s_ok != 0;
-}
-
-__device__ __forceinline__ float warp_sum(float v)
-{
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-struct SolveArgs {
-    int64_t N, bw, W;
-    const float *band;
-    const float *b;
-    float *x;
-    float *part;  // [2][kMaxCta][kTri]
-    BarState *st;
-};
-
-constexpr int64_t kMinCols = 64;  // columns per worker at least: few partials for CTA 0 to add
-
-// Columns that the workers sum for block kn (all rows of the band solved
-// before the block that precedes kn in the sweep) and their split.
-struct Split {
-    int64_t c0, c1, chunk, nact;
-};
-
-__device__ __forceinline__ Split worker_split(const SolveArgs &A, int64_t kn, bool fwd, int workers)
-{
-    const int64_t Rn = kn * kTri;
-    Split sp;
-    if (fwd) {
-        sp.c0 = Rn - A.bw > 0 ? Rn - A.bw : 0;
-        sp.c1 = Rn - kTri;
-    } else {
-        sp.c0 = Rn + 2 * kTri < A.N ? Rn + 2 * kTri : A.N;
-        sp.c1 = Rn + kTri + A.bw < A.N ? Rn + kTri + A.bw : A.N;
-    }
-    const int64_t len = sp.c1 > sp.c0 ? sp.c1 - sp.c0 : 0;
-    const int64_t even = cdiv(len, workers);
-    sp.chunk = even > kMinCols ? even : kMinCols;
-    sp.nact = cdiv(len, sp.chunk);
-    return sp;
-}
-
-// Partial sums of block rows [R, R+nb) over columns [c0, c1) (this worker's
-// slice), each row restricted to its band.
-__device__ __forceinline__ void block_partials(const SolveArgs &A, int64_t R, int nb, int64_t c0, int64_t c1,
-                                               bool forward, float *out)
-{
+    __shared__ double s_w[32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = warp; i < kTri; i += kSolveThreads / 32) {
-        float s = 0.0f;
-        if (i < nb) {
-            const int64_t r = R + i;
-            const int64_t lo = forward ? (c0 > r - A.bw ? c0 : r - A.bw) : c0;
-            const int64_t hi = forward ? c1 : (c1 < r + A.bw + 1 ? c1 : r + A.bw + 1);
-            const float *row = A.band + r * A.W + A.bw - r;
-            for (int64_t c = lo + lane; c < hi; c += 32) s += __ldg(row + c) * __ldcg(A.x + c);
+    for (int64_t r = threadIdx.x; r < N; r += blockDim.x) y[r] = (double)b[r];
+    __syncthreads();
+    for (int64_t ro = 0; ro < N; ++ro) {
+        const int64_t p = piv[ro];
+        if (p != ro && threadIdx.x == 0) {
+            const double t = y[ro];
+            y[ro] = y[p];
+            y[p] = t;
         }
-        s = warp_sum(s);
-        if (lane == 0) out[i] = s;
+        __syncthreads();
+        const double yr = y[ro];
+        const int64_t span = N - 1 - ro < bw ? N - 1 - ro : bw;
+        if (yr != 0.0)
+            for (int64_t t = 1 + threadIdx.x; t <= span; t += blockDim.x) y[ro + t] = fma(-Lc[ro * bw + t - 1], yr, y[ro + t]);
+        __syncthreads();
     }
+    // back substitution: y[r] becomes x[r]
+    for (int64_t r = N - 1; r >= 0; --r) {
+        const int64_t cend = N - 1 - r < 2 * bw ? N - 1 - r : 2 * bw;
+        const double *u = band + r * W + bw;  // u[j] = U(r, r+j)
+        double s = 0.0;
+        for (int64_t j = 1 + threadIdx.x; j <= cend; j += blockDim.x) s = fma(u[j], y[r + j], s);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) s_w[warp] = s;
+        __syncthreads();
+        if (warp == 0) {
+            s = lane < (int)(blockDim.x >> 5) ? s_w[lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) y[r] = (y[r] - s) / u[0];
+        }
+        __syncthreads();
+    }
+    for (int64_t r = threadIdx.x; r < N; r += blockDim.x) x[r] = (float)y[r];
 }
 
-__global__ void __launch_bounds__(kSolveThreads) k_band_solve(SolveArgs A)
-{
-    __shared__ float s_tri[kTri][kTri + 1];
-    __shared__ float s_sum[kTri];
-    __shared__ int s_ok;
-    const int64_t N = A.N, bw = A.bw, W = A.W;
-    const int64_t nblk = cdiv(N, kTri);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int workers = (int)gridDim.x - 1;
-    for (int sweep = 0; sweep < 2; ++sweep) {
-        const bool fwd = sweep == 0;
-        for (int64_t it = 0; it < nblk; ++it) {
-            const int64_t k = fwd ? it : nblk - 1 - it;
-            const int64_t R = k * kTri;
-            const int nb = (int)(N - R < kTri ? N - R : kTri);
-            const int buf = (int)(it & 1);
-            if (blockIdx.x > 0) {
-                // partial sums of the next block over the blocks solved before this one
-                const int64_t w = blockIdx.x - 1;
-                if (it + 1 < nblk) {
-                    const int64_t kn = fwd ? k + 1 : k - 1, Rn = kn * kTri;
-                    const Split sp = worker_split(A, kn, fwd, workers);
-                    if (w < sp.nact) {
-                        const int64_t a0 = sp.c0 + w * sp.chunk, a1 = a0 + sp.chunk < sp.c1 ? a0 + sp.chunk : sp.c1;
-                        block_partials(A, Rn, (int)(N - Rn < kTri ? N - Rn : kTri), a0, a1, fwd,
-                                       A.part + ((size_t)(buf ^ 1) * kMaxCta + blockIdx.x) * kTri);
-                    }
-                }
-            } else {
-                // block k: the workers' sums, the block solved last, the triangle
-                const bool has_prev = it > 0;
-                const int64_t nact = has_prev ? worker_split(A, k, fwd, workers).nact : 0;
-                const int64_t Rp = (fwd ? k - 1 : k + 1) * kTri;
-                float acc[kTri / (kSolveThreads / 32)];
-#pragma unroll
-                for (int q = 0; q < kTri / (kSolveThreads / 32); ++q) {
-                    const int i = warp + q * (kSolveThreads / 32);
-                    float s = 0.0f;
-                    if (i < nb && has_prev) {
-                        const float *pp = A.part + (size_t)buf * kMaxCta * kTri + i;
-                        if (lane < nact) s += __ldcg(pp + (size_t)(1 + lane) * kTri);
-                        for (int64_t g = 33 + lane; g <= nact; g += 32) s += __ldcg(pp + (size_t)g * kTri);
-                        const int64_t r = R + i, c = Rp + lane;
-                        const bool in = fwd ? (c >= r - bw) : (c < N && c <= r + bw);
-                        if (in) s += __ldg(A.band + r * W + (c - r + bw)) * __ldcg(A.x + c);
-                    }
-                    acc[q] = s;
-                }
-#pragma unroll
-                for (int q = 0; q < kTri / (kSolveThreads / 32); ++q) {
-                    const float s = warp_sum(acc[q]);
-                    if (lane == 0) s_sum[warp + q * (kSolveThreads / 32)] = s;
-                }
-                for (int t = threadIdx.x; t < kTri * kTri; t += kSolveThreads) {
-                    const int i = t / kTri, j = t % kTri;
-                    const bool in = i < nb && j < nb && (fwd ? (j < i && i - j <= bw) : (j >= i && j - i <= bw));
-                    s_tri[i][j] = in ? __ldg(A.band + (R + i) * W + (j - i + bw)) : 0.0f;
-                }
-                __syncthreads();
-                if (warp == 0) {
-                    float v = lane < nb ? (fwd ? __ldg(A.b + R + lane) : __ldcg(A.x + R + lane)) - s_sum[lane] : 0.0f;
-                    if (fwd) {
-                        for (int j = 0; j < nb; ++j) {
-                            const float xj = __shfl_sync(0xffffffffu, v, j);
-                            if (lane > j) v -= s_tri[lane][j] * xj;
-                        }
-                    } else {
-                        for (int j = nb - 1; j >= 0; --j) {
-                            if (lane == j) v = v / s_tri[j][j];
-                            const float xj = __shfl_sync(0xffffffffu, v, j);
-                            if (lane < j) v -= s_tri[lane][j] * xj;
-                        }
-                    }
-                    if (lane < nb) __stcg(A.x + R + lane, v);
-                }
-            }
-            if (!grid_barrier(A.st, &s_ok)) return;
-        }
-    }
-}
+// Device layout of the factor buffer: band double[N][3bw+1], Lc double[N][bw],
+// y double[N] (the solve's workspace), piv int32[N], err int[2].
+struct LupLayout {
+    int64_t W;
+    size_t band, lc, y, piv, err, total;  // byte offsets
+};
 
-int band_layout(int64_t N, int64_t bw, int64_t *W, size_t *band_floats)
+int lup_layout(int64_t N, int64_t bw, LupLayout *L)
 {
     if (N < 1 || bw < 1) return PIRO_ERR_ARG;
-    if (bw > N - 1) bw = N - 1 > 0 ? N - 1 : 1;
-    *W = 2 * bw + 1;
-    *band_floats = (size_t)N * (size_t)(*W);
+    L->W = 3 * bw + 1;
+    auto up = [](size_t v) { return (v + 255) / 256 * 256; };
+    L->band = 0;
+    L->lc = up(sizeof(double) * (size_t)N * (size_t)L->W);
+    L->y = L->lc + up(sizeof(double) * (size_t)N * (size_t)bw);
+    L->piv = L->y + up(sizeof(double) * (size_t)N);
+    L->err = L->piv + up(sizeof(int32_t) * (size_t)N);
+    L->total = L->err + 256;
     return PIRO_OK;
 }
-
-constexpr size_t kScratchBytes = sizeof(float) * 2 * kMaxCta * kTri + 256;  // partial sums, barrier state
-
-size_t scratch_offset(size_t band_floats) { return (sizeof(float) * band_floats + 255) / 256 * 256; }
 
 }  // namespace
 }  // namespace piro
@@ -578,31 +518,35 @@ extern "C" int piro_ht_lu_reference(int64_t N, int64_t *keys, float *vals, int64
 
 extern "C" int piro_ht_lu_band_bytes(int64_t N, int64_t bw, size_t *bytes)
 {
-    int64_t W;
-    size_t nf;
-    PIRO_ARG(bytes && band_layout(N, bw, &W, &nf) == PIRO_OK, "piro_ht_lu_band_bytes: bad arguments");
-    *bytes = scratch_offset(nf) + kScratchBytes;
+    LupLayout L;
+    PIRO_ARG(bytes && N >= 1 && bw >= 1 && bw <= N && lup_layout(N, bw, &L) == PIRO_OK,
+             "piro_ht_lu_band_bytes: bad arguments");
+    *bytes = L.total;
     return PIRO_OK;
 }
 
 extern "C" int piro_ht_lu_factor(int64_t N, int64_t bw, const int64_t *keys, const float *vals, int64_t ts,
                                  float shift, float scale, void *band, size_t band_bytes, piro_stream_t stream)
 {
-    int64_t W;
-    size_t nf;
-    PIRO_ARG(keys && vals && ts > 0 && band && band_layout(N, bw, &W, &nf) == PIRO_OK && N < ((int64_t)1 << 31),
+    LupLayout L;
+    PIRO_ARG(keys && vals && ts > 0 && band && N >= 1 && bw >= 1 && bw <= N && N < ((int64_t)1 << 31) &&
+                 lup_layout(N, bw, &L) == PIRO_OK,
              "piro_ht_lu_factor: bad arguments");
-    PIRO_ARG(band_bytes >= scratch_offset(nf) + kScratchBytes, "piro_ht_lu_factor: band buffer too small");
-    PIRO_ARG((W - 1) / 2 <= 65535, "piro_ht_lu_factor: bandwidth above 65535");
-    bw = (W - 1) / 2;
+    PIRO_ARG(band_bytes >= L.total, "piro_ht_lu_factor: band buffer too small (piro_ht_lu_band_bytes)");
+    PIRO_ARG(bw <= 65535, "piro_ht_lu_factor: bandwidth above 65535");
     cudaStream_t st = as_stream(stream);
-    float *AB = static_cast<float *>(band);
-    int *err = reinterpret_cast<int *>(static_cast<char *>(band) + scratch_offset(nf));
-    PIRO_CUDA(cudaMemsetAsync(AB, 0, sizeof(float) * nf, st));
+    char *base = static_cast<char *>(band);
+    double *AB = reinterpret_cast<double *>(base + L.band);
+    double *Lc = reinterpret_cast<double *>(base + L.lc);
+    int32_t *piv = reinterpret_cast<int32_t *>(base + L.piv);
+    int *err = reinterpret_cast<int *>(base + L.err);
+    const int64_t W = L.W;
+    PIRO_CUDA(cudaMemsetAsync(AB, 0, sizeof(double) * (size_t)N * (size_t)W, st));
     PIRO_CUDA(cudaMemsetAsync(err, 0, 2 * sizeof(int), st));
-    k_band_diag<<<grid_for(N, 256, 8), 256, 0, st>>>(N, W, bw, shift, AB);
-    k_band_scatter<<<grid_for(ts, 256, 8), 256, 0, st>>>(N, bw, W, keys, vals, ts, shift, scale, AB, err);
-    PIRO_CHECK_LAUNCH("k_band_scatter");
+    k_lup_diag<<<grid_for(N, 256, 8), 256, 0, st>>>(N, W, bw, (double)shift, AB);
+    k_lup_scatter<<<grid_for(ts, 256, 8), 256, 0, st>>>(N, bw, W, keys, vals, ts, (double)shift, (double)scale, AB,
+                                                        err);
+    PIRO_CHECK_LAUNCH("k_lup_scatter");
     int herr[2] = {0, 0};
     PIRO_CUDA(cudaMemcpyAsync(herr, err, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     PIRO_CUDA(cudaStreamSynchronize(st));
@@ -611,15 +555,19 @@ extern "C" int piro_ht_lu_factor(int64_t N, int64_t bw, const int64_t *keys, con
         return PIRO_ERR_ARG;
     }
     for (int64_t ro = 0; ro < N; ++ro) {
+        k_lup_pivot<<<1, kPivThreads, 0, st>>>(N, bw, W, AB, Lc, piv, ro, err);
         const int64_t span = N - 1 - ro < bw ? N - 1 - ro : bw;
-        const dim3 grid((unsigned)(span > 0 ? cdiv(span, kRoundCols) : 1), (unsigned)(span > 0 ? span : 1));
-        k_band_round<<<grid, kRoundThreads, 0, st>>>(N, bw, W, AB, ro, err);
+        const int64_t cend = N - 1 - ro < 2 * bw ? N - 1 - ro : 2 * bw;
+        if (span > 0 && cend > 0) {
+            const dim3 grid((unsigned)cdiv(cend, kUpdThreads), (unsigned)span);
+            k_lup_update<<<grid, kUpdThreads, 0, st>>>(N, bw, W, AB, ro, err);
+        }
     }
-    PIRO_CHECK_LAUNCH("k_band_round");
+    PIRO_CHECK_LAUNCH("k_lup_update");
     PIRO_CUDA(cudaMemcpyAsync(herr, err, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     PIRO_CUDA(cudaStreamSynchronize(st));
     if (herr[0] == 3) {
-        set_error("piro_ht_lu_factor: zero pivot at row %d (elimination without pivoting)", herr[1]);
+        set_error("piro_ht_lu_factor: singular matrix: column %d has no nonzero at or below the diagonal", herr[1]);
         return PIRO_ERR_ZERO_PIVOT;
     }
     return PIRO_OK;
@@ -628,49 +576,27 @@ extern "C" int piro_ht_lu_factor(int64_t N, int64_t bw, const int64_t *keys, con
 extern "C" int piro_ht_lu_solve(int64_t N, int64_t bw, void *band, size_t band_bytes, const float *b, float *x,
                                 piro_stream_t stream)
 {
-    int64_t W;
-    size_t nf;
-    PIRO_ARG(band && b && x && b != x && band_layout(N, bw, &W, &nf) == PIRO_OK, "piro_ht_lu_solve: bad arguments");
-    PIRO_ARG(band_bytes >= scratch_offset(nf) + kScratchBytes, "piro_ht_lu_solve: band buffer too small");
+    LupLayout L;
+    PIRO_ARG(band && b && x && N >= 1 && bw >= 1 && bw <= N && lup_layout(N, bw, &L) == PIRO_OK,
+             "piro_ht_lu_solve: bad arguments");
+    PIRO_ARG(band_bytes >= L.total, "piro_ht_lu_solve: band buffer too small (piro_ht_lu_band_bytes)");
     cudaStream_t st = as_stream(stream);
-    static int grid[kMaxDevices] = {0};
-    static DeviceOnce once;
-    int dev = 0;
-    PIRO_CUDA(cudaGetDevice(&dev));
-    const int rc = device_once(once, dev, [dev]() -> int {
-        int per_sm = 0;
-        PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_band_solve, kSolveThreads, 0));
-        const int g = sm_count();  // at most one CTA per SM
-        if (per_sm < 1) {
-            set_error("piro_ht_lu_solve: the solve kernel cannot be resident");
-            return PIRO_ERR_CUDA;
-        }
-        grid[dev] = g < 2 ? 2 : (g > kMaxCta ? kMaxCta : g);
-        return PIRO_OK;
-    });
-    if (rc != PIRO_OK) return rc;
-    char *scratch = static_cast<char *>(band) + scratch_offset(nf);
-    SolveArgs A;
-    A.N = N;
-    A.bw = (W - 1) / 2;
-    A.W = W;
-    A.band = static_cast<const float *>(band);
-    A.b = b;
-    A.x = x;
-    A.part = reinterpret_cast<float *>(scratch + 256);
-    A.st = reinterpret_cast<BarState *>(scratch + 64);
-    PIRO_CUDA(cudaMemsetAsync(A.st, 0, sizeof(BarState), st));
-    void *args[] = {&A};
-    // CTA 0 and enough workers for kMinCols columns each
-    int64_t g = 1 + cdiv(A.bw, kMinCols);
-    g = g < 2 ? 2 : (g > grid[dev] ? grid[dev] : g);
-    PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_band_solve, dim3((unsigned)g), dim3(kSolveThreads), args, 0, st));
-    BarState h;
-    PIRO_CUDA(cudaMemcpyAsync(&h, A.st, sizeof(BarState), cudaMemcpyDeviceToHost, st));
-    PIRO_CUDA(cudaStreamSynchronize(st));
-    if (h.err) {
-        set_error("piro_ht_lu_solve: grid barrier timed out");
-        return PIRO_ERR_CUDA;
-    }
+    char *base = static_cast<char *>(band);
+    k_lup_solve<<<1, kPivThreads, 0, st>>>(N, bw, L.W, reinterpret_cast<const double *>(base + L.band),
+                                          reinterpret_cast<const double *>(base + L.lc),
+                                          reinterpret_cast<const int32_t *>(base + L.piv), b,
+                                          reinterpret_cast<double *>(base + L.y), x);
+    PIRO_CHECK_LAUNCH("k_lup_solve");
+    return PIRO_OK;
+}
+
+extern "C" int piro_ht_lu_pivots(int64_t N, int64_t bw, const void *band, size_t band_bytes, int32_t *piv_host)
+{
+    LupLayout L;
+    PIRO_ARG(band && piv_host && N >= 1 && bw >= 1 && bw <= N && lup_layout(N, bw, &L) == PIRO_OK &&
+                 band_bytes >= L.total,
+             "piro_ht_lu_pivots: bad arguments");
+    PIRO_CUDA(cudaMemcpy(piv_host, static_cast<const char *>(band) + L.piv, sizeof(int32_t) * (size_t)N,
+                         cudaMemcpyDeviceToHost));
     return PIRO_OK;
 }

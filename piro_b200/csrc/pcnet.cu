@@ -24,7 +24,11 @@
 // masked MSE loss against a target error, backward through the four layers
 // (data gradient = the transposed convolution times GELU'; weight gradient =
 // per-block partial correlations reduced in a fixed order, so gradients are
-// deterministic), and Adam.
+// deterministic), and Adam.  With the tensor-core engine (the default) every
+// convolution of training runs on tcgen05: the forward and the data gradient
+// as the implicit GEMM of conv_tc.cuh (the data gradient with the weights
+// transposed and the taps reversed), the weight gradient as the GEMM over
+// cells of wgrad_tc.cuh.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -35,6 +39,7 @@
 
 #include "common.cuh"
 #include "conv_tc.cuh"
+#include "wgrad_tc.cuh"
 
 namespace piro {
 namespace {
@@ -454,6 +459,36 @@ __global__ void k_pack_wtc(const float *__restrict__ wq, Layout L, bf16 *__restr
     }
 }
 
+// The data gradient of layer l as a forward convolution: input channels =
+// the layer's outputs, output channels = its inputs, tap t reading the
+// gradient at c + off(t) with the weights of tap 26 - t (off(26 - t) =
+// -off(t)).  Per layer l = 1..3 and tap: [channel group 2][out 16][8 in] BF16,
+// channels beyond the layer's zero.
+__global__ void k_pack_wtc_t(const float *__restrict__ wq, Layout L, bf16 *__restrict__ wpk_t)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (kLayers - 1) * kTaps * 256; i += gridDim.x * blockDim.x) {
+        const int l = 1 + i / (kTaps * 256), rem = i % (kTaps * 256);
+        const int tap = rem / 256, r2 = rem % 256;
+        const int gin = (r2 / 128) * 8 + (r2 % 8), gout = (r2 / 8) % 16;  // gin: the layer's co, gout: its ci
+        const int CI = l == 0 ? 2 : 16, CO = l == kLayers - 1 ? 1 : 16;
+        const float v = (gin < CO && gout < CI) ? wq[L.w[l] + ((kTaps - 1 - tap) * CI + gout) * CO + gin] : 0.0f;
+        wpk_t[i] = __float2bfloat16_rn(v);
+    }
+}
+
+// The loss gradient (FP32, one channel) as a 16-channel BF16 array: channel 0
+// = bf16(gout), the rest 0 -- the input of the last layer's data gradient and
+// weight gradient on the tensor cores.
+__global__ void k_pack_grad16(int64_t n, const float *__restrict__ gout, bf16 *__restrict__ g16)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(gout[i], 0.0f);
+        uint4 *dst = reinterpret_cast<uint4 *>(g16 + i * 16);
+        dst[0] = make_uint4(*reinterpret_cast<const uint32_t *>(&h), 0, 0, 0);
+        dst[1] = make_uint4(0, 0, 0, 0);
+    }
+}
+
 // Tensor-core input: x16[b][c] = (r s_b, r s_b f, 0 x 14) on interior cells,
 // zeros elsewhere (32 bytes per cell, the layout of the hidden activations).
 __global__ void k_pack_input16(GridDiv g, int64_t N, const float *__restrict__ r, const float *__restrict__ feat,
@@ -508,6 +543,7 @@ struct piro_pcnet {
     Layout L;
     float *w = nullptr, *wq = nullptr, *m = nullptr, *v = nullptr, *g = nullptr;
     bf16 *wpk = nullptr;  // BF16 tensor-core operands of the four layers
+    bf16 *wpk_t = nullptr;  // the same, transposed and tap-reversed, of layers 2-4 (data gradients)
     int *d_err = nullptr; // raised by a tensor-core launch whose bounded wait ran out
     int engine = PIRO_PCNET_TENSOR_CORES;
     float *partials = nullptr;
@@ -517,6 +553,7 @@ struct piro_pcnet {
     int64_t cap = 0;
     bf16 *x0 = nullptr, *y[3] = {nullptr, nullptr, nullptr}, *a[3] = {nullptr, nullptr, nullptr};
     bf16 *g16[2] = {nullptr, nullptr};
+    bf16 *x16 = nullptr, *go16 = nullptr;  // tensor-core training: 16-channel input and loss gradient
     float *out = nullptr, *gout = nullptr;
     long long launches = 0;
 };
@@ -530,11 +567,14 @@ static void net_free_ws(piro_pcnet *n)
     }
     cudaFree(n->g16[0]);
     cudaFree(n->g16[1]);
+    cudaFree(n->x16);
+    cudaFree(n->go16);
     cudaFree(n->out);
     cudaFree(n->gout);
     n->x0 = nullptr;
     for (int i = 0; i < 3; ++i) n->y[i] = n->a[i] = nullptr;
     n->g16[0] = n->g16[1] = nullptr;
+    n->x16 = n->go16 = nullptr;
     n->out = n->gout = nullptr;
     n->cap = 0;
 }
@@ -551,6 +591,12 @@ static int net_reserve(piro_pcnet *n, int64_t cells, bool training)
         for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaMalloc(&n->y[i], c * 16 * sizeof(bf16));
         for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMalloc(&n->g16[i], c * 16 * sizeof(bf16));
         if (e == cudaSuccess) e = cudaMalloc(&n->gout, c * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&n->x16, c * 16 * sizeof(bf16));
+        if (e == cudaSuccess) e = cudaMalloc(&n->go16, c * 16 * sizeof(bf16));
+        // the tensor-core layers never write the boundary planes of their outputs
+        for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaMemset(n->y[i], 0, c * 16 * sizeof(bf16));
+        for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMemset(n->g16[i], 0, c * 16 * sizeof(bf16));
+        if (e == cudaSuccess) e = cudaMemset(n->out, 0, c * sizeof(float));
     }
     for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaMemset(n->a[i], 0, c * 16 * sizeof(bf16));
     if (e != cudaSuccess) {
@@ -622,23 +668,27 @@ static Acts infer_acts(void *work, int64_t cells)
 
 // TMA descriptor of an activation array of `rows` cells (16 BF16 channels
 // each) as the 3-D view (8 channels, rows at 32 bytes, 2 groups at 16 bytes)
-// with box {8, 130, 2}: the line blocks of conv_tc.cuh.
-static int encode_rows_map(CUtensorMap *m, const void *base, int64_t rows)
+// with box {8, box_rows, 2}: the line blocks of conv_tc.cuh (130 rows) or the
+// tiles of wgrad_tc.cuh (128 rows).
+static int encode_rows_map(CUtensorMap *m, const void *base, int64_t rows, int box_rows)
 {
+    // the driver entry point, resolved once for all host threads
+    static std::once_flag resolved;
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
+    std::call_once(resolved, []() {
         void *fn = nullptr;
         cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess || !fn) {
-            set_error("cuTensorMapEncodeTiled is not available");
-            return PIRO_ERR_CUDA;
-        }
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess && fn)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    if (!encode) {
+        set_error("cuTensorMapEncodeTiled is not available");
+        return PIRO_ERR_CUDA;
     }
     const cuuint64_t dims[3] = {8, (cuuint64_t)rows, 2};
     const cuuint64_t strides[2] = {32, 16};
-    const cuuint32_t box[3] = {8, (cuuint32_t)tc::kLineRows, 2};
+    const cuuint32_t box[3] = {8, (cuuint32_t)box_rows, 2};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUresult r = encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void *>(base), dims, strides, box,
                               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -656,7 +706,8 @@ static int encode_rows_map(CUtensorMap *m, const void *base, int64_t rows)
 // z = 0 and nz - 1 are not written (they must already be zero).
 template <int kEpi>
 static int conv_tc(const bf16 *in, bf16 *out, float *zout, const bf16 *wpk, const GridDiv &g, int64_t N, int batch,
-                   const double *rr, double n_int, const int *skip, int *err, cudaStream_t st)
+                   const double *rr, double n_int, const int *skip, int *err, cudaStream_t st,
+                   bf16 *yout = nullptr, const bf16 *yprev = nullptr)
 {
     static DeviceOnce once;
     int dev = 0;
@@ -668,14 +719,14 @@ static int conv_tc(const bf16 *in, bf16 *out, float *zout, const bf16 *wpk, cons
     });
     if (rc != PIRO_OK) return rc;
     CUtensorMap map;
-    rc = encode_rows_map(&map, in, N * batch);
+    rc = encode_rows_map(&map, in, N * batch, tc::kLineRows);
     if (rc) return rc;
     const int64_t nxy = (int64_t)g.nx * g.ny;
     const int ncol = (int)cdiv(nxy, tc::kRows);
     const int planes = g.nz - 2;
     const int zchunk = planes < kTcZChunk ? planes : kTcZChunk;
     const int nzc = (int)cdiv(planes, zchunk);
-    tc::Args a{g, N, nxy, ncol, zchunk, wpk, out, zout, rr, n_int, skip, err};
+    tc::Args a{g, N, nxy, ncol, zchunk, wpk, out, zout, rr, n_int, skip, err, yout, yprev};
     tc::k_conv16_tc<kEpi><<<dim3((unsigned)(ncol * nzc), (unsigned)batch), tc::kThreads, tc::kSmemBytes, st>>>(map, a);
     PIRO_CHECK_LAUNCH("k_conv16_tc");
     return PIRO_OK;
@@ -703,6 +754,42 @@ static int net_pack(piro_pcnet *n, cudaStream_t st)
 {
     k_pack_wtc<<<cdiv(kLayers * kTaps * 256, 256), 256, 0, st>>>(n->wq, n->L, n->wpk);
     PIRO_CHECK_LAUNCH("k_pack_wtc");
+    k_pack_wtc_t<<<cdiv((kLayers - 1) * kTaps * 256, 256), 256, 0, st>>>(n->wq, n->L, n->wpk_t);
+    PIRO_CHECK_LAUNCH("k_pack_wtc_t");
+    return PIRO_OK;
+}
+
+// Weight gradient of one layer on the tensor cores (wgrad_tc.cuh): x and gy
+// are 16-channel BF16 arrays of `cells` rows; the layer's dW (CI x CO kept of
+// the 16 x 16 per tap) goes to grad_w through per-CTA partials reduced in a
+// fixed order.
+static int launch_wgrad_tc(piro_pcnet *n, const GridDiv &g, int64_t cells, const bf16 *x, const bf16 *gy, int CI,
+                           int CO, float *grad_w, cudaStream_t st)
+{
+    static DeviceOnce once;
+    int dev = 0;
+    PIRO_CUDA(cudaGetDevice(&dev));
+    int rc = device_once(once, dev, []() -> int {
+        PIRO_CUDA(cudaFuncSetAttribute(tc::k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       tc::kWgSmemBytes));
+        return PIRO_OK;
+    });
+    if (rc != PIRO_OK) return rc;
+    CUtensorMap xmap, gmap;
+    rc = encode_rows_map(&xmap, x, cells, tc::kWgRows);
+    if (!rc) rc = encode_rows_map(&gmap, gy, cells, tc::kWgRows);
+    if (rc) return rc;
+    const int64_t ntiles = cdiv(cells, tc::kWgRows);
+    int64_t grid = sm_count();
+    if (grid > kRedBlocks) grid = kRedBlocks;
+    if (grid > ntiles) grid = ntiles;
+    tc::WgArgs a{g.nx, (int64_t)g.nx * g.ny, ntiles, CI, CO, n->partials, n->d_err};
+    tc::k_wgrad_tc<<<(unsigned)grid, tc::kWgThreads, tc::kWgSmemBytes, st>>>(xmap, gmap, a);
+    PIRO_CHECK_LAUNCH("k_wgrad_tc");
+    const int P = kTaps * CI * CO;
+    k_reduce_partials<<<(P + 255) / 256, 256, 0, st>>>(n->partials, (int)grid, P, grad_w);
+    PIRO_CHECK_LAUNCH("k_reduce_partials");
+    n->launches += 2;
     return PIRO_OK;
 }
 
@@ -752,6 +839,7 @@ extern "C" int piro_pcnet_create(uint64_t seed, piro_pcnet **out)
     if (e == cudaSuccess) e = cudaMalloc(&n->partials, (size_t)pmax * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&n->red, (kRedBlocks + 8) * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&n->wpk, sizeof(bf16) * kLayers * kTaps * 256);
+    if (e == cudaSuccess) e = cudaMalloc(&n->wpk_t, sizeof(bf16) * (kLayers - 1) * kTaps * 256);
     if (e == cudaSuccess) e = cudaMalloc(&n->d_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(n->d_err, 0, sizeof(int));
     if (e != cudaSuccess) {
@@ -897,9 +985,26 @@ extern "C" int piro_pcnet_loss_grad(piro_pcnet *n, int batch, int nx, int ny, in
     const Layout &L = n->L;
     const GridDiv g(nx, ny, nz);
     const int64_t cells = N * batch;
-    k_pack_input<<<dim3(net_grid(N, 256), batch), 256, 0, st>>>(g, N, r, feat, nullptr, 1.0, n->x0, nullptr);
-    PIRO_CHECK_LAUNCH("k_pack_input");
-    rc = net_forward(n->wq, train_acts(n), batch, g, N, true, n->out, nullptr, 1.0, nullptr, st);
+    const bool tcore = n->engine == PIRO_PCNET_TENSOR_CORES;
+    const int64_t W = (int64_t)kTaps * 256;
+    if (tcore) {
+        // forward on the tensor cores, keeping each hidden layer's y and a
+        k_pack_input16<<<dim3(net_grid(N, 256), batch), 256, 0, st>>>(g, N, r, feat, nullptr, 1.0, n->x16, nullptr);
+        PIRO_CHECK_LAUNCH("k_pack_input16");
+        rc = conv_tc<2>(n->x16, n->a[0], nullptr, n->wpk, g, N, batch, nullptr, 0.0, nullptr, n->d_err, st, n->y[0]);
+        if (!rc)
+            rc = conv_tc<2>(n->a[0], n->a[1], nullptr, n->wpk + W, g, N, batch, nullptr, 0.0, nullptr, n->d_err, st,
+                            n->y[1]);
+        if (!rc)
+            rc = conv_tc<2>(n->a[1], n->a[2], nullptr, n->wpk + 2 * W, g, N, batch, nullptr, 0.0, nullptr, n->d_err,
+                            st, n->y[2]);
+        if (!rc)
+            rc = conv_tc<1>(n->a[2], nullptr, n->out, n->wpk + 3 * W, g, N, batch, nullptr, 0.0, nullptr, n->d_err, st);
+    } else {
+        k_pack_input<<<dim3(net_grid(N, 256), batch), 256, 0, st>>>(g, N, r, feat, nullptr, 1.0, n->x0, nullptr);
+        PIRO_CHECK_LAUNCH("k_pack_input");
+        rc = net_forward(n->wq, train_acts(n), batch, g, N, true, n->out, nullptr, 1.0, nullptr, st);
+    }
     n->launches += 5;
     if (rc) return rc;
     k_mask_sum<<<kRedBlocks, 256, 0, st>>>(cells, mask, n->red);
@@ -908,6 +1013,36 @@ extern "C" int piro_pcnet_loss_grad(piro_pcnet *n, int batch, int nx, int ny, in
     k_finish_sum<<<1, 32, 0, st>>>(n->red, 1);
     PIRO_CHECK_LAUNCH("k_loss");
     const dim3 grid(net_grid(N, 128), batch);
+    if (tcore) {
+        // backward on the tensor cores: per layer the weight gradient (GEMM over
+        // the cells), then the data gradient into the previous layer's
+        // pre-activation (transposed, tap-reversed convolution times GELU')
+        k_pack_grad16<<<net_grid(cells, 256), 256, 0, st>>>(cells, n->gout, n->go16);
+        PIRO_CHECK_LAUNCH("k_pack_grad16");
+        rc = launch_wgrad_tc(n, g, cells, n->a[2], n->go16, 16, 1, n->g + L.w[3], st);
+        if (!rc)
+            rc = conv_tc<3>(n->go16, n->g16[0], nullptr, n->wpk_t + 2 * W, g, N, batch, nullptr, 0.0, nullptr,
+                            n->d_err, st, nullptr, n->y[2]);
+        if (!rc) rc = launch_wgrad_tc(n, g, cells, n->a[1], n->g16[0], 16, 16, n->g + L.w[2], st);
+        if (!rc)
+            rc = conv_tc<3>(n->g16[0], n->g16[1], nullptr, n->wpk_t + W, g, N, batch, nullptr, 0.0, nullptr, n->d_err,
+                            st, nullptr, n->y[1]);
+        if (!rc) rc = launch_wgrad_tc(n, g, cells, n->a[0], n->g16[1], 16, 16, n->g + L.w[1], st);
+        if (!rc)
+            rc = conv_tc<3>(n->g16[1], n->g16[0], nullptr, n->wpk_t, g, N, batch, nullptr, 0.0, nullptr, n->d_err, st,
+                            nullptr, n->y[0]);
+        if (!rc) rc = launch_wgrad_tc(n, g, cells, n->x16, n->g16[0], 2, 16, n->g + L.w[0], st);
+        if (rc) return rc;
+        n->launches += 4;
+        if (loss) {
+            PIRO_CUDA(cudaMemcpyAsync(loss, n->red + kRedBlocks + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+        }
+        if (grad) {
+            PIRO_CUDA(cudaMemcpyAsync(grad, n->g, (size_t)L.total * sizeof(float), cudaMemcpyDeviceToHost, st));
+        }
+        if (loss || grad) return pcnet_take_error(n, st);  // synchronises the stream
+        return PIRO_OK;
+    }
     // layer 4 (16 -> 1): weight gradient, then the data gradient into layer 3's output
     rc = launch_bwd_w<16, 1, float>(n, g, N, batch, n->a[2], n->gout, n->g + L.w[3], st);
     if (rc) return rc;
@@ -966,6 +1101,7 @@ extern "C" int piro_pcnet_destroy(piro_pcnet *n)
     cudaFree(n->partials);
     cudaFree(n->red);
     cudaFree(n->wpk);
+    cudaFree(n->wpk_t);
     cudaFree(n->d_err);
     delete n;
     return PIRO_OK;

@@ -148,7 +148,8 @@ def dense_check():
 
 class HtLu:
     """Scheme 27 with a solution: shift*I + scale*M (M the table's matrix)
-    factorized in a dense band of bandwidth bw; solve(b) -> x."""
+    factorized in FP64 with partial pivoting in a band of bandwidth bw;
+    solve(b) -> x (FP64 solve, x rounded to FP32)."""
 
     def __init__(self, N, bw, keys, vals, ts, shift=1.0, scale=1.0):
         n = C.c_size_t()
@@ -164,6 +165,15 @@ class HtLu:
         check(lib().piro_ht_lu_solve(self.N, self.bw, _p(self.band), self.nbytes, _p(b), _p(x), _stream()),
               "piro_ht_lu_solve")
         return x
+
+    def pivots(self):
+        """Pivot row of each elimination step (0-based), as numpy int32."""
+        import numpy as np
+        torch.cuda.synchronize()
+        piv = np.empty(self.N, np.int32)
+        check(lib().piro_ht_lu_pivots(self.N, self.bw, _p(self.band), self.nbytes, piv.ctypes.data_as(C.c_void_p)),
+              "piro_ht_lu_pivots")
+        return piv
 
 
 # ----------------------------------------------------------------- steps
@@ -468,7 +478,7 @@ class PCNet:
         return (loss.value if want_loss else None), g
 
     def set_engine(self, tensor_cores: bool) -> None:
-        """Inference engine: tcgen05 tensor cores for the 16 -> 16 layers, or CUDA cores."""
+        """Engine of inference and training: tcgen05 tensor cores (the default) or CUDA cores."""
         check(lib().piro_pcnet_set_engine(self.h, 1 if tensor_cores else 0), "piro_pcnet_set_engine")
 
     def adam_step(self, lr: float) -> None:

@@ -53,11 +53,17 @@ def test_forward_matches_oracle(cuda, net, n, B):
     assert np.all(got[:, b] == 0.0)
 
 
-def test_gradient_matches_oracle(cuda, net):
+@pytest.mark.parametrize("tensor_cores", [True, False])
+@pytest.mark.parametrize("n,B", [((9, 8, 10), 2), ((20, 17, 13), 3)])
+def test_gradient_matches_oracle(cuda, net, tensor_cores, n, B):
+    """Loss and per-layer gradients of the device's training pass against the
+    oracle's analytic gradient, on the tensor cores (tcgen05 forward, data
+    gradient and weight gradient; the loss gradient enters the last layer in
+    BF16) and on the CUDA cores."""
     import torch
-    n, B = (9, 8, 10), 2
     p = P.init_params(5).astype(np.float32)
     net.set_params(p)
+    net.set_engine(tensor_cores)
     r, f, t, m = _inputs(2, n, B)
     T = lambda a: torch.from_numpy(a.reshape(-1)).cuda()  # noqa: E731
     loss, g = net.loss_grad(*n, T(r), T(f), T(t), T(m), batch=B, want_grad=True)
@@ -69,17 +75,45 @@ def test_gradient_matches_oracle(cuda, net):
         a, b = g[wo[l]:ends[l]].astype(np.float64), rg[wo[l]:ends[l]]
         rel = np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-30))
         assert rel < 2e-2, (l, rel)
+    net.set_engine(True)
 
 
-def test_gradient_is_deterministic(cuda, net):
+@pytest.mark.parametrize("tensor_cores", [True, False])
+def test_gradient_is_deterministic(cuda, net, tensor_cores):
     import torch
     n, B = (12, 11, 10), 3
     net.set_params(P.init_params(6).astype(np.float32))
+    net.set_engine(tensor_cores)
     r, f, t, m = _inputs(3, n, B)
     T = lambda a: torch.from_numpy(a.reshape(-1)).cuda()  # noqa: E731
     _, g1 = net.loss_grad(*n, T(r), T(f), T(t), T(m), batch=B, want_grad=True)
     _, g2 = net.loss_grad(*n, T(r), T(f), T(t), T(m), batch=B, want_grad=True)
     assert np.array_equal(g1, g2)
+    net.set_engine(True)
+
+
+def test_tensor_core_and_cuda_core_gradients_agree(cuda, net):
+    """The two training engines give the same gradient up to BF16 rounding of
+    intermediate values (the tensor cores sum in another order and take the
+    loss gradient in BF16)."""
+    import torch
+    n, B = (18, 14, 12), 2
+    net.set_params(P.init_params(8).astype(np.float32))
+    r, f, t, m = _inputs(6, n, B)
+    T = lambda a: torch.from_numpy(a.reshape(-1)).cuda()  # noqa: E731
+    out = []
+    for tc in (True, False):
+        net.set_engine(tc)
+        out.append(net.loss_grad(*n, T(r), T(f), T(t), T(m), batch=B, want_grad=True))
+    net.set_engine(True)
+    (l1, g1), (l2, g2) = out
+    assert abs(l1 - l2) <= 1e-3 * abs(l2)
+    wo, total = P.layout()
+    ends = wo[1:] + [total]
+    for l in range(4):
+        a, b = g1[wo[l]:ends[l]].astype(np.float64), g2[wo[l]:ends[l]].astype(np.float64)
+        rel = np.sqrt(((a - b) ** 2).sum() / max((b ** 2).sum(), 1e-30))
+        assert rel < 2e-2, (l, rel)
 
 
 def test_training_reduces_loss(cuda):
