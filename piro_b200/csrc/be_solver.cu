@@ -1057,6 +1057,146 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
     }
 }
 
+// The Jacobi iterations of a learned sweep in one cooperative launch: flexible
+// CG (the k_fcg_* iteration above) resumed from the state the network-
+// preconditioned iterations left -- r, the last direction p in p0 and its
+// q = A p, <p, S p> in st->pq, d, the sweep's rr0, tol2 and cap -- and run to
+// the sweep's inner tolerance with z = D^-1 r, two grid barriers per
+// iteration instead of three kernel launches:
+//   z = D^-1 r, beta = -<z, S p_old> / <p_old, S p_old> (0 on a sweep's first
+//   iteration); A: p = z + beta p_old, q = A p, <p, S p>, <p, s>; a =
+//   <p, s> / <p, S p>; B: d += a p, r -= a q, z = D^-1 r, |r|^2, <z, S p>.
+// Global arrays only (the state lives in them between launches); barrier
+// waits bounded like k_be_persistent's.
+struct FArgs {
+    GridDiv g;
+    int64_t N;
+    float mdt, vself, vnb;
+    const float *alpha, *dinv;
+    float *r, *z, *q, *d, *p0, *p1;
+    double *partials;
+    DevState *st;
+    long long spin_limit;
+};
+
+__global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(FArgs F)
+{
+    __shared__ double s_warp[32];
+    __shared__ double s_red[4 * 32];
+    __shared__ double s_b;
+    __shared__ double s_bn[4];
+    __shared__ int s_ok;
+    const GridDiv g = F.g;
+    const int64_t N = F.N, sxy = (int64_t)g.nx * g.ny;
+    const int64_t c_beg = (int64_t)blockIdx.x * kPT + threadIdx.x, c_step = (int64_t)gridDim.x * kPT;
+    DevState *st = F.st;
+    if (*((volatile int *)&st->done)) return;  // the same in every block: written before this launch
+    const int max_iters = st->max_iters;
+    const double tol2 = st->tol2, rr0 = st->rr0;
+    double t_pq = st->pq, t_rr = st->rr;
+    int iters = st->iters;
+    unsigned bar_target = 0;
+    auto inter = [&](int64_t i) {
+        int x, y, zc;
+        g.coords((uint32_t)i, x, y, zc);
+        return x > 0 && x < g.nx - 1 && y > 0 && y < g.ny - 1 && zc > 0 && zc < g.nz - 1;
+    };
+    // z = D^-1 r and <z, S p_old> with S p_old = q / alpha
+    double zq = 0.0;
+    for (int64_t i = c_beg; i < N; i += c_step) {
+        const float dv = __ldg(F.dinv + i);
+        const float zi = F.r[i] * dv;  // dinv = 0 on the boundary: z = 0 there
+        F.z[i] = zi;
+        if (dv != 0.0f) zq += (double)zi * (double)F.q[i] / (double)__ldg(F.alpha + i);
+    }
+    put_partial(F.partials, 0, zq, s_warp);
+    bool ok = grid_barrier(st, bar_target, F.spin_limit, &s_ok);
+    double beta = 0.0, a = 0.0;
+    bool broken = false;
+    if (ok) {
+        const double t_zq = all_sum(F.partials, 0, s_warp, &s_b);
+        beta = iters == 0 ? 0.0 : -t_zq / t_pq;
+        broken = !isfinite(beta);
+    }
+    float *pold = F.p0, *pnew = F.p1;
+    while (ok && !broken) {
+        // A: p = z + beta p_old, q = A p, <p, S p>, <p, s>
+        const float fb = (float)beta;
+        double pv[2] = {0.0, 0.0};
+        for (int64_t i = c_beg; i < N; i += c_step) {
+            if (!inter(i)) {
+                pnew[i] = 0.0f;
+                F.q[i] = 0.0f;
+                continue;
+            }
+            const float al = __ldg(F.alpha + i);
+            const float cur = ld_(F.z + i) + fb * ld_(pold + i);
+            const float xm = ld_(F.z + i - 1) + fb * ld_(pold + i - 1);
+            const float xp = ld_(F.z + i + 1) + fb * ld_(pold + i + 1);
+            const float ym = ld_(F.z + i - g.nx) + fb * ld_(pold + i - g.nx);
+            const float yp = ld_(F.z + i + g.nx) + fb * ld_(pold + i + g.nx);
+            const float zm = ld_(F.z + i - sxy) + fb * ld_(pold + i - sxy);
+            const float zp = ld_(F.z + i + sxy) + fb * ld_(pold + i + sxy);
+            const float cd = __fadd_rn(1.0f, __fmul_rn(F.mdt, __fmul_rn(al, F.vself)));
+            const float co = __fmul_rn(F.mdt, __fmul_rn(al, F.vnb));
+            const float qv = cd * cur + co * (((xm + xp) + (ym + yp)) + (zm + zp));
+            pnew[i] = cur;
+            F.q[i] = qv;
+            pv[0] += (double)cur * (double)qv / (double)al;
+            pv[1] += (double)cur * (double)F.r[i] / (double)al;
+        }
+        put_partials<2>(F.partials, 1, pv, s_red);
+        if (!(ok = grid_barrier(st, bar_target, F.spin_limit, &s_ok))) break;
+        double at[2];
+        all_sums<2>(F.partials, 1, at, s_red, s_bn);
+        t_pq = at[0];
+        a = at[1] / at[0];
+        if (!isfinite(a) || at[0] <= 0.0) {
+            broken = true;
+            break;
+        }
+        // B: d += a p, r -= a q, z = D^-1 r, |r|^2, <z, S p>
+        const float fa = (float)a;
+        double bv[2] = {0.0, 0.0};
+        for (int64_t i = c_beg; i < N; i += c_step) {
+            const float dv = __ldg(F.dinv + i);
+            if (dv == 0.0f) continue;
+            const float qi = F.q[i];
+            F.d[i] += fa * pnew[i];
+            const float ri = F.r[i] - fa * qi;
+            const float zi = ri * dv;
+            F.r[i] = ri;
+            F.z[i] = zi;
+            bv[0] += (double)ri * (double)ri;
+            bv[1] += (double)zi * (double)qi / (double)__ldg(F.alpha + i);
+        }
+        put_partials<2>(F.partials, 3, bv, s_red);
+        if (!(ok = grid_barrier(st, bar_target, F.spin_limit, &s_ok))) break;
+        double btot[2];
+        all_sums<2>(F.partials, 3, btot, s_red, s_bn);
+        t_rr = btot[0];
+        beta = -btot[1] / t_pq;
+        ++iters;
+        float *t = pold;
+        pold = pnew;
+        pnew = t;
+        if (!isfinite(t_rr) || !isfinite(beta)) {
+            broken = true;
+            break;
+        }
+        if (t_rr <= tol2 * rr0 || iters >= max_iters) break;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->iters = iters;
+        st->rr = t_rr;
+        st->pq = t_pq;
+        st->a = a;
+        st->beta = beta;
+        if (broken) st->broken = 1;
+        st->done = 1;
+    }
+}
+
 // Interior-boundary coupling of A: per row, the entries of interior rows whose
 // column is a boundary cell.  Count pass writes ib_ptr[r+1]; fill after scan.
 __global__ void k_ib_count(GridDiv g, int64_t N, const int32_t *__restrict__ rowptr, const int32_t *__restrict__ col,
@@ -1156,6 +1296,7 @@ struct piro_be_solver {
     int32_t *ib_ptr, *ib_col;
     float *ib_val;
     double *beff;
+    unsigned grid_fp;   // k_fcg_persistent: co-resident blocks (0: use the graph-launched chunks)
     int64_t res_cells;  // resident variant: cells per block, 0 if it does not fit
     size_t res_smem;
     cudaEvent_t pev0, pev1;
@@ -1357,6 +1498,10 @@ static int be_setup_persistent(piro_be_solver *s, bool allow_resident)
     if (grid > need) grid = need;
     s->grid_p = (unsigned)grid;
     s->persist = 1;
+    int per_sm_f = 0;
+    PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_fcg_persistent, kPT, 0));
+    const int64_t fgrid = (int64_t)nsm * per_sm_f;
+    s->grid_fp = (unsigned)(fgrid < grid ? fgrid : grid);
     // resident variant: every block's r, d, q in shared memory, if they fit
     // with the same grid still co-resident
     s->res_cells = 0;
@@ -1719,6 +1864,41 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
         while (true) {
             const bool with_net = net_iters;
             net_iters = false;
+            if (learned && !with_net && s->persist && s->grid_fp > 0) {
+                // the rest of the sweep: Jacobi flexible CG in one cooperative launch
+                FArgs F;
+                F.g = GridDiv(s->nx, s->ny, s->nz);
+                F.N = N;
+                F.mdt = s->mdt;
+                F.vself = s->vself;
+                F.vnb = s->vnb;
+                F.alpha = s->alpha;
+                F.dinv = s->dinv;
+                F.r = s->r;
+                F.z = s->z;
+                F.q = s->q;
+                F.d = s->d;
+                F.p0 = s->p[0];
+                F.p1 = s->p[1];
+                F.partials = s->partials;
+                F.st = s->st;
+                F.spin_limit = wait_limit(1ll << 22);
+                void *fargs[] = {&F};
+                PIRO_CUDA(cudaMemsetAsync(&s->st->bar_count, 0, 2 * sizeof(unsigned) + sizeof(int), st));
+                PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_fcg_persistent, dim3(s->grid_fp), dim3(kPT),
+                                                      fargs, 0, st));
+                s->kernel_launches += 1;
+                PIRO_CUDA(cudaMemcpyAsync(s->h_st, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, st));
+                PIRO_CUDA(cudaStreamSynchronize(st));
+                if (s->h_st->bar_err) {
+                    piro::set_error("piro_be_solve: grid barrier timed out");
+                    inf.status = PIRO_ERR_CUDA;
+                    if (info) *info = inf;
+                    return PIRO_ERR_CUDA;
+                }
+                seen = s->h_st->iters;
+                break;
+            }
             const int chunk = learned ? (with_net ? kLearnedIters : kChunkF) : kChunk;
             PIRO_CUDA(cudaGraphLaunch(learned ? (with_net ? s->exec_l : s->exec_f) : s->exec, st));
             s->kernel_launches += learned ? (with_net ? 9 * kLearnedIters : 3 * kChunkF) : 2 * kChunk;
