@@ -903,6 +903,95 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_sharded(args):
+    """One grid over all ranks: the backward-Euler configuration's family at
+    256^3 (smoothed log-normal alpha, sigma 1.5, filter 8, seed 2; dt = 50x
+    the explicit limit) split into z-slabs, one per GPU
+    (piro_b200/slab.py SlabBE: halo planes and FP64 sums over NCCL, the CG
+    scalars kept on the device and the done flag read every 8 iterations).
+    A step is one backward-Euler solve to a 1e-8 FP64 relative residual, the
+    next step starting from its result; strong scaling (the grid is fixed)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from piro_b200 import slab
+    from piro_b200 import workloads as W
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        comm = slab.TorchComm()
+    else:
+        comm = slab.LocalComm(slab.LocalGroup(1), 0)
+    n = args.sharded
+    cfg = W.heat_be_128(n=n)
+    nx = ny = nz = n
+    plane = nx * ny
+    z0, z1 = slab.split_planes(nz, world)[rank]
+    lo, hi = (z0 - 1) * plane, (z1 + 1) * plane
+
+    def local_of(full):
+        out = np.zeros(hi - lo, np.float32)
+        s0, s1 = max(lo, 0), min(hi, nx * ny * nz)
+        out[s0 - lo:s1 - lo] = full[s0:s1]
+        return torch.from_numpy(out).cuda()
+    be = slab.CudaBackend()
+    sv = slab.SlabBE(be, comm, nx, ny, nz, z0, z1, float(cfg["dt"]), 1.0, local_of(cfg["alpha"]))
+    b0 = local_of(cfg["u0"])
+    b = b0.clone()
+    traj = cfg["steps"]
+    iters = []
+
+    def step():
+        x64, info = sv.solve(b, rtol=1e-8, device_scalars=True, check_every=8)
+        if info["status"] != "ok":
+            raise RuntimeError(f"sharded solve: {info}")
+        iters.append(info["inner"])
+        b.copy_(x64.float())
+    for i in range(args.warmup):
+        if i % traj == 0:
+            b.copy_(b0)
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    iters.clear()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for i in range(args.steps):
+        if i % traj == 0:
+            b.copy_(b0)
+        ev[i][0].record()
+        step()
+        ev[i][1].record()
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(c) for a, c in ev) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": f"BE {n}^3 step ms at 1e-8 FP64 residual, one grid in z-slabs over {world} GPU(s)",
+        "value": round(ms, 4), "unit": "ms/step", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 4), "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32 Krylov + f64 refinement", "data": "synthetic (seeded numpy)",
+        "config": {"workload": f"heat backward Euler {n}^3, smoothed log-normal alpha (sigma 1.5, filter 8, seed 2), "
+                               "dt = 50x explicit limit", "grid": [nx, ny, nz], "parallelism": f"z-slab x{world}",
+                   "slab_planes": [z1 - z0 for z0, z1 in slab.split_planes(nz, world)]},
+        "solver": {"inner_iterations_mean": float(np.mean(iters)) if iters else None,
+                   "scalars": "on the device (all-reduced sums read by the next kernel), done flag read every 8 "
+                              "iterations"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_profile_case(args):
     """Small fixed cases for ncu captures (no timing, no JSON): `be` solves the
     128^3 backward-Euler step twice, `spmv` runs the 256^3 forward-Euler
@@ -1004,6 +1093,8 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="piro", choices=["piro", "reference"])
+    ap.add_argument("--sharded", type=int, default=0, metavar="N",
+                    help="one N^3 backward-Euler grid in z-slabs over the ranks (strong scaling) instead of replicas")
     ap.add_argument("--profile", choices=["be", "spmv", "dense", "learned", "batched", "train"],
                     help="run a small fixed case for ncu, print no JSON")
     args = ap.parse_args()
@@ -1014,6 +1105,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.sharded:
+        run_sharded(args)
     else:
         run_piro(args)
 

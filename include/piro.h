@@ -497,6 +497,24 @@ int piro_slab_cg_update(int nx, int ny, int nz, int z0, int z1, float dt, float 
                         piro_stream_t stream);
 /* x64 += d, d = 0 on owned interior cells. */
 int piro_slab_x_update(int nx, int ny, int nz, int z0, int z1, double *x64, float *d, piro_stream_t stream);
+/* The CG steps with their scalars kept on the device, so that an iteration
+ * needs no host round trip: state is a device double[8] -- 0 <r/alpha, z>,
+ * 1 beta, 2 a, 3 the inner stop threshold (tol2 * rr0), 4 done, 5 iterations,
+ * 6 |r|^2, 7 broken -- identical on every rank because it is formed from
+ * all-reduced sums.  piro_slab_cg_spmv_dev is piro_slab_cg_spmv with beta
+ * from state; piro_slab_cg_update_dev is piro_slab_cg_update with a =
+ * state[0] / pq[0] (pq: the all-reduced sums of the spmv step); both return
+ * at once when state says done.  piro_slab_cg_scalars (one thread) then
+ * forms a, beta and the stop and breakdown tests from pq and up (the
+ * all-reduced sums of the update step).  No counterpart in the reference,
+ * which runs one grid in one process (src/solve.cpp:11-48). */
+int piro_slab_cg_spmv_dev(int nx, int ny, int nz, int z0, int z1, float dt, float norm, const double *state,
+                          const float *alpha, const float *z, const float *p_old, float *p_new, float *q,
+                          double *work, double *sums, piro_stream_t stream);
+int piro_slab_cg_update_dev(int nx, int ny, int nz, int z0, int z1, float dt, float norm, const double *state,
+                            const double *pq, const float *alpha, const float *p, const float *q, float *d, float *r,
+                            float *z, double *work, double *sums, piro_stream_t stream);
+int piro_slab_cg_scalars(double *state, const double *pq, const double *up, piro_stream_t stream);
 
 /* -- batched stepping: many independent problems in one persistent launch ----
  *

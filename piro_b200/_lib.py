@@ -127,6 +127,10 @@ SIGNATURES = {
     "piro_slab_cg_spmv": (i32, [i32, i32, i32, i32, i32, f32, f32, f32, vp, vp, vp, vp, vp, vp, vp, vp]),
     "piro_slab_cg_update": (i32, [i32, i32, i32, i32, i32, f32, f32, f32, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "piro_slab_x_update": (i32, [i32, i32, i32, i32, i32, vp, vp, vp]),
+    "piro_slab_cg_spmv_dev": (i32, [i32, i32, i32, i32, i32, f32, f32, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "piro_slab_cg_update_dev": (i32, [i32, i32, i32, i32, i32, f32, f32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                      vp]),
+    "piro_slab_cg_scalars": (i32, [vp, vp, vp, vp]),
     "piro_batch_create": (i32, [i32, vp, vp, vp, vp, vp, C.POINTER(vp)]),
     "piro_batch_layout": (i32, [vp, vp, pi64]),
     "piro_batch_set_fields": (i32, [vp, vp, i32]),

@@ -93,14 +93,33 @@ __global__ void __launch_bounds__(kSlabThreads) k_slab_residual(Slab S, const fl
     block_partials(part, 4, v);
 }
 
+// Device-resident CG scalars of one slab solve (state[kSlabStateLen], the
+// same on every rank since it is formed from all-reduced sums):
+enum : int {
+    kStRz = 0,    // <r/alpha, z> of the current iterate
+    kStBeta = 1,  // direction update of the next iteration
+    kStA = 2,     // step length of the last iteration
+    kStStop = 3,  // inner stop: |r|^2 <= this (tol2 * rr0)
+    kStDone = 4,  // nonzero: the inner solve has stopped (steps are no-ops)
+    kStIters = 5, // iterations taken
+    kStRr = 6,    // |r|^2 after the last iteration
+    kStBroken = 7 // nonzero: a non-finite or non-positive scalar appeared
+};
+
 // p = z + beta*p_old on interior cells of the owned and halo planes (0 on the
-// boundary); q = A p on owned interior cells; partial <p, q/alpha>.
-__global__ void __launch_bounds__(kSlabThreads) k_slab_cg_spmv(Slab S, float beta, const float *__restrict__ alpha,
+// boundary); q = A p on owned interior cells; partial <p, q/alpha>.  With a
+// device state, beta comes from it and a finished solve returns at once.
+__global__ void __launch_bounds__(kSlabThreads) k_slab_cg_spmv(Slab S, float beta, const double *__restrict__ state,
+                                                               const float *__restrict__ alpha,
                                                                const float *__restrict__ z,
                                                                const float *__restrict__ p_old,
                                                                float *__restrict__ p_new, float *__restrict__ q,
                                                                double *__restrict__ part)
 {
+    if (state) {
+        if (state[kStDone] != 0.0) return;
+        beta = (float)state[kStBeta];
+    }
     const int64_t sxy = (int64_t)S.g.nx * S.g.ny;
     const int64_t N = sxy * S.g.nz;
     double v[4] = {0.0, 0.0, 0.0, 0.0};
@@ -126,13 +145,23 @@ __global__ void __launch_bounds__(kSlabThreads) k_slab_cg_spmv(Slab S, float bet
 }
 
 // d += a p, r -= a q, z = r / A_rr on owned interior cells; partials
-// <r/alpha, z>, |r|^2.
-__global__ void __launch_bounds__(kSlabThreads) k_slab_cg_update(Slab S, float a, const float *__restrict__ alpha,
+// <r/alpha, z>, |r|^2.  With a device state, a = rz / <p, S p> (pq: the
+// all-reduced sum of the operator step) and a finished or broken-down solve
+// returns at once.
+__global__ void __launch_bounds__(kSlabThreads) k_slab_cg_update(Slab S, float a, const double *__restrict__ state,
+                                                                 const double *__restrict__ pq,
+                                                                 const float *__restrict__ alpha,
                                                                  const float *__restrict__ p,
                                                                  const float *__restrict__ q, float *__restrict__ d,
                                                                  float *__restrict__ r, float *__restrict__ z,
                                                                  double *__restrict__ part)
 {
+    if (state) {
+        if (state[kStDone] != 0.0) return;
+        const double ad = state[kStRz] / pq[0];
+        if (!isfinite(ad) || !(pq[0] > 0.0)) return;  // k_slab_cg_scalars records the breakdown
+        a = (float)ad;
+    }
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     for (int64_t l = S.own0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < S.own1;
          l += (int64_t)gridDim.x * blockDim.x) {
@@ -149,6 +178,34 @@ __global__ void __launch_bounds__(kSlabThreads) k_slab_cg_update(Slab S, float a
         v[1] += (double)ri * (double)ri;
     }
     block_partials(part, 2, v);
+}
+
+// One CG iteration's scalars from its all-reduced sums (one thread): a =
+// rz / pq, then beta = rz' / rz, rz = rz' from up = {rz', |r|^2}; the stop
+// and breakdown tests set done.
+__global__ void k_slab_cg_scalars(double *__restrict__ st, const double *__restrict__ pq,
+                                  const double *__restrict__ up)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0 || st[kStDone] != 0.0) return;
+    const double a = st[kStRz] / pq[0];
+    if (!isfinite(a) || !(pq[0] > 0.0)) {
+        st[kStBroken] = 1.0;
+        st[kStDone] = 1.0;
+        return;
+    }
+    st[kStA] = a;
+    const double rzn = up[0], rr = up[1];
+    const double beta = rzn / st[kStRz];
+    st[kStIters] += 1.0;
+    st[kStRr] = rr;
+    if (!isfinite(rr) || !isfinite(beta)) {
+        st[kStBroken] = 1.0;
+        st[kStDone] = 1.0;
+        return;
+    }
+    st[kStBeta] = beta;
+    st[kStRz] = rzn;
+    if (rr <= st[kStStop]) st[kStDone] = 1.0;
 }
 
 // x64 += d, d = 0 on owned interior cells.
@@ -230,7 +287,7 @@ extern "C" int piro_slab_cg_spmv(int nx, int ny, int nz, int z0, int z1, float d
     PIRO_ARG(alpha && z && p_old && p_new && q && work && sums && p_old != p_new, "piro_slab_cg_spmv: bad pointers");
     cudaStream_t st = as_stream(stream);
     const unsigned grid = slab_grid();
-    k_slab_cg_spmv<<<grid, kSlabThreads, 0, st>>>(S, beta, alpha, z, p_old, p_new, q, work);
+    k_slab_cg_spmv<<<grid, kSlabThreads, 0, st>>>(S, beta, nullptr, alpha, z, p_old, p_new, q, work);
     PIRO_CHECK_LAUNCH("k_slab_cg_spmv");
     k_slab_finish<<<1, 32, 0, st>>>(work, (int)grid, 1, sums);
     PIRO_CHECK_LAUNCH("k_slab_finish");
@@ -247,7 +304,7 @@ extern "C" int piro_slab_cg_update(int nx, int ny, int nz, int z0, int z1, float
     PIRO_ARG(alpha && p && q && d && r && z && work && sums, "piro_slab_cg_update: null pointer");
     cudaStream_t st = as_stream(stream);
     const unsigned grid = slab_grid();
-    k_slab_cg_update<<<grid, kSlabThreads, 0, st>>>(S, a, alpha, p, q, d, r, z, work);
+    k_slab_cg_update<<<grid, kSlabThreads, 0, st>>>(S, a, nullptr, nullptr, alpha, p, q, d, r, z, work);
     PIRO_CHECK_LAUNCH("k_slab_cg_update");
     k_slab_finish<<<1, 64, 0, st>>>(work, (int)grid, 2, sums);
     PIRO_CHECK_LAUNCH("k_slab_finish");
@@ -262,5 +319,49 @@ extern "C" int piro_slab_x_update(int nx, int ny, int nz, int z0, int z1, double
     PIRO_ARG(x64 && d, "piro_slab_x_update: null pointer");
     k_slab_x_update<<<slab_grid(), kSlabThreads, 0, as_stream(stream)>>>(S, x64, d);
     PIRO_CHECK_LAUNCH("k_slab_x_update");
+    return PIRO_OK;
+}
+
+extern "C" int piro_slab_cg_spmv_dev(int nx, int ny, int nz, int z0, int z1, float dt, float norm,
+                                     const double *state, const float *alpha, const float *z, const float *p_old,
+                                     float *p_new, float *q, double *work, double *sums, piro_stream_t stream)
+{
+    Slab S;
+    int rc = slab_make(nx, ny, nz, z0, z1, dt, norm, &S);
+    if (rc) return rc;
+    PIRO_ARG(state && alpha && z && p_old && p_new && q && work && sums && p_old != p_new,
+             "piro_slab_cg_spmv_dev: bad pointers");
+    cudaStream_t st = as_stream(stream);
+    const unsigned grid = slab_grid();
+    k_slab_cg_spmv<<<grid, kSlabThreads, 0, st>>>(S, 0.0f, state, alpha, z, p_old, p_new, q, work);
+    PIRO_CHECK_LAUNCH("k_slab_cg_spmv");
+    k_slab_finish<<<1, 32, 0, st>>>(work, (int)grid, 1, sums);
+    PIRO_CHECK_LAUNCH("k_slab_finish");
+    return PIRO_OK;
+}
+
+extern "C" int piro_slab_cg_update_dev(int nx, int ny, int nz, int z0, int z1, float dt, float norm,
+                                       const double *state, const double *pq, const float *alpha, const float *p,
+                                       const float *q, float *d, float *r, float *z, double *work, double *sums,
+                                       piro_stream_t stream)
+{
+    Slab S;
+    int rc = slab_make(nx, ny, nz, z0, z1, dt, norm, &S);
+    if (rc) return rc;
+    PIRO_ARG(state && pq && alpha && p && q && d && r && z && work && sums, "piro_slab_cg_update_dev: null pointer");
+    cudaStream_t st = as_stream(stream);
+    const unsigned grid = slab_grid();
+    k_slab_cg_update<<<grid, kSlabThreads, 0, st>>>(S, 0.0f, state, pq, alpha, p, q, d, r, z, work);
+    PIRO_CHECK_LAUNCH("k_slab_cg_update");
+    k_slab_finish<<<1, 64, 0, st>>>(work, (int)grid, 2, sums);
+    PIRO_CHECK_LAUNCH("k_slab_finish");
+    return PIRO_OK;
+}
+
+extern "C" int piro_slab_cg_scalars(double *state, const double *pq, const double *up, piro_stream_t stream)
+{
+    PIRO_ARG(state && pq && up, "piro_slab_cg_scalars: null pointer");
+    k_slab_cg_scalars<<<1, 32, 0, as_stream(stream)>>>(state, pq, up);
+    PIRO_CHECK_LAUNCH("k_slab_cg_scalars");
     return PIRO_OK;
 }

@@ -202,6 +202,22 @@ class CudaBackend:
         self.check(self.lib().piro_slab_x_update(nx, ny, nz, z0, z1, self._p(x64), self._p(d), self._stream()),
                    "piro_slab_x_update")
 
+    # steps with the CG scalars on the device (state: double[8], see include/piro.h)
+    def cg_spmv_dev(self, S, state, alpha, z, p_old, p_new, q, sums):
+        self.check(self.lib().piro_slab_cg_spmv_dev(*S, self._p(state), self._p(alpha), self._p(z), self._p(p_old),
+                                                    self._p(p_new), self._p(q), self._p(self.work), self._p(sums),
+                                                    self._stream()), "piro_slab_cg_spmv_dev")
+
+    def cg_update_dev(self, S, state, pq, alpha, p, q, d, r, z, sums):
+        self.check(self.lib().piro_slab_cg_update_dev(*S, self._p(state), self._p(pq), self._p(alpha), self._p(p),
+                                                      self._p(q), self._p(d), self._p(r), self._p(z),
+                                                      self._p(self.work), self._p(sums), self._stream()),
+                   "piro_slab_cg_update_dev")
+
+    def cg_scalars(self, state, pq, up):
+        self.check(self.lib().piro_slab_cg_scalars(self._p(state), self._p(pq), self._p(up), self._stream()),
+                   "piro_slab_cg_scalars")
+
 
 # ------------------------------------------------------------------ solvers
 class SlabFE:
@@ -261,7 +277,77 @@ class SlabBE:
     def _sum(self, t):
         return self.comm.allsum(t).cpu().numpy().astype(np.float64)
 
-    def solve(self, b, rtol=1e-8, max_outer=20, max_inner=20000, inner_floor=1e-6):
+    def solve(self, b, rtol=1e-8, max_outer=20, max_inner=20000, inner_floor=1e-6, device_scalars=False,
+              check_every=8):
+        """device_scalars: the CG step lengths, directions and stop test stay
+        on the device (all-reduced into device buffers, read by the next
+        kernel); the host looks at the done flag every `check_every`
+        iterations, so an iteration costs no host round trip."""
+        if device_scalars:
+            return self._solve_dev(b, rtol, max_outer, max_inner, inner_floor, check_every)
+        return self._solve_host(b, rtol, max_outer, max_inner, inner_floor)
+
+    def _solve_dev(self, b, rtol, max_outer, max_inner, inner_floor, check_every):
+        S, B = self.S, self.b
+        self.comm.halo(b, self.plane)
+        self.x64.copy_(b)
+        self.d.zero_()
+        state = B.empty(8, "f64")
+        pq, up = B.empty(1, "f64"), B.empty(2, "f64")
+        info = dict(status="not converged", outer=0, inner=0, rel=math.inf)
+        prev = math.inf
+        for outer in range(max_outer + 1):
+            self.comm.halo(self.x64, self.plane)
+            s = self._sum(B.residual(S, self.alpha, b, self.x64, self.r, self.z))  # one host sync per sweep
+            bn = math.sqrt(s[1]) if s[1] > 0 else 1.0
+            rel = math.sqrt(s[0]) / bn
+            info["rel"] = rel
+            if not math.isfinite(rel):
+                info["status"] = "stalled"
+                break
+            if rel <= rtol:
+                info["status"] = "ok"
+                break
+            if outer == max_outer or info["inner"] >= max_inner:
+                break
+            if outer > 0 and rel > 0.5 * prev:
+                info["status"] = "stalled"
+                break
+            prev = rel
+            info["outer"] = outer + 1
+            itol = min(0.1, max(inner_floor, 0.5 * rtol / rel)) if rel > 0 else 1.0
+            st = np.zeros(8)
+            st[0], st[3] = s[2], itol * itol * s[3]
+            st[4] = 1.0 if s[3] <= 0.0 else 0.0
+            state.copy_(self.b_tensor(st, state))
+            k, taken = 0, 0
+            while True:
+                for _ in range(check_every):
+                    self.comm.halo(self.z, self.plane)
+                    p_old, p_new = self.p[k & 1], self.p[(k + 1) & 1]
+                    B.cg_spmv_dev(S, state, self.alpha, self.z, p_old, p_new, self.q, pq)
+                    self.comm.allsum(pq)
+                    B.cg_update_dev(S, state, pq, self.alpha, p_new, self.q, self.d, self.r, self.z, up)
+                    self.comm.allsum(up)
+                    B.cg_scalars(state, pq, up)
+                    k += 1
+                h = state.cpu().numpy()  # the host's look at the flags
+                taken = int(h[5])
+                if h[4] != 0.0 or info["inner"] + taken >= max_inner:
+                    break
+            info["inner"] += taken
+            if h[7] != 0.0:
+                info["status"] = "stalled"
+                break
+            B.x_update(S, self.x64, self.d)
+        return self.x64, info
+
+    @staticmethod
+    def b_tensor(values, like):
+        import torch
+        return torch.as_tensor(values, dtype=torch.float64).to(like.device)
+
+    def _solve_host(self, b, rtol=1e-8, max_outer=20, max_inner=20000, inner_floor=1e-6):
         """x64 (owned planes valid) for A x = b; b's halo planes are exchanged here."""
         S, B = self.S, self.b
         self.comm.halo(b, self.plane)

@@ -131,3 +131,39 @@ class NumpyBackend:
         l = np.nonzero(inter & own)[0]
         x64.numpy()[l] += d.numpy()[l].astype(np.float64)
         d.numpy()[l] = 0.0
+
+    # ---- the same steps with the CG scalars in a state vector (piro_slab_*_dev)
+    def cg_spmv_dev(self, S, state, alpha, z, p_old, p_new, q, sums):
+        st = state.numpy()
+        if st[4] != 0.0:
+            return
+        sums.copy_(self.cg_spmv(S, float(np.float32(st[1])), alpha, z, p_old, p_new, q))
+
+    def cg_update_dev(self, S, state, pq, alpha, p, q, d, r, z, sums):
+        st, t = state.numpy(), float(pq.numpy()[0])
+        if st[4] != 0.0:
+            return
+        a = st[0] / t if t != 0.0 else np.inf
+        if not np.isfinite(a) or not t > 0.0:
+            return
+        sums.copy_(self.cg_update(S, float(np.float32(a)), alpha, p, q, d, r, z))
+
+    def cg_scalars(self, state, pq, up):
+        st, t = state.numpy(), float(pq.numpy()[0])
+        if st[4] != 0.0:
+            return
+        a = st[0] / t if t != 0.0 else np.inf
+        if not np.isfinite(a) or not t > 0.0:
+            st[7] = st[4] = 1.0
+            return
+        st[2] = a
+        rzn, rr = (float(v) for v in up.numpy()[:2])
+        beta = rzn / st[0]
+        st[5] += 1.0
+        st[6] = rr
+        if not np.isfinite(rr) or not np.isfinite(beta):
+            st[7] = st[4] = 1.0
+            return
+        st[1], st[0] = beta, rzn
+        if rr <= st[3]:
+            st[4] = 1.0

@@ -111,8 +111,11 @@ def test_slab_advection_bitexact(cuda, world, scheme):
     assert np.array_equal(got[inter], ref[inter])
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_slab_be_matches_single_grid(cuda, world):
+@pytest.mark.parametrize("world,device_scalars", [(2, False), (3, False), (2, True), (3, True)])
+def test_slab_be_matches_single_grid(cuda, world, device_scalars):
+    """device_scalars: the CG scalars formed on the device from all-reduced
+    sums (piro_slab_*_dev), the host looking at the done flag every 8
+    iterations."""
     import torch
     from piro_b200 import learned, ops, slab
     n = 34
@@ -131,7 +134,8 @@ def test_slab_be_matches_single_grid(cuda, world):
         z0, z1 = parts[r]
         be = slab.CudaBackend()
         s = slab.SlabBE(be, comm, n, n, n, z0, z1, dt, 1.0, torch.from_numpy(_local(alpha, z0, z1, plane)).cuda())
-        x64, info = s.solve(torch.from_numpy(_local(b, z0, z1, plane)).cuda(), rtol=1e-10)
+        x64, info = s.solve(torch.from_numpy(_local(b, z0, z1, plane)).cuda(), rtol=1e-10,
+                            device_scalars=device_scalars)
         assert info["status"] == "ok", info
         return x64.cpu().numpy()[plane:(z1 - z0 + 1) * plane]
 

@@ -78,8 +78,9 @@ def _rank_main(rank, world, port, task, out_dir):
             fe.step(u, out, 0.01)
             res = out.numpy()[plane:(z1 - z0 + 1) * plane]
         else:
-            sv = slab.SlabBE(be, comm, nx, ny, nz, z0, z1, arg, 1.0, torch.from_numpy(a_loc))
-            x64, info = sv.solve(torch.from_numpy(loc), rtol=1e-10)
+            dt, dev = arg if isinstance(arg, tuple) else (arg, False)
+            sv = slab.SlabBE(be, comm, nx, ny, nz, z0, z1, dt, 1.0, torch.from_numpy(a_loc))
+            x64, info = sv.solve(torch.from_numpy(loc), rtol=1e-10, device_scalars=dev, check_every=3)
             assert info["status"] == "ok", info
             res = x64.numpy()[plane:(z1 - z0 + 1) * plane]
         np.save(os.path.join(out_dir, f"r{rank}.npy"), res)
@@ -114,11 +115,14 @@ def test_slab_fe_matches_whole_grid(oracle, world, scheme):
     assert np.array_equal(got[inter], ref[inter])  # bit for bit on every stepped row
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_slab_be_matches_whole_grid(oracle, world):
+@pytest.mark.parametrize("world,device_scalars", [(2, False), (3, False), (2, True), (3, True)])
+def test_slab_be_matches_whole_grid(oracle, world, device_scalars):
+    """device_scalars: the CG scalars stay in a device state vector formed from
+    all-reduced sums (piro_slab_*_dev); the host looks at the flags every 3
+    iterations and finished iterations are no-ops on every rank."""
     nx, ny, nz = 8, 7, 10
     dt = 2.0
-    got = _run(world, ("be", nx, ny, nz, dt))
+    got = _run(world, ("be", nx, ny, nz, (dt, device_scalars)))
     O = oracle
     u, alpha = _fields(nx, ny, nz, True)
     N = nx * ny * nz
