@@ -331,6 +331,29 @@ def assembly_section(torch, ops, peak):
         out[f"csr_laplacian_{n}"] = {"ms": round(ms, 4), "nnz": nnz, "bytes_written": byt,
                                      "gbs": round(byt / ms / 1e6, 1), "frac": round(byt / ms / 1e6 / peak, 4)}
         del A
+    # v . grad merge (operator&, csrgeam count + scan + fill) at 256^3 of the
+    # upwind gradients; bytes: sum 8 nnz_in + 12 N (v) + 8 nnz_out + 4 (N+1)
+    n = 256
+    N = n ** 3
+    G = [ops.csr_gradient(n, n, n, 1, a, 2.0) for a in range(3)]
+    v = torch.rand(3 * N, device="cuda")
+    for _ in range(2):
+        D = ops.csrgeam3(N, *G, v)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        D = ops.csrgeam3(N, *G, v)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 5
+    nnz_in = sum(int(g[2].numel()) for g in G)
+    byt = 8 * nnz_in + 12 * N + 8 * int(D[2].numel()) + 4 * (N + 1)
+    out["csrgeam3_256"] = {"ms": round(ms, 4), "nnz_out": int(D[2].numel()), "bytes": byt,
+                           "gbs": round(byt / ms / 1e6, 1), "frac": round(byt / ms / 1e6 / peak, 4),
+                           "note": "count, one device scan, fill (the reference: N scan launches)"}
+    del G, D, v
+    torch.cuda.empty_cache()
     try:  # PIRO's own host code (oracle/_ref), when it was built
         from oracle import oracle as O
         R = O.Ref()

@@ -20,14 +20,32 @@ constexpr int kMaxPerRow = 7;
 struct Grid {
     int nx, ny, nz;
     int64_t sxy;
+    FastDiv fx, fxy;  // division by nx and nx*ny for cell indices below 2^31
 };
 
+Grid make_grid(int nx, int ny, int nz)
+{
+    Grid g;
+    g.nx = nx;
+    g.ny = ny;
+    g.nz = nz;
+    g.sxy = (int64_t)nx * ny;
+    g.fx = FastDiv((uint32_t)nx);
+    g.fxy = FastDiv((uint32_t)g.sxy);
+    return g;
+}
+
+// Cell coordinates by multiply-shift division (every grid here has fewer
+// than 2^31 cells), not 64-bit division.
 __device__ __forceinline__ void coords(int64_t i, const Grid &g, int &x, int &y, int &z)
 {
-    z = (int)(i / g.sxy);
-    int64_t rem = i - (int64_t)z * g.sxy;
-    y = (int)(rem / g.nx);
-    x = (int)(rem - (int64_t)y * g.nx);
+    const uint32_t u = (uint32_t)i;
+    const uint32_t zz = g.fxy.div(u);
+    const uint32_t rem = u - zz * (uint32_t)g.sxy;
+    const uint32_t yy = g.fx.div(rem);
+    z = (int)zz;
+    y = (int)yy;
+    x = (int)(rem - yy * (uint32_t)g.nx);
 }
 
 // Sum of 7-point row lengths over all rows before (x, y, z) in row-major
@@ -110,6 +128,8 @@ __global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, 
         base0 = lap_prefix(x, y, z, g);
     }
     const int64_t R1 = row0 + N;
+    const bool vec_ok = ((reinterpret_cast<uintptr_t>(col) | reinterpret_cast<uintptr_t>(val) |
+                          reinterpret_cast<uintptr_t>(rows)) & 15) == 0;
     for (int64_t r0 = row0 + (int64_t)blockIdx.x * kRowsPerBlock; r0 < R1; r0 += (int64_t)gridDim.x * kRowsPerBlock) {
         const int64_t i = r0 + threadIdx.x;
         const int64_t rlast = (r0 + kRowsPerBlock < R1 ? r0 + kRowsPerBlock : R1) - 1;
@@ -142,11 +162,29 @@ __global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, 
             }
         }
         __syncthreads();
+        // the block's entries leave as 16-byte stores from the first entry
+        // whose index is a multiple of 4 on (scalar head and tail), when the
+        // arrays themselves are 16-byte aligned
         const int cnt = (int)(s_end - s_base);
-        for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-            col[s_base - base0 + t] = s_col[t];
-            val[s_base - base0 + t] = s_val[t];
-            if (rows) rows[s_base - base0 + t] = s_row[t];
+        const int64_t dst = s_base - base0;
+        int head = vec_ok ? (int)((4 - (dst & 3)) & 3) : cnt;
+        head = head < cnt ? head : cnt;
+        const int body = (cnt - head) & ~3;
+        for (int t = threadIdx.x; t < head; t += blockDim.x) {
+            col[dst + t] = s_col[t];
+            val[dst + t] = s_val[t];
+            if (rows) rows[dst + t] = s_row[t];
+        }
+        for (int t = head + 4 * threadIdx.x; t < head + body; t += 4 * blockDim.x) {
+            *reinterpret_cast<int4 *>(col + dst + t) = make_int4(s_col[t], s_col[t + 1], s_col[t + 2], s_col[t + 3]);
+            *reinterpret_cast<float4 *>(val + dst + t) = make_float4(s_val[t], s_val[t + 1], s_val[t + 2], s_val[t + 3]);
+            if (rows)
+                *reinterpret_cast<int4 *>(rows + dst + t) = make_int4(s_row[t], s_row[t + 1], s_row[t + 2], s_row[t + 3]);
+        }
+        for (int t = head + body + threadIdx.x; t < cnt; t += blockDim.x) {
+            col[dst + t] = s_col[t];
+            val[dst + t] = s_val[t];
+            if (rows) rows[dst + t] = s_row[t];
         }
         __syncthreads();
     }
@@ -290,7 +328,7 @@ static int launch_laplacian(int nx, int ny, int nz, int scheme, float norm, int3
         piro::set_error("laplacian: space scheme %d not in {1 uw, 2 dw, 3 cd}", scheme);
         return PIRO_ERR_SCHEME;
     }
-    Grid g{nx, ny, nz, (int64_t)nx * ny};
+    Grid g = make_grid(nx, ny, nz);
     const int64_t N = (int64_t)nx * ny * nz;
     // The literals are double in stencils.cpp:245,250: (float)(-6.0/norm).
     const float vself = (float)(-6.0 / (double)norm);
@@ -307,7 +345,7 @@ extern "C" int piro_laplacian_nnz_rows(int nx, int ny, int nz, int64_t row0, int
     const int64_t N = (int64_t)nx * ny * nz;
     PIRO_ARG(nnz && grid_ok(nx, ny, nz) && row0 >= 0 && nrows >= 0 && row0 + nrows <= N,
              "piro_laplacian_nnz_rows: bad arguments");
-    const Grid g{nx, ny, nz, (int64_t)nx * ny};
+    const Grid g = make_grid(nx, ny, nz);
     auto prefix = [&](int64_t i) -> int64_t {
         if (i >= N) return 7 * N - 2 * ((int64_t)nx * ny + (int64_t)ny * nz + (int64_t)nx * nz);
         const int z = (int)(i / g.sxy);
@@ -332,7 +370,7 @@ extern "C" int piro_csr_laplacian_rows(int nx, int ny, int nz, int space_scheme,
         piro::set_error("laplacian: space scheme %d not in {1 uw, 2 dw, 3 cd}", space_scheme);
         return PIRO_ERR_SCHEME;
     }
-    Grid g{nx, ny, nz, (int64_t)nx * ny};
+    Grid g = make_grid(nx, ny, nz);
     const float vself = (float)(-6.0 / (double)norm);
     const float vnb = (float)(1.0 / (double)norm);
     unsigned grid = grid_for(nrows, kRowsPerBlock, 4);
@@ -374,7 +412,7 @@ extern "C" int piro_csr_gradient(int nx, int ny, int nz, int space_scheme, int a
         piro::set_error("piro_csr_gradient: space scheme %d not in {1,2,3}", space_scheme);
         return PIRO_ERR_SCHEME;
     }
-    Grid g{nx, ny, nz, (int64_t)nx * ny};
+    Grid g = make_grid(nx, ny, nz);
     const int64_t N = (int64_t)nx * ny * nz;
     // -1/norm and 1/norm are float divisions (int operand promoted), stencils.cpp:17,24.
     const float vm = -1 / norm, vp = 1 / norm;
@@ -389,7 +427,7 @@ extern "C" int piro_gradient_nnz_rows(int nx, int ny, int nz, int axis, int64_t 
     const int64_t N = (int64_t)nx * ny * nz;
     PIRO_ARG(nnz && grid_ok(nx, ny, nz) && axis >= 0 && axis <= 2 && row0 >= 0 && nrows >= 0 && row0 + nrows <= N,
              "piro_gradient_nnz_rows: bad arguments");
-    const Grid g{nx, ny, nz, (int64_t)nx * ny};
+    const Grid g = make_grid(nx, ny, nz);
     *nnz = grad_prefix_host(row0 + nrows, axis, g, N) - grad_prefix_host(row0, axis, g, N);
     return PIRO_OK;
 }
@@ -407,7 +445,7 @@ extern "C" int piro_csr_gradient_rows(int nx, int ny, int nz, int space_scheme, 
         piro::set_error("piro_csr_gradient_rows: space scheme %d not in {1,2,3}", space_scheme);
         return PIRO_ERR_SCHEME;
     }
-    Grid g{nx, ny, nz, (int64_t)nx * ny};
+    Grid g = make_grid(nx, ny, nz);
     const float vm = -1 / norm, vp = 1 / norm;
     const int64_t p0 = grad_prefix_host(row0, axis, g, N);
     k_gradient<<<grid_for(nrows, 256, 8), 256, 0, as_stream(stream)>>>(g, nrows, space_scheme, axis, vm, vp, rowptr,
@@ -449,7 +487,7 @@ extern "C" int piro_face_count(int nx, int ny, int nz, int64_t *q, int64_t face_
 extern "C" int piro_face_lists(int nx, int ny, int nz, uint32_t *idx, piro_stream_t stream)
 {
     PIRO_ARG(idx && grid_ok(nx, ny, nz), "piro_face_lists: bad arguments");
-    Grid g{nx, ny, nz, (int64_t)nx * ny};
+    Grid g = make_grid(nx, ny, nz);
     const int64_t a = (int64_t)(ny - 2) * (nz - 2), b = (int64_t)(nx - 2) * (nz - 2), c = (int64_t)(nx - 2) * (ny - 2);
     const int64_t Q = 2 * (a + b + c);
     k_faces<<<grid_for(Q, 256, 4), 256, 0, as_stream(stream)>>>(g, a, b, c, idx);

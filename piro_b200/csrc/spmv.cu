@@ -181,6 +181,124 @@ __global__ void k_coo_segsum(int64_t N, int64_t nnz, const int32_t *__restrict__
     if (bad) atomicOr(err, bad);
 }
 
+// The same sum with 8 consecutive entries per lane (a warp covers 256 per
+// pass): 16-byte loads of rows, cols and vals, runs of equal row ids summed
+// sequentially in the lane, and one segmented scan per warp over the lanes'
+// last runs instead of one per entry.  With ascending row ids a row's entries
+// are contiguous, so a run that starts and ends inside a lane is the whole
+// row (a plain store); a lane's last run continues into the next lane when
+// that lane starts with the same row, and the scan carries its sum there.  A
+// row that touches either end of the warp's 256-entry span is added
+// atomically in every span it appears in (at most two contributions for rows
+// of <= 256 entries, so the sum does not depend on their order).  Same input
+// checks as k_coo_segsum.  Requires 16-byte aligned arrays; acc must be zero.
+constexpr int kCooPer = 8;
+
+__global__ void __launch_bounds__(256) k_coo_segsum8(int64_t N, int64_t nnz, const int32_t *__restrict__ rows,
+                                                     const int32_t *__restrict__ cols,
+                                                     const float *__restrict__ vals, const float *__restrict__ u,
+                                                     float *__restrict__ acc, int *__restrict__ err)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    constexpr int kSpan = 32 * kCooPer;
+    constexpr int kNone = INT32_MAX;  // row id of entries past the end
+    int bad = 0;
+    for (int64_t base = warp * kSpan; base < nnz; base += nwarps * kSpan) {
+        const int64_t k0 = base + (int64_t)lane * kCooPer;
+        int r[kCooPer], c[kCooPer];
+        float v[kCooPer];
+        if (k0 + kCooPer <= nnz) {
+            const int4 *R4 = reinterpret_cast<const int4 *>(rows + k0), *C4 = reinterpret_cast<const int4 *>(cols + k0);
+            const float4 *V4 = reinterpret_cast<const float4 *>(vals + k0);
+#pragma unroll
+            for (int h = 0; h < kCooPer / 4; ++h) {
+                const int4 ra = __ldcs(R4 + h), ca = __ldcs(C4 + h);
+                const float4 va = __ldcs(V4 + h);
+                r[4 * h] = ra.x; r[4 * h + 1] = ra.y; r[4 * h + 2] = ra.z; r[4 * h + 3] = ra.w;
+                c[4 * h] = ca.x; c[4 * h + 1] = ca.y; c[4 * h + 2] = ca.z; c[4 * h + 3] = ca.w;
+                v[4 * h] = va.x; v[4 * h + 1] = va.y; v[4 * h + 2] = va.z; v[4 * h + 3] = va.w;
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < kCooPer; ++t) {
+                const int64_t k = k0 + t;
+                const bool in = k < nnz;
+                r[t] = in ? __ldcs(rows + k) : kNone;
+                c[t] = in ? __ldcs(cols + k) : 0;
+                v[t] = in ? __ldcs(vals + k) : 0.0f;
+            }
+        }
+        // input checks: ids in [0, N), row ids ascending (within the lane and
+        // from the entry before it); an entry out of range adds nothing
+        int prev = __shfl_up_sync(0xffffffffu, r[kCooPer - 1], 1);
+        if (lane == 0) prev = base > 0 ? __ldg(rows + (base - 1)) : INT32_MIN;
+#pragma unroll
+        for (int t = 0; t < kCooPer; ++t) {
+            if (k0 + t >= nnz) continue;
+            if (r[t] < prev) bad |= 2;
+            prev = r[t];
+            if (r[t] < 0 || r[t] >= N || c[t] < 0 || c[t] >= N) {
+                bad |= 1;
+                v[t] = 0.0f;
+                c[t] = 0;
+            }
+        }
+        // runs of equal row ids: runs strictly inside the lane are whole rows
+        const int first = r[0];
+        int cur = r[0];
+        float s_run = 0.0f, head = 0.0f;
+        bool multi = false;
+#pragma unroll
+        for (int t = 0; t < kCooPer; ++t) {
+            const float pv = r[t] != kNone ? __fmul_rn(v[t], __ldg(u + c[t])) : 0.0f;
+            if (r[t] != cur) {
+                if (!multi) head = s_run;                                  // the lane's first run
+                else if (cur >= 0 && cur < N) acc[cur] = s_run;            // a whole row inside the lane
+                multi = true;
+                cur = r[t];
+                s_run = 0.0f;
+            }
+            s_run = __fadd_rn(s_run, pv);
+        }
+        const int last = cur;
+        // inclusive segmented scan of the lanes' last runs: a lane that is one
+        // run throughout continues its predecessor's run of the same row
+        float carry = s_run;
+        bool joins = !multi;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const float cq = __shfl_up_sync(0xffffffffu, carry, o);
+            const int kq = __shfl_up_sync(0xffffffffu, last, o);
+            const int jq = __shfl_up_sync(0xffffffffu, (int)joins, o);
+            if (lane >= o && joins && kq == last) {
+                carry = __fadd_rn(cq, carry);
+                joins = jq != 0;
+            }
+        }
+        const float cin = __shfl_up_sync(0xffffffffu, carry, 1);
+        const int kin = __shfl_up_sync(0xffffffffu, last, 1);
+        const int next_first = __shfl_down_sync(0xffffffffu, first, 1);
+        const int64_t span_end = base + kSpan < nnz ? base + kSpan : nnz;
+        const int left_row = base > 0 ? __ldg(rows + (base - 1)) : INT32_MIN;   // row of the entry before the span
+        const int right_row = span_end < nnz ? __ldg(rows + span_end) : kNone;  // row of the entry after it
+        if (multi && first >= 0 && first < N) {
+            // the lane's first run ends here: add what the lanes before carried in
+            const float h = (lane > 0 && kin == first) ? __fadd_rn(cin, head) : head;
+            if (first == left_row) atomicAdd(acc + first, h);
+            else acc[first] = h;
+        }
+        // the lane's last run ends here unless the next lane starts with it
+        const bool ends_here = lane == 31 || k0 + kCooPer >= span_end || next_first != last;
+        if (ends_here && last >= 0 && last < N) {
+            if (last == left_row || last == right_row) atomicAdd(acc + last, carry);
+            else acc[last] = carry;
+        }
+    }
+    if (bad) atomicOr(err, bad);
+}
+
 // out = dt*acc (SpMVCOO's C[row] = deltat*result) or u + dt*acc.
 // acc and out may be the same buffer (element-wise, same index).
 __global__ void k_scale_add(int64_t n, float dt, const float *acc, const float *u, float *out)
@@ -736,8 +854,15 @@ static int coo_common(int64_t N, int64_t nnz, const int32_t *rows, const int32_t
     PIRO_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * N, s));
     if (nnz > 0) {
         PIRO_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-        k_coo_segsum<<<grid_for(nnz, 256, 8), 256, 0, s>>>(N, nnz, rows, cols, vals, u, out, err);
-        PIRO_CHECK_LAUNCH("k_coo_segsum");
+        const bool al16 = ((reinterpret_cast<uintptr_t>(rows) | reinterpret_cast<uintptr_t>(cols) |
+                            reinterpret_cast<uintptr_t>(vals)) & 15) == 0;
+        if (al16) {
+            k_coo_segsum8<<<grid_for(cdiv(nnz, kCooPer), 256, 8), 256, 0, s>>>(N, nnz, rows, cols, vals, u, out, err);
+            PIRO_CHECK_LAUNCH("k_coo_segsum8");
+        } else {
+            k_coo_segsum<<<grid_for(nnz, 256, 8), 256, 0, s>>>(N, nnz, rows, cols, vals, u, out, err);
+            PIRO_CHECK_LAUNCH("k_coo_segsum");
+        }
     }
     k_scale_add<<<grid_for(N, 256, 8), 256, 0, s>>>(N, dt, out, fe ? u : nullptr, out);
     PIRO_CHECK_LAUNCH("k_scale_add");

@@ -191,6 +191,11 @@ def test_csr_and_coo_steps_on_wide_rows_bitexact(cuda, oracle):
     want_coo = oracle.spmv_coo(N, (rows, col, val), dt, u)
     ops.coo_step_indexed(N, Ad[0], Ad[1], Ad[2], dt, dev(torch, u), out)
     assert f32_bits_equal(h(out), want_coo)
+    # the segmented sum (8 entries per lane, rows across lanes and 256-entry
+    # spans): FP32 tolerance, since it adds in another order
+    ops.coo_spmv(N, (dev(torch, rows), Ad[1], Ad[2]), dt, dev(torch, u), out)
+    scale = np.abs(val).reshape(-1).max() * np.abs(u).max() * lengths.max() * abs(float(dt))
+    np.testing.assert_allclose(h(out), want_coo, rtol=1e-5, atol=1e-6 * scale)
 
 
 def test_csrgeam3_vs_golden(cuda, golden_grids):
