@@ -1021,7 +1021,8 @@ def run_profile_case(args):
     kernels (CSR, matrix-free, fused CSR + setBC, indexed COO, ordered HT), `dense` three DENSE steps at N = 12,288 (a 604 MB
     matrix), `learned` two learned-preconditioner solves of the 128^3 step,
     `batched` two steps of a 64-member batch, `train` four training steps of
-    the network on 8 crops of 34^3 cells."""
+    the network on 8 crops of 34^3 cells, `ht` three ordered hash-table steps
+    at 192^3."""
     import torch
 
     from piro_b200 import ops
@@ -1061,6 +1062,20 @@ def run_profile_case(args):
         print("learned", info.inner_iterations, info.rel_residual)
         s.close()
         net.close()
+    elif args.profile == "ht":
+        n = 192  # 7.1M rows, a 0.85 GB table: larger than L2, small enough to capture
+        N = n ** 3
+        A = ops.csr_laplacian(n, n, n, 3, 1.0)
+        ts = ops.ht_table_size(A[2].numel(), N, 1)
+        keys, vals = ops.ht_build(N, *A, ts)
+        del A
+        order = ops.ht_row_order(N, ts)
+        u = torch.rand(N, device="cuda")
+        out = torch.empty_like(u)
+        for _ in range(3):
+            ops.ht_spmv_ordered(n, n, n, keys, vals, 0.01, order, u, out, fe=True)
+        torch.cuda.synchronize()
+        print("ht ok", ts)
     elif args.profile == "train":
         m, batch = 34, 8
         N = m ** 3
@@ -1118,7 +1133,7 @@ def main():
     ap.add_argument("--impl", default="piro", choices=["piro", "reference"])
     ap.add_argument("--sharded", type=int, default=0, metavar="N",
                     help="one N^3 backward-Euler grid in z-slabs over the ranks (strong scaling) instead of replicas")
-    ap.add_argument("--profile", choices=["be", "spmv", "dense", "learned", "batched", "train"],
+    ap.add_argument("--profile", choices=["be", "spmv", "dense", "learned", "batched", "train", "ht"],
                     help="run a small fixed case for ncu, print no JSON")
     args = ap.parse_args()
     if args.profile:
