@@ -1018,7 +1018,8 @@ def run_sharded(args):
 def run_profile_case(args):
     """Small fixed cases for ncu captures (no timing, no JSON): `be` solves the
     128^3 backward-Euler step twice, `spmv` runs the 256^3 forward-Euler
-    kernels (CSR, matrix-free, fused CSR + setBC, indexed COO, ordered HT), `dense` three DENSE steps at N = 12,288 (a 604 MB
+    kernels (CSR, matrix-free, fused CSR + setBC, indexed COO; about 1.5 GB
+    on the device), `dense` three DENSE steps at N = 12,288 (a 604 MB
     matrix), `learned` two learned-preconditioner solves of the 128^3 step,
     `batched` two steps of a 64-member batch, `train` four training steps of
     the network on 8 crops of 34^3 cells, `ht` three ordered hash-table steps
@@ -1116,11 +1117,6 @@ def run_profile_case(args):
         for _ in range(2):
             ops.coo_step_indexed(N, rowstart, A[1], A[2], 0.01, u, out, fe=True)
         del rows, rowstart
-        ts = ops.ht_table_size(A[2].numel(), N, 1)
-        keys, vals = ops.ht_build(N, *A, ts)
-        order = ops.ht_row_order(N, ts)
-        for _ in range(2):
-            ops.ht_spmv_ordered(nx, ny, nz, keys, vals, 0.01, order, u, out, fe=True)
         torch.cuda.synchronize()
         print("spmv ok")
 
