@@ -31,8 +31,8 @@
 //
 // Warp roles (192 threads): warps 0-3 read the accumulator (TMEM lanes
 // 32w..32w+31), apply GELU and store; warp 4 lane 0 issues the TMA loads;
-// warp 5 lane 0 issues the MMAs.  Two TMEM accumulators (2 x 16 columns)
-// overlap a tile's epilogue with the next tile's MMAs.  mbarriers: full[slot]
+// warp 5 lane 0 issues the MMAs.  Four TMEM accumulators (4 x 16 columns)
+// let the MMAs of the next tiles run while a tile's epilogue reads its own.  mbarriers: full[slot]
 // (TMA bytes landed), empty[slot] (the MMAs reading a plane completed),
 // acc_full[b] (a tile's MMAs completed), acc_empty[b] (its epilogue read it).
 // Every wait is bounded: on timeout the kernel raises *err and every role
@@ -58,7 +58,9 @@ constexpr int kPlaneBytes = 3 * kLineStride;  // the 3 line blocks (dy = -1, 0, 
 constexpr int kWBytes = 27 * 512;             // one layer's weights: per tap [group][co 16][8 ci] BF16
 constexpr int kThreads = 192;
 constexpr int kBarOff = kSlots * kPlaneBytes + kWBytes;
-constexpr int kSmemBytes = kBarOff + 16 * 8 + 16 + 128;  // + barriers, TMEM address, alignment slack
+constexpr int kAcc = 4;                       // TMEM accumulators (16 columns each) per CTA
+constexpr int kBarSlots = 2 * kSlots + 2 * kAcc + 1;  // full, empty, acc_full, acc_empty, drain
+constexpr int kSmemBytes = kBarOff + kBarSlots * 8 + 16 + 128;  // + barriers, TMEM address, alignment slack
 constexpr long long kSpin = 1ll << 24;        // polls before a wait gives up
 
 struct Args {
@@ -207,13 +209,13 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
     unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
     const uint32_t planes_s = smem_u32(sm);
     const uint32_t w_s = planes_s + kSlots * kPlaneBytes;
-    const uint32_t bar_s = planes_s + kBarOff;  // full[4], empty[4], acc_full[2], acc_empty[2]
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sm + kBarOff + 16 * 8);
+    const uint32_t bar_s = planes_s + kBarOff;  // full[kSlots], empty[kSlots], acc_full[kAcc], acc_empty[kAcc], drain
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sm + kBarOff + kBarSlots * 8);
     auto full = [&](int i) { return bar_s + 8u * i; };
     auto empty = [&](int i) { return bar_s + 8u * (kSlots + i); };
     auto accf = [&](int b) { return bar_s + 8u * (2 * kSlots + b); };
-    auto acce = [&](int b) { return bar_s + 8u * (2 * kSlots + 2 + b); };
-    const uint32_t drain_s = bar_s + 8u * (2 * kSlots + 4);
+    auto acce = [&](int b) { return bar_s + 8u * (2 * kSlots + kAcc + b); };
+    const uint32_t drain_s = bar_s + 8u * (2 * kSlots + 2 * kAcc);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t boff = (int64_t)blockIdx.y * a.N;  // batch member: rows b*N ..
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
             mbar_init(full(i), 1);
             mbar_init(empty(i), 1);
         }
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < kAcc; ++b) {
             mbar_init(accf(b), 1);
             mbar_init(acce(b), 4);
         }
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(32)
+                     "r"(kAcc * 16)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -281,8 +283,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
                         ok = mbar_wait(full(waited % kSlots), (waited / kSlots) & 1, a.err);
                         ++waited;
                     }
-                    const int buf = j & 1;
-                    if (ok && j >= 2) ok = mbar_wait(acce(buf), ((j >> 1) - 1) & 1, a.err);
+                    const int buf = j % kAcc;
+                    if (ok && j >= kAcc) ok = mbar_wait(acce(buf), ((j / kAcc) - 1) & 1, a.err);
                     if (!ok) break;
                     fence_after();
                     const uint32_t d_tmem = tmem + (uint32_t)(buf * 16);
@@ -310,8 +312,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
         } else {
             // epilogue: warp w holds tile rows 32w .. 32w+31
             for (int j = 0; j < P; ++j) {
-                const int buf = j & 1;
-                if (!mbar_wait(accf(buf), (j >> 1) & 1, a.err)) break;
+                const int buf = j % kAcc;
+                if (!mbar_wait(accf(buf), (j / kAcc) & 1, a.err)) break;
                 fence_after();
                 uint32_t v[16];
                 tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * 16), v);
@@ -375,7 +377,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
     __syncthreads();
     if (warp == 0) {
         fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kAcc * 16) : "memory");
     }
 }
 
