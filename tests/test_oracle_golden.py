@@ -177,3 +177,27 @@ def test_case_oracle_runs_every_test_case(oracle):
     T = r["fields"][1]
     assert np.all(T[idx[fs[5]:fs[6]]] == np.float32(1.0))
     assert T[0] == 0.0
+
+
+@pytest.mark.skipif(not __import__("oracle.oracle", fromlist=["ref_available"]).ref_available(),
+                    reason="the reference build (oracle/_ref) is absent")
+def test_reference_spmv_over_threads_equals_sequential(oracle):
+    """The CPU baseline runs PIRO's SpMVCSR/SpMVCOO/SpMVHT NDRanges over the
+    OpenMP threads; every work-item writes only its own row, so the result
+    must equal the sequential NDRange bit for bit."""
+    R = oracle.Ref()
+    nx, ny, nz = 9, 8, 7
+    N = nx * ny * nz
+    A = oracle.laplacian(nx, ny, nz, 3, np.float32(1.0))
+    u = np.random.default_rng(2).random(N).astype(np.float32)
+    seq = R.spmvcsr(nx, ny, nz, A, 0.01, u, np.zeros(N, np.float32))
+    assert np.array_equal(seq.view(np.uint32), R.spmv_par("csr", nx, ny, nz, A, 0.01, u).view(np.uint32))
+    rows = np.repeat(np.arange(N, dtype=np.int32), np.diff(A[0]))
+    seq = R.spmvcoo(nx, ny, nz, (rows, A[1], A[2]), 0.01, u)
+    par = R.spmv_par("coo", nx, ny, nz, (rows, A[1], A[2]), 0.01, u)
+    assert np.array_equal(seq.view(np.uint32), par.view(np.uint32))
+    ts = oracle.ht_table_size_build(len(A[2]))
+    keys, vals = oracle.ht_build(N, *A, ts)
+    seq = R.spmvht(N, keys.astype(np.int32), vals, 0.01, u)
+    par = R.spmv_par("ht", nx, ny, nz, (keys.astype(np.int32), vals), 0.01, u)
+    assert np.array_equal(seq.view(np.uint32), par.view(np.uint32))
