@@ -552,6 +552,15 @@ int piro_batch_member_info(piro_batch *s, int *status, int *sweeps, int *inner, 
  * each tile size (2048 .. 16384 cells) and blocks-per-SM (1, 2, 4) the
  * occupancy allows and keeps the fastest. */
 int piro_batch_autotune(piro_batch *s, double rtol, int *tile, int *blocks_per_sm);
+/* Schedule of the step: 0 lockstep (k_batch_step: every backward-Euler
+ * member advances one phase per grid-wide round), 1 grouped (k_batch_groups:
+ * each large member on a group of CTAs of its own with group-local barriers,
+ * small members packed onto the other CTAs; no grid-wide barrier).  The
+ * autotuner picks the faster; piro_batch_set_schedule forces one, with the
+ * given CTAs per SM.  Results agree to rounding (the same arithmetic per
+ * member, sums over other partitions). */
+int piro_batch_schedule(piro_batch *s, int *grouped);
+int piro_batch_set_schedule(piro_batch *s, int grouped, int blocks_per_sm);
 int piro_batch_destroy(piro_batch *s);
 
 /* Reference JLI iteration (scheme 12 + solver 40, src/kernelprocess.cpp:123-209)

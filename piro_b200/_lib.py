@@ -139,6 +139,8 @@ SIGNATURES = {
     "piro_batch_step": (i32, [vp, i32, f64, C.POINTER(C.c_double)]),
     "piro_batch_member_info": (i32, [vp, vp, vp, vp, vp]),
     "piro_batch_autotune": (i32, [vp, f64, pint, pint]),
+    "piro_batch_schedule": (i32, [vp, pint]),
+    "piro_batch_set_schedule": (i32, [vp, i32, i32]),
     "piro_batch_destroy": (i32, [vp]),
     "piro_open": (i32, [C.c_char_p, C.c_char_p, C.POINTER(vp)]),
     "piro_close": (None, [vp]),

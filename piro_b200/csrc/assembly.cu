@@ -117,9 +117,12 @@ __global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, 
                                                              float *__restrict__ val, int64_t row0,
                                                              int64_t col_shift)
 {
-    __shared__ int32_t s_col[kRowsPerBlock * kMaxPerRow];
-    __shared__ float s_val[kRowsPerBlock * kMaxPerRow];
-    __shared__ int32_t s_row[kRowsPerBlock * kMaxPerRow];
+    // staged at index (global entry index) mod 4 + position in the block, so
+    // that shared and global indices agree mod 4 and both sides move as
+    // aligned 16-byte vectors
+    __shared__ __align__(16) int32_t s_col[kRowsPerBlock * kMaxPerRow + 4];
+    __shared__ __align__(16) float s_val[kRowsPerBlock * kMaxPerRow + 4];
+    __shared__ __align__(16) int32_t s_row[kRowsPerBlock * kMaxPerRow + 4];
     __shared__ int64_t s_base, s_end;
     int64_t base0;
     {
@@ -150,7 +153,7 @@ __global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, 
             int32_t c[kMaxPerRow];
             float v[kMaxPerRow];
             const int n = lap_row(i, g, scheme, vself, vnb, c, v);
-            const int off = (int)(p - s_base);
+            const int off = (int)(p - s_base) + (vec_ok ? (int)((s_base - base0) & 3) : 0);
             for (int t = 0; t < n; ++t) {
                 s_col[off + t] = (int32_t)(c[t] - col_shift);
                 s_val[off + t] = v[t];
@@ -162,29 +165,27 @@ __global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, 
             }
         }
         __syncthreads();
-        // the block's entries leave as 16-byte stores from the first entry
-        // whose index is a multiple of 4 on (scalar head and tail), when the
-        // arrays themselves are 16-byte aligned
+        // the block's entries leave as 16-byte stores (scalar head and tail)
+        // when the arrays are 16-byte aligned
         const int cnt = (int)(s_end - s_base);
-        const int64_t dst = s_base - base0;
-        int head = vec_ok ? (int)((4 - (dst & 3)) & 3) : cnt;
-        head = head < cnt ? head : cnt;
-        const int body = (cnt - head) & ~3;
-        for (int t = threadIdx.x; t < head; t += blockDim.x) {
-            col[dst + t] = s_col[t];
-            val[dst + t] = s_val[t];
-            if (rows) rows[dst + t] = s_row[t];
+        const int sh = vec_ok ? (int)((s_base - base0) & 3) : 0;  // shared index of the first entry
+        const int64_t g0 = s_base - base0 - sh;                   // global index of shared index 0
+        const int j0 = vec_ok ? (sh + 3) & ~3 : sh + cnt, j1 = vec_ok ? (sh + cnt) & ~3 : sh + cnt;
+        const int head_end = j0 < sh + cnt ? j0 : sh + cnt;
+        for (int j = sh + threadIdx.x; j < head_end; j += blockDim.x) {
+            col[g0 + j] = s_col[j];
+            val[g0 + j] = s_val[j];
+            if (rows) rows[g0 + j] = s_row[j];
         }
-        for (int t = head + 4 * threadIdx.x; t < head + body; t += 4 * blockDim.x) {
-            *reinterpret_cast<int4 *>(col + dst + t) = make_int4(s_col[t], s_col[t + 1], s_col[t + 2], s_col[t + 3]);
-            *reinterpret_cast<float4 *>(val + dst + t) = make_float4(s_val[t], s_val[t + 1], s_val[t + 2], s_val[t + 3]);
-            if (rows)
-                *reinterpret_cast<int4 *>(rows + dst + t) = make_int4(s_row[t], s_row[t + 1], s_row[t + 2], s_row[t + 3]);
+        for (int j = j0 + 4 * threadIdx.x; j < j1; j += 4 * blockDim.x) {
+            *reinterpret_cast<int4 *>(col + g0 + j) = *reinterpret_cast<const int4 *>(s_col + j);
+            *reinterpret_cast<float4 *>(val + g0 + j) = *reinterpret_cast<const float4 *>(s_val + j);
+            if (rows) *reinterpret_cast<int4 *>(rows + g0 + j) = *reinterpret_cast<const int4 *>(s_row + j);
         }
-        for (int t = head + body + threadIdx.x; t < cnt; t += blockDim.x) {
-            col[dst + t] = s_col[t];
-            val[dst + t] = s_val[t];
-            if (rows) rows[dst + t] = s_row[t];
+        for (int j = (j1 > head_end ? j1 : head_end) + threadIdx.x; j < sh + cnt; j += blockDim.x) {
+            col[g0 + j] = s_col[j];
+            val[g0 + j] = s_val[j];
+            if (rows) rows[g0 + j] = s_row[j];
         }
         __syncthreads();
     }

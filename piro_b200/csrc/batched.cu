@@ -452,6 +452,306 @@ __global__ void __launch_bounds__(kThreads) k_batch_step(BArgs A)
     }
 }
 
+// ---------------------------------------------------------------------------
+// The grouped step (k_batch_groups): the same arithmetic as k_batch_step per
+// member, without grid-wide lockstep.  Forward-Euler tiles are stepped by all
+// CTAs first.  Each backward-Euler member is a job: a large member gets a
+// contiguous group of CTAs (about one per average CTA's share of the cells)
+// that split its cells into 64-cell aligned chunks and meet at a group
+// barrier -- a monotonic arrival counter per job -- between phases; small
+// members are packed onto the other CTAs (longest first, to the least loaded)
+// and solved one after another with block barriers only.  No CTA waits for
+// a member it does not work on, so members finish at their own pace and the
+// step ends when the most loaded CTA is done.  Group sums are per-CTA block
+// sums read by every CTA of the group in rank order (identical decisions in
+// all of them, results independent of scheduling).  Each phase writes its own
+// partial slots (RESID 0-3, the operator step 4, the update 5-6): a CTA that
+// runs ahead cannot overwrite a sum another CTA of its group has not read,
+// since it reaches the next writes of a slot only after that CTA arrived at
+// the barrier that follows the read.
+struct BJob {
+    int member;
+    int gbase, gsize;  // first CTA of the group and its CTAs
+    int part_off;      // first double of its partials: 7 slots x gsize
+};
+
+struct GArgs {
+    const BMember *mem;
+    const int *fe_tile_m;
+    const int64_t *fe_tile_s;
+    int nfe, tile;
+    const BJob *jobs;
+    const int *cta_ptr, *cta_jobs;  // CTA c works on jobs cta_jobs[cta_ptr[c] .. cta_ptr[c+1])
+    unsigned *job_bar;              // arrival counters (zeroed before the launch)
+    double *job_part;
+    const float *u;
+    float *out, *b, *r, *p0, *p1, *q, *d;
+    double *x64;
+    BState *st;
+    BarrierState *bar;  // err: a group barrier wait ran out
+    double rtol, inner_floor;
+    int max_sweeps, max_inner;
+    long long spin_limit;
+};
+
+// Group barrier of one job: arrivals only grow within a launch; barrier k of
+// the job waits for k * gsize of them.  A single-CTA group is a block barrier.
+__device__ __forceinline__ bool group_sync(const GArgs &A, unsigned *count, int gsize, unsigned &target, int *s_ok)
+{
+    __syncthreads();
+    if (gsize == 1) return true;
+    target += (unsigned)gsize;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(count, 1u);
+        volatile unsigned *vc = count;
+        volatile int *verr = &A.bar->err;
+        int ok = 1;
+        long long spins = 0;
+        while ((int)(*vc - target) < 0) {
+            if (*verr || ++spins > A.spin_limit) {
+                ok = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        if (*verr) ok = 0;
+        if (!ok) atomicExch(&A.bar->err, 1);
+        __threadfence();
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+// kN group sums: this CTA's block sums into slots first.. (rank q), then,
+// after the group barrier, every CTA adds the gsize partials of each slot in
+// rank order.  Returns false if the barrier wait ran out.
+template <int kN>
+__device__ __forceinline__ bool group_sums(const GArgs &A, double *part, int first, int q, int gsize, unsigned *count,
+                                           unsigned &target, double (&v)[kN], double *s_red, double *s_tot,
+                                           int *s_ok)
+{
+    block_sums<kN>(v, s_red);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int t = 0; t < kN; ++t) part[(first + t) * gsize + q] = v[t];
+    if (!group_sync(A, count, gsize, target, s_ok)) return false;
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+#pragma unroll
+        for (int t = 0; t < kN; ++t) {
+            double a = 0.0;
+            for (int k = lane; k < gsize; k += 32) a += ((volatile const double *)part)[(first + t) * gsize + k];
+            a = warp_sum(a);
+            if (lane == 0) s_tot[t] = a;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < kN; ++t) v[t] = s_tot[t];
+    __syncthreads();
+    return true;
+}
+
+__global__ void __launch_bounds__(kThreads) k_batch_groups(GArgs A)
+{
+    __shared__ double s_red[4 * 32];
+    __shared__ double s_tot[4];
+    __shared__ int s_ok;
+    // forward-Euler members: one pass over their tiles by every CTA
+    for (int t = blockIdx.x; t < A.nfe; t += gridDim.x) {
+        const BMember m = A.mem[A.fe_tile_m[t]];
+        const int64_t s0 = A.fe_tile_s[t], s1 = min(s0 + (int64_t)A.tile, m.N);
+        const int64_t sxy = (int64_t)m.g.nx * m.g.ny;
+        const float *u = A.u + m.off;
+        float *o = A.out + m.off;
+        for (int64_t i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+            const float c = u[i];
+            if (m.g.interior(i)) {
+                const float c2 = __fmul_rn(2.0f, c);
+                const float lx = __fsub_rn(__fadd_rn(u[i + 1], u[i - 1]), c2);
+                const float ly = __fsub_rn(__fadd_rn(u[i + m.g.nx], u[i - m.g.nx]), c2);
+                const float lz = __fsub_rn(__fadd_rn(u[i + sxy], u[i - sxy]), c2);
+                const float lap = __fadd_rn(__fadd_rn(lx, ly), lz);
+                o[i] = __fadd_rn(c, __fmul_rn(m.dt, __fmul_rn(m.alpha, lap)));
+            } else {
+                o[i] = c;
+            }
+        }
+    }
+    // backward-Euler jobs of this CTA
+    for (int jj = A.cta_ptr[blockIdx.x]; jj < A.cta_ptr[blockIdx.x + 1]; ++jj) {
+        const BJob J = A.jobs[A.cta_jobs[jj]];
+        const BMember m = A.mem[J.member];
+        const int G = J.gsize, q = (int)blockIdx.x - J.gbase;
+        unsigned *count = A.job_bar + A.cta_jobs[jj];
+        double *part = A.job_part + J.part_off;
+        unsigned target = 0;
+        const int64_t chunk = cdiv(cdiv(m.N, G), 64) * 64;
+        const int64_t c0 = min((int64_t)q * chunk, m.N), c1 = min(c0 + chunk, m.N);
+        const int64_t sxy = (int64_t)m.g.nx * m.g.ny;
+        const int nx = m.g.nx;
+        const float *uu = A.u + m.off;
+        float *bb = A.b + m.off, *rr = A.r + m.off, *dd = A.d + m.off, *qq = A.q + m.off, *oo = A.out + m.off;
+        double *x = A.x64 + m.off;
+        for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+            const float v = uu[i];
+            bb[i] = v;
+            x[i] = (double)v;
+            dd[i] = 0.0f;
+        }
+        BState s{};
+        s.status = PIRO_ERR_NOT_CONVERGED;
+        s.prev_rel = INFINITY;
+        bool ok = group_sync(A, count, G, target, &s_ok);
+        bool finished = false;
+        while (ok && !finished) {
+            // RESID: r = b - A (x64 + d) in FP64 on the chunk
+            double v[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+                if (!m.g.interior(i)) {
+                    rr[i] = 0.0f;
+                    continue;
+                }
+                const double xc = x[i] + (double)dd[i];
+                const double nb = ((x[i - 1] + (double)dd[i - 1]) + (x[i + 1] + (double)dd[i + 1])) +
+                                  ((x[i - nx] + (double)dd[i - nx]) + (x[i + nx] + (double)dd[i + nx])) +
+                                  ((x[i - sxy] + (double)dd[i - sxy]) + (x[i + sxy] + (double)dd[i + sxy]));
+                const double bi = (double)bb[i];
+                const double ri = bi - (m.cd64 * xc + m.co64 * nb);
+                const float rf = (float)ri;
+                rr[i] = rf;
+                v[0] += ri * ri;
+                v[1] += bi * bi;
+                v[2] += (double)rf * (double)(rf * m.dinv);
+                v[3] += (double)rf * (double)rf;
+            }
+            if (!(ok = group_sums<4>(A, part, 0, q, G, count, target, v, s_red, s_tot, &s_ok))) break;
+            const double bn = sqrt(v[1]) > 0.0 ? sqrt(v[1]) : 1.0;
+            const double rel = sqrt(v[0]) / bn;
+            s.rel = rel;
+            if (!isfinite(rel)) {
+                s.status = PIRO_STATUS_STALLED;
+                finished = true;
+            } else if (rel <= A.rtol) {
+                s.status = PIRO_OK;
+                finished = true;
+            } else if (s.sweep >= A.max_sweeps || s.inner_total >= A.max_inner) {
+                s.status = PIRO_ERR_NOT_CONVERGED;
+                finished = true;
+            } else if (s.sweep > 0 && rel > 0.5 * s.prev_rel) {
+                s.status = PIRO_STATUS_STALLED;
+                finished = true;
+            }
+            // the pending correction joins x (read next by the sweep after this one)
+            for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+                const double xn = x[i] + (double)dd[i];
+                x[i] = xn;
+                dd[i] = 0.0f;
+                if (finished) oo[i] = (float)xn;
+            }
+            if (finished || v[3] <= 0.0) {
+                if (!finished) {
+                    for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) oo[i] = (float)x[i];
+                    finished = true;
+                }
+                break;
+            }
+            double itol = rel > 0.0 ? 0.5 * A.rtol / rel : 1.0;
+            itol = itol > 0.1 ? 0.1 : itol;
+            itol = itol < A.inner_floor ? A.inner_floor : itol;
+            s.tol2 = itol * itol;
+            s.rz = v[2];
+            s.rr0 = v[3];
+            s.beta = 0.0;
+            s.it = 0;
+            s.prev_rel = rel;
+            s.sweep += 1;
+            // CG on the correction d
+            while (true) {
+                // V1: p = z + beta p_old (z = r / A_rr), q = A p, <p, q>
+                const float beta = (float)s.beta;
+                const float *po = ((s.it & 1) ? A.p1 : A.p0) + m.off;
+                float *pn = ((s.it & 1) ? A.p0 : A.p1) + m.off;
+                double w[1] = {0.0};
+                for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+                    if (!m.g.interior(i)) {
+                        pn[i] = 0.0f;
+                        qq[i] = 0.0f;
+                        continue;
+                    }
+                    auto pv = [&](int64_t j) { return rr[j] * m.dinv + beta * po[j]; };
+                    const float c = pv(i);
+                    const float nb = ((pv(i - 1) + pv(i + 1)) + (pv(i - nx) + pv(i + nx))) + (pv(i - sxy) + pv(i + sxy));
+                    const float qv = m.cd * c + m.co * nb;
+                    pn[i] = c;
+                    qq[i] = qv;
+                    w[0] += (double)c * (double)qv;
+                }
+                if (!(ok = group_sums<1>(A, part, 4, q, G, count, target, w, s_red, s_tot, &s_ok))) break;
+                const double a = s.rz / w[0];
+                if (!isfinite(a) || w[0] <= 0.0) {
+                    // breakdown: the member ends with the correction it has (as k_batch_step's S1)
+                    s.status = PIRO_STATUS_STALLED;
+                    for (int64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+                        const double xn = x[i] + (double)dd[i];
+                        x[i] = xn;
+                        dd[i] = 0.0f;
+                        oo[i] = (float)xn;
+                    }
+                    finished = true;
+                    break;
+                }
+                // V2: d += a p, r -= a q; <r, z>, |r|^2 (boundary cells carry p = q = r = 0)
+                const float fa = (float)a;
+                double u2[2] = {0.0, 0.0};
+                const int64_t g0 = c0 >> 2, g1 = c1 >> 2;  // c0 % 4 == 0
+                for (int64_t gi = g0 + threadIdx.x; gi < g1; gi += blockDim.x) {
+                    const float4 p4 = reinterpret_cast<const float4 *>(pn)[gi];
+                    const float4 q4 = reinterpret_cast<const float4 *>(qq)[gi];
+                    float4 d4 = reinterpret_cast<float4 *>(dd)[gi];
+                    float4 r4 = reinterpret_cast<float4 *>(rr)[gi];
+                    d4.x += fa * p4.x; d4.y += fa * p4.y; d4.z += fa * p4.z; d4.w += fa * p4.w;
+                    r4.x = r4.x - fa * q4.x; r4.y = r4.y - fa * q4.y; r4.z = r4.z - fa * q4.z; r4.w = r4.w - fa * q4.w;
+                    reinterpret_cast<float4 *>(dd)[gi] = d4;
+                    reinterpret_cast<float4 *>(rr)[gi] = r4;
+                    u2[0] += (double)r4.x * (double)(r4.x * m.dinv) + (double)r4.y * (double)(r4.y * m.dinv) +
+                             (double)r4.z * (double)(r4.z * m.dinv) + (double)r4.w * (double)(r4.w * m.dinv);
+                    u2[1] += (double)r4.x * (double)r4.x + (double)r4.y * (double)r4.y + (double)r4.z * (double)r4.z +
+                             (double)r4.w * (double)r4.w;
+                }
+                for (int64_t i = (g1 << 2) + threadIdx.x; i < c1; i += blockDim.x) {
+                    dd[i] += fa * pn[i];
+                    const float ri = rr[i] - fa * qq[i];
+                    rr[i] = ri;
+                    u2[0] += (double)ri * (double)(ri * m.dinv);
+                    u2[1] += (double)ri * (double)ri;
+                }
+                if (!(ok = group_sums<2>(A, part, 5, q, G, count, target, u2, s_red, s_tot, &s_ok))) break;
+                s.it += 1;
+                s.inner_total += 1;
+                const double beta_n = u2[0] / s.rz;
+                if (!isfinite(u2[1]) || !isfinite(beta_n)) {
+                    s.status = PIRO_STATUS_STALLED;
+                    break;
+                }
+                if (u2[1] <= s.tol2 * s.rr0 || s.inner_total >= A.max_inner) break;
+                s.beta = beta_n;
+                s.rz = u2[0];
+            }
+            // the update's group sum was the barrier: every CTA's d and r are
+            // written before the residual reads its neighbours
+            if (!ok) break;
+        }
+        if (q == 0 && threadIdx.x == 0) {
+            s.mode = kDone;
+            A.st[J.member] = s;
+        }
+        if (!ok) return;
+    }
+}
+
 }  // namespace
 }  // namespace piro
 
@@ -483,7 +783,115 @@ struct piro_batch {
     double step_ms = 0.0;
     long long steps = 0;
     double rtol = 1e-8;
+    // the grouped step (k_batch_groups): used when grouped = 1
+    int grouped = 0;
+    unsigned grid_g = 0;
+    int njobs = 0;
+    BJob *d_jobs = nullptr;
+    int *d_cta_ptr = nullptr, *d_cta_jobs = nullptr;
+    unsigned *d_job_bar = nullptr;
+    double *d_job_part = nullptr;
 };
+
+static void batch_free_groups(piro_batch *s)
+{
+    cudaFree(s->d_jobs);
+    cudaFree(s->d_cta_ptr);
+    cudaFree(s->d_cta_jobs);
+    cudaFree(s->d_job_bar);
+    cudaFree(s->d_job_part);
+    s->d_jobs = nullptr;
+    s->d_cta_ptr = s->d_cta_jobs = nullptr;
+    s->d_job_bar = nullptr;
+    s->d_job_part = nullptr;
+    s->njobs = 0;
+    s->grid_g = 0;
+}
+
+// Jobs of the grouped step for a grid of sm_count * blocks_per_sm CTAs: with
+// T the backward-Euler cells per CTA on average, a member of at least 2T
+// cells gets floor(cells / T) CTAs of its own (T grows until the groups
+// leave a CTA for the small members); the others go, largest first, to the
+// least loaded of the remaining CTAs.
+static int batch_groups_setup(piro_batch *s, int blocks_per_sm)
+{
+    batch_free_groups(s);
+    int per_sm = 0;
+    PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_groups, kThreads, 0));
+    if (per_sm < 1) {
+        set_error("piro_batch: the grouped step cannot be resident");
+        return PIRO_ERR_CUDA;
+    }
+    const int C = sm_count() * std::min(per_sm, blocks_per_sm);
+    std::vector<int> be;
+    double total = 0.0;
+    for (int k = 0; k < s->M; ++k)
+        if (s->mem[k].scheme == 1) {
+            be.push_back(k);
+            total += (double)s->mem[k].N;
+        }
+    std::sort(be.begin(), be.end(), [&](int a, int b) { return s->mem[a].N > s->mem[b].N || (s->mem[a].N == s->mem[b].N && a < b); });
+    double T = std::max(total / C, 1.0);
+    std::vector<int> gsz(be.size(), 1);
+    for (int guard = 0; guard < 64; ++guard) {
+        int used = 0, small = 0;
+        for (size_t i = 0; i < be.size(); ++i) {
+            const int g = (int)std::floor((double)s->mem[be[i]].N / T);
+            gsz[i] = g >= 2 ? g : 1;
+            if (gsz[i] > 1) used += gsz[i];
+            else ++small;
+        }
+        if (used + (small > 0 ? 1 : 0) <= C) break;
+        T *= 1.25;
+    }
+    std::vector<BJob> jobs;
+    std::vector<std::vector<int>> cta(C);
+    int next = 0, part = 0;
+    for (size_t i = 0; i < be.size(); ++i) {
+        if (gsz[i] < 2) continue;
+        BJob J{be[i], next, gsz[i], part};
+        for (int c = next; c < next + gsz[i]; ++c) cta[c].push_back((int)jobs.size());
+        jobs.push_back(J);
+        next += gsz[i];
+        part += 7 * gsz[i];
+    }
+    std::vector<double> load(C, 0.0);
+    for (size_t i = 0; i < be.size(); ++i) {
+        if (gsz[i] >= 2) continue;
+        int best = next;
+        for (int c = next + 1; c < C; ++c)
+            if (load[c] < load[best]) best = c;
+        BJob J{be[i], best, 1, part};
+        cta[best].push_back((int)jobs.size());
+        jobs.push_back(J);
+        load[best] += (double)s->mem[be[i]].N;
+        part += 7;
+    }
+    std::vector<int> ptr(C + 1, 0), list;
+    for (int c = 0; c < C; ++c) {
+        ptr[c] = (int)list.size();
+        list.insert(list.end(), cta[c].begin(), cta[c].end());
+    }
+    ptr[C] = (int)list.size();
+    auto up = [](void **dst, const void *src, size_t bytes) -> cudaError_t {
+        cudaError_t e = cudaMalloc(dst, bytes > 0 ? bytes : 8);
+        if (e == cudaSuccess && bytes > 0) e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+        return e;
+    };
+    cudaError_t e = up((void **)&s->d_jobs, jobs.data(), jobs.size() * sizeof(BJob));
+    if (e == cudaSuccess) e = up((void **)&s->d_cta_ptr, ptr.data(), ptr.size() * sizeof(int));
+    if (e == cudaSuccess) e = up((void **)&s->d_cta_jobs, list.data(), list.size() * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_job_bar, sizeof(unsigned) * std::max<size_t>(1, jobs.size()));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_job_part, sizeof(double) * std::max(1, part));
+    if (e != cudaSuccess) {
+        batch_free_groups(s);
+        set_error("piro_batch: grouped step setup failed: %s", cudaGetErrorString(e));
+        return PIRO_ERR_CUDA;
+    }
+    s->njobs = (int)jobs.size();
+    s->grid_g = (unsigned)C;
+    return PIRO_OK;
+}
 
 static void batch_drop_graph(piro_batch *s)
 {
@@ -661,8 +1069,45 @@ extern "C" int piro_batch_field_ptr(piro_batch *s, float **u)
     return PIRO_OK;
 }
 
+static int batch_launch_groups(piro_batch *s, const float *u, float *out, cudaStream_t st)
+{
+    GArgs A;
+    A.mem = s->d_mem;
+    A.fe_tile_m = s->d_fe_m;
+    A.fe_tile_s = s->d_fe_s;
+    A.nfe = s->nfe;
+    A.tile = s->tile;
+    A.jobs = s->d_jobs;
+    A.cta_ptr = s->d_cta_ptr;
+    A.cta_jobs = s->d_cta_jobs;
+    A.job_bar = s->d_job_bar;
+    A.job_part = s->d_job_part;
+    A.u = u;
+    A.out = out;
+    A.b = s->b;
+    A.r = s->r;
+    A.p0 = s->p0;
+    A.p1 = s->p1;
+    A.q = s->q;
+    A.d = s->d;
+    A.x64 = s->x64;
+    A.st = s->st;
+    A.bar = s->bar;
+    A.rtol = s->rtol;
+    A.inner_floor = 1e-6;
+    A.max_sweeps = 20;
+    A.max_inner = 20000;
+    A.spin_limit = wait_limit(1ll << 22);  // ~2 s of polling per barrier wait
+    void *args[] = {&A};
+    PIRO_CUDA(cudaMemsetAsync(s->bar, 0, sizeof(BarrierState), st));
+    PIRO_CUDA(cudaMemsetAsync(s->d_job_bar, 0, sizeof(unsigned) * (size_t)std::max(1, s->njobs), st));
+    PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_batch_groups, dim3(s->grid_g), dim3(kThreads), args, 0, st));
+    return PIRO_OK;
+}
+
 static int batch_launch(piro_batch *s, const float *u, float *out, cudaStream_t st)
 {
+    if (s->grouped) return batch_launch_groups(s, u, out, st);
     BArgs A;
     A.mem = s->d_mem;
     A.M = s->M;
@@ -782,11 +1227,13 @@ extern "C" int piro_batch_member_info(piro_batch *s, int *status, int *sweeps, i
 }
 
 // Autotuner: time one step (from the current fields, result discarded) for
-// each tile size and blocks-per-SM candidate and keep the fastest.
+// each tile size and blocks-per-SM candidate of the lockstep step and for the
+// grouped step at 2 and 4 CTAs per SM, and keep the fastest.
 extern "C" int piro_batch_autotune(piro_batch *s, double rtol, int *tile_out, int *blocks_per_sm_out)
 {
     PIRO_ARG(s && rtol > 0.0, "piro_batch_autotune: bad arguments");
     s->rtol = rtol;
+    s->grouped = 0;  // the lockstep candidates first
     const int tiles[] = {2048, 4096, 8192, 16384};
     const int bps[] = {1, 2, 4};
     double best = INFINITY;
@@ -811,16 +1258,73 @@ extern "C" int piro_batch_autotune(piro_batch *s, double rtol, int *tile_out, in
                 bb = b;
             }
         }
+    // the grouped step (FE tiles of the best tiling), 2 or 4 CTAs per SM
     int rc = batch_tiles(s, bt, bb);
     if (rc) return rc;
+    int bg = 0;
+    for (int b : {2, 4}) {
+        rc = batch_groups_setup(s, b);
+        if (rc) return rc;
+        s->grouped = 1;
+        float ms = INFINITY;
+        for (int rep = 0; rep < 2; ++rep) {
+            PIRO_CUDA(cudaEventRecord(s->e0, s->stream));
+            rc = batch_launch(s, s->f[s->cur], s->f[s->cur ^ 1], s->stream);
+            if (rc) {
+                s->grouped = 0;
+                return rc;
+            }
+            PIRO_CUDA(cudaEventRecord(s->e1, s->stream));
+            PIRO_CUDA(cudaStreamSynchronize(s->stream));
+            PIRO_CUDA(cudaEventElapsedTime(&ms, s->e0, s->e1));
+        }
+        s->grouped = 0;
+        if (ms < best) {
+            best = ms;
+            bg = b;
+        }
+    }
+    if (bg) {
+        rc = batch_groups_setup(s, bg);
+        if (rc) return rc;
+        s->grouped = 1;
+        bb = bg;
+    } else {
+        batch_free_groups(s);
+    }
+    batch_drop_graph(s);
     if (tile_out) *tile_out = bt;
     if (blocks_per_sm_out) *blocks_per_sm_out = bb;
+    return PIRO_OK;
+}
+
+extern "C" int piro_batch_schedule(piro_batch *s, int *grouped)
+{
+    PIRO_ARG(s && grouped, "piro_batch_schedule: bad arguments");
+    *grouped = s->grouped;
+    return PIRO_OK;
+}
+
+extern "C" int piro_batch_set_schedule(piro_batch *s, int grouped, int blocks_per_sm)
+{
+    PIRO_ARG(s && (grouped == 0 || grouped == 1) && blocks_per_sm >= 1, "piro_batch_set_schedule: bad arguments");
+    batch_drop_graph(s);
+    if (grouped) {
+        int rc = batch_groups_setup(s, blocks_per_sm);
+        if (rc) return rc;
+    } else {
+        int rc = batch_tiles(s, s->tile, blocks_per_sm);
+        if (rc) return rc;
+        batch_free_groups(s);
+    }
+    s->grouped = grouped;
     return PIRO_OK;
 }
 
 extern "C" int piro_batch_destroy(piro_batch *s)
 {
     if (!s) return PIRO_OK;
+    batch_free_groups(s);
     batch_free_tiles(s);
     cudaFree(s->d_mem);
     cudaFree(s->f[0]);

@@ -31,8 +31,8 @@
 //
 // Warp roles (192 threads): warps 0-3 read the accumulator (TMEM lanes
 // 32w..32w+31), apply GELU and store; warp 4 lane 0 issues the TMA loads;
-// warp 5 lane 0 issues the MMAs.  Four TMEM accumulators (4 x 16 columns)
-// let the MMAs of the next tiles run while a tile's epilogue reads its own.  mbarriers: full[slot]
+// warp 5 lane 0 issues the MMAs.  Two TMEM accumulators (2 x 16 columns)
+// overlap a tile's epilogue with the next tile's MMAs (four measured slower).  mbarriers: full[slot]
 // (TMA bytes landed), empty[slot] (the MMAs reading a plane completed),
 // acc_full[b] (a tile's MMAs completed), acc_empty[b] (its epilogue read it).
 // Every wait is bounded: on timeout the kernel raises *err and every role
@@ -58,7 +58,7 @@ constexpr int kPlaneBytes = 3 * kLineStride;  // the 3 line blocks (dy = -1, 0, 
 constexpr int kWBytes = 27 * 512;             // one layer's weights: per tap [group][co 16][8 ci] BF16
 constexpr int kThreads = 192;
 constexpr int kBarOff = kSlots * kPlaneBytes + kWBytes;
-constexpr int kAcc = 4;                       // TMEM accumulators (16 columns each) per CTA
+constexpr int kAcc = 2;                       // TMEM accumulators (16 columns each) per CTA
 constexpr int kBarSlots = 2 * kSlots + 2 * kAcc + 1;  // full, empty, acc_full, acc_empty, drain
 constexpr int kSmemBytes = kBarOff + kBarSlots * 8 + 16 + 128;  // + barriers, TMEM address, alignment slack
 constexpr long long kSpin = 1ll << 24;        // polls before a wait gives up
@@ -310,6 +310,27 @@ __global__ void __launch_bounds__(kThreads, 3) k_conv16_tc(const __grid_constant
                 mbar_drain(drain_s, 0);
             }
         } else {
+            // the boundary planes z = 0 and nz - 1 of this column hold zeros
+            // in every output (no tile computes them; a buffer reused for
+            // another grid must not keep values there)
+            for (int e = 0; e < 2; ++e) {
+                if ((e == 0 && zb != 1) || (e == 1 && ze != a.g.nz - 1)) continue;
+                const int64_t inplane = (int64_t)col * kRows + warp * 32 + lane;
+                if (inplane >= a.nxy) continue;
+                const int64_t c = (e == 0 ? 0 : (int64_t)(a.g.nz - 1) * a.nxy) + inplane;
+                if (kEpi == 1) {
+                    a.zout[boff + c] = 0.0f;
+                } else {
+                    uint4 *o = reinterpret_cast<uint4 *>(a.out + (boff + c) * 16);
+                    o[0] = make_uint4(0, 0, 0, 0);
+                    o[1] = make_uint4(0, 0, 0, 0);
+                    if (kEpi == 2) {
+                        uint4 *oy = reinterpret_cast<uint4 *>(a.yout + (boff + c) * 16);
+                        oy[0] = make_uint4(0, 0, 0, 0);
+                        oy[1] = make_uint4(0, 0, 0, 0);
+                    }
+                }
+            }
             // epilogue: warp w holds tile rows 32w .. 32w+31
             for (int j = 0; j < P; ++j) {
                 const int buf = j % kAcc;

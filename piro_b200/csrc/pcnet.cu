@@ -593,7 +593,7 @@ static int net_reserve(piro_pcnet *n, int64_t cells, bool training)
         if (e == cudaSuccess) e = cudaMalloc(&n->gout, c * sizeof(float));
         if (e == cudaSuccess) e = cudaMalloc(&n->x16, c * 16 * sizeof(bf16));
         if (e == cudaSuccess) e = cudaMalloc(&n->go16, c * 16 * sizeof(bf16));
-        // the tensor-core layers never write the boundary planes of their outputs
+        // defined contents before the first pass (every layer writes all of its output)
         for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaMemset(n->y[i], 0, c * 16 * sizeof(bf16));
         for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMemset(n->g16[i], 0, c * 16 * sizeof(bf16));
         if (e == cudaSuccess) e = cudaMemset(n->out, 0, c * sizeof(float));
@@ -702,8 +702,8 @@ static int encode_rows_map(CUtensorMap *m, const void *base, int64_t rows, int b
 
 // One layer on the tensor cores over `batch` grids of N cells: in (16 BF16
 // channels per cell) -> out (GELU, 16 BF16 channels) or, for the last layer,
-// zout (FP32 channel 0 times sqrt(rr / n_int)).  Cells of the boundary planes
-// z = 0 and nz - 1 are not written (they must already be zero).
+// zout (FP32 channel 0 times sqrt(rr / n_int)).  Every cell of the output is
+// written, the boundary planes z = 0 and nz - 1 with zeros.
 template <int kEpi>
 static int conv_tc(const bf16 *in, bf16 *out, float *zout, const bf16 *wpk, const GridDiv &g, int64_t N, int batch,
                    const double *rr, double n_int, const int *skip, int *err, cudaStream_t st,
@@ -904,12 +904,6 @@ extern "C" int piro_pcnet_forward(piro_pcnet *n, int batch, int nx, int ny, int 
     n->launches += 5;
     const Acts A{n->x0, {nullptr, nullptr, nullptr}, {n->a[0], n->a[1], n->a[2]}};
     if (n->engine == PIRO_PCNET_TENSOR_CORES) {
-        // the tensor-core layers leave the boundary planes of out unwritten
-        const int64_t nxy = (int64_t)nx * ny;
-        for (int b = 0; b < batch; ++b) {
-            PIRO_CUDA(cudaMemsetAsync(out + b * N, 0, sizeof(float) * nxy, st));
-            PIRO_CUDA(cudaMemsetAsync(out + b * N + N - nxy, 0, sizeof(float) * nxy, st));
-        }
         rc = net_forward_tc(n, A, batch, g, N, r, feat, out, nullptr, 1.0, nullptr, st);
         if (rc) return rc;
         int err = 0;
@@ -935,9 +929,7 @@ extern "C" int piro_pcnet_set_engine(piro_pcnet *n, int engine)
 }
 
 namespace piro {
-// Device bytes of the caller-owned workspace of pcnet_apply for N cells; the
-// caller zeroes it once (boundary planes of the tensor-core layers' outputs
-// are never written).
+// Device bytes of the caller-owned workspace of pcnet_apply for N cells.
 size_t pcnet_apply_bytes(int64_t N) { return sizeof(bf16) * (size_t)(cdiv(N * 2, 128) * 128 + 2 * N * 16); }
 
 // Tensor-core pipeline error of the network (a bounded wait ran out); clears it.
@@ -958,8 +950,7 @@ int pcnet_take_error(const piro_pcnet *n, cudaStream_t st)
 // every launch returning at once when *skip is set.  Reads only the net's
 // weight vectors (allocated once per network), so a CUDA graph that captured
 // it stays valid while the network is trained or reloaded.  Five kernel
-// launches.  z's boundary planes must be zero already (the tensor-core
-// engine does not write them).
+// launches; every cell of z is written (zeros on the boundary).
 int pcnet_apply(const piro_pcnet *n, void *work, const GridDiv &g, int64_t N, const float *r, const float *feat,
                 const double *rr, double n_int, float *z, const int *skip, cudaStream_t st)
 {

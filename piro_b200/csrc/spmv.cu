@@ -973,11 +973,6 @@ extern "C" int piro_ht_row_order(int64_t N, int64_t ts, int32_t *order, void *wo
     return PIRO_OK;
 }
 
-// Per device: bytes of L2 that persisting accesses may hold (0: none), set
-// once to the device maximum.
-static size_t ht_l2_persist[kMaxDevices] = {}, ht_l2_window[kMaxDevices] = {};
-static DeviceOnce ht_l2_once;
-
 extern "C" int piro_ht_spmv_ordered(int nx, int ny, int nz, const int64_t *keys, const float *vals, int64_t ts,
                                     float dt, int fe, const int32_t *order, const float *u, float *out,
                                     piro_stream_t stream)
@@ -985,43 +980,9 @@ extern "C" int piro_ht_spmv_ordered(int nx, int ny, int nz, const int64_t *keys,
     PIRO_ARG(grid_ok(nx, ny, nz) && keys && vals && ts > 0 && order && u && out && u != out,
              "piro_ht_spmv_ordered: bad arguments");
     const int64_t N = (int64_t)nx * ny * nz;
-    // In home-slot order the table streams through L2 once, while each row
-    // gathers its seven u values at random: u is marked persisting in L2 for
-    // this launch (an access-policy window on the kernel alone), so the
-    // gathers hit L2 instead of re-reading u from HBM as the table evicts it.
-    int dev = 0;
-    PIRO_CUDA(cudaGetDevice(&dev));
-    int rc = device_once(ht_l2_once, dev, [dev]() -> int {
-        int maxp = 0, maxw = 0;
-        if (cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, dev) == cudaSuccess && maxp > 0 &&
-            cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, dev) == cudaSuccess && maxw > 0 &&
-            cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, (size_t)maxp) == cudaSuccess) {
-            ht_l2_persist[dev] = (size_t)maxp;
-            ht_l2_window[dev] = (size_t)maxw;
-        }
-        (void)cudaGetLastError();
-        return PIRO_OK;
-    });
-    if (rc != PIRO_OK) return rc;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid_for(N, 256, 8));
-    cfg.blockDim = dim3(256);
-    cfg.stream = as_stream(stream);
-    cudaLaunchAttribute attr[1];
-    size_t ubytes = sizeof(float) * (size_t)N;
-    if (ubytes > ht_l2_window[dev]) ubytes = ht_l2_window[dev];
-    if (ht_l2_persist[dev] > 0) {
-        attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
-        attr[0].val.accessPolicyWindow.base_ptr = const_cast<float *>(u);
-        attr[0].val.accessPolicyWindow.num_bytes = ubytes;
-        attr[0].val.accessPolicyWindow.hitRatio =
-            ubytes <= ht_l2_persist[dev] ? 1.0f : (float)((double)ht_l2_persist[dev] / (double)ubytes);
-        attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-        attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-    }
-    PIRO_CUDA(cudaLaunchKernelEx(&cfg, k_ht_spmv<true>, nx, ny, nz, N, keys, vals, ts, dt, fe, order, u, out));
+    k_ht_spmv<true><<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(nx, ny, nz, N, keys, vals, ts, dt, fe, order,
+                                                                        u, out);
+    PIRO_CHECK_LAUNCH("k_ht_spmv");
     return PIRO_OK;
 }
 

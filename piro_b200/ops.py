@@ -558,6 +558,16 @@ class Batch:
         check(lib().piro_batch_member_info(self.h, vp(st), vp(sw), vp(it), vp(rel)), "piro_batch_member_info")
         return dict(status=st, sweeps=sw, inner=it, rel=rel)
 
+    def schedule(self):
+        """'grouped' or 'lockstep' (piro_batch_schedule)."""
+        g = C.c_int()
+        check(lib().piro_batch_schedule(self.h, C.byref(g)), "piro_batch_schedule")
+        return "grouped" if g.value else "lockstep"
+
+    def set_schedule(self, grouped, blocks_per_sm=4):
+        check(lib().piro_batch_set_schedule(self.h, int(bool(grouped)), int(blocks_per_sm)),
+              "piro_batch_set_schedule")
+
     def autotune(self, rtol=1e-8):
         t, b = C.c_int(), C.c_int()
         check(lib().piro_batch_autotune(self.h, float(rtol), C.byref(t), C.byref(b)), "piro_batch_autotune")

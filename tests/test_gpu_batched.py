@@ -34,12 +34,18 @@ def _small_batch(seed=7, count=10):
     return W.batched(seed=seed, count=count, lo=8, hi=22)
 
 
-def test_batch_matches_oracle(cuda):
+@pytest.mark.parametrize("schedule", ["lockstep", "grouped"])
+def test_batch_matches_oracle(cuda, schedule):
+    """Both schedules: the lockstep rounds of k_batch_step and the grouped
+    k_batch_groups (each member on a CTA group of its own with group-local
+    barriers, small members packed onto single CTAs)."""
     from piro_b200 import ops
     from piro_b200 import workloads as W
     cfg = _small_batch()
     assert set(cfg["scheme"]) == {0, 1}
     B = ops.Batch(cfg["n"], cfg["alpha"], cfg["dt"], cfg["scheme"])
+    B.set_schedule(schedule == "grouped", 2)
+    assert B.schedule() == schedule
     B.set_fields(W.pack_batch(cfg["fields"], B.offsets, B.total))
     B.step(2, rtol=1e-8)
     out = B.get_fields()
@@ -66,13 +72,15 @@ def test_batch_matches_oracle(cuda):
             assert err < 1e-6, (k, err)
 
 
-def test_batch_is_deterministic(cuda):
+@pytest.mark.parametrize("schedule", ["lockstep", "grouped"])
+def test_batch_is_deterministic(cuda, schedule):
     from piro_b200 import ops
     from piro_b200 import workloads as W
     cfg = _small_batch(seed=8, count=14)
     res = []
     for _ in range(2):
         B = ops.Batch(cfg["n"], cfg["alpha"], cfg["dt"], cfg["scheme"])
+        B.set_schedule(schedule == "grouped", 4)
         B.set_fields(W.pack_batch(cfg["fields"], B.offsets, B.total))
         B.step(3)
         res.append(B.get_fields())
@@ -92,6 +100,7 @@ def test_batch_autotune(cuda):
     B.set_fields(u0)
     tile, bps = B.autotune()
     assert tile in (2048, 4096, 8192, 16384) and bps in (1, 2, 4)
+    assert B.schedule() in ("lockstep", "grouped")
     B.set_fields(u0)
     B.step(1)
     got = B.get_fields()
@@ -104,3 +113,33 @@ def test_batch_autotune(cuda):
             assert np.abs(a - b).max() <= 1e-6 * max(1e-30, np.abs(b).max())
         else:
             assert np.array_equal(a, b)
+
+
+def test_grouped_schedule_large_members_vs_lockstep(cuda):
+    """Members large enough to get CTA groups of their own (sides up to 60):
+    the grouped step agrees with the lockstep one to rounding, forward-Euler
+    members bit for bit, for two steps in a row."""
+    from piro_b200 import ops
+    from piro_b200 import workloads as W
+    cfg = W.batched(seed=11, count=24, lo=12, hi=60)
+    u0 = None
+    out = {}
+    for grouped in (False, True):
+        B = ops.Batch(cfg["n"], cfg["alpha"], cfg["dt"], cfg["scheme"])
+        u0 = W.pack_batch(cfg["fields"], B.offsets, B.total)
+        B.set_schedule(grouped, 2)
+        B.set_fields(u0)
+        B.step(2)
+        out[grouped] = (B.get_fields(), B.member_info())
+        offs = B.offsets
+        B.close()
+    be = cfg["scheme"] == 1
+    (a, ia), (b, ib) = out[False], out[True]
+    assert np.all(ib["status"] == 0) and np.all(ib["rel"][be] <= 1e-8)
+    for k in range(len(cfg["n"])):
+        n3 = int(cfg["n"][k]) ** 3
+        x, y = a[offs[k]:offs[k] + n3], b[offs[k]:offs[k] + n3]
+        if be[k]:
+            assert np.abs(x - y).max() <= 1e-6 * max(1e-30, np.abs(x).max()), k
+        else:
+            assert np.array_equal(x, y), k
