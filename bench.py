@@ -585,6 +585,7 @@ def batched_section(torch, ops, peak, steps=4):
     u0 = W.pack_batch(cfg["fields"], B.offsets, B.total)
     B.set_fields(u0)
     tile, bps = B.autotune()
+    schedule = B.schedule()
     # one step from u0 for the error check
     B.set_fields(u0)
     B.step(1)
@@ -635,7 +636,7 @@ def batched_section(torch, ops, peak, steps=4):
         "members": int(len(n)), "backward_euler_members": int(be.sum()), "cells": cells,
         "ms_per_step": round(ms, 3), "cell_updates_per_s": cells / ms * 1e3,
         "gbs": round(byt / ms / 1e6, 1), "frac": round(byt / ms / 1e6 / peak, 4),
-        "autotuned": {"tile_cells": tile, "blocks_per_sm": bps},
+        "autotuned": {"tile_cells": tile, "blocks_per_sm": bps, "schedule": schedule},
         "be_cg_iterations": {"mean": float(info["inner"][be].mean()), "max": int(info["inner"][be].max())},
         "be_sweeps_max": int(info["sweeps"][be].max()),
         "worst_rel_residual": float(info["rel"][be].max()), "all_converged": bool(np.all(info["status"] == 0)),
