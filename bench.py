@@ -181,10 +181,17 @@ def spmv_section(torch, ops, steps, warmup, peak):
     # read, out written, the row order read
     byt = 12 * ts + 12 * N
     order = ops.ht_row_order(N, ts)
-    ms = timeit(lambda: ops.ht_spmv_ordered(nx, ny, nz, keys, vals, dt, order, u, out, fe=True), steps)
+    stage = ops.ht_stage(N)
+    ms = timeit(lambda: ops.ht_spmv_staged(nx, ny, nz, keys, vals, dt, order, stage, u, out, fe=True), steps)
     res["ht"] = {"ms": ms, "gbs": byt / ms / 1e6, "frac": byt / ms / 1e6 / peak, "bytes": byt, "slots": ts,
-                 "rows": "in home-slot order (piro_ht_row_order, once per table)",
-                 "bytes_definition": "12 ts (keys and values, every slot) + 12 N (u, out, row order)"}
+                 "rows": "table read with the rows in home-slot order (piro_ht_row_order, once per table), "
+                         "each row's values staged in a 32-byte record, then applied in row order",
+                 "stage_bytes": 32 * N,
+                 "bytes_definition": "12 ts (keys and values, every slot) + 12 N (u, out, row order); the "
+                                     "stage's 64 N bytes (written, read back) are not counted"}
+    del stage
+    ms = timeit(lambda: ops.ht_spmv_ordered(nx, ny, nz, keys, vals, dt, order, u, out, fe=True), steps)
+    res["ht_one_pass"] = {"ms": ms, "gbs": byt / ms / 1e6, "frac": byt / ms / 1e6 / peak}
     ms = timeit(lambda: ops.ht_spmv(nx, ny, nz, keys, vals, dt, u, out, fe=True), max(3, steps // 4))
     res["ht_row_major"] = {"ms": ms, "gbs": byt / ms / 1e6, "frac": byt / ms / 1e6 / peak}
     del order
@@ -465,8 +472,8 @@ def learned_section(torch, ops, cfg, A, alpha, plain_ms, plain_iters, steps, tfl
     """Configuration 4: the backward-Euler step with the learned preconditioner
     (the network trained on the device on seeds 100-199 by
     `python -m piro_b200.learned`, weights in piro_b200/data) inside flexible
-    CG, against plain Jacobi-PCG on the same step; plus held-out fields
-    (seeds 200-202) solved both ways."""
+    CG, against plain Jacobi-PCG on the same step; plus the held-out fields
+    (seeds 200-209) solved both ways."""
     from piro_b200 import learned as LP
     nx, ny, nz = cfg["n"]
     N = nx * ny * nz
@@ -504,7 +511,9 @@ def learned_section(torch, ops, cfg, A, alpha, plain_ms, plain_iters, steps, tfl
     n_int = (nx - 2) * (ny - 2) * (nz - 2)
     alg_flops = 2 * 27 * (2 * 16 + 16 * 16 + 16 * 16 + 16 * 1) * n_int  # the network's multiply-adds
     avg_apply = apply_ms / max(1, napply)
-    held = LP.compare(torch, ops, net, nx, [200, 201, 202])
+    held_seeds = list(range(200, 210))
+    LP.prefetch_alpha(nx, held_seeds)
+    held = LP.compare(torch, ops, net, nx, held_seeds)
     net.close()
     return {
         "ms_per_step": round(ms, 4), "inner_iterations_mean": float(np.mean(iters)), "fallbacks": fb,
@@ -514,7 +523,7 @@ def learned_section(torch, ops, cfg, A, alpha, plain_ms, plain_iters, steps, tfl
         "apply_tflops": round(alg_flops / avg_apply / 1e9, 1),
         "apply_frac_of_bf16_peak": round(alg_flops / avg_apply / 1e9 / tflops_peak, 4),
         "kernel_launches_per_step": launches / steps,
-        "held_out": LP.summary(held),
+        "held_out": dict(LP.summary(held), seeds=[held_seeds[0], held_seeds[-1]]),
         "note": "network applies on the tensor cores (tcgen05, 4 layers); the network preconditions the first 2 "
                 "flexible-CG iterations of each refinement sweep, Jacobi the rest; plain = Jacobi-PCG in the "
                 "persistent single-launch solver",
@@ -1031,9 +1040,13 @@ def run_profile_case(args):
     kernels (CSR, matrix-free, fused CSR + setBC, indexed COO; about 1.5 GB
     on the device), `dense` three DENSE steps at N = 12,288 (a 604 MB
     matrix), `learned` two learned-preconditioner solves of the 128^3 step,
-    `batched` two steps of a 64-member batch, `train` four training steps of
-    the network on 8 crops of 34^3 cells, `ht` three ordered hash-table steps
-    at 192^3."""
+    `batched` two steps of a 64-member batch
+    in each schedule (lockstep, then grouped), `train` four training steps of
+    the network on 8 crops of 34^3 cells, `ht` three staged and three one-pass
+    ordered hash-table steps at 192^3, `fe160` the forward-Euler kernels one format at a time at 160^3
+    (CSR, matrix-free, segmented COO, three launches each), three
+    Laplacian assemblies and three v.grad merges (csrgeam3) of the upwind
+    gradients."""
     import torch
 
     from piro_b200 import ops
@@ -1083,6 +1096,9 @@ def run_profile_case(args):
         order = ops.ht_row_order(N, ts)
         u = torch.rand(N, device="cuda")
         out = torch.empty_like(u)
+        stage = ops.ht_stage(N)
+        for _ in range(3):
+            ops.ht_spmv_staged(n, n, n, keys, vals, 0.01, order, stage, u, out, fe=True)
         for _ in range(3):
             ops.ht_spmv_ordered(n, n, n, keys, vals, 0.01, order, u, out, fe=True)
         torch.cuda.synchronize()
@@ -1103,9 +1119,38 @@ def run_profile_case(args):
     elif args.profile == "batched":
         cfg = W.batched(count=64)
         B = ops.Batch(cfg["n"], cfg["alpha"], cfg["dt"], cfg["scheme"])
-        B.set_fields(W.pack_batch(cfg["fields"], B.offsets, B.total))
-        B.step(2)
+        u0 = W.pack_batch(cfg["fields"], B.offsets, B.total)
+        for grouped in (False, True):
+            B.set_schedule(grouped, 4)
+            B.set_fields(u0)
+            B.step(2)
         print("batched ok")
+    elif args.profile == "fe160":
+        cfg = W.spmv_256(n=160)  # 4.1M rows, 28.4M nonzeros: above L2, well under a GB
+        nx, ny, nz = cfg["n"]
+        N = nx * ny * nz
+        u = torch.from_numpy(cfg["u"]).cuda()
+        alpha = torch.from_numpy(cfg["alpha"]).cuda()
+        out = torch.empty_like(u)
+        A = ops.csr_laplacian(nx, ny, nz, 3, 1.0)
+        ops.csr_rowscale(A[0], A[2], alpha)
+        for _ in range(3):
+            ops.csr_fe_step(nx, ny, nz, A, 0.01, u, out)
+        for _ in range(3):
+            ops.stencil_fe_step(nx, ny, nz, 0.01, u, out, alpha=alpha)
+        rows = torch.repeat_interleave(torch.arange(N, device="cuda", dtype=torch.int32),
+                                       (A[0][1:] - A[0][:-1]).to(torch.int64))
+        for _ in range(3):
+            ops.coo_spmv(N, (rows, A[1], A[2]), 0.01, u, out, fe=True)
+        for _ in range(3):
+            ops.csr_laplacian(nx, ny, nz, 3, 1.0)
+        del A, rows
+        G = [ops.csr_gradient(nx, ny, nz, 1, a, 2.0) for a in range(3)]
+        v = torch.rand(3 * N, device="cuda")
+        for _ in range(3):
+            ops.csrgeam3(N, *G, v)
+        torch.cuda.synchronize()
+        print("fe160 ok")
     else:
         cfg = W.spmv_256()
         nx, ny, nz = cfg["n"]
@@ -1139,7 +1184,7 @@ def main():
     ap.add_argument("--impl", default="piro", choices=["piro", "reference"])
     ap.add_argument("--sharded", type=int, default=0, metavar="N",
                     help="one N^3 backward-Euler grid in z-slabs over the ranks (strong scaling) instead of replicas")
-    ap.add_argument("--profile", choices=["be", "spmv", "dense", "learned", "batched", "train", "ht"],
+    ap.add_argument("--profile", choices=["be", "spmv", "fe160", "dense", "learned", "batched", "train", "ht"],
                     help="run a small fixed case for ncu, print no JSON")
     args = ap.parse_args()
     if args.profile:

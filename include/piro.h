@@ -196,6 +196,16 @@ int piro_ht_row_order_workspace(int64_t N, int64_t ts, size_t *bytes);
 int piro_ht_row_order(int64_t N, int64_t ts, int32_t *order, void *work, size_t work_bytes, piro_stream_t stream);
 int piro_ht_spmv_ordered(int nx, int ny, int nz, const int64_t *keys, const float *vals, int64_t ts, float dt, int fe,
                          const int32_t *order, const float *u, float *out, piro_stream_t stream);
+/* The same step in two passes over a caller-owned stage of
+ * piro_ht_stage_bytes(N) bytes (32 per row, 16-byte aligned): the table is
+ * read in home-slot order as above and each row's seven stencil values land
+ * in a 32-byte record, then the rows are applied in index order, so that u
+ * and out are read and written coalesced instead of at the scattered
+ * home-slot rows.  Same results bit for bit; N < 2^31. */
+int piro_ht_stage_bytes(int64_t N, size_t *bytes);
+int piro_ht_spmv_staged(int nx, int ny, int nz, const int64_t *keys, const float *vals, int64_t ts, float dt, int fe,
+                        const int32_t *order, void *stage, size_t stage_bytes, const float *u, float *out,
+                        piro_stream_t stream);
 
 /* Scheme 27 (TIMESCHEME 12 + solver 27) on a table built by piro_ht_build
  * (int64 keys, -1 empty; -2 marks a deleted key).  piro_ht_lu_reference is

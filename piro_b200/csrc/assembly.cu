@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, 
     __shared__ __align__(16) int32_t s_col[kRowsPerBlock * kMaxPerRow + 4];
     __shared__ __align__(16) float s_val[kRowsPerBlock * kMaxPerRow + 4];
     __shared__ __align__(16) int32_t s_row[kRowsPerBlock * kMaxPerRow + 4];
-    __shared__ int64_t s_base, s_end;
+    __shared__ int64_t s_end;
     int64_t base0;
     {
         int x, y, z;
@@ -136,16 +136,14 @@ __global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, 
     for (int64_t r0 = row0 + (int64_t)blockIdx.x * kRowsPerBlock; r0 < R1; r0 += (int64_t)gridDim.x * kRowsPerBlock) {
         const int64_t i = r0 + threadIdx.x;
         const int64_t rlast = (r0 + kRowsPerBlock < R1 ? r0 + kRowsPerBlock : R1) - 1;
-        if (threadIdx.x == 0) {
+        // the block's first entry, the same in every thread (no serial section)
+        int64_t s_base;
+        {
             int x, y, z;
             coords(r0, g, x, y, z);
             s_base = lap_prefix(x, y, z, g);
-            int32_t c[kMaxPerRow];
-            float v[kMaxPerRow];
-            coords(rlast, g, x, y, z);
-            s_end = lap_prefix(x, y, z, g) + lap_row(rlast, g, scheme, vself, vnb, c, v);
         }
-        __syncthreads();
+        const int sh = vec_ok ? (int)((s_base - base0) & 3) : 0;  // shared index of the first entry
         if (i < R1) {
             int x, y, z;
             coords(i, g, x, y, z);
@@ -153,22 +151,23 @@ __global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, 
             int32_t c[kMaxPerRow];
             float v[kMaxPerRow];
             const int n = lap_row(i, g, scheme, vself, vnb, c, v);
-            const int off = (int)(p - s_base) + (vec_ok ? (int)((s_base - base0) & 3) : 0);
+            const int off = (int)(p - s_base) + sh;
             for (int t = 0; t < n; ++t) {
                 s_col[off + t] = (int32_t)(c[t] - col_shift);
                 s_val[off + t] = v[t];
-                s_row[off + t] = (int32_t)(i - col_shift);
             }
+            if (rows)
+                for (int t = 0; t < n; ++t) s_row[off + t] = (int32_t)(i - col_shift);
             if (rowptr) {
                 rowptr[i - row0 + 1] = (int32_t)(p + n - base0);
                 if (i == row0) rowptr[0] = 0;
             }
+            if (i == rlast) s_end = p + n;
         }
         __syncthreads();
         // the block's entries leave as 16-byte stores (scalar head and tail)
         // when the arrays are 16-byte aligned
         const int cnt = (int)(s_end - s_base);
-        const int sh = vec_ok ? (int)((s_base - base0) & 3) : 0;  // shared index of the first entry
         const int64_t g0 = s_base - base0 - sh;                   // global index of shared index 0
         const int j0 = vec_ok ? (sh + 3) & ~3 : sh + cnt, j1 = vec_ok ? (sh + cnt) & ~3 : sh + cnt;
         const int head_end = j0 < sh + cnt ? j0 : sh + cnt;

@@ -554,7 +554,7 @@ __device__ __forceinline__ bool group_sums(const GArgs &A, double *part, int fir
     return true;
 }
 
-__global__ void __launch_bounds__(kThreads) k_batch_groups(GArgs A)
+__global__ void __launch_bounds__(kThreads, 4) k_batch_groups(GArgs A)
 {
     __shared__ double s_red[4 * 32];
     __shared__ double s_tot[4];

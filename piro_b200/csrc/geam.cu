@@ -109,33 +109,101 @@ __global__ void k_geam3_count(int64_t N, const int32_t *__restrict__ rpA, const 
     }
 }
 
-// csrgeam_3.cl:21-88: three-way merge, ties A before B before C, tails
-// appended A, B, C; values scaled by v[row + comp*N].
-__global__ void k_geam3_fill(int64_t N, const int32_t *__restrict__ rpA, const int32_t *__restrict__ cA,
-                             const float *__restrict__ vA, const int32_t *__restrict__ rpB,
-                             const int32_t *__restrict__ cB, const float *__restrict__ vB,
-                             const int32_t *__restrict__ rpC, const int32_t *__restrict__ cC,
-                             const float *__restrict__ vC, const float *__restrict__ v,
-                             const int32_t *__restrict__ rpD, int32_t *__restrict__ cD, float *__restrict__ vD)
+// csrgeam_3.cl:21-88: three-way merge per row, ties A before B before C,
+// tails appended A, B, C; values scaled by v[row + comp*N].  A warp takes 32
+// consecutive rows.  Their entries in each input are one contiguous segment,
+// and so are their outputs: the warp loads the three input segments into
+// shared memory with consecutive lanes on consecutive entries, each lane
+// merges its row there, and the warp stores the output segment the same
+// coalesced way.  A chunk whose segments exceed the staging capacity (or
+// whose row pointers are not monotone) runs the same merge per lane on
+// global memory instead.
+constexpr int kGeamWarps = 8;
+constexpr int kGeamCap = 128;  // staged entries per input and warp (about 4 per row)
+
+__global__ void __launch_bounds__(kGeamWarps * 32) k_geam3_fill_warp(
+    int64_t N, const int32_t *__restrict__ rpA, const int32_t *__restrict__ cA, const float *__restrict__ vA,
+    const int32_t *__restrict__ rpB, const int32_t *__restrict__ cB, const float *__restrict__ vB,
+    const int32_t *__restrict__ rpC, const int32_t *__restrict__ cC, const float *__restrict__ vC,
+    const float *__restrict__ v, const int32_t *__restrict__ rpD, int32_t *__restrict__ cD, float *__restrict__ vD)
 {
-    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < N;
-         row += (int64_t)gridDim.x * blockDim.x) {
-        int32_t i = rpA[row], ie = rpA[row + 1];
-        int32_t j = rpB[row], je = rpB[row + 1];
-        int32_t k = rpC[row], ke = rpC[row + 1];
-        int64_t d = rpD[row];
-        const float sa = v[row], sb = v[N + row], sc = v[2 * N + row];
-        while (i < ie && j < je && k < ke) {
-            const int32_t a = cA[i], b = cB[j], c = cC[k];
-            const int32_t m = min(a, min(c, b));
-            if (a == m) { cD[d] = a; vD[d] = __fmul_rn(vA[i], sa); ++i; }
-            else if (b == m) { cD[d] = b; vD[d] = __fmul_rn(vB[j], sb); ++j; }
-            else { cD[d] = c; vD[d] = __fmul_rn(vC[k], sc); ++k; }
-            ++d;
+    __shared__ int32_t s_c[kGeamWarps][6 * kGeamCap];  // A, B, C inputs, then the 3 * kGeamCap outputs
+    __shared__ float s_v[kGeamWarps][6 * kGeamCap];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int32_t *sc = s_c[w];
+    float *sv = s_v[w];
+    const int64_t nchunk = (N + 31) >> 5;
+    for (int64_t ch = (int64_t)blockIdx.x * kGeamWarps + w; ch < nchunk; ch += (int64_t)gridDim.x * kGeamWarps) {
+        const int64_t r0 = ch << 5, r1 = r0 + 32 < N ? r0 + 32 : N;
+        const int64_t row = r0 + lane;
+        const bool live = row < r1;
+        const int32_t a0 = rpA[r0], a1 = rpA[r1], b0 = rpB[r0], b1 = rpB[r1], c0 = rpC[r0], c1 = rpC[r1];
+        const int32_t d0 = rpD[r0], d1 = rpD[r1];
+        int32_t i = 0, ie = 0, j = 0, je = 0, k = 0, ke = 0;
+        float sa = 0.0f, sb = 0.0f, sc_ = 0.0f;
+        if (live) {
+            i = rpA[row]; ie = rpA[row + 1];
+            j = rpB[row]; je = rpB[row + 1];
+            k = rpC[row]; ke = rpC[row + 1];
+            sa = v[row]; sb = v[N + row]; sc_ = v[2 * N + row];
         }
-        for (; i < ie; ++i, ++d) { cD[d] = cA[i]; vD[d] = __fmul_rn(vA[i], sa); }
-        for (; j < je; ++j, ++d) { cD[d] = cB[j]; vD[d] = __fmul_rn(vB[j], sb); }
-        for (; k < ke; ++k, ++d) { cD[d] = cC[k]; vD[d] = __fmul_rn(vC[k], sc); }
+        // stage only when every lane's ranges lie inside the chunk's segments (a
+        // monotone row pointer) and the segments fit; else the global loop
+        const bool inside = !live || (a0 <= i && i <= ie && ie <= a1 && b0 <= j && j <= je && je <= b1 &&
+                                      c0 <= k && k <= ke && ke <= c1 && d0 <= rpD[row] && d1 <= d0 + 3 * kGeamCap);
+        const bool fits = (uint32_t)(a1 - a0) <= (uint32_t)kGeamCap && (uint32_t)(b1 - b0) <= (uint32_t)kGeamCap &&
+                          (uint32_t)(c1 - c0) <= (uint32_t)kGeamCap;
+        if (!__all_sync(0xffffffffu, inside && fits)) {
+            if (live) {
+                int64_t d = rpD[row];
+                while (i < ie && j < je && k < ke) {
+                    const int32_t a = cA[i], b = cB[j], c = cC[k];
+                    const int32_t m = min(a, min(c, b));
+                    if (a == m) { cD[d] = a; vD[d] = __fmul_rn(vA[i], sa); ++i; }
+                    else if (b == m) { cD[d] = b; vD[d] = __fmul_rn(vB[j], sb); ++j; }
+                    else { cD[d] = c; vD[d] = __fmul_rn(vC[k], sc_); ++k; }
+                    ++d;
+                }
+                for (; i < ie; ++i, ++d) { cD[d] = cA[i]; vD[d] = __fmul_rn(vA[i], sa); }
+                for (; j < je; ++j, ++d) { cD[d] = cB[j]; vD[d] = __fmul_rn(vB[j], sb); }
+                for (; k < ke; ++k, ++d) { cD[d] = cC[k]; vD[d] = __fmul_rn(vC[k], sc_); }
+            }
+            continue;
+        }
+        for (int t = lane; t < a1 - a0; t += 32) { sc[t] = cA[a0 + t]; sv[t] = vA[a0 + t]; }
+        for (int t = lane; t < b1 - b0; t += 32) { sc[kGeamCap + t] = cB[b0 + t]; sv[kGeamCap + t] = vB[b0 + t]; }
+        for (int t = lane; t < c1 - c0; t += 32) {
+            sc[2 * kGeamCap + t] = cC[c0 + t];
+            sv[2 * kGeamCap + t] = vC[c0 + t];
+        }
+        __syncwarp();
+        if (live) {
+            int32_t *oc = sc + 3 * kGeamCap;
+            float *ov = sv + 3 * kGeamCap;
+            int d = rpD[row] - d0;
+            i -= a0; ie -= a0;
+            j -= b0; je -= b0;
+            k -= c0; ke -= c0;
+            const int32_t *lc_a = sc, *lc_b = sc + kGeamCap, *lc_c = sc + 2 * kGeamCap;
+            const float *lv_a = sv, *lv_b = sv + kGeamCap, *lv_c = sv + 2 * kGeamCap;
+            while (i < ie && j < je && k < ke) {
+                const int32_t a = lc_a[i], b = lc_b[j], c = lc_c[k];
+                const int32_t m = min(a, min(c, b));
+                if (a == m) { oc[d] = a; ov[d] = __fmul_rn(lv_a[i], sa); ++i; }
+                else if (b == m) { oc[d] = b; ov[d] = __fmul_rn(lv_b[j], sb); ++j; }
+                else { oc[d] = c; ov[d] = __fmul_rn(lv_c[k], sc_); ++k; }
+                ++d;
+            }
+            for (; i < ie; ++i, ++d) { oc[d] = lc_a[i]; ov[d] = __fmul_rn(lv_a[i], sa); }
+            for (; j < je; ++j, ++d) { oc[d] = lc_b[j]; ov[d] = __fmul_rn(lv_b[j], sb); }
+            for (; k < ke; ++k, ++d) { oc[d] = lc_c[k]; ov[d] = __fmul_rn(lv_c[k], sc_); }
+        }
+        __syncwarp();
+        for (int t = lane; t < d1 - d0; t += 32) {
+            cD[d0 + t] = sc[3 * kGeamCap + t];
+            vD[d0 + t] = sv[3 * kGeamCap + t];
+        }
+        __syncwarp();
     }
 }
 
@@ -247,8 +315,9 @@ extern "C" int piro_csrgeam3(int64_t N, const int32_t *rpA, const int32_t *cA, c
     PIRO_CHECK_LAUNCH("k_geam3_count");
     int rc = scan_rowptr_inplace(N, rpD, work, work_bytes, s);
     if (rc) return rc;
-    k_geam3_fill<<<grid_for(N, 128, 8), 128, 0, s>>>(N, rpA, cA, vA, rpB, cB, vB, rpC, cC, vC, v, rpD, cD, vD);
-    PIRO_CHECK_LAUNCH("k_geam3_fill");
+    k_geam3_fill_warp<<<grid_for(cdiv(N, 32) * 32, kGeamWarps * 32, 4), kGeamWarps * 32, 0, s>>>(
+        N, rpA, cA, vA, rpB, cB, vB, rpC, cC, vC, v, rpD, cD, vD);
+    PIRO_CHECK_LAUNCH("k_geam3_fill_warp");
     return PIRO_OK;
 }
 

@@ -332,7 +332,7 @@ __device__ __forceinline__ float ht_get_from(int64_t key, int64_t h, const int64
 // are issued together, then the seven value loads; only a collision (a first
 // probe holding another key) walks on.
 template <bool kOrdered>
-__global__ void k_ht_spmv(int nx, int ny, int nz, int64_t N, const int64_t *__restrict__ keys,
+__global__ void __launch_bounds__(256, 4) k_ht_spmv(int nx, int ny, int nz, int64_t N, const int64_t *__restrict__ keys,
                           const float *__restrict__ vals, int64_t ts, float dt, int fe,
                           const int32_t *__restrict__ order, const float *__restrict__ u, float *__restrict__ out)
 {
@@ -348,6 +348,7 @@ __global__ void k_ht_spmv(int nx, int ny, int nz, int64_t N, const int64_t *__re
         const bool ok[7] = {z > 0, y > 0, x > 0, true, x < nx - 1, y < ny - 1, z < nz - 1};
         const int64_t kd = i * N + i, base = kd % ts;
         int64_t h[7], k[7];
+        float v[7];
 #pragma unroll
         for (int t = 0; t < 7; ++t) {
             if (ok[t]) {
@@ -356,21 +357,97 @@ __global__ void k_ht_spmv(int nx, int ny, int nz, int64_t N, const int64_t *__re
                 hh -= hh >= ts ? ts : 0;
                 h[t] = hh;
                 k[t] = __ldg(keys + hh);
+                v[t] = __ldg(vals + hh);  // with the key, not after it: one round trip
             }
         }
-        float v[7];
 #pragma unroll
         for (int t = 0; t < 7; ++t) {
             if (ok[t]) {
                 const int64_t key = kd + off[t];
-                if (k[t] == key)
-                    v[t] = __ldg(vals + h[t]);
-                else if (k[t] == -1)
+                if (k[t] == key) {
+                } else if (k[t] == -1) {
                     v[t] = 0.0f;
-                else
+                } else {
                     v[t] = ht_get_from(key, h[t] + 1 == ts ? 0 : h[t] + 1, keys, vals, ts);
+                }
             }
         }
+        float sum = 0.0f;
+#pragma unroll
+        for (int t = 0; t < 7; ++t)
+            if (ok[t]) sum = __fadd_rn(sum, __fmul_rn(v[t], __ldg(u + i + off[t])));
+        const float c = __fmul_rn(dt, sum);
+        out[i] = fe ? __fadd_rn(u[i], c) : c;
+    }
+}
+
+// The same step in two passes, so that neither u nor out is touched in the
+// scattered home-slot order.  Pass 1 (rows in home-slot order) streams the
+// table through its moving window and writes each row's seven values, absent
+// keys as 0, into a 32-byte record stage[8 i .. 8 i + 7] (two full 16-byte
+// stores: whole sectors, no read-modify-write of a partly written sector).
+// Pass 2 (rows in index order) reads the records and u coalesced and writes
+// out coalesced.  The per-row arithmetic is the one above, term for term.
+__global__ void __launch_bounds__(256, 4) k_ht_stage(int nx, int ny, int nz, int64_t N, const int64_t *__restrict__ keys,
+                           const float *__restrict__ vals, int64_t ts, const int32_t *__restrict__ order,
+                           float4 *__restrict__ stage)
+{
+    const int64_t sxy = (int64_t)nx * ny;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < N; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = (int64_t)__ldg(order + j);
+        const int z = (int)(i / sxy);
+        const int64_t rem = i - (int64_t)z * sxy;
+        const int y = (int)(rem / nx);
+        const int x = (int)(rem - (int64_t)y * nx);
+        const int64_t off[7] = {-sxy, -(int64_t)nx, -1, 0, 1, (int64_t)nx, sxy};
+        const bool ok[7] = {z > 0, y > 0, x > 0, true, x < nx - 1, y < ny - 1, z < nz - 1};
+        const int64_t kd = i * N + i, base = kd % ts;
+        int64_t h[7], k[7];
+        float v[8];
+        v[7] = 0.0f;
+#pragma unroll
+        for (int t = 0; t < 7; ++t) {
+            v[t] = 0.0f;
+            if (ok[t]) {
+                int64_t hh = base + off[t];
+                hh += hh < 0 ? ts : 0;
+                hh -= hh >= ts ? ts : 0;
+                h[t] = hh;
+                k[t] = __ldg(keys + hh);
+                v[t] = __ldg(vals + hh);  // with the key: one round trip
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 7; ++t) {
+            if (ok[t]) {
+                const int64_t key = kd + off[t];
+                if (k[t] == key) {
+                } else if (k[t] == -1) {
+                    v[t] = 0.0f;
+                } else {
+                    v[t] = ht_get_from(key, h[t] + 1 == ts ? 0 : h[t] + 1, keys, vals, ts);
+                }
+            }
+        }
+        stage[2 * i] = make_float4(v[0], v[1], v[2], v[3]);
+        stage[2 * i + 1] = make_float4(v[4], v[5], v[6], v[7]);
+    }
+}
+
+__global__ void k_ht_stage_apply(int nx, int ny, int nz, float dt, int fe, const float4 *__restrict__ stage,
+                                 const float *__restrict__ u, float *__restrict__ out)
+{
+    const int sxy = nx * ny;
+    const int N = sxy * nz;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const int z = i / sxy;
+        const int rem = i - z * sxy;
+        const int y = rem / nx;
+        const int x = rem - y * nx;
+        const float4 lo = __ldcs(stage + 2 * (int64_t)i), hi = __ldcs(stage + 2 * (int64_t)i + 1);
+        const float v[7] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z};
+        const int off[7] = {-sxy, -nx, -1, 0, 1, nx, sxy};
+        const bool ok[7] = {z > 0, y > 0, x > 0, true, x < nx - 1, y < ny - 1, z < nz - 1};
         float sum = 0.0f;
 #pragma unroll
         for (int t = 0; t < 7; ++t)
@@ -983,6 +1060,32 @@ extern "C" int piro_ht_spmv_ordered(int nx, int ny, int nz, const int64_t *keys,
     k_ht_spmv<true><<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(nx, ny, nz, N, keys, vals, ts, dt, fe, order,
                                                                         u, out);
     PIRO_CHECK_LAUNCH("k_ht_spmv");
+    return PIRO_OK;
+}
+
+extern "C" int piro_ht_stage_bytes(int64_t N, size_t *bytes)
+{
+    PIRO_ARG(bytes && N > 0, "piro_ht_stage_bytes: bad arguments");
+    *bytes = 32 * (size_t)N;
+    return PIRO_OK;
+}
+
+extern "C" int piro_ht_spmv_staged(int nx, int ny, int nz, const int64_t *keys, const float *vals, int64_t ts,
+                                   float dt, int fe, const int32_t *order, void *stage, size_t stage_bytes,
+                                   const float *u, float *out, piro_stream_t stream)
+{
+    PIRO_ARG(grid_ok(nx, ny, nz) && keys && vals && ts > 0 && order && stage && u && out && u != out,
+             "piro_ht_spmv_staged: bad arguments");
+    const int64_t N = (int64_t)nx * ny * nz;
+    PIRO_ARG(N < INT32_MAX, "piro_ht_spmv_staged: more than 2^31 - 1 rows");
+    PIRO_ARG(stage_bytes >= 32 * (size_t)N && ((uintptr_t)stage & 15) == 0,
+             "piro_ht_spmv_staged: stage smaller than 32 bytes per row or not 16-byte aligned");
+    cudaStream_t s = as_stream(stream);
+    float4 *st = static_cast<float4 *>(stage);
+    k_ht_stage<<<grid_for(N, 256, 8), 256, 0, s>>>(nx, ny, nz, N, keys, vals, ts, order, st);
+    PIRO_CHECK_LAUNCH("k_ht_stage");
+    k_ht_stage_apply<<<grid_for(N, 256, 8), 256, 0, s>>>(nx, ny, nz, dt, fe, st, u, out);
+    PIRO_CHECK_LAUNCH("k_ht_stage_apply");
     return PIRO_OK;
 }
 

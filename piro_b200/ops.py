@@ -240,6 +240,20 @@ def ht_spmv_ordered(nx, ny, nz, keys, vals, dt, order, u, out, fe=False):
     return out
 
 
+def ht_stage(N):
+    """The 32-byte-per-row stage piro_ht_spmv_staged writes and reads."""
+    n = C.c_size_t()
+    check(lib().piro_ht_stage_bytes(N, C.byref(n)), "piro_ht_stage_bytes")
+    return torch.empty(n.value // 4, dtype=torch.float32, device="cuda")
+
+
+def ht_spmv_staged(nx, ny, nz, keys, vals, dt, order, stage, u, out, fe=False):
+    check(lib().piro_ht_spmv_staged(nx, ny, nz, _p(keys), _p(vals), keys.numel(), float(dt), int(fe), _p(order),
+                                    _p(stage), stage.numel() * stage.element_size(), _p(u), _p(out), _stream()),
+          "piro_ht_spmv_staged")
+    return out
+
+
 def stencil_fe_step(nx, ny, nz, dt, u, out, alpha=None, idx2=1.0, idy2=1.0, idz2=1.0):
     check(lib().piro_stencil_fe_step(nx, ny, nz, idx2, idy2, idz2, float(dt), _p(alpha), _p(u), _p(out), _stream()),
           "piro_stencil_fe_step")
