@@ -159,9 +159,13 @@ int piro_csr_i1(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *co
                 const float *u, float *out, piro_stream_t stream);
 
 /* SpMVCOO.cl:12-24 semantics with a warp-segmented reduction: out[r] =
- * dt * sum of vals*u[cols] over the entries of row r, for every row.  rows
- * must be sorted ascending (the Laplacian assembly order).  Summation order
- * differs from the sequential kernel (results agree to FP32 rounding). */
+ * dt * sum of vals*u[cols] over the entries of row r, for every row (rows
+ * without entries get dt*0).  rows must be sorted ascending (the Laplacian
+ * assembly order); ids outside [0, N) or unsorted rows return PIRO_ERR_ARG
+ * (the call synchronizes the stream to read the check).  Summation order
+ * differs from the sequential kernel (results agree to FP32 rounding) but is
+ * fixed: results do not vary from run to run.  With 16-byte aligned arrays
+ * the step is finished inside the reduction (no accumulator pass). */
 int piro_coo_spmv(int64_t N, int64_t nnz, const int32_t *rows, const int32_t *cols, const float *vals, float dt,
                   const float *u, float *out, piro_stream_t stream);
 
@@ -223,8 +227,11 @@ int piro_ht_spmv_staged(int nx, int ny, int nz, const int64_t *keys, const float
  * bandwidth bw (nx*ny for the 7-point grid), then factorizes it by Gaussian
  * elimination with partial pivoting in FP64, as LAPACK's banded LU (dgbtrf):
  * P A = L U with U's upper bandwidth 2bw, the first row of largest magnitude
- * chosen on a tie.  band is a device buffer of piro_ht_lu_band_bytes bytes
- * (band, multipliers, pivots and the solve's workspace).  PIRO_ERR_ARG when a
+ * chosen on a tie, by panels of 16 columns (8 or 4 for bands wider than
+ * about 1 600); the environment variable PIRO_LU_UNBLOCKED=1 selects the
+ * column-by-column form, which gives the same bits.  band is a device buffer
+ * of piro_ht_lu_band_bytes bytes (band, multipliers, pivots, the panels'
+ * multipliers and the solve's workspace).  PIRO_ERR_ARG when a
  * table entry lies outside the band; PIRO_ERR_ZERO_PIVOT when a column has no
  * nonzero at or below the diagonal (a singular matrix).  piro_ht_lu_solve
  * solves A x = b (b, x device float[N]) in FP64 -- the row exchanges and

@@ -258,21 +258,43 @@ __global__ void __launch_bounds__(kThreads) k_batch_step(BArgs A)
                 float *pn = ((s.it & 1) ? A.p0 : A.p1) + m.off;
                 float *qq = A.q + m.off;
                 const int nx = m.g.nx;
-                for (int64_t i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
-                    if (!m.g.interior(i)) {
+                // p = z + beta p_old at the cell and its six neighbours (boundary
+                // neighbours carry r = 0 and p_old = 0).  Two cells per
+                // iteration (i and i + blockDim.x, the thread's cells in their
+                // usual order) so that both cells' 14 loads are in flight together.
+                auto pv = [&](int64_t j) { return rr[j] * m.dinv + beta * po[j]; };
+                for (int64_t i = s0 + threadIdx.x; i < s1; i += 2 * blockDim.x) {
+                    const int64_t i2 = i + blockDim.x;
+                    const bool in1 = m.g.interior(i), in2 = i2 < s1 && m.g.interior(i2);
+                    float c1 = 0.0f, nb1 = 0.0f, c2 = 0.0f, nb2 = 0.0f;
+                    if (in1) {
+                        c1 = pv(i);
+                        nb1 = ((pv(i - 1) + pv(i + 1)) + (pv(i - nx) + pv(i + nx))) + (pv(i - sxy) + pv(i + sxy));
+                    }
+                    if (in2) {
+                        c2 = pv(i2);
+                        nb2 = ((pv(i2 - 1) + pv(i2 + 1)) + (pv(i2 - nx) + pv(i2 + nx))) + (pv(i2 - sxy) + pv(i2 + sxy));
+                    }
+                    if (in1) {
+                        const float qv = m.cd * c1 + m.co * nb1;
+                        pn[i] = c1;
+                        qq[i] = qv;
+                        v0 += (double)c1 * (double)qv;
+                    } else {
                         pn[i] = 0.0f;
                         qq[i] = 0.0f;
-                        continue;
                     }
-                    // p = z + beta p_old at the cell and its six neighbours (boundary
-                    // neighbours carry r = 0 and p_old = 0)
-                    auto pv = [&](int64_t j) { return rr[j] * m.dinv + beta * po[j]; };
-                    const float c = pv(i);
-                    const float nb = ((pv(i - 1) + pv(i + 1)) + (pv(i - nx) + pv(i + nx))) + (pv(i - sxy) + pv(i + sxy));
-                    const float qv = m.cd * c + m.co * nb;
-                    pn[i] = c;
-                    qq[i] = qv;
-                    v0 += (double)c * (double)qv;
+                    if (i2 < s1) {
+                        if (in2) {
+                            const float qv = m.cd * c2 + m.co * nb2;
+                            pn[i2] = c2;
+                            qq[i2] = qv;
+                            v0 += (double)c2 * (double)qv;
+                        } else {
+                            pn[i2] = 0.0f;
+                            qq[i2] = 0.0f;
+                        }
+                    }
                 }
             } else {
                 continue;

@@ -116,6 +116,22 @@ struct FastDiv {
     __device__ __forceinline__ uint32_t div(uint32_t n) const { return d == 1 ? n : __umulhi(n, m) >> sh; }
 };
 
+// x mod d for 64-bit x and d >= 1 by a multiply-high with floor((2^64-1)/d)
+// (Barrett reduction): the estimated quotient is at most 2 below the true one,
+// so two conditional subtractions give the exact remainder.
+struct ModU64 {
+    uint64_t d, m;
+    ModU64() = default;
+    __host__ explicit ModU64(uint64_t div) : d(div), m(div > 1 ? ~0ull / div : 0) {}
+    __device__ __forceinline__ uint64_t mod(uint64_t x) const
+    {
+        if (d == 1) return 0;
+        uint64_t r = x - __umul64hi(x, m) * d;
+        r = r >= d ? r - d : r;
+        return r >= d ? r - d : r;
+    }
+};
+
 // Grid with fast coordinate decomposition of a linear index i < 2^31.
 struct GridDiv {
     int nx, ny, nz;

@@ -119,9 +119,9 @@ __global__ void k_geam3_count(int64_t N, const int32_t *__restrict__ rpA, const 
 // whose row pointers are not monotone) runs the same merge per lane on
 // global memory instead.
 constexpr int kGeamWarps = 8;
-constexpr int kGeamCap = 128;  // staged entries per input and warp (about 4 per row)
+constexpr int kGeamCap = 64;  // staged entries per input and warp (2 per row: a gradient matrix)
 
-__global__ void __launch_bounds__(kGeamWarps * 32) k_geam3_fill_warp(
+__global__ void __launch_bounds__(kGeamWarps * 32, 6) k_geam3_fill_warp(
     int64_t N, const int32_t *__restrict__ rpA, const int32_t *__restrict__ cA, const float *__restrict__ vA,
     const int32_t *__restrict__ rpB, const int32_t *__restrict__ cB, const float *__restrict__ vB,
     const int32_t *__restrict__ rpC, const int32_t *__restrict__ cC, const float *__restrict__ vC,

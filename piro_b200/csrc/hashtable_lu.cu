@@ -33,10 +33,12 @@
 // r*N + c of one row are contiguous, so at load 0.7 the rows' runs of slots
 // merge and a table lookup walks thousands of slots.  The factorization is
 // Gaussian elimination with partial pivoting in FP64 (LAPACK's banded LU,
-// dgbtrf): per pivot row one launch chooses the pivot, exchanges the two
-// rows and forms the multipliers, a second applies the rank-1 update to the
-// (bw x 2bw) block below and right of it.  The solve (one block, FP64)
-// replays the exchanges and Gauss transforms on b and back-substitutes.
+// dgbtrf), by panels of 16 columns: one block factors the panel in shared
+// memory, then the exchanges and the pivot rows' U part right of it, then a
+// tiled update of the (bw x 2bw) block below and right of it (the column-by-
+// column form -- one pivot launch and one rank-1 update launch per row --
+// remains, and gives the same bits).  The solve (one block, FP64) replays the
+// exchanges and Gauss transforms on b and back-substitutes.
 #include "common.cuh"
 
 namespace piro {
@@ -398,6 +400,269 @@ __global__ void __launch_bounds__(kUpdThreads) k_lup_update(int64_t N, int64_t b
         a[j] = fma(-l, u[j], a[j]);
 }
 
+// The same factorization by panels of nb columns (LAPACK's blocked dgbtrf
+// scheme), bit for bit the result of the column-by-column launches above:
+//   1. k_lupb_panel (one block): the panel's rows j0 .. j0+nb-1+bw and
+//      columns j0 .. j0+nb-1 in shared memory; per column the pivot search,
+//      the exchange inside the panel, the multipliers (to the band and Lc)
+//      and the rank-1 update of the panel's later columns, each element by
+//      the same fma as the column launches.  The exchanges of the columns
+//      right of the panel are deferred; Lw gets the multipliers as the later
+//      exchanges of the panel see them (the multiplier of step k for the row
+//      that ends at position r is the one stored at the position that row
+//      held at step k).
+//   2. k_lupb_rows (a thread per column right of the panel): the panel's nb
+//      exchanges in order, then the pivot rows j0 .. j0+nb-1 updated with
+//      Lw (forward substitution with the unit lower triangle).
+//   3. k_lupb_update (64 x 64 tiles): a(r, c) -= sum over k of Lw(r, k) *
+//      a(j0+k, c) for the rows below the panel, k ascending, as the column
+//      launches apply their steps.
+// Every update is skipped where the column launches skip it: a zero
+// multiplier, or a column more than 2bw right of the step's pivot.
+constexpr int kLuNbMax = 16;
+constexpr int kLuTile = 64;
+
+__device__ __forceinline__ double *band_at(double *band, int64_t W, int64_t bw, int64_t r, int64_t c)
+{
+    return band + r * W + (c - r + bw);
+}
+
+__device__ __forceinline__ bool in_band(int64_t bw, int64_t r, int64_t c)
+{
+    const int64_t d = c - r + bw;
+    return d >= 0 && d <= 3 * bw;
+}
+
+__global__ void __launch_bounds__(kPivThreads) k_lupb_panel(int64_t N, int64_t bw, int64_t W,
+                                                            double *__restrict__ band, double *__restrict__ Lc,
+                                                            int32_t *__restrict__ piv, double *__restrict__ Lw,
+                                                            int64_t j0, int nbp, int nb, int *err)
+{
+    extern __shared__ double s_p[];  // [R][ld], ld = nb + 1: a column read across rows is bank-conflict free
+    __shared__ double s_v[32];
+    __shared__ int s_i[32];
+    __shared__ int s_prow;
+    __shared__ int32_t s_piv[kLuNbMax];
+    if (*((volatile int *)err)) return;
+    const int ld = nb + 1;
+    const int64_t rmax = j0 + nbp - 1 + bw < N - 1 ? j0 + nbp - 1 + bw : N - 1;
+    const int R = (int)(rmax - j0 + 1);
+    for (int idx = threadIdx.x; idx < R * nbp; idx += blockDim.x) {
+        const int r = idx / nbp, cc = idx - r * nbp;
+        const int64_t gr = j0 + r, gc = j0 + cc;
+        s_p[r * ld + cc] = in_band(bw, gr, gc) ? *band_at(band, W, bw, gr, gc) : 0.0;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // argmax of |column jj| over rows jj .. jj+span (first on a tie), from the
+    // per-thread candidates (best, bi) of the caller; the result in s_prow
+    auto pick = [&](double best, int bi, int jj) {
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_down_sync(0xffffffffu, best, o);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) {
+                best = ov;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            s_v[warp] = best;
+            s_i[warp] = bi;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            best = lane < (int)(blockDim.x >> 5) ? s_v[lane] : -1.0;
+            bi = lane < (int)(blockDim.x >> 5) ? s_i[lane] : 0;
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_down_sync(0xffffffffu, best, o);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+                if (ov > best || (ov == best && oi < bi)) {
+                    best = ov;
+                    bi = oi;
+                }
+            }
+            if (lane == 0) {
+                const int64_t j = j0 + jj;
+                s_prow = best > 0.0 ? bi : -1;
+                piv[j] = (int32_t)(j + (best > 0.0 ? bi : 0));
+                s_piv[jj] = (int32_t)(j + (best > 0.0 ? bi : 0));
+                if (best <= 0.0 && atomicCAS(err, 0, 3) == 0) err[1] = (int)j;
+            }
+        }
+        __syncthreads();
+    };
+    {   // the first column's pivot
+        const int span0 = (int)(N - 1 - j0 < bw ? N - 1 - j0 : bw);
+        double best = -1.0;
+        int bi = 0;
+        for (int t = threadIdx.x; t <= span0; t += blockDim.x) {
+            const double v = fabs(s_p[t * ld]);
+            if (v > best) {
+                best = v;
+                bi = t;
+            }
+        }
+        pick(best, bi, 0);
+    }
+    for (int jj = 0; jj < nbp; ++jj) {
+        const int64_t j = j0 + jj;
+        const int span = (int)(N - 1 - j < bw ? N - 1 - j : bw);
+        const int64_t cend = N - 1 - j < 2 * bw ? N - 1 - j : 2 * bw;  // columns j .. j+cend take part
+        const int p = s_prow;
+        if (p < 0) return;  // singular: the later launches see *err and return
+        const int ccend = (int)(jj + cend < nbp - 1 ? jj + cend : nbp - 1);  // last panel column of this step
+        if (p > 0)
+            for (int cc = jj + threadIdx.x; cc <= ccend; cc += blockDim.x) {
+                const double t = s_p[jj * ld + cc];
+                s_p[jj * ld + cc] = s_p[(jj + p) * ld + cc];
+                s_p[(jj + p) * ld + cc] = t;
+            }
+        __syncthreads();
+        // per row below the pivot: the multiplier, the update of the row's later
+        // panel columns, and the row's candidate for the next column's pivot
+        const double pv = s_p[jj * ld + jj];
+        const bool next = jj + 1 < nbp;
+        const int span_n = next ? (int)(N - 1 - (j + 1) < bw ? N - 1 - (j + 1) : bw) : -1;  // next column's rows
+        double best = -1.0;
+        int bi = 0;
+        for (int t = 1 + threadIdx.x; t <= span || (next && t <= span_n + 1); t += blockDim.x) {
+            double *row = s_p + (jj + t) * ld;
+            if (t <= span) {
+                const double l = row[jj] / pv;
+                row[jj] = l;
+                Lc[j * bw + t - 1] = l;
+                if (l != 0.0)
+                    for (int cc = jj + 1; cc <= ccend; ++cc) row[cc] = fma(-l, s_p[jj * ld + cc], row[cc]);
+            }
+            if (next && t <= span_n + 1) {  // row j + t is candidate t - 1 of column j + 1
+                const double v = fabs(row[jj + 1]);
+                if (v > best) {
+                    best = v;
+                    bi = t - 1;
+                }
+            }
+        }
+        if (next) pick(best, bi, jj + 1);
+        else __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < R * nbp; idx += blockDim.x) {
+        const int r = idx / nbp, cc = idx - r * nbp;
+        const int64_t gr = j0 + r, gc = j0 + cc;
+        if (in_band(bw, gr, gc)) *band_at(band, W, bw, gr, gc) = s_p[r * ld + cc];
+    }
+    // Lw[r][k]: the multiplier of step k for the row that ends at position j0 + r
+    for (int idx = threadIdx.x; idx < R * nbp; idx += blockDim.x) {
+        const int r = idx / nbp, k = idx - r * nbp;
+        int64_t q = j0 + r;
+        for (int kk = nbp - 1; kk > k; --kk) {
+            const int64_t pk = s_piv[kk];
+            if (q == j0 + kk) q = pk;
+            else if (q == pk) q = j0 + kk;
+        }
+        const int64_t rel = q - (j0 + k);
+        const int64_t span_k = N - 1 - (j0 + k) < bw ? N - 1 - (j0 + k) : bw;
+        Lw[(int64_t)r * kLuNbMax + k] = rel >= 1 && rel <= span_k ? s_p[(q - j0) * ld + k] : 0.0;
+    }
+}
+
+// Right of the panel: the deferred exchanges, then the pivot rows' U part.
+__global__ void k_lupb_rows(int64_t N, int64_t bw, int64_t W, double *__restrict__ band,
+                            const int32_t *__restrict__ piv, const double *__restrict__ Lw, int64_t j0, int nbp,
+                            const int *err)
+{
+    if (*((volatile const int *)err)) return;
+    const int64_t cmax = j0 + nbp - 1 + 2 * bw < N - 1 ? j0 + nbp - 1 + 2 * bw : N - 1;
+    const int64_t c = j0 + nbp + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > cmax) return;
+    for (int k = 0; k < nbp; ++k) {
+        const int64_t j = j0 + k, p = piv[j];
+        if (p != j && c <= j + 2 * bw) {
+            double *a = band_at(band, W, bw, j, c), *b = band_at(band, W, bw, p, c);
+            const double t = *a;
+            *a = *b;
+            *b = t;
+        }
+    }
+    for (int i = 1; i < nbp; ++i) {
+        double *a = band_at(band, W, bw, j0 + i, c);
+        if (!in_band(bw, j0 + i, c)) continue;
+        double acc = *a;
+        for (int k = 0; k < i; ++k) {
+            const double l = Lw[(int64_t)i * kLuNbMax + k];
+            if (l != 0.0 && c <= j0 + k + 2 * bw) acc = fma(-l, *band_at(band, W, bw, j0 + k, c), acc);
+        }
+        *a = acc;
+    }
+}
+
+// Rows below the panel: 64 x 64 tiles, 256 threads, 4 x 4 elements each
+// (rows ty + 16 m, columns tx + 16 n: consecutive threads on consecutive
+// columns).
+__global__ void __launch_bounds__(256) k_lupb_update(int64_t N, int64_t bw, int64_t W, double *__restrict__ band,
+                                                     const double *__restrict__ Lw, int64_t j0, int nbp,
+                                                     const int *err)
+{
+    __shared__ double s_l[kLuTile][kLuNbMax + 1];
+    __shared__ double s_u[kLuNbMax][kLuTile];
+    if (*((volatile const int *)err)) return;
+    const int64_t rfirst = j0 + nbp;
+    const int64_t rmax = j0 + nbp - 1 + bw < N - 1 ? j0 + nbp - 1 + bw : N - 1;
+    const int64_t cmax = j0 + nbp - 1 + 2 * bw < N - 1 ? j0 + nbp - 1 + 2 * bw : N - 1;
+    const int64_t r0 = rfirst + (int64_t)blockIdx.y * kLuTile, c0 = rfirst + (int64_t)blockIdx.x * kLuTile;
+    if (r0 > rmax || c0 > cmax) return;
+    for (int idx = threadIdx.x; idx < kLuTile * kLuNbMax; idx += blockDim.x) {
+        const int r = idx / kLuNbMax, k = idx - r * kLuNbMax;
+        const int64_t gr = r0 + r;
+        s_l[r][k] = (k < nbp && gr <= rmax) ? Lw[(gr - j0) * kLuNbMax + k] : 0.0;
+    }
+    for (int idx = threadIdx.x; idx < kLuNbMax * kLuTile; idx += blockDim.x) {
+        const int k = idx / kLuTile, cc = idx - k * kLuTile;
+        const int64_t gc = c0 + cc;
+        s_u[k][cc] = (k < nbp && gc <= cmax && gc <= j0 + k + 2 * bw) ? *band_at(band, W, bw, j0 + k, gc) : 0.0;
+    }
+    __syncthreads();
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    // all 16 elements loaded first (16 loads in flight per thread), then the
+    // steps in order on the 16 accumulators
+    double acc[4][4];
+    unsigned ok = 0, upd = 0;
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            const int64_t gr = r0 + ty + 16 * m, gc = c0 + tx + 16 * n;
+            const bool e = gr <= rmax && gc <= cmax && in_band(bw, gr, gc);
+            acc[m][n] = e ? *band_at(band, W, bw, gr, gc) : 0.0;
+            ok |= e ? 1u << (4 * m + n) : 0u;
+        }
+    for (int k = 0; k < nbp; ++k) {
+        double l[4], u[4];
+        bool cu[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) l[m] = s_l[ty + 16 * m][k];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            u[n] = s_u[k][tx + 16 * n];
+            cu[n] = c0 + tx + 16 * n <= j0 + k + 2 * bw;
+        }
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+#pragma unroll
+            for (int n = 0; n < 4; ++n)
+                if (l[m] != 0.0 && cu[n]) {
+                    acc[m][n] = fma(-l[m], u[n], acc[m][n]);
+                    upd |= 1u << (4 * m + n);
+                }
+    }
+    upd &= ok;
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int n = 0; n < 4; ++n)
+            if (upd & (1u << (4 * m + n)))
+                *band_at(band, W, bw, r0 + ty + 16 * m, c0 + tx + 16 * n) = acc[m][n];
+}
+
 // Solve with the factor (one block): y = b in FP64; per step ro the row
 // exchange and the Gauss transform y[ro+t] -= l(t) y[ro]; then x from U,
 // row by row from the last (each row a block-wide dot product over its at
@@ -445,11 +710,172 @@ __global__ void __launch_bounds__(kPivThreads) k_lup_solve(int64_t N, int64_t bw
     for (int64_t r = threadIdx.x; r < N; r += blockDim.x) x[r] = (float)y[r];
 }
 
+// The solve by the same 16-row panels.  Lp holds, per panel of 16 steps
+// starting at j0, the multipliers as the panel's later exchanges see them
+// ([bw + 16][16] doubles per panel, row r = position j0 + r), built once per
+// factorization from Lc and the pivots.  The forward pass per panel: the 16
+// exchanges on y, the unit lower triangle (one thread, steps in order), then
+// the rows below it (a thread per row, steps in order); the backward pass per
+// panel from the last: for each of its rows the dot product with the solved
+// x right of the panel (a warp per row), then the triangle (one thread).  Two
+// block barriers per panel and pass, against two per row in k_lup_solve.
+constexpr int kLuSolveNb = 16;
+
+__global__ void k_lup_lw_from_lc(int64_t N, int64_t bw, const double *__restrict__ Lc,
+                                 const int32_t *__restrict__ piv, double *__restrict__ Lp)
+{
+    const int64_t R = bw + kLuSolveNb;
+    const int64_t npan = cdiv(N, kLuSolveNb);
+    const int64_t total = npan * R * kLuSolveNb;
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pi = idx / (R * kLuSolveNb);
+        const int64_t rem = idx - pi * R * kLuSolveNb;
+        const int r = (int)(rem / kLuSolveNb), k = (int)(rem - (int64_t)r * kLuSolveNb);
+        const int64_t j0 = pi * kLuSolveNb;
+        const int nbp = (int)(N - j0 < kLuSolveNb ? N - j0 : kLuSolveNb);
+        double v = 0.0;
+        if (k < nbp && j0 + r < N) {
+            int64_t q = j0 + r;
+            for (int kk = nbp - 1; kk > k; --kk) {
+                const int64_t pk = piv[j0 + kk];
+                if (q == j0 + kk) q = pk;
+                else if (q == pk) q = j0 + kk;
+            }
+            const int64_t rel = q - (j0 + k);
+            const int64_t span_k = N - 1 - (j0 + k) < bw ? N - 1 - (j0 + k) : bw;
+            if (rel >= 1 && rel <= span_k) v = Lc[(j0 + k) * bw + rel - 1];
+        }
+        Lp[idx] = v;
+    }
+}
+
+__global__ void __launch_bounds__(kPivThreads) k_lup_solve_panels(int64_t N, int64_t bw, int64_t W,
+                                                                  const double *__restrict__ band,
+                                                                  const double *__restrict__ Lp,
+                                                                  const int32_t *__restrict__ piv,
+                                                                  const float *__restrict__ b, double *__restrict__ y,
+                                                                  float *__restrict__ x)
+{
+    // The sequential parts of a panel (its exchanges, its triangle) run in one
+    // thread on shared-memory copies that the block loads in parallel first,
+    // so that no dependent chain waits on global memory.
+    constexpr int P = kLuSolveNb;
+    __shared__ double s_y[P];        // y of the panel's rows
+    __shared__ double s_t[P][P + 1]; // the panel's triangle: Lw (forward) or U (backward)
+    __shared__ double s_far[P];      // y at each step's pivot row, before the panel's exchanges
+    __shared__ int64_t s_pos[P];     // rows outside the panel that the exchanges touch, and their values
+    __shared__ double s_val[P];
+    __shared__ int32_t s_piv[P];
+    __shared__ double s_dot[P];
+    const int64_t R = bw + P;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int64_t r = threadIdx.x; r < N; r += blockDim.x) y[r] = (double)b[r];
+    __syncthreads();
+    const int64_t npan = cdiv(N, P);
+    for (int64_t pi = 0; pi < npan; ++pi) {
+        const int64_t j0 = pi * P;
+        const int nbp = (int)(N - j0 < P ? N - j0 : P);
+        const double *lw = Lp + pi * R * P;
+        // parallel loads: pivots, y of the panel and of the pivot rows, the triangle of Lw
+        if (threadIdx.x < nbp) {
+            const int32_t p = piv[j0 + threadIdx.x];
+            s_piv[threadIdx.x] = p;
+            s_y[threadIdx.x] = y[j0 + threadIdx.x];
+            s_far[threadIdx.x] = y[p];
+        }
+        for (int t = threadIdx.x; t < P * P; t += blockDim.x) {
+            const int i = t / P, k = t - i * P;
+            s_t[i][k] = (i < nbp && k < i) ? lw[i * P + k] : 0.0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int nfar = 0;
+            for (int k = 0; k < nbp; ++k) {
+                const int64_t p = s_piv[k];
+                if (p == j0 + k) continue;
+                double *vb;
+                if (p < j0 + nbp) {
+                    vb = &s_y[p - j0];
+                } else {
+                    int f = 0;
+                    while (f < nfar && s_pos[f] != p) ++f;
+                    if (f == nfar) {  // first touch in this panel: y[p] as loaded
+                        s_pos[f] = p;
+                        s_val[f] = s_far[k];
+                        ++nfar;
+                    }
+                    vb = &s_val[f];
+                }
+                const double t = s_y[k];
+                s_y[k] = *vb;
+                *vb = t;
+            }
+            for (int f = 0; f < nfar; ++f) y[s_pos[f]] = s_val[f];
+            for (int i = 0; i < nbp; ++i) {
+                double acc = s_y[i];
+                for (int k = 0; k < i; ++k) {
+                    const double l = s_t[i][k];
+                    if (l != 0.0 && s_y[k] != 0.0) acc = fma(-l, s_y[k], acc);
+                }
+                s_y[i] = acc;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < nbp) y[j0 + threadIdx.x] = s_y[threadIdx.x];
+        const int64_t rmax = j0 + nbp - 1 + bw < N - 1 ? j0 + nbp - 1 + bw : N - 1;
+        for (int64_t r = j0 + nbp + threadIdx.x; r <= rmax; r += blockDim.x) {
+            double acc = y[r];
+            for (int k = 0; k < nbp; ++k) {
+                const double l = lw[(r - j0) * P + k];
+                if (l != 0.0 && s_y[k] != 0.0) acc = fma(-l, s_y[k], acc);
+            }
+            y[r] = acc;
+        }
+        __syncthreads();
+    }
+    // back substitution, panels from the last; y[r] becomes x[r]
+    for (int64_t pi = npan - 1; pi >= 0; --pi) {
+        const int64_t j0 = pi * P;
+        const int nbp = (int)(N - j0 < P ? N - j0 : P);
+        const int64_t jend = j0 + nbp;  // first column right of the panel
+        for (int i = warp; i < nbp; i += nwarp) {
+            const int64_t r = j0 + i;
+            const int64_t cmax = r + 2 * bw < N - 1 ? r + 2 * bw : N - 1;
+            double sum = 0.0;
+            for (int64_t c = jend + lane; c <= cmax; c += 32) sum = fma(band[r * W + (c - r + bw)], y[c], sum);
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if (lane == 0) s_dot[i] = sum;
+        }
+        // U of the panel's rows and columns (diagonal included), and their y
+        for (int t = threadIdx.x; t < P * P; t += blockDim.x) {
+            const int i = t / P, c = t - i * P;
+            const int64_t r = j0 + i, gc = j0 + c;
+            s_t[i][c] = (i < nbp && c < nbp && c >= i && gc <= r + 2 * bw) ? band[r * W + (gc - r + bw)] : 0.0;
+        }
+        if (threadIdx.x < nbp) s_y[threadIdx.x] = y[j0 + threadIdx.x];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int i = nbp - 1; i >= 0; --i) {
+                double sum = s_dot[i];
+                for (int c = i + 1; c < nbp; ++c) sum = fma(s_t[i][c], s_y[c], sum);
+                s_y[i] = (s_y[i] - sum) / s_t[i][i];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < nbp) y[j0 + threadIdx.x] = s_y[threadIdx.x];
+        __syncthreads();
+    }
+    for (int64_t r = threadIdx.x; r < N; r += blockDim.x) x[r] = (float)y[r];
+}
+
 // Device layout of the factor buffer: band double[N][3bw+1], Lc double[N][bw],
-// y double[N] (the solve's workspace), piv int32[N], err int[2].
+// y double[N] (the solve's workspace), piv int32[N], err int[2], Lw
+// double[bw + 16][16] (the blocked factorization's panel multipliers), Lp
+// double[ceil(N/16)][bw + 16][16] (the solve's panel multipliers).
 struct LupLayout {
     int64_t W;
-    size_t band, lc, y, piv, err, total;  // byte offsets
+    size_t band, lc, y, piv, err, lw, lp, total;  // byte offsets
 };
 
 int lup_layout(int64_t N, int64_t bw, LupLayout *L)
@@ -462,7 +888,9 @@ int lup_layout(int64_t N, int64_t bw, LupLayout *L)
     L->y = L->lc + up(sizeof(double) * (size_t)N * (size_t)bw);
     L->piv = L->y + up(sizeof(double) * (size_t)N);
     L->err = L->piv + up(sizeof(int32_t) * (size_t)N);
-    L->total = L->err + 256;
+    L->lw = L->err + 256;
+    L->lp = L->lw + up(sizeof(double) * (size_t)(bw + kLuNbMax) * kLuNbMax);
+    L->total = L->lp + up(sizeof(double) * (size_t)cdiv(N, kLuSolveNb) * (size_t)(bw + kLuSolveNb) * kLuSolveNb);
     return PIRO_OK;
 }
 
@@ -554,22 +982,53 @@ extern "C" int piro_ht_lu_factor(int64_t N, int64_t bw, const int64_t *keys, con
         set_error("piro_ht_lu_factor: the table holds an entry outside the bandwidth %lld", (long long)bw);
         return PIRO_ERR_ARG;
     }
-    for (int64_t ro = 0; ro < N; ++ro) {
-        k_lup_pivot<<<1, kPivThreads, 0, st>>>(N, bw, W, AB, Lc, piv, ro, err);
-        const int64_t span = N - 1 - ro < bw ? N - 1 - ro : bw;
-        const int64_t cend = N - 1 - ro < 2 * bw ? N - 1 - ro : 2 * bw;
-        if (span > 0 && cend > 0) {
-            const dim3 grid((unsigned)cdiv(cend, kUpdThreads), (unsigned)span);
-            k_lup_update<<<grid, kUpdThreads, 0, st>>>(N, bw, W, AB, ro, err);
+    // panel width: the widest of 16, 8, 4 whose panel (bw + nb rows) fits in
+    // 200 KB of shared memory; PIRO_LU_UNBLOCKED=1 forces the column launches
+    int nb = 0;
+    for (int t = kLuNbMax; t >= 4 && !nb; t /= 2)
+        if ((size_t)(bw + t) * (t + 1) * sizeof(double) <= 200 * 1024) nb = t;
+    const char *ub = getenv("PIRO_LU_UNBLOCKED");
+    if (ub && ub[0] == '1') nb = 0;
+    if (nb) {
+        double *Lw = reinterpret_cast<double *>(base + L.lw);
+        const size_t smem = (size_t)(bw + nb) * (nb + 1) * sizeof(double);
+        PIRO_CUDA(cudaFuncSetAttribute(k_lupb_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        for (int64_t j0 = 0; j0 < N; j0 += nb) {
+            const int nbp = (int)(N - j0 < nb ? N - j0 : nb);
+            k_lupb_panel<<<1, kPivThreads, smem, st>>>(N, bw, W, AB, Lc, piv, Lw, j0, nbp, nb, err);
+            const int64_t rmax = j0 + nbp - 1 + bw < N - 1 ? j0 + nbp - 1 + bw : N - 1;
+            const int64_t cmax = j0 + nbp - 1 + 2 * bw < N - 1 ? j0 + nbp - 1 + 2 * bw : N - 1;
+            const int64_t ncols = cmax - (j0 + nbp) + 1, nrows = rmax - (j0 + nbp) + 1;
+            if (ncols > 0) {
+                k_lupb_rows<<<(unsigned)cdiv(ncols, 128), 128, 0, st>>>(N, bw, W, AB, piv, Lw, j0, nbp, err);
+                if (nrows > 0)
+                    k_lupb_update<<<dim3((unsigned)cdiv(ncols, kLuTile), (unsigned)cdiv(nrows, kLuTile)), 256, 0,
+                                    st>>>(N, bw, W, AB, Lw, j0, nbp, err);
+            }
         }
+        PIRO_CHECK_LAUNCH("k_lupb_update");
+    } else {
+        for (int64_t ro = 0; ro < N; ++ro) {
+            k_lup_pivot<<<1, kPivThreads, 0, st>>>(N, bw, W, AB, Lc, piv, ro, err);
+            const int64_t span = N - 1 - ro < bw ? N - 1 - ro : bw;
+            const int64_t cend = N - 1 - ro < 2 * bw ? N - 1 - ro : 2 * bw;
+            if (span > 0 && cend > 0) {
+                const dim3 grid((unsigned)cdiv(cend, kUpdThreads), (unsigned)span);
+                k_lup_update<<<grid, kUpdThreads, 0, st>>>(N, bw, W, AB, ro, err);
+            }
+        }
+        PIRO_CHECK_LAUNCH("k_lup_update");
     }
-    PIRO_CHECK_LAUNCH("k_lup_update");
     PIRO_CUDA(cudaMemcpyAsync(herr, err, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     PIRO_CUDA(cudaStreamSynchronize(st));
     if (herr[0] == 3) {
         set_error("piro_ht_lu_factor: singular matrix: column %d has no nonzero at or below the diagonal", herr[1]);
         return PIRO_ERR_ZERO_PIVOT;
     }
+    const int64_t lp_items = cdiv(N, kLuSolveNb) * (bw + kLuSolveNb) * kLuSolveNb;
+    k_lup_lw_from_lc<<<grid_for(lp_items, 256, 8), 256, 0, st>>>(N, bw, Lc, piv,
+                                                                   reinterpret_cast<double *>(base + L.lp));
+    PIRO_CHECK_LAUNCH("k_lup_lw_from_lc");
     return PIRO_OK;
 }
 
@@ -582,11 +1041,20 @@ extern "C" int piro_ht_lu_solve(int64_t N, int64_t bw, void *band, size_t band_b
     PIRO_ARG(band_bytes >= L.total, "piro_ht_lu_solve: band buffer too small (piro_ht_lu_band_bytes)");
     cudaStream_t st = as_stream(stream);
     char *base = static_cast<char *>(band);
-    k_lup_solve<<<1, kPivThreads, 0, st>>>(N, bw, L.W, reinterpret_cast<const double *>(base + L.band),
-                                          reinterpret_cast<const double *>(base + L.lc),
-                                          reinterpret_cast<const int32_t *>(base + L.piv), b,
-                                          reinterpret_cast<double *>(base + L.y), x);
-    PIRO_CHECK_LAUNCH("k_lup_solve");
+    const char *ub = getenv("PIRO_LU_UNBLOCKED");
+    if (ub && ub[0] == '1') {
+        k_lup_solve<<<1, kPivThreads, 0, st>>>(N, bw, L.W, reinterpret_cast<const double *>(base + L.band),
+                                              reinterpret_cast<const double *>(base + L.lc),
+                                              reinterpret_cast<const int32_t *>(base + L.piv), b,
+                                              reinterpret_cast<double *>(base + L.y), x);
+        PIRO_CHECK_LAUNCH("k_lup_solve");
+    } else {
+        k_lup_solve_panels<<<1, kPivThreads, 0, st>>>(N, bw, L.W, reinterpret_cast<const double *>(base + L.band),
+                                                     reinterpret_cast<const double *>(base + L.lp),
+                                                     reinterpret_cast<const int32_t *>(base + L.piv), b,
+                                                     reinterpret_cast<double *>(base + L.y), x);
+        PIRO_CHECK_LAUNCH("k_lup_solve_panels");
+    }
     return PIRO_OK;
 }
 

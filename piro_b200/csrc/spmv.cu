@@ -181,32 +181,54 @@ __global__ void k_coo_segsum(int64_t N, int64_t nnz, const int32_t *__restrict__
     if (bad) atomicOr(err, bad);
 }
 
-// The same sum with 8 consecutive entries per lane (a warp covers 256 per
-// pass): 16-byte loads of rows, cols and vals, runs of equal row ids summed
-// sequentially in the lane, and one segmented scan per warp over the lanes'
-// last runs instead of one per entry.  With ascending row ids a row's entries
-// are contiguous, so a run that starts and ends inside a lane is the whole
-// row (a plain store); a lane's last run continues into the next lane when
-// that lane starts with the same row, and the scan carries its sum there.  A
-// row that touches either end of the warp's 256-entry span is added
-// atomically in every span it appears in (at most two contributions for rows
-// of <= 256 entries, so the sum does not depend on their order).  Same input
-// checks as k_coo_segsum.  Requires 16-byte aligned arrays; acc must be zero.
+// The same sum with 8 consecutive entries per lane (a warp covers a 256-entry
+// span per pass), and the step finished in place: 16-byte loads of rows,
+// cols and vals, runs of equal row ids summed sequentially in the lane, and
+// one segmented scan per warp over the lanes' last runs instead of one per
+// entry.  With ascending row ids a row's entries are contiguous, so a run
+// that starts and ends inside a lane is the whole row; a lane's last run
+// continues into the next lane when that lane starts with the same row, and
+// the scan carries its sum there.  A row complete inside the span is
+// written at once, out = dt*sum or u + dt*sum (SpMVCOO's C[row] =
+// deltat*result, then addVectors); rows without entries get dt*0 (+ u).  A
+// row that crosses a span boundary leaves its part in this span as
+// part_first[span] (the row began in an earlier span) or part_last[span]
+// (it begins here), and k_coo_span_fixup adds the parts in span order: no
+// atomics, so the sums do not depend on scheduling.  Same input checks as
+// k_coo_segsum.  Requires 16-byte aligned arrays.
 constexpr int kCooPer = 8;
+constexpr int kCooSpan = 32 * kCooPer;
+
+__device__ __forceinline__ float coo_finish(float sum, float dt, int fe, const float *__restrict__ u, int64_t r)
+{
+    const float c = __fmul_rn(dt, sum);
+    return fe ? __fadd_rn(__ldg(u + r), c) : c;
+}
+
+// rows [r0, r1) hold no entry (clamped to [0, N))
+__device__ __forceinline__ void coo_empty_rows(int64_t r0, int64_t r1, int64_t N, float dt, int fe,
+                                               const float *__restrict__ u, float *__restrict__ out)
+{
+    r0 = r0 < 0 ? 0 : r0;
+    r1 = r1 > N ? N : r1;
+    for (int64_t r = r0; r < r1; ++r) out[r] = coo_finish(0.0f, dt, fe, u, r);
+}
 
 __global__ void __launch_bounds__(256) k_coo_segsum8(int64_t N, int64_t nnz, const int32_t *__restrict__ rows,
                                                      const int32_t *__restrict__ cols,
                                                      const float *__restrict__ vals, const float *__restrict__ u,
-                                                     float *__restrict__ acc, int *__restrict__ err)
+                                                     float dt, int fe, float *__restrict__ out,
+                                                     float *__restrict__ part_first, float *__restrict__ part_last,
+                                                     int *__restrict__ err)
 {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    constexpr int kSpan = 32 * kCooPer;
     constexpr int kNone = INT32_MAX;  // row id of entries past the end
     int bad = 0;
-    for (int64_t base = warp * kSpan; base < nnz; base += nwarps * kSpan) {
+    for (int64_t base = warp * kCooSpan; base < nnz; base += nwarps * kCooSpan) {
         const int64_t k0 = base + (int64_t)lane * kCooPer;
+        const int64_t sidx = base / kCooSpan;
         int r[kCooPer], c[kCooPer];
         float v[kCooPer];
         if (k0 + kCooPer <= nnz) {
@@ -254,8 +276,9 @@ __global__ void __launch_bounds__(256) k_coo_segsum8(int64_t N, int64_t nnz, con
         for (int t = 0; t < kCooPer; ++t) {
             const float pv = r[t] != kNone ? __fmul_rn(v[t], __ldg(u + c[t])) : 0.0f;
             if (r[t] != cur) {
-                if (!multi) head = s_run;                                  // the lane's first run
-                else if (cur >= 0 && cur < N) acc[cur] = s_run;            // a whole row inside the lane
+                if (!multi) head = s_run;                                               // the lane's first run
+                else if (cur >= 0 && cur < N) out[cur] = coo_finish(s_run, dt, fe, u, cur);  // a whole row
+                if (r[t] != kNone) coo_empty_rows((int64_t)cur + 1, r[t], N, dt, fe, u, out);
                 multi = true;
                 cur = r[t];
                 s_run = 0.0f;
@@ -280,23 +303,60 @@ __global__ void __launch_bounds__(256) k_coo_segsum8(int64_t N, int64_t nnz, con
         const float cin = __shfl_up_sync(0xffffffffu, carry, 1);
         const int kin = __shfl_up_sync(0xffffffffu, last, 1);
         const int next_first = __shfl_down_sync(0xffffffffu, first, 1);
-        const int64_t span_end = base + kSpan < nnz ? base + kSpan : nnz;
+        const int64_t span_end = base + kCooSpan < nnz ? base + kCooSpan : nnz;
         const int left_row = base > 0 ? __ldg(rows + (base - 1)) : INT32_MIN;   // row of the entry before the span
         const int right_row = span_end < nnz ? __ldg(rows + span_end) : kNone;  // row of the entry after it
         if (multi && first >= 0 && first < N) {
             // the lane's first run ends here: add what the lanes before carried in
             const float h = (lane > 0 && kin == first) ? __fadd_rn(cin, head) : head;
-            if (first == left_row) atomicAdd(acc + first, h);
-            else acc[first] = h;
+            if (first == left_row) part_first[sidx] = h;  // the tail of a row begun in an earlier span
+            else out[first] = coo_finish(h, dt, fe, u, first);
         }
         // the lane's last run ends here unless the next lane starts with it
         const bool ends_here = lane == 31 || k0 + kCooPer >= span_end || next_first != last;
         if (ends_here && last >= 0 && last < N) {
-            if (last == left_row || last == right_row) atomicAdd(acc + last, carry);
-            else acc[last] = carry;
+            if (last == left_row) part_first[sidx] = carry;       // begun earlier (its tail, or the whole span)
+            else if (last == right_row) part_last[sidx] = carry;  // begins here, goes on in the next span
+            else out[last] = coo_finish(carry, dt, fe, u, last);
         }
+        // rows without entries after this lane's: up to the next lane's first
+        // row, or from the span's last entry to the next span's first row (to
+        // N after the last entry); before the first entry, in span 0
+        if (k0 < span_end) {
+            if (k0 + kCooPer >= span_end)
+                coo_empty_rows((int64_t)__ldg(rows + (span_end - 1)) + 1, span_end < nnz ? (int64_t)right_row : N, N,
+                               dt, fe, u, out);
+            else
+                coo_empty_rows((int64_t)last + 1, next_first, N, dt, fe, u, out);
+        }
+        if (base == 0 && lane == 0) coo_empty_rows(0, r[0], N, dt, fe, u, out);
     }
     if (bad) atomicOr(err, bad);
+}
+
+// Rows that cross span boundaries, one thread per span that begins such a
+// row: its part here plus the parts of the following spans, in span order,
+// while the row goes on; then the finished value.
+__global__ void k_coo_span_fixup(int64_t N, int64_t nnz, const int32_t *__restrict__ rows,
+                                 const float *__restrict__ u, float dt, int fe, const float *__restrict__ part_first,
+                                 const float *__restrict__ part_last, float *__restrict__ out)
+{
+    const int64_t nspan = cdiv(nnz, kCooSpan);
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nspan; s += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t base = s * kCooSpan, end = base + kCooSpan < nnz ? base + kCooSpan : nnz;
+        if (end >= nnz) continue;
+        const int lr = __ldg(rows + (end - 1));
+        if (__ldg(rows + end) != lr || lr < 0 || lr >= N) continue;  // the last row ends in this span
+        const int fr = __ldg(rows + base);
+        if (fr == lr && base > 0 && __ldg(rows + (base - 1)) == lr) continue;  // a middle part: not the row's start
+        float total = part_last[s];
+        for (int64_t t = s + 1; t < nspan; ++t) {
+            total = __fadd_rn(total, part_first[t]);
+            const int64_t te = (t + 1) * kCooSpan < nnz ? (t + 1) * kCooSpan : nnz;
+            if (!(te < nnz && __ldg(rows + (te - 1)) == lr && __ldg(rows + te) == lr)) break;
+        }
+        out[lr] = coo_finish(total, dt, fe, u, lr);
+    }
 }
 
 // out = dt*acc (SpMVCOO's C[row] = deltat*result) or u + dt*acc.
@@ -332,21 +392,20 @@ __device__ __forceinline__ float ht_get_from(int64_t key, int64_t h, const int64
 // are issued together, then the seven value loads; only a collision (a first
 // probe holding another key) walks on.
 template <bool kOrdered>
-__global__ void __launch_bounds__(256, 4) k_ht_spmv(int nx, int ny, int nz, int64_t N, const int64_t *__restrict__ keys,
-                          const float *__restrict__ vals, int64_t ts, float dt, int fe,
+__global__ void __launch_bounds__(256, 4) k_ht_spmv(GridDiv g, int64_t N, const int64_t *__restrict__ keys,
+                          const float *__restrict__ vals, int64_t ts, ModU64 mts, float dt, int fe,
                           const int32_t *__restrict__ order, const float *__restrict__ u, float *__restrict__ out)
 {
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int64_t sxy = (int64_t)nx * ny;
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < N; j += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = kOrdered ? (int64_t)__ldg(order + j) : j;
-        const int z = (int)(i / sxy);
-        const int64_t rem = i - (int64_t)z * sxy;
-        const int y = (int)(rem / nx);
-        const int x = (int)(rem - (int64_t)y * nx);
+        int x, y, z;
+        g.coords((uint32_t)i, x, y, z);
         // the seven directions in ascending column order, each present or not
         const int64_t off[7] = {-sxy, -(int64_t)nx, -1, 0, 1, (int64_t)nx, sxy};
         const bool ok[7] = {z > 0, y > 0, x > 0, true, x < nx - 1, y < ny - 1, z < nz - 1};
-        const int64_t kd = i * N + i, base = kd % ts;
+        const int64_t kd = i * N + i, base = (int64_t)mts.mod((uint64_t)kd);
         int64_t h[7], k[7];
         float v[7];
 #pragma unroll
@@ -388,20 +447,19 @@ __global__ void __launch_bounds__(256, 4) k_ht_spmv(int nx, int ny, int nz, int6
 // stores: whole sectors, no read-modify-write of a partly written sector).
 // Pass 2 (rows in index order) reads the records and u coalesced and writes
 // out coalesced.  The per-row arithmetic is the one above, term for term.
-__global__ void __launch_bounds__(256, 4) k_ht_stage(int nx, int ny, int nz, int64_t N, const int64_t *__restrict__ keys,
-                           const float *__restrict__ vals, int64_t ts, const int32_t *__restrict__ order,
+__global__ void __launch_bounds__(256, 4) k_ht_stage(GridDiv g, int64_t N, const int64_t *__restrict__ keys,
+                           const float *__restrict__ vals, int64_t ts, ModU64 mts, const int32_t *__restrict__ order,
                            float4 *__restrict__ stage)
 {
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int64_t sxy = (int64_t)nx * ny;
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < N; j += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = (int64_t)__ldg(order + j);
-        const int z = (int)(i / sxy);
-        const int64_t rem = i - (int64_t)z * sxy;
-        const int y = (int)(rem / nx);
-        const int x = (int)(rem - (int64_t)y * nx);
+        int x, y, z;
+        g.coords((uint32_t)i, x, y, z);
         const int64_t off[7] = {-sxy, -(int64_t)nx, -1, 0, 1, (int64_t)nx, sxy};
         const bool ok[7] = {z > 0, y > 0, x > 0, true, x < nx - 1, y < ny - 1, z < nz - 1};
-        const int64_t kd = i * N + i, base = kd % ts;
+        const int64_t kd = i * N + i, base = (int64_t)mts.mod((uint64_t)kd);
         int64_t h[7], k[7];
         float v[8];
         v[7] = 0.0f;
@@ -434,16 +492,15 @@ __global__ void __launch_bounds__(256, 4) k_ht_stage(int nx, int ny, int nz, int
     }
 }
 
-__global__ void k_ht_stage_apply(int nx, int ny, int nz, float dt, int fe, const float4 *__restrict__ stage,
+__global__ void k_ht_stage_apply(GridDiv g, float dt, int fe, const float4 *__restrict__ stage,
                                  const float *__restrict__ u, float *__restrict__ out)
 {
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int sxy = nx * ny;
     const int N = sxy * nz;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        const int z = i / sxy;
-        const int rem = i - z * sxy;
-        const int y = rem / nx;
-        const int x = rem - y * nx;
+        int x, y, z;
+        g.coords((uint32_t)i, x, y, z);
         const float4 lo = __ldcs(stage + 2 * (int64_t)i), hi = __ldcs(stage + 2 * (int64_t)i + 1);
         const float v[7] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z};
         const int off[7] = {-sxy, -nx, -1, 0, 1, nx, sxy};
@@ -911,6 +968,9 @@ extern "C" int piro_csr_i1(int nx, int ny, int nz, const int32_t *rowptr, const 
 // Per device: the input-check flags of k_coo_segsum.
 static int *coo_err_dev[kMaxDevices] = {};
 static DeviceOnce coo_err_once;
+static std::mutex coo_part_mu;
+static float *coo_part_dev[kMaxDevices] = {};
+static int64_t coo_part_cap[kMaxDevices] = {};
 
 static int coo_common(int64_t N, int64_t nnz, const int32_t *rows, const int32_t *cols, const float *vals, float dt,
                       const float *u, float *out, bool fe, piro_stream_t stream)
@@ -927,22 +987,41 @@ static int coo_common(int64_t N, int64_t nnz, const int32_t *rows, const int32_t
     });
     if (rc != PIRO_OK) return rc;
     int *err = coo_err_dev[dev];
-    // out doubles as the accumulator: zero it, sum into it, then scale in place.
-    PIRO_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * N, s));
-    if (nnz > 0) {
-        PIRO_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-        const bool al16 = ((reinterpret_cast<uintptr_t>(rows) | reinterpret_cast<uintptr_t>(cols) |
-                            reinterpret_cast<uintptr_t>(vals)) & 15) == 0;
-        if (al16) {
-            k_coo_segsum8<<<grid_for(cdiv(nnz, kCooPer), 256, 8), 256, 0, s>>>(N, nnz, rows, cols, vals, u, out, err);
-            PIRO_CHECK_LAUNCH("k_coo_segsum8");
-        } else {
+    const bool al16 = ((reinterpret_cast<uintptr_t>(rows) | reinterpret_cast<uintptr_t>(cols) |
+                        reinterpret_cast<uintptr_t>(vals)) & 15) == 0;
+    if (nnz > 0) PIRO_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    if (nnz > 0 && al16) {
+        // the span parts of rows that cross spans: a per-device buffer that grows
+        const int64_t nspan = cdiv(nnz, kCooSpan);
+        float *parts = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(coo_part_mu);
+            if (coo_part_cap[dev] < nspan) {
+                if (coo_part_dev[dev]) PIRO_CUDA(cudaFree(coo_part_dev[dev]));
+                coo_part_dev[dev] = nullptr;
+                coo_part_cap[dev] = 0;
+                PIRO_CUDA(cudaMalloc(&coo_part_dev[dev], 2 * sizeof(float) * (size_t)nspan));
+                coo_part_cap[dev] = nspan;
+            }
+            parts = coo_part_dev[dev];
+        }
+        float *part_first = parts, *part_last = parts + coo_part_cap[dev];
+        k_coo_segsum8<<<grid_for(cdiv(nnz, kCooPer), 256, 8), 256, 0, s>>>(N, nnz, rows, cols, vals, u, dt, fe ? 1 : 0,
+                                                                         out, part_first, part_last, err);
+        PIRO_CHECK_LAUNCH("k_coo_segsum8");
+        k_coo_span_fixup<<<grid_for(nspan, 256, 4), 256, 0, s>>>(N, nnz, rows, u, dt, fe ? 1 : 0, part_first, part_last,
+                                                                out);
+        PIRO_CHECK_LAUNCH("k_coo_span_fixup");
+    } else {
+        // out doubles as the accumulator: zero it, sum into it, then scale in place.
+        PIRO_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * N, s));
+        if (nnz > 0) {
             k_coo_segsum<<<grid_for(nnz, 256, 8), 256, 0, s>>>(N, nnz, rows, cols, vals, u, out, err);
             PIRO_CHECK_LAUNCH("k_coo_segsum");
         }
+        k_scale_add<<<grid_for(N, 256, 8), 256, 0, s>>>(N, dt, out, fe ? u : nullptr, out);
+        PIRO_CHECK_LAUNCH("k_scale_add");
     }
-    k_scale_add<<<grid_for(N, 256, 8), 256, 0, s>>>(N, dt, out, fe ? u : nullptr, out);
-    PIRO_CHECK_LAUNCH("k_scale_add");
     if (nnz > 0) {
         int h = 0;
         PIRO_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1013,7 +1092,8 @@ extern "C" int piro_ht_spmv(int nx, int ny, int nz, const int64_t *keys, const f
 {
     PIRO_ARG(grid_ok(nx, ny, nz) && keys && vals && ts > 0 && u && out && u != out, "piro_ht_spmv: bad arguments");
     const int64_t N = (int64_t)nx * ny * nz;
-    k_ht_spmv<false><<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(nx, ny, nz, N, keys, vals, ts, dt, fe, nullptr,
+    k_ht_spmv<false><<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(GridDiv(nx, ny, nz), N, keys, vals, ts,
+                                                                         ModU64((uint64_t)ts), dt, fe, nullptr,
                                                                          u, out);
     PIRO_CHECK_LAUNCH("k_ht_spmv");
     return PIRO_OK;
@@ -1057,7 +1137,8 @@ extern "C" int piro_ht_spmv_ordered(int nx, int ny, int nz, const int64_t *keys,
     PIRO_ARG(grid_ok(nx, ny, nz) && keys && vals && ts > 0 && order && u && out && u != out,
              "piro_ht_spmv_ordered: bad arguments");
     const int64_t N = (int64_t)nx * ny * nz;
-    k_ht_spmv<true><<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(nx, ny, nz, N, keys, vals, ts, dt, fe, order,
+    k_ht_spmv<true><<<grid_for(N, 256, 8), 256, 0, as_stream(stream)>>>(GridDiv(nx, ny, nz), N, keys, vals, ts,
+                                                                        ModU64((uint64_t)ts), dt, fe, order,
                                                                         u, out);
     PIRO_CHECK_LAUNCH("k_ht_spmv");
     return PIRO_OK;
@@ -1082,9 +1163,10 @@ extern "C" int piro_ht_spmv_staged(int nx, int ny, int nz, const int64_t *keys, 
              "piro_ht_spmv_staged: stage smaller than 32 bytes per row or not 16-byte aligned");
     cudaStream_t s = as_stream(stream);
     float4 *st = static_cast<float4 *>(stage);
-    k_ht_stage<<<grid_for(N, 256, 8), 256, 0, s>>>(nx, ny, nz, N, keys, vals, ts, order, st);
+    const GridDiv g(nx, ny, nz);
+    k_ht_stage<<<grid_for(N, 256, 8), 256, 0, s>>>(g, N, keys, vals, ts, ModU64((uint64_t)ts), order, st);
     PIRO_CHECK_LAUNCH("k_ht_stage");
-    k_ht_stage_apply<<<grid_for(N, 256, 8), 256, 0, s>>>(nx, ny, nz, dt, fe, st, u, out);
+    k_ht_stage_apply<<<grid_for(N, 256, 8), 256, 0, s>>>(g, dt, fe, st, u, out);
     PIRO_CHECK_LAUNCH("k_ht_stage_apply");
     return PIRO_OK;
 }

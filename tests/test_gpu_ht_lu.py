@@ -117,3 +117,33 @@ def test_ht_lu_entry_outside_band_is_reported(cuda):
     with pytest.raises(PiroError, match="outside the bandwidth") as e:
         ops.HtLu(N, nx, keys, vals, ts, 1.0, -0.05)  # the z neighbours sit nx*ny away
     assert e.value.status == 1
+
+
+@pytest.mark.parametrize("n,dt", [((8, 7, 6), 0.7), ((12, 10, 9), 0.05), ((3, 3, 40), 0.05), ((3, 2, 20), 0.7),
+                                  ((40, 3, 3), 0.1), ((9, 9, 9), 0.7)])
+def test_ht_lu_panels_equal_column_launches(cuda, n, dt, monkeypatch):
+    """The blocked factorization (16-column panels, or 8/4 for wide bands)
+    gives the band, the multipliers and the pivots of the column-by-column
+    launches bit for bit (PIRO_LU_UNBLOCKED=1 selects those)."""
+    from piro_b200 import ops
+    nx, ny, nz = n
+    N = nx * ny * nz
+    bw = nx * ny
+    L = ops.csr_laplacian(nx, ny, nz, 3, 1.0)
+    ts = ops.ht_table_size(L[2].numel(), N, 1)
+    keys, vals = ops.ht_build(N, *L, ts)
+    band_bytes = 8 * N * (3 * bw + 1)
+    lc_off = (band_bytes + 255) // 256 * 256
+    blk = ops.HtLu(N, bw, keys, vals, ts, 1.0, -dt)
+    monkeypatch.setenv("PIRO_LU_UNBLOCKED", "1")
+    col = ops.HtLu(N, bw, keys, vals, ts, 1.0, -dt)
+    assert np.array_equal(blk.pivots(), col.pivots())
+    # the band (zeroed before the factorization, every entry defined)
+    a, b = blk.band[:band_bytes].cpu().numpy(), col.band[:band_bytes].cpu().numpy()
+    assert np.array_equal(a, b), int(np.count_nonzero(a != b))
+    # the multipliers of step r: Lc[r][t - 1] for t <= min(bw, N - 1 - r)
+    la = blk.band[lc_off:lc_off + 8 * N * bw].cpu().numpy().view(np.float64).reshape(N, bw)
+    lb = col.band[lc_off:lc_off + 8 * N * bw].cpu().numpy().view(np.float64).reshape(N, bw)
+    span = np.minimum(bw, N - 1 - np.arange(N))
+    defined = np.arange(bw)[None, :] < span[:, None]
+    assert np.array_equal(la[defined].view(np.uint64), lb[defined].view(np.uint64))

@@ -176,6 +176,7 @@ def test_csr_and_coo_steps_on_wide_rows_bitexact(cuda, oracle):
     lengths = rng.choice([0, 1, 3, 7, 31, 32, 33, 64, 100, 257, 1000], size=N,
                          p=[.05, .05, .1, .3, .05, .05, .1, .1, .1, .07, .03]).astype(np.int64)
     lengths[5] = 5000  # one very long row
+    lengths[[0, N - 2, N - 1]] = 0  # rows without entries at both ends
     rp = np.zeros(N + 1, np.int64)
     rp[1:] = np.cumsum(lengths)
     nnz = int(rp[-1])
@@ -196,9 +197,21 @@ def test_csr_and_coo_steps_on_wide_rows_bitexact(cuda, oracle):
     assert f32_bits_equal(h(out), want_coo)
     # the segmented sum (8 entries per lane, rows across lanes and 256-entry
     # spans): FP32 tolerance, since it adds in another order
-    ops.coo_spmv(N, (dev(torch, rows), Ad[1], Ad[2]), dt, dev(torch, u), out)
+    coo = (dev(torch, rows), Ad[1], Ad[2])
+    ops.coo_spmv(N, coo, dt, dev(torch, u), out)
     scale = np.abs(val).reshape(-1).max() * np.abs(u).max() * lengths.max() * abs(float(dt))
     np.testing.assert_allclose(h(out), want_coo, rtol=1e-5, atol=1e-6 * scale)
+    assert np.all(h(out)[lengths == 0] == 0.0)
+    # the fused forward-Euler form, and the same bits on every run (the parts of
+    # rows that cross spans are added in span order, not by atomics)
+    runs = []
+    for _ in range(3):
+        o = torch.full_like(out, float("nan"))
+        ops.coo_spmv(N, coo, dt, dev(torch, u), o, fe=True)
+        runs.append(h(o))
+    np.testing.assert_allclose(runs[0], u + want_coo, rtol=1e-5, atol=1e-6 * scale)
+    assert np.array_equal(runs[0][lengths == 0], u[lengths == 0])
+    assert all(np.array_equal(runs[0], r) for r in runs[1:])
 
 
 def test_csrgeam3_vs_golden(cuda, golden_grids):
