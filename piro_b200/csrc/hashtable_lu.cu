@@ -433,7 +433,9 @@ __device__ __forceinline__ bool in_band(int64_t bw, int64_t r, int64_t c)
     return d >= 0 && d <= 3 * bw;
 }
 
-__global__ void __launch_bounds__(kPivThreads) k_lupb_panel(int64_t N, int64_t bw, int64_t W,
+constexpr int kPanelThreads = 512;
+
+__global__ void __launch_bounds__(kPanelThreads) k_lupb_panel(int64_t N, int64_t bw, int64_t W,
                                                             double *__restrict__ band, double *__restrict__ Lc,
                                                             int32_t *__restrict__ piv, double *__restrict__ Lw,
                                                             int64_t j0, int nbp, int nb, int *err)
@@ -812,14 +814,18 @@ __global__ void __launch_bounds__(kPivThreads) k_lup_solve_panels(int64_t N, int
                 *vb = t;
             }
             for (int f = 0; f < nfar; ++f) y[s_pos[f]] = s_val[f];
-            for (int i = 0; i < nbp; ++i) {
-                double acc = s_y[i];
-                for (int k = 0; k < i; ++k) {
-                    const double l = s_t[i][k];
-                    if (l != 0.0 && s_y[k] != 0.0) acc = fma(-l, s_y[k], acc);
-                }
-                s_y[i] = acc;
+        }
+        __syncwarp();
+        if (warp == 0) {
+            // the unit lower triangle by columns: lane i takes row i, step k's
+            // y_k reaches the lanes by a shuffle (each row's updates in k order)
+            double yi = lane < nbp ? s_y[lane] : 0.0;
+            for (int k = 0; k < nbp - 1; ++k) {
+                const double yk = __shfl_sync(0xffffffffu, yi, k);
+                const double l = lane > k && lane < nbp ? s_t[lane][k] : 0.0;
+                if (l != 0.0 && yk != 0.0) yi = fma(-l, yk, yi);
             }
+            if (lane < nbp) s_y[lane] = yi;
         }
         __syncthreads();
         if (threadIdx.x < nbp) y[j0 + threadIdx.x] = s_y[threadIdx.x];
@@ -855,12 +861,16 @@ __global__ void __launch_bounds__(kPivThreads) k_lup_solve_panels(int64_t N, int
         }
         if (threadIdx.x < nbp) s_y[threadIdx.x] = y[j0 + threadIdx.x];
         __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int i = nbp - 1; i >= 0; --i) {
-                double sum = s_dot[i];
-                for (int c = i + 1; c < nbp; ++c) sum = fma(s_t[i][c], s_y[c], sum);
-                s_y[i] = (s_y[i] - sum) / s_t[i][i];
+        if (warp == 0) {
+            // U by columns from the last: lane i holds row i's sum; x_c, once
+            // solved, reaches the lanes above it by a shuffle
+            double sum = lane < nbp ? s_dot[lane] : 0.0, yi = lane < nbp ? s_y[lane] : 0.0;
+            for (int c = nbp - 1; c >= 0; --c) {
+                if (lane == c) yi = (yi - sum) / s_t[c][c];
+                const double xc = __shfl_sync(0xffffffffu, yi, c);
+                if (lane < c) sum = fma(s_t[lane][c], xc, sum);
             }
+            if (lane < nbp) s_y[lane] = yi;
         }
         __syncthreads();
         if (threadIdx.x < nbp) y[j0 + threadIdx.x] = s_y[threadIdx.x];
@@ -995,7 +1005,7 @@ extern "C" int piro_ht_lu_factor(int64_t N, int64_t bw, const int64_t *keys, con
         PIRO_CUDA(cudaFuncSetAttribute(k_lupb_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         for (int64_t j0 = 0; j0 < N; j0 += nb) {
             const int nbp = (int)(N - j0 < nb ? N - j0 : nb);
-            k_lupb_panel<<<1, kPivThreads, smem, st>>>(N, bw, W, AB, Lc, piv, Lw, j0, nbp, nb, err);
+            k_lupb_panel<<<1, kPanelThreads, smem, st>>>(N, bw, W, AB, Lc, piv, Lw, j0, nbp, nb, err);
             const int64_t rmax = j0 + nbp - 1 + bw < N - 1 ? j0 + nbp - 1 + bw : N - 1;
             const int64_t cmax = j0 + nbp - 1 + 2 * bw < N - 1 ? j0 + nbp - 1 + 2 * bw : N - 1;
             const int64_t ncols = cmax - (j0 + nbp) + 1, nrows = rmax - (j0 + nbp) + 1;

@@ -199,25 +199,28 @@ __global__ void k_coo_segsum(int64_t N, int64_t nnz, const int32_t *__restrict__
 constexpr int kCooPer = 8;
 constexpr int kCooSpan = 32 * kCooPer;
 
-__device__ __forceinline__ float coo_finish(float sum, float dt, int fe, const float *__restrict__ u, int64_t r)
+template <bool kFe>
+__device__ __forceinline__ float coo_finish(float sum, float dt, const float *__restrict__ u, int64_t r)
 {
     const float c = __fmul_rn(dt, sum);
-    return fe ? __fadd_rn(__ldg(u + r), c) : c;
+    return kFe ? __fadd_rn(__ldg(u + r), c) : c;
 }
 
-// rows [r0, r1) hold no entry (clamped to [0, N))
-__device__ __forceinline__ void coo_empty_rows(int64_t r0, int64_t r1, int64_t N, float dt, int fe,
-                                               const float *__restrict__ u, float *__restrict__ out)
+// rows [r0, r1) hold no entry (clamped to [0, N)); callers test for a gap first
+template <bool kFe>
+__device__ __forceinline__ void coo_empty_rows(int64_t r0, int64_t r1, int64_t N, float dt, const float *__restrict__ u,
+                                            float *__restrict__ out)
 {
     r0 = r0 < 0 ? 0 : r0;
     r1 = r1 > N ? N : r1;
-    for (int64_t r = r0; r < r1; ++r) out[r] = coo_finish(0.0f, dt, fe, u, r);
+    for (int64_t r = r0; r < r1; ++r) out[r] = coo_finish<kFe>(0.0f, dt, u, r);
 }
 
-__global__ void __launch_bounds__(256) k_coo_segsum8(int64_t N, int64_t nnz, const int32_t *__restrict__ rows,
+template <bool kFe>
+__global__ void __launch_bounds__(256, 5) k_coo_segsum8(int64_t N, int64_t nnz, const int32_t *__restrict__ rows,
                                                      const int32_t *__restrict__ cols,
                                                      const float *__restrict__ vals, const float *__restrict__ u,
-                                                     float dt, int fe, float *__restrict__ out,
+                                                     float dt, float *__restrict__ out,
                                                      float *__restrict__ part_first, float *__restrict__ part_last,
                                                      int *__restrict__ err)
 {
@@ -277,8 +280,8 @@ __global__ void __launch_bounds__(256) k_coo_segsum8(int64_t N, int64_t nnz, con
             const float pv = r[t] != kNone ? __fmul_rn(v[t], __ldg(u + c[t])) : 0.0f;
             if (r[t] != cur) {
                 if (!multi) head = s_run;                                               // the lane's first run
-                else if (cur >= 0 && cur < N) out[cur] = coo_finish(s_run, dt, fe, u, cur);  // a whole row
-                if (r[t] != kNone) coo_empty_rows((int64_t)cur + 1, r[t], N, dt, fe, u, out);
+                else if (cur >= 0 && cur < N) out[cur] = coo_finish<kFe>(s_run, dt, u, cur);  // a whole row
+                if (r[t] != kNone && r[t] > cur + 1) coo_empty_rows<kFe>((int64_t)cur + 1, r[t], N, dt, u, out);
                 multi = true;
                 cur = r[t];
                 s_run = 0.0f;
@@ -310,26 +313,27 @@ __global__ void __launch_bounds__(256) k_coo_segsum8(int64_t N, int64_t nnz, con
             // the lane's first run ends here: add what the lanes before carried in
             const float h = (lane > 0 && kin == first) ? __fadd_rn(cin, head) : head;
             if (first == left_row) part_first[sidx] = h;  // the tail of a row begun in an earlier span
-            else out[first] = coo_finish(h, dt, fe, u, first);
+            else out[first] = coo_finish<kFe>(h, dt, u, first);
         }
         // the lane's last run ends here unless the next lane starts with it
         const bool ends_here = lane == 31 || k0 + kCooPer >= span_end || next_first != last;
         if (ends_here && last >= 0 && last < N) {
             if (last == left_row) part_first[sidx] = carry;       // begun earlier (its tail, or the whole span)
             else if (last == right_row) part_last[sidx] = carry;  // begins here, goes on in the next span
-            else out[last] = coo_finish(carry, dt, fe, u, last);
+            else out[last] = coo_finish<kFe>(carry, dt, u, last);
         }
         // rows without entries after this lane's: up to the next lane's first
         // row, or from the span's last entry to the next span's first row (to
         // N after the last entry); before the first entry, in span 0
         if (k0 < span_end) {
-            if (k0 + kCooPer >= span_end)
-                coo_empty_rows((int64_t)__ldg(rows + (span_end - 1)) + 1, span_end < nnz ? (int64_t)right_row : N, N,
-                               dt, fe, u, out);
-            else
-                coo_empty_rows((int64_t)last + 1, next_first, N, dt, fe, u, out);
+            if (k0 + kCooPer >= span_end) {
+                const int64_t a = (int64_t)__ldg(rows + (span_end - 1)) + 1, b = span_end < nnz ? (int64_t)right_row : N;
+                if (b > a) coo_empty_rows<kFe>(a, b, N, dt, u, out);
+            } else if (next_first > last + 1) {
+                coo_empty_rows<kFe>((int64_t)last + 1, next_first, N, dt, u, out);
+            }
         }
-        if (base == 0 && lane == 0) coo_empty_rows(0, r[0], N, dt, fe, u, out);
+        if (base == 0 && lane == 0 && r[0] > 0) coo_empty_rows<kFe>(0, r[0], N, dt, u, out);
     }
     if (bad) atomicOr(err, bad);
 }
@@ -337,8 +341,9 @@ __global__ void __launch_bounds__(256) k_coo_segsum8(int64_t N, int64_t nnz, con
 // Rows that cross span boundaries, one thread per span that begins such a
 // row: its part here plus the parts of the following spans, in span order,
 // while the row goes on; then the finished value.
+template <bool kFe>
 __global__ void k_coo_span_fixup(int64_t N, int64_t nnz, const int32_t *__restrict__ rows,
-                                 const float *__restrict__ u, float dt, int fe, const float *__restrict__ part_first,
+                                 const float *__restrict__ u, float dt, const float *__restrict__ part_first,
                                  const float *__restrict__ part_last, float *__restrict__ out)
 {
     const int64_t nspan = cdiv(nnz, kCooSpan);
@@ -355,7 +360,7 @@ __global__ void k_coo_span_fixup(int64_t N, int64_t nnz, const int32_t *__restri
             const int64_t te = (t + 1) * kCooSpan < nnz ? (t + 1) * kCooSpan : nnz;
             if (!(te < nnz && __ldg(rows + (te - 1)) == lr && __ldg(rows + te) == lr)) break;
         }
-        out[lr] = coo_finish(total, dt, fe, u, lr);
+        out[lr] = coo_finish<kFe>(total, dt, u, lr);
     }
 }
 
@@ -406,15 +411,18 @@ __global__ void __launch_bounds__(256, 4) k_ht_spmv(GridDiv g, int64_t N, const 
         const int64_t off[7] = {-sxy, -(int64_t)nx, -1, 0, 1, (int64_t)nx, sxy};
         const bool ok[7] = {z > 0, y > 0, x > 0, true, x < nx - 1, y < ny - 1, z < nz - 1};
         const int64_t kd = i * N + i, base = (int64_t)mts.mod((uint64_t)kd);
-        int64_t h[7], k[7];
+        auto home = [&](int t) {  // the first probe of candidate t (recomputed on a collision, not kept)
+            int64_t hh = base + off[t];
+            hh += hh < 0 ? ts : 0;
+            hh -= hh >= ts ? ts : 0;
+            return hh;
+        };
+        int64_t k[7];
         float v[7];
 #pragma unroll
         for (int t = 0; t < 7; ++t) {
             if (ok[t]) {
-                int64_t hh = base + off[t];
-                hh += hh < 0 ? ts : 0;
-                hh -= hh >= ts ? ts : 0;
-                h[t] = hh;
+                const int64_t hh = home(t);
                 k[t] = __ldg(keys + hh);
                 v[t] = __ldg(vals + hh);  // with the key, not after it: one round trip
             }
@@ -427,7 +435,8 @@ __global__ void __launch_bounds__(256, 4) k_ht_spmv(GridDiv g, int64_t N, const 
                 } else if (k[t] == -1) {
                     v[t] = 0.0f;
                 } else {
-                    v[t] = ht_get_from(key, h[t] + 1 == ts ? 0 : h[t] + 1, keys, vals, ts);
+                    const int64_t hh = home(t);
+                    v[t] = ht_get_from(key, hh + 1 == ts ? 0 : hh + 1, keys, vals, ts);
                 }
             }
         }
@@ -453,24 +462,31 @@ __global__ void __launch_bounds__(256, 4) k_ht_stage(GridDiv g, int64_t N, const
 {
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int64_t sxy = (int64_t)nx * ny;
-    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < N; j += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = (int64_t)__ldg(order + j);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t next_i = j < N ? __ldg(order + j) : 0;  // the row of the next iteration, loaded one ahead
+    for (; j < N; j += stride) {
+        const int64_t i = next_i;
+        if (j + stride < N) next_i = __ldg(order + j + stride);
         int x, y, z;
         g.coords((uint32_t)i, x, y, z);
         const int64_t off[7] = {-sxy, -(int64_t)nx, -1, 0, 1, (int64_t)nx, sxy};
         const bool ok[7] = {z > 0, y > 0, x > 0, true, x < nx - 1, y < ny - 1, z < nz - 1};
         const int64_t kd = i * N + i, base = (int64_t)mts.mod((uint64_t)kd);
-        int64_t h[7], k[7];
+        auto home = [&](int t) {  // the first probe of candidate t (recomputed on a collision, not kept)
+            int64_t hh = base + off[t];
+            hh += hh < 0 ? ts : 0;
+            hh -= hh >= ts ? ts : 0;
+            return hh;
+        };
+        int64_t k[7];
         float v[8];
         v[7] = 0.0f;
 #pragma unroll
         for (int t = 0; t < 7; ++t) {
             v[t] = 0.0f;
             if (ok[t]) {
-                int64_t hh = base + off[t];
-                hh += hh < 0 ? ts : 0;
-                hh -= hh >= ts ? ts : 0;
-                h[t] = hh;
+                const int64_t hh = home(t);
                 k[t] = __ldg(keys + hh);
                 v[t] = __ldg(vals + hh);  // with the key: one round trip
             }
@@ -483,7 +499,8 @@ __global__ void __launch_bounds__(256, 4) k_ht_stage(GridDiv g, int64_t N, const
                 } else if (k[t] == -1) {
                     v[t] = 0.0f;
                 } else {
-                    v[t] = ht_get_from(key, h[t] + 1 == ts ? 0 : h[t] + 1, keys, vals, ts);
+                    const int64_t hh = home(t);
+                    v[t] = ht_get_from(key, hh + 1 == ts ? 0 : hh + 1, keys, vals, ts);
                 }
             }
         }
@@ -1006,12 +1023,15 @@ static int coo_common(int64_t N, int64_t nnz, const int32_t *rows, const int32_t
             parts = coo_part_dev[dev];
         }
         float *part_first = parts, *part_last = parts + coo_part_cap[dev];
-        k_coo_segsum8<<<grid_for(cdiv(nnz, kCooPer), 256, 8), 256, 0, s>>>(N, nnz, rows, cols, vals, u, dt, fe ? 1 : 0,
-                                                                         out, part_first, part_last, err);
+        const unsigned g1 = grid_for(cdiv(nnz, kCooPer), 256, 8), g2 = grid_for(nspan, 256, 4);
+        if (fe) {
+            k_coo_segsum8<true><<<g1, 256, 0, s>>>(N, nnz, rows, cols, vals, u, dt, out, part_first, part_last, err);
+            k_coo_span_fixup<true><<<g2, 256, 0, s>>>(N, nnz, rows, u, dt, part_first, part_last, out);
+        } else {
+            k_coo_segsum8<false><<<g1, 256, 0, s>>>(N, nnz, rows, cols, vals, u, dt, out, part_first, part_last, err);
+            k_coo_span_fixup<false><<<g2, 256, 0, s>>>(N, nnz, rows, u, dt, part_first, part_last, out);
+        }
         PIRO_CHECK_LAUNCH("k_coo_segsum8");
-        k_coo_span_fixup<<<grid_for(nspan, 256, 4), 256, 0, s>>>(N, nnz, rows, u, dt, fe ? 1 : 0, part_first, part_last,
-                                                                out);
-        PIRO_CHECK_LAUNCH("k_coo_span_fixup");
     } else {
         // out doubles as the accumulator: zero it, sum into it, then scale in place.
         PIRO_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * N, s));
