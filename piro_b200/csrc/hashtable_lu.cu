@@ -879,6 +879,136 @@ __global__ void __launch_bounds__(kPivThreads) k_lup_solve_panels(int64_t N, int
     for (int64_t r = threadIdx.x; r < N; r += blockDim.x) x[r] = (float)y[r];
 }
 
+// The same solve with y kept in shared memory: a ring of WS = 2bw + 16
+// doubles holds rows [j0, j0 + WS) while panel j0 is worked on (every row a
+// panel step touches lies within bw + 15 of j0 in the forward pass and within
+// 2bw + 15 in the backward pass); rows leave for global memory as the panels
+// move on and enter from b (forward) or from the forward result (backward).
+// Only the multipliers, the pivots and U's rows are read from global memory.
+// Same arithmetic as k_lup_solve_panels, bit for bit.
+__global__ void __launch_bounds__(kPivThreads) k_lup_solve_ring(int64_t N, int64_t bw, int64_t W,
+                                                                const double *__restrict__ band,
+                                                                const double *__restrict__ Lp,
+                                                                const int32_t *__restrict__ piv,
+                                                                const float *__restrict__ b, double *__restrict__ y,
+                                                                float *__restrict__ x)
+{
+    constexpr int P = kLuSolveNb;
+    extern __shared__ double s_ring[];
+    __shared__ double s_y[P];
+    __shared__ double s_t[P][P + 1];
+    __shared__ int32_t s_piv[P];
+    __shared__ double s_dot[P];
+    const uint32_t WS = (uint32_t)(2 * bw + P);
+    auto slot = [WS](int64_t r) { return (uint32_t)((uint64_t)r % WS); };
+    const int64_t R = bw + P;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int64_t npan = cdiv(N, P);
+    for (int64_t r = threadIdx.x; r < N && r < (int64_t)WS; r += blockDim.x) s_ring[r] = (double)b[r];
+    __syncthreads();
+    for (int64_t pi = 0; pi < npan; ++pi) {
+        const int64_t j0 = pi * P;
+        const int nbp = (int)(N - j0 < P ? N - j0 : P);
+        const double *lw = Lp + pi * R * P;
+        if (threadIdx.x < nbp) s_piv[threadIdx.x] = piv[j0 + threadIdx.x];
+        for (int t = threadIdx.x; t < P * P; t += blockDim.x) {
+            const int i = t / P, k = t - i * P;
+            s_t[i][k] = (i < nbp && k < i) ? lw[i * P + k] : 0.0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int k = 0; k < nbp; ++k) {
+                const int64_t p = s_piv[k];
+                if (p == j0 + k) continue;
+                double *a = &s_ring[slot(j0 + k)], *c = &s_ring[slot(p)];
+                const double t = *a;
+                *a = *c;
+                *c = t;
+            }
+        __syncwarp();
+        if (warp == 0) {
+            double yi = lane < nbp ? s_ring[slot(j0 + lane)] : 0.0;
+            for (int k = 0; k < nbp - 1; ++k) {
+                const double yk = __shfl_sync(0xffffffffu, yi, k);
+                const double l = lane > k && lane < nbp ? s_t[lane][k] : 0.0;
+                if (l != 0.0 && yk != 0.0) yi = fma(-l, yk, yi);
+            }
+            if (lane < nbp) {
+                s_y[lane] = yi;
+                s_ring[slot(j0 + lane)] = yi;
+            }
+        }
+        __syncthreads();
+        const int64_t rmax = j0 + nbp - 1 + bw < N - 1 ? j0 + nbp - 1 + bw : N - 1;
+        for (int64_t r = j0 + nbp + threadIdx.x; r <= rmax; r += blockDim.x) {
+            double *yr = &s_ring[slot(r)];
+            double acc = *yr;
+            for (int k = 0; k < nbp; ++k) {
+                const double l = lw[(r - j0) * P + k];
+                if (l != 0.0 && s_y[k] != 0.0) acc = fma(-l, s_y[k], acc);
+            }
+            *yr = acc;
+        }
+        __syncthreads();
+        // rows j0 .. j0+nbp-1 are done with the forward pass; rows WS further on enter
+        if (threadIdx.x < nbp) {
+            const int64_t r = j0 + threadIdx.x, rn = r + WS;
+            y[r] = s_ring[slot(r)];
+            if (rn < N) s_ring[slot(rn)] = (double)b[rn];
+        }
+    }
+    __syncthreads();
+    // back substitution, panels from the last; the ring holds rows [j0, j0 + WS)
+    for (int64_t pi = npan - 1; pi >= 0; --pi) {
+        const int64_t j0 = pi * P;
+        const int nbp = (int)(N - j0 < P ? N - j0 : P);
+        const int64_t jend = j0 + nbp;
+        if (pi == npan - 1) {
+            for (int64_t r = j0 + threadIdx.x; r < N; r += blockDim.x) s_ring[slot(r)] = y[r];
+        } else if (threadIdx.x < nbp) {  // row r + WS (solved) leaves, row r (forward result) enters
+            const int64_t r = j0 + threadIdx.x, ro = r + WS;
+            if (ro < N) y[ro] = s_ring[slot(ro)];
+            s_ring[slot(r)] = y[r];
+        }
+        __syncthreads();
+        for (int i = warp; i < nbp; i += nwarp) {
+            const int64_t r = j0 + i;
+            const int64_t cmax = r + 2 * bw < N - 1 ? r + 2 * bw : N - 1;
+            const double *u = band + r * W + (bw - r);  // u[c] = U(r, c)
+            double sum = 0.0;
+            int64_t c = jend + lane;
+            uint32_t sc = slot(c);
+#pragma unroll 4
+            for (; c <= cmax; c += 32) {
+                sum = fma(u[c], s_ring[sc], sum);
+                sc += 32;
+                sc = sc >= WS ? sc - WS : sc;
+            }
+            for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if (lane == 0) s_dot[i] = sum;
+        }
+        for (int t = threadIdx.x; t < P * P; t += blockDim.x) {
+            const int i = t / P, c = t - i * P;
+            const int64_t r = j0 + i, gc = j0 + c;
+            s_t[i][c] = (i < nbp && c < nbp && c >= i && gc <= r + 2 * bw) ? band[r * W + (gc - r + bw)] : 0.0;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double sum = lane < nbp ? s_dot[lane] : 0.0, yi = lane < nbp ? s_ring[slot(j0 + lane)] : 0.0;
+            for (int c = nbp - 1; c >= 0; --c) {
+                if (lane == c) yi = (yi - sum) / s_t[c][c];
+                const double xc = __shfl_sync(0xffffffffu, yi, c);
+                if (lane < c) sum = fma(s_t[lane][c], xc, sum);
+            }
+            if (lane < nbp) s_ring[slot(j0 + lane)] = yi;
+        }
+        __syncthreads();
+    }
+    for (int64_t r = threadIdx.x; r < N && r < (int64_t)WS; r += blockDim.x) y[r] = s_ring[slot(r)];
+    __syncthreads();
+    for (int64_t r = threadIdx.x; r < N; r += blockDim.x) x[r] = (float)y[r];
+}
+
 // Device layout of the factor buffer: band double[N][3bw+1], Lc double[N][bw],
 // y double[N] (the solve's workspace), piv int32[N], err int[2], Lw
 // double[bw + 16][16] (the blocked factorization's panel multipliers), Lp
@@ -1058,6 +1188,14 @@ extern "C" int piro_ht_lu_solve(int64_t N, int64_t bw, void *band, size_t band_b
                                               reinterpret_cast<const int32_t *>(base + L.piv), b,
                                               reinterpret_cast<double *>(base + L.y), x);
         PIRO_CHECK_LAUNCH("k_lup_solve");
+    } else if ((size_t)(2 * bw + kLuSolveNb) * sizeof(double) <= 160 * 1024) {
+        const size_t smem = (size_t)(2 * bw + kLuSolveNb) * sizeof(double);
+        PIRO_CUDA(cudaFuncSetAttribute(k_lup_solve_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_lup_solve_ring<<<1, kPivThreads, smem, st>>>(N, bw, L.W, reinterpret_cast<const double *>(base + L.band),
+                                                       reinterpret_cast<const double *>(base + L.lp),
+                                                       reinterpret_cast<const int32_t *>(base + L.piv), b,
+                                                       reinterpret_cast<double *>(base + L.y), x);
+        PIRO_CHECK_LAUNCH("k_lup_solve_ring");
     } else {
         k_lup_solve_panels<<<1, kPivThreads, 0, st>>>(N, bw, L.W, reinterpret_cast<const double *>(base + L.band),
                                                      reinterpret_cast<const double *>(base + L.lp),
