@@ -433,7 +433,7 @@ __device__ __forceinline__ bool in_band(int64_t bw, int64_t r, int64_t c)
     return d >= 0 && d <= 3 * bw;
 }
 
-constexpr int kPanelThreads = 512;
+constexpr int kPanelThreads = 1024;
 
 __global__ void __launch_bounds__(kPanelThreads) k_lupb_panel(int64_t N, int64_t bw, int64_t W,
                                                             double *__restrict__ band, double *__restrict__ Lc,
@@ -445,6 +445,7 @@ __global__ void __launch_bounds__(kPanelThreads) k_lupb_panel(int64_t N, int64_t
     __shared__ int s_i[32];
     __shared__ int s_prow;
     __shared__ int32_t s_piv[kLuNbMax];
+    __shared__ double s_pr[kLuNbMax];  // the pivot row (after its exchange), columns jj .. of the step
     if (*((volatile int *)err)) return;
     const int ld = nb + 1;
     const int64_t rmax = j0 + nbp - 1 + bw < N - 1 ? j0 + nbp - 1 + bw : N - 1;
@@ -483,13 +484,20 @@ __global__ void __launch_bounds__(kPanelThreads) k_lupb_panel(int64_t N, int64_t
                     bi = oi;
                 }
             }
+            const int64_t j = j0 + jj;
             if (lane == 0) {
-                const int64_t j = j0 + jj;
                 s_prow = best > 0.0 ? bi : -1;
                 piv[j] = (int32_t)(j + (best > 0.0 ? bi : 0));
                 s_piv[jj] = (int32_t)(j + (best > 0.0 ? bi : 0));
                 if (best <= 0.0 && atomicCAS(err, 0, 3) == 0) err[1] = (int)j;
             }
+            // the pivot row as the step's exchange leaves it: row jj + p over the
+            // columns jj .. jj + cend of the panel
+            const int p = __shfl_sync(0xffffffffu, bi, 0);
+            const int64_t cend = N - 1 - j < 2 * bw ? N - 1 - j : 2 * bw;
+            const int ccend = (int)(jj + cend < nbp - 1 ? jj + cend : nbp - 1);
+            const int cc = jj + lane;
+            if (cc <= ccend) s_pr[cc] = s_p[(jj + p) * ld + cc];
         }
         __syncthreads();
     };
@@ -513,16 +521,12 @@ __global__ void __launch_bounds__(kPanelThreads) k_lupb_panel(int64_t N, int64_t
         const int p = s_prow;
         if (p < 0) return;  // singular: the later launches see *err and return
         const int ccend = (int)(jj + cend < nbp - 1 ? jj + cend : nbp - 1);  // last panel column of this step
-        if (p > 0)
-            for (int cc = jj + threadIdx.x; cc <= ccend; cc += blockDim.x) {
-                const double t = s_p[jj * ld + cc];
-                s_p[jj * ld + cc] = s_p[(jj + p) * ld + cc];
-                s_p[(jj + p) * ld + cc] = t;
-            }
-        __syncthreads();
         // per row below the pivot: the multiplier, the update of the row's later
-        // panel columns, and the row's candidate for the next column's pivot
-        const double pv = s_p[jj * ld + jj];
+        // panel columns, and the row's candidate for the next column's pivot.
+        // The exchange happens here: the thread of row jj + p takes row jj's
+        // entries as its own and writes the pivot row (s_pr) to position jj; no
+        // other thread reads either position in this phase.
+        const double pv = s_pr[jj];
         const bool next = jj + 1 < nbp;
         const int span_n = next ? (int)(N - 1 - (j + 1) < bw ? N - 1 - (j + 1) : bw) : -1;  // next column's rows
         double best = -1.0;
@@ -530,11 +534,16 @@ __global__ void __launch_bounds__(kPanelThreads) k_lupb_panel(int64_t N, int64_t
         for (int t = 1 + threadIdx.x; t <= span || (next && t <= span_n + 1); t += blockDim.x) {
             double *row = s_p + (jj + t) * ld;
             if (t <= span) {
+                if (t == p)
+                    for (int cc = jj; cc <= ccend; ++cc) {
+                        row[cc] = s_p[jj * ld + cc];
+                        s_p[jj * ld + cc] = s_pr[cc];
+                    }
                 const double l = row[jj] / pv;
                 row[jj] = l;
                 Lc[j * bw + t - 1] = l;
                 if (l != 0.0)
-                    for (int cc = jj + 1; cc <= ccend; ++cc) row[cc] = fma(-l, s_p[jj * ld + cc], row[cc]);
+                    for (int cc = jj + 1; cc <= ccend; ++cc) row[cc] = fma(-l, s_pr[cc], row[cc]);
             }
             if (next && t <= span_n + 1) {  // row j + t is candidate t - 1 of column j + 1
                 const double v = fabs(row[jj + 1]);
@@ -900,7 +909,8 @@ __global__ void __launch_bounds__(kPivThreads) k_lup_solve_ring(int64_t N, int64
     __shared__ int32_t s_piv[P];
     __shared__ double s_dot[P];
     const uint32_t WS = (uint32_t)(2 * bw + P);
-    auto slot = [WS](int64_t r) { return (uint32_t)((uint64_t)r % WS); };
+    auto slot = [WS](int64_t r) { return (uint32_t)r % WS; };  // rows < 2^31
+    const uint32_t step_b = blockDim.x % WS, step_w = 32u % WS;  // ring moves of a block / warp stride
     const int64_t R = bw + P;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int64_t npan = cdiv(N, P);
@@ -940,8 +950,11 @@ __global__ void __launch_bounds__(kPivThreads) k_lup_solve_ring(int64_t N, int64
         }
         __syncthreads();
         const int64_t rmax = j0 + nbp - 1 + bw < N - 1 ? j0 + nbp - 1 + bw : N - 1;
+        uint32_t sr = slot(j0 + nbp + threadIdx.x);
         for (int64_t r = j0 + nbp + threadIdx.x; r <= rmax; r += blockDim.x) {
-            double *yr = &s_ring[slot(r)];
+            double *yr = &s_ring[sr];
+            sr += step_b;
+            sr = sr >= WS ? sr - WS : sr;
             double acc = *yr;
             for (int k = 0; k < nbp; ++k) {
                 const double l = lw[(r - j0) * P + k];
@@ -981,7 +994,7 @@ __global__ void __launch_bounds__(kPivThreads) k_lup_solve_ring(int64_t N, int64
 #pragma unroll 4
             for (; c <= cmax; c += 32) {
                 sum = fma(u[c], s_ring[sc], sum);
-                sc += 32;
+                sc += step_w;
                 sc = sc >= WS ? sc - WS : sc;
             }
             for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);

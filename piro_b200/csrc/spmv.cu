@@ -222,6 +222,7 @@ __global__ void __launch_bounds__(256, 5) k_coo_segsum8(int64_t N, int64_t nnz, 
                                                      const float *__restrict__ vals, const float *__restrict__ u,
                                                      float dt, float *__restrict__ out,
                                                      float *__restrict__ part_first, float *__restrict__ part_last,
+                                                     int32_t *__restrict__ span_row, int32_t *__restrict__ span_whole,
                                                      int *__restrict__ err)
 {
     const int lane = threadIdx.x & 31;
@@ -325,10 +326,17 @@ __global__ void __launch_bounds__(256, 5) k_coo_segsum8(int64_t N, int64_t nnz, 
         // rows without entries after this lane's: up to the next lane's first
         // row, or from the span's last entry to the next span's first row (to
         // N after the last entry); before the first entry, in span 0
+        const int span_first = __shfl_sync(0xffffffffu, first, 0);
         if (k0 < span_end) {
-            if (k0 + kCooPer >= span_end) {
-                const int64_t a = (int64_t)__ldg(rows + (span_end - 1)) + 1, b = span_end < nnz ? (int64_t)right_row : N;
+            if (k0 + kCooPer >= span_end) {  // the lane with the span's last entry
+                const int lr = __ldg(rows + (span_end - 1));
+                const int64_t a = (int64_t)lr + 1, b = span_end < nnz ? (int64_t)right_row : N;
                 if (b > a) coo_empty_rows<kFe>(a, b, N, dt, u, out);
+                // for k_coo_span_fixup: the row that begins here and goes on (or -1),
+                // and whether one row covers the whole span and goes on
+                const bool cont_in = span_first == lr && left_row == lr, cont_out = right_row == lr;
+                span_row[sidx] = cont_out && !cont_in && lr >= 0 && lr < N ? lr : -1;
+                span_whole[sidx] = cont_in && cont_out ? 1 : 0;
             } else if (next_first > last + 1) {
                 coo_empty_rows<kFe>((int64_t)last + 1, next_first, N, dt, u, out);
             }
@@ -342,23 +350,18 @@ __global__ void __launch_bounds__(256, 5) k_coo_segsum8(int64_t N, int64_t nnz, 
 // row: its part here plus the parts of the following spans, in span order,
 // while the row goes on; then the finished value.
 template <bool kFe>
-__global__ void k_coo_span_fixup(int64_t N, int64_t nnz, const int32_t *__restrict__ rows,
-                                 const float *__restrict__ u, float dt, const float *__restrict__ part_first,
-                                 const float *__restrict__ part_last, float *__restrict__ out)
+__global__ void k_coo_span_fixup(int64_t nspan, const float *__restrict__ u, float dt,
+                                 const float *__restrict__ part_first, const float *__restrict__ part_last,
+                                 const int32_t *__restrict__ span_row, const int32_t *__restrict__ span_whole,
+                                 float *__restrict__ out)
 {
-    const int64_t nspan = cdiv(nnz, kCooSpan);
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nspan; s += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t base = s * kCooSpan, end = base + kCooSpan < nnz ? base + kCooSpan : nnz;
-        if (end >= nnz) continue;
-        const int lr = __ldg(rows + (end - 1));
-        if (__ldg(rows + end) != lr || lr < 0 || lr >= N) continue;  // the last row ends in this span
-        const int fr = __ldg(rows + base);
-        if (fr == lr && base > 0 && __ldg(rows + (base - 1)) == lr) continue;  // a middle part: not the row's start
+        const int lr = span_row[s];
+        if (lr < 0) continue;  // no row begins in this span and goes on
         float total = part_last[s];
         for (int64_t t = s + 1; t < nspan; ++t) {
             total = __fadd_rn(total, part_first[t]);
-            const int64_t te = (t + 1) * kCooSpan < nnz ? (t + 1) * kCooSpan : nnz;
-            if (!(te < nnz && __ldg(rows + (te - 1)) == lr && __ldg(rows + te) == lr)) break;
+            if (!span_whole[t]) break;  // the row ends in span t
         }
         out[lr] = coo_finish<kFe>(total, dt, u, lr);
     }
@@ -1017,19 +1020,24 @@ static int coo_common(int64_t N, int64_t nnz, const int32_t *rows, const int32_t
                 if (coo_part_dev[dev]) PIRO_CUDA(cudaFree(coo_part_dev[dev]));
                 coo_part_dev[dev] = nullptr;
                 coo_part_cap[dev] = 0;
-                PIRO_CUDA(cudaMalloc(&coo_part_dev[dev], 2 * sizeof(float) * (size_t)nspan));
+                PIRO_CUDA(cudaMalloc(&coo_part_dev[dev], 4 * sizeof(float) * (size_t)nspan));
                 coo_part_cap[dev] = nspan;
             }
             parts = coo_part_dev[dev];
         }
-        float *part_first = parts, *part_last = parts + coo_part_cap[dev];
+        const int64_t cap = coo_part_cap[dev];
+        float *part_first = parts, *part_last = parts + cap;
+        int32_t *span_row = reinterpret_cast<int32_t *>(parts + 2 * cap);
+        int32_t *span_whole = reinterpret_cast<int32_t *>(parts + 3 * cap);
         const unsigned g1 = grid_for(cdiv(nnz, kCooPer), 256, 8), g2 = grid_for(nspan, 256, 4);
         if (fe) {
-            k_coo_segsum8<true><<<g1, 256, 0, s>>>(N, nnz, rows, cols, vals, u, dt, out, part_first, part_last, err);
-            k_coo_span_fixup<true><<<g2, 256, 0, s>>>(N, nnz, rows, u, dt, part_first, part_last, out);
+            k_coo_segsum8<true><<<g1, 256, 0, s>>>(N, nnz, rows, cols, vals, u, dt, out, part_first, part_last, span_row,
+                                                   span_whole, err);
+            k_coo_span_fixup<true><<<g2, 256, 0, s>>>(nspan, u, dt, part_first, part_last, span_row, span_whole, out);
         } else {
-            k_coo_segsum8<false><<<g1, 256, 0, s>>>(N, nnz, rows, cols, vals, u, dt, out, part_first, part_last, err);
-            k_coo_span_fixup<false><<<g2, 256, 0, s>>>(N, nnz, rows, u, dt, part_first, part_last, out);
+            k_coo_segsum8<false><<<g1, 256, 0, s>>>(N, nnz, rows, cols, vals, u, dt, out, part_first, part_last,
+                                                    span_row, span_whole, err);
+            k_coo_span_fixup<false><<<g2, 256, 0, s>>>(nspan, u, dt, part_first, part_last, span_row, span_whole, out);
         }
         PIRO_CHECK_LAUNCH("k_coo_segsum8");
     } else {
