@@ -986,11 +986,7 @@ extern "C" int piro_csr_i1(int nx, int ny, int nz, const int32_t *rowptr, const 
 }
 
 // Per device: the input-check flags of k_coo_segsum.
-static int *coo_err_dev[kMaxDevices] = {};
-static DeviceOnce coo_err_once;
-static std::mutex coo_part_mu;
-static float *coo_part_dev[kMaxDevices] = {};
-static int64_t coo_part_cap[kMaxDevices] = {};
+
 
 static int coo_common(int64_t N, int64_t nnz, const int32_t *rows, const int32_t *cols, const float *vals, float dt,
                       const float *u, float *out, bool fe, piro_stream_t stream)
@@ -999,36 +995,28 @@ static int coo_common(int64_t N, int64_t nnz, const int32_t *rows, const int32_t
              "coo spmv: bad arguments");
     PIRO_ARG(u != out, "coo spmv: u and out must differ");
     cudaStream_t s = as_stream(stream);
-    int dev = 0;
-    PIRO_CUDA(cudaGetDevice(&dev));
-    int rc = device_once(coo_err_once, dev, [dev]() -> int {
-        if (!coo_err_dev[dev]) PIRO_CUDA(cudaMalloc(&coo_err_dev[dev], sizeof(int)));
+    if (nnz == 0) {  // every row empty: dt*0 (+ u)
+        PIRO_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * N, s));
+        k_scale_add<<<grid_for(N, 256, 8), 256, 0, s>>>(N, dt, out, fe ? u : nullptr, out);
+        PIRO_CHECK_LAUNCH("k_scale_add");
         return PIRO_OK;
-    });
-    if (rc != PIRO_OK) return rc;
-    int *err = coo_err_dev[dev];
+    }
+    // per-call scratch, stream-ordered (calls on different streams do not share
+    // it): the input-check flag, then for the 16-byte path the per-span parts
+    // and records of rows that cross spans
     const bool al16 = ((reinterpret_cast<uintptr_t>(rows) | reinterpret_cast<uintptr_t>(cols) |
                         reinterpret_cast<uintptr_t>(vals)) & 15) == 0;
-    if (nnz > 0) PIRO_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-    if (nnz > 0 && al16) {
-        // the span parts of rows that cross spans: a per-device buffer that grows
-        const int64_t nspan = cdiv(nnz, kCooSpan);
-        float *parts = nullptr;
-        {
-            std::lock_guard<std::mutex> lk(coo_part_mu);
-            if (coo_part_cap[dev] < nspan) {
-                if (coo_part_dev[dev]) PIRO_CUDA(cudaFree(coo_part_dev[dev]));
-                coo_part_dev[dev] = nullptr;
-                coo_part_cap[dev] = 0;
-                PIRO_CUDA(cudaMalloc(&coo_part_dev[dev], 4 * sizeof(float) * (size_t)nspan));
-                coo_part_cap[dev] = nspan;
-            }
-            parts = coo_part_dev[dev];
-        }
-        const int64_t cap = coo_part_cap[dev];
-        float *part_first = parts, *part_last = parts + cap;
-        int32_t *span_row = reinterpret_cast<int32_t *>(parts + 2 * cap);
-        int32_t *span_whole = reinterpret_cast<int32_t *>(parts + 3 * cap);
+    const int64_t nspan = cdiv(nnz, kCooSpan);
+    const size_t scratch = 256 + (al16 ? 16 * (size_t)nspan : 0);
+    void *mem = nullptr;
+    PIRO_CUDA(cudaMallocAsync(&mem, scratch, s));
+    int *err = static_cast<int *>(mem);
+    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), s);
+    if (e == cudaSuccess && al16) {
+        float *parts = reinterpret_cast<float *>(static_cast<char *>(mem) + 256);
+        float *part_first = parts, *part_last = parts + nspan;
+        int32_t *span_row = reinterpret_cast<int32_t *>(parts + 2 * nspan);
+        int32_t *span_whole = reinterpret_cast<int32_t *>(parts + 3 * nspan);
         const unsigned g1 = grid_for(cdiv(nnz, kCooPer), 256, 8), g2 = grid_for(nspan, 256, 4);
         if (fe) {
             k_coo_segsum8<true><<<g1, 256, 0, s>>>(N, nnz, rows, cols, vals, u, dt, out, part_first, part_last, span_row,
@@ -1039,24 +1027,27 @@ static int coo_common(int64_t N, int64_t nnz, const int32_t *rows, const int32_t
                                                     span_row, span_whole, err);
             k_coo_span_fixup<false><<<g2, 256, 0, s>>>(nspan, u, dt, part_first, part_last, span_row, span_whole, out);
         }
-        PIRO_CHECK_LAUNCH("k_coo_segsum8");
-    } else {
+        e = cudaGetLastError();
+    } else if (e == cudaSuccess) {
         // out doubles as the accumulator: zero it, sum into it, then scale in place.
-        PIRO_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * N, s));
-        if (nnz > 0) {
+        e = cudaMemsetAsync(out, 0, sizeof(float) * N, s);
+        if (e == cudaSuccess) {
             k_coo_segsum<<<grid_for(nnz, 256, 8), 256, 0, s>>>(N, nnz, rows, cols, vals, u, out, err);
-            PIRO_CHECK_LAUNCH("k_coo_segsum");
+            k_scale_add<<<grid_for(N, 256, 8), 256, 0, s>>>(N, dt, out, fe ? u : nullptr, out);
+            e = cudaGetLastError();
         }
-        k_scale_add<<<grid_for(N, 256, 8), 256, 0, s>>>(N, dt, out, fe ? u : nullptr, out);
-        PIRO_CHECK_LAUNCH("k_scale_add");
     }
-    if (nnz > 0) {
-        int h = 0;
-        PIRO_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s));
-        PIRO_CUDA(cudaStreamSynchronize(s));
-        PIRO_ARG(!(h & 1), "coo spmv: a row or column id outside [0, N)");
-        PIRO_ARG(!(h & 2), "coo spmv: row ids not sorted ascending (use piro_coo_row_index for its check)");
+    int h = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    const cudaError_t ef = cudaFreeAsync(mem, s);
+    if (e == cudaSuccess) e = ef;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_error("coo spmv: %s", cudaGetErrorString(e));
+        return PIRO_ERR_CUDA;
     }
+    PIRO_ARG(!(h & 1), "coo spmv: a row or column id outside [0, N)");
+    PIRO_ARG(!(h & 2), "coo spmv: row ids not sorted ascending (use piro_coo_row_index for its check)");
     return PIRO_OK;
 }
 
