@@ -236,6 +236,9 @@ int piro_ht_spmv_staged(int nx, int ny, int nz, const int64_t *keys, const float
  * nonzero at or below the diagonal (a singular matrix).  piro_ht_lu_solve
  * solves A x = b (b, x device float[N]) in FP64 -- the row exchanges and
  * Gauss transforms, then back substitution -- and rounds x to FP32.
+ * The solve runs by 16-row panels with y in a shared-memory ring of 2bw + 16
+ * rows (bands up to about 10 000 wide; wider ones, or PIRO_LU_NO_RING=1, keep
+ * y in global memory, same bits).
  * piro_ht_lu_pivots copies the pivot rows (0-based, LAPACK's ipiv - 1) to the
  * host. */
 int piro_ht_lu_reference(int64_t N, int64_t *keys, float *vals, int64_t ts, piro_stream_t stream);

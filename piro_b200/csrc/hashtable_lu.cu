@@ -1201,7 +1201,8 @@ extern "C" int piro_ht_lu_solve(int64_t N, int64_t bw, void *band, size_t band_b
                                               reinterpret_cast<const int32_t *>(base + L.piv), b,
                                               reinterpret_cast<double *>(base + L.y), x);
         PIRO_CHECK_LAUNCH("k_lup_solve");
-    } else if ((size_t)(2 * bw + kLuSolveNb) * sizeof(double) <= 160 * 1024) {
+    } else if ((size_t)(2 * bw + kLuSolveNb) * sizeof(double) <= 160 * 1024 &&
+               !(getenv("PIRO_LU_NO_RING") && getenv("PIRO_LU_NO_RING")[0] == '1')) {
         const size_t smem = (size_t)(2 * bw + kLuSolveNb) * sizeof(double);
         PIRO_CUDA(cudaFuncSetAttribute(k_lup_solve_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_lup_solve_ring<<<1, kPivThreads, smem, st>>>(N, bw, L.W, reinterpret_cast<const double *>(base + L.band),

@@ -988,6 +988,10 @@ extern "C" int piro_csr_i1(int nx, int ny, int nz, const int32_t *rowptr, const 
 // Per device: the input-check flags of k_coo_segsum.
 
 
+static std::mutex coo_scratch_mu[kMaxDevices];
+static void *coo_scratch_buf[kMaxDevices] = {};
+static size_t coo_scratch_cap[kMaxDevices] = {};
+
 static int coo_common(int64_t N, int64_t nnz, const int32_t *rows, const int32_t *cols, const float *vals, float dt,
                       const float *u, float *out, bool fe, piro_stream_t stream)
 {
@@ -1001,15 +1005,27 @@ static int coo_common(int64_t N, int64_t nnz, const int32_t *rows, const int32_t
         PIRO_CHECK_LAUNCH("k_scale_add");
         return PIRO_OK;
     }
-    // per-call scratch, stream-ordered (calls on different streams do not share
-    // it): the input-check flag, then for the 16-byte path the per-span parts
-    // and records of rows that cross spans
+    // scratch: the input-check flag, then for the 16-byte path the per-span
+    // parts and records of rows that cross spans.  One buffer per device,
+    // grown on demand and held under a lock for the whole call (the call
+    // ends with a stream synchronize), so calls from several host threads or
+    // streams never share it while in flight.
     const bool al16 = ((reinterpret_cast<uintptr_t>(rows) | reinterpret_cast<uintptr_t>(cols) |
                         reinterpret_cast<uintptr_t>(vals)) & 15) == 0;
     const int64_t nspan = cdiv(nnz, kCooSpan);
     const size_t scratch = 256 + (al16 ? 16 * (size_t)nspan : 0);
-    void *mem = nullptr;
-    PIRO_CUDA(cudaMallocAsync(&mem, scratch, s));
+    int dev = 0;
+    PIRO_CUDA(cudaGetDevice(&dev));
+    PIRO_ARG(dev >= 0 && dev < kMaxDevices, "coo spmv: device index out of range");
+    std::lock_guard<std::mutex> lk(coo_scratch_mu[dev]);
+    if (coo_scratch_cap[dev] < scratch) {
+        if (coo_scratch_buf[dev]) PIRO_CUDA(cudaFree(coo_scratch_buf[dev]));
+        coo_scratch_buf[dev] = nullptr;
+        coo_scratch_cap[dev] = 0;
+        PIRO_CUDA(cudaMalloc(&coo_scratch_buf[dev], scratch));
+        coo_scratch_cap[dev] = scratch;
+    }
+    void *mem = coo_scratch_buf[dev];
     int *err = static_cast<int *>(mem);
     cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), s);
     if (e == cudaSuccess && al16) {
@@ -1039,8 +1055,6 @@ static int coo_common(int64_t N, int64_t nnz, const int32_t *rows, const int32_t
     }
     int h = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);
-    const cudaError_t ef = cudaFreeAsync(mem, s);
-    if (e == cudaSuccess) e = ef;
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         set_error("coo spmv: %s", cudaGetErrorString(e));

@@ -147,3 +147,26 @@ def test_ht_lu_panels_equal_column_launches(cuda, n, dt, monkeypatch):
     span = np.minimum(bw, N - 1 - np.arange(N))
     defined = np.arange(bw)[None, :] < span[:, None]
     assert np.array_equal(la[defined].view(np.uint64), lb[defined].view(np.uint64))
+
+
+@pytest.mark.parametrize("n,dt", [((8, 7, 6), 0.7), ((12, 10, 9), 0.05), ((3, 3, 40), 0.1)])
+def test_ht_lu_ring_and_global_solves_agree(cuda, n, dt, monkeypatch):
+    """The solve with y in a shared-memory ring and the one with y in global
+    memory (PIRO_LU_NO_RING=1, the form bands wider than the ring take) give
+    the same bits; both match an FP64 dense solve."""
+    import torch
+    from piro_b200 import ops
+    nx, ny, nz = n
+    N = nx * ny * nz
+    L, Ad = _dense(ops, n, dt)
+    ts = ops.ht_table_size(L[2].numel(), N, 1)
+    keys, vals = ops.ht_build(N, *L, ts)
+    lu = ops.HtLu(N, nx * ny, keys, vals, ts, 1.0, -dt)
+    b = torch.from_numpy(np.random.default_rng(5).random(N).astype(np.float32)).cuda()
+    x_ring = lu.solve(b).cpu().numpy()
+    monkeypatch.setenv("PIRO_LU_NO_RING", "1")
+    x_glob = lu.solve(b).cpu().numpy()
+    assert np.array_equal(x_ring.view(np.uint32), x_glob.view(np.uint32))
+    ref = np.linalg.solve(Ad, b.cpu().numpy().astype(np.float64))
+    cond = np.linalg.cond(Ad)
+    assert np.abs(x_ring - ref).max() <= (1.2e-7 + 64 * cond * 1.2e-16) * np.abs(ref).max()
