@@ -126,18 +126,24 @@ __global__ void __launch_bounds__(kSlabThreads) k_slab_cg_spmv(Slab S, float bet
     const int64_t lo = max(S.own0 - sxy, -S.lbase), hi = min(S.own1 + sxy, N - S.lbase);
     for (int64_t l = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < hi;
          l += (int64_t)gridDim.x * blockDim.x) {
-        const bool in = S.g.interior(l + S.lbase);
+        int x, y, zc;
+        S.g.coords((uint32_t)(l + S.lbase), x, y, zc);
+        const bool in = x > 0 && x < S.g.nx - 1 && y > 0 && y < S.g.ny - 1 && zc > 0 && zc < S.g.nz - 1;
         const float pc = in ? z[l] + beta * p_old[l] : 0.0f;
         p_new[l] = pc;
         if (!in || l < S.own0 || l >= S.own1) continue;
         const int nx = S.g.nx;
-        // neighbours' p formed from z and p_old (p_new of other threads is not read)
-        auto pv = [&](int64_t j) { return S.g.interior(j + S.lbase) ? z[j] + beta * p_old[j] : 0.0f; };
+        // neighbours' p formed from z and p_old (p_new of other threads is not read);
+        // the cell is interior, so a neighbour is interior when its one moved
+        // coordinate is
+        auto pv = [&](int64_t j, bool nin) { return nin ? z[j] + beta * p_old[j] : 0.0f; };
         const float a = alpha[l];
         float cd, co;
         coef(S, a, cd, co);
         const float qv =
-            cd * pc + co * (((pv(l - 1) + pv(l + 1)) + (pv(l - nx) + pv(l + nx))) + (pv(l - sxy) + pv(l + sxy)));
+            cd * pc + co * (((pv(l - 1, x > 1) + pv(l + 1, x < nx - 2)) +
+                             (pv(l - nx, y > 1) + pv(l + nx, y < S.g.ny - 2))) +
+                            (pv(l - sxy, zc > 1) + pv(l + sxy, zc < S.g.nz - 2)));
         q[l] = qv;
         v[0] += (double)pc * (double)qv / (double)a;
     }

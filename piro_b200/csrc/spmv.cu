@@ -257,15 +257,19 @@ __global__ void __launch_bounds__(256, 5) k_coo_segsum8(int64_t N, int64_t nnz, 
             }
         }
         // input checks: ids in [0, N), row ids ascending (within the lane and
-        // from the entry before it); an entry out of range adds nothing
+        // from the entry before it); an entry out of range adds nothing.  A
+        // lane with all 8 entries inside the array (every lane but the last
+        // one of the array) skips the per-entry end test.
+        const bool full = k0 + kCooPer <= nnz;
         int prev = __shfl_up_sync(0xffffffffu, r[kCooPer - 1], 1);
         if (lane == 0) prev = base > 0 ? __ldg(rows + (base - 1)) : INT32_MIN;
+        const uint32_t un = (uint32_t)N;
 #pragma unroll
         for (int t = 0; t < kCooPer; ++t) {
-            if (k0 + t >= nnz) continue;
+            if (!full && k0 + t >= nnz) continue;
             if (r[t] < prev) bad |= 2;
             prev = r[t];
-            if (r[t] < 0 || r[t] >= N || c[t] < 0 || c[t] >= N) {
+            if ((uint32_t)r[t] >= un || (uint32_t)c[t] >= un) {  // negative ids wrap above N
                 bad |= 1;
                 v[t] = 0.0f;
                 c[t] = 0;
@@ -278,7 +282,7 @@ __global__ void __launch_bounds__(256, 5) k_coo_segsum8(int64_t N, int64_t nnz, 
         bool multi = false;
 #pragma unroll
         for (int t = 0; t < kCooPer; ++t) {
-            const float pv = r[t] != kNone ? __fmul_rn(v[t], __ldg(u + c[t])) : 0.0f;
+            const float pv = (full || r[t] != kNone) ? __fmul_rn(v[t], __ldg(u + c[t])) : 0.0f;
             if (r[t] != cur) {
                 if (!multi) head = s_run;                                               // the lane's first run
                 else if (cur >= 0 && cur < N) out[cur] = coo_finish<kFe>(s_run, dt, u, cur);  // a whole row
