@@ -109,7 +109,7 @@ enum : int {
 // p = z + beta*p_old on interior cells of the owned and halo planes (0 on the
 // boundary); q = A p on owned interior cells; partial <p, q/alpha>.  With a
 // device state, beta comes from it and a finished solve returns at once.
-__global__ void __launch_bounds__(kSlabThreads) k_slab_cg_spmv(Slab S, float beta, const double *__restrict__ state,
+__global__ void __launch_bounds__(kSlabThreads, 4) k_slab_cg_spmv(Slab S, float beta, const double *__restrict__ state,
                                                                const float *__restrict__ alpha,
                                                                const float *__restrict__ z,
                                                                const float *__restrict__ p_old,
@@ -124,6 +124,61 @@ __global__ void __launch_bounds__(kSlabThreads) k_slab_cg_spmv(Slab S, float bet
     const int64_t N = sxy * S.g.nz;
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     const int64_t lo = max(S.own0 - sxy, -S.lbase), hi = min(S.own1 + sxy, N - S.lbase);
+    const int nx = S.g.nx;
+    const bool vec = (nx & 3) == 0 && ((lo | hi | S.own0 | S.own1 | S.lbase) & 3) == 0 &&
+                     ((reinterpret_cast<uintptr_t>(alpha) | reinterpret_cast<uintptr_t>(z) |
+                       reinterpret_cast<uintptr_t>(p_old) | reinterpret_cast<uintptr_t>(p_new) |
+                       reinterpret_cast<uintptr_t>(q)) & 15) == 0;
+    if (vec) {
+        // groups of 4 x-adjacent cells (nx % 4 == 0: a group never leaves its
+        // x-row): z and p_old at the group and its y/z neighbours as 16-byte
+        // loads, the x halo as two scalars; the same arithmetic per cell
+        const float4 *Z = reinterpret_cast<const float4 *>(z), *Po = reinterpret_cast<const float4 *>(p_old);
+        const int64_t rx = nx >> 2, rxy = sxy >> 2;
+        for (int64_t g4 = (lo >> 2) + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g4 < (hi >> 2);
+             g4 += (int64_t)gridDim.x * blockDim.x) {
+            const int64_t l = g4 << 2;
+            int x0, y, zc;
+            S.g.coords((uint32_t)(l + S.lbase), x0, y, zc);
+            const bool yz = y > 0 && y < S.g.ny - 1 && zc > 0 && zc < S.g.nz - 1;
+            bool in[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) in[k] = yz && x0 + k > 0 && x0 + k < nx - 1;
+            const float4 zc4 = Z[g4], pc4 = Po[g4];
+            const float zz[4] = {zc4.x, zc4.y, zc4.z, zc4.w}, pp[4] = {pc4.x, pc4.y, pc4.z, pc4.w};
+            float pc[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) pc[k] = in[k] ? zz[k] + beta * pp[k] : 0.0f;
+            reinterpret_cast<float4 *>(p_new)[g4] = make_float4(pc[0], pc[1], pc[2], pc[3]);
+            if (l < S.own0 || l >= S.own1 || !(in[0] || in[1] || in[2] || in[3])) continue;
+            auto vp = [&](float4 a4, float4 b4, int k) {
+                const float za[4] = {a4.x, a4.y, a4.z, a4.w}, pb[4] = {b4.x, b4.y, b4.z, b4.w};
+                return za[k] + beta * pb[k];
+            };
+            const float4 zym = Z[g4 - rx], pym = Po[g4 - rx], zyp = Z[g4 + rx], pyp = Po[g4 + rx];
+            const float4 zzm = Z[g4 - rxy], pzm = Po[g4 - rxy], zzp = Z[g4 + rxy], pzp = Po[g4 + rxy];
+            const float xl = x0 > 1 ? z[l - 1] + beta * p_old[l - 1] : 0.0f;
+            const float xr = x0 + 4 < nx - 1 ? z[l + 4] + beta * p_old[l + 4] : 0.0f;
+            const float4 al4 = reinterpret_cast<const float4 *>(alpha)[g4];
+            const float al[4] = {al4.x, al4.y, al4.z, al4.w};
+            float qo[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                qo[k] = 0.0f;
+                if (!in[k]) continue;
+                const float xm = k > 0 ? pc[k - 1] : xl, xp = k < 3 ? pc[k + 1] : xr;
+                const float ym = y > 1 ? vp(zym, pym, k) : 0.0f, yp = y < S.g.ny - 2 ? vp(zyp, pyp, k) : 0.0f;
+                const float zm = zc > 1 ? vp(zzm, pzm, k) : 0.0f, zp = zc < S.g.nz - 2 ? vp(zzp, pzp, k) : 0.0f;
+                float cd, co;
+                coef(S, al[k], cd, co);
+                qo[k] = cd * pc[k] + co * (((xm + xp) + (ym + yp)) + (zm + zp));
+                v[0] += (double)pc[k] * (double)qo[k] / (double)al[k];
+            }
+            reinterpret_cast<float4 *>(q)[g4] = make_float4(qo[0], qo[1], qo[2], qo[3]);
+        }
+        block_partials(part, 1, v);
+        return;
+    }
     for (int64_t l = lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < hi;
          l += (int64_t)gridDim.x * blockDim.x) {
         int x, y, zc;
@@ -132,7 +187,6 @@ __global__ void __launch_bounds__(kSlabThreads) k_slab_cg_spmv(Slab S, float bet
         const float pc = in ? z[l] + beta * p_old[l] : 0.0f;
         p_new[l] = pc;
         if (!in || l < S.own0 || l >= S.own1) continue;
-        const int nx = S.g.nx;
         // neighbours' p formed from z and p_old (p_new of other threads is not read);
         // the cell is interior, so a neighbour is interior when its one moved
         // coordinate is
@@ -169,19 +223,49 @@ __global__ void __launch_bounds__(kSlabThreads) k_slab_cg_update(Slab S, float a
         a = (float)ad;
     }
     double v[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int64_t l = S.own0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < S.own1;
-         l += (int64_t)gridDim.x * blockDim.x) {
-        if (!S.g.interior(l + S.lbase)) continue;
-        const float al = alpha[l];
+    auto one = [&](float al, float pv, float qv, float &dv, float &rv, float &zv) {
         float cd, co;
         coef(S, al, cd, co);
-        d[l] += a * p[l];
-        const float ri = r[l] - a * q[l];
-        const float zi = ri / cd;
-        r[l] = ri;
-        z[l] = zi;
-        v[0] += (double)ri / (double)al * (double)zi;
-        v[1] += (double)ri * (double)ri;
+        dv += a * pv;
+        rv = rv - a * qv;
+        zv = rv / cd;
+        v[0] += (double)rv / (double)al * (double)zv;
+        v[1] += (double)rv * (double)rv;
+    };
+    const bool vec = ((S.own0 | S.own1) & 3) == 0 &&
+                     ((reinterpret_cast<uintptr_t>(alpha) | reinterpret_cast<uintptr_t>(p) |
+                       reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(d) |
+                       reinterpret_cast<uintptr_t>(r) | reinterpret_cast<uintptr_t>(z)) & 15) == 0;
+    if (vec) {
+        // groups of 4 cells, all five inputs (and z, kept where the cell is not
+        // interior) as 16-byte loads: four times the bytes in flight per thread
+        for (int64_t g4 = (S.own0 >> 2) + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g4 < (S.own1 >> 2);
+             g4 += (int64_t)gridDim.x * blockDim.x) {
+            const float4 al = reinterpret_cast<const float4 *>(alpha)[g4];
+            const float4 pv = reinterpret_cast<const float4 *>(p)[g4];
+            const float4 qv = reinterpret_cast<const float4 *>(q)[g4];
+            float4 dv = reinterpret_cast<float4 *>(d)[g4];
+            float4 rv = reinterpret_cast<float4 *>(r)[g4];
+            float4 zv = reinterpret_cast<float4 *>(z)[g4];
+            const int64_t l = g4 << 2;
+            if (S.g.interior(l + S.lbase)) one(al.x, pv.x, qv.x, dv.x, rv.x, zv.x);
+            if (S.g.interior(l + 1 + S.lbase)) one(al.y, pv.y, qv.y, dv.y, rv.y, zv.y);
+            if (S.g.interior(l + 2 + S.lbase)) one(al.z, pv.z, qv.z, dv.z, rv.z, zv.z);
+            if (S.g.interior(l + 3 + S.lbase)) one(al.w, pv.w, qv.w, dv.w, rv.w, zv.w);
+            reinterpret_cast<float4 *>(d)[g4] = dv;
+            reinterpret_cast<float4 *>(r)[g4] = rv;
+            reinterpret_cast<float4 *>(z)[g4] = zv;
+        }
+    } else {
+        for (int64_t l = S.own0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < S.own1;
+             l += (int64_t)gridDim.x * blockDim.x) {
+            if (!S.g.interior(l + S.lbase)) continue;
+            float dv = d[l], rv = r[l], zv;
+            one(alpha[l], p[l], q[l], dv, rv, zv);
+            d[l] = dv;
+            r[l] = rv;
+            z[l] = zv;
+        }
     }
     block_partials(part, 2, v);
 }
