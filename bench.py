@@ -182,20 +182,13 @@ def spmv_section(torch, ops, steps, warmup, peak):
     byt = 12 * ts + 12 * N
     order = ops.ht_row_order(N, ts)
     stage = ops.ht_stage(N)
-    packed = ops.ht_pack(keys, vals)
-    ms = timeit(lambda: ops.ht_spmv_packed(nx, ny, nz, packed, dt, order, stage, u, out, fe=True), steps)
+    ms = timeit(lambda: ops.ht_spmv_staged(nx, ny, nz, keys, vals, dt, order, stage, u, out, fe=True), steps)
     res["ht"] = {"ms": ms, "gbs": byt / ms / 1e6, "frac": byt / ms / 1e6 / peak, "bytes": byt, "slots": ts,
                  "rows": "table read with the rows in home-slot order (piro_ht_row_order, once per table), "
                          "each row's values staged in a 32-byte record, then applied in row order",
-                 "table": "16-byte slots {key, value} (piro_ht_pack, once per table): one load per probe",
                  "stage_bytes": 32 * N,
-                 "bytes_definition": "12 ts (key and value of every slot) + 12 N (u, out, row order); the "
-                                     "slots' 4 padding bytes and the stage's 64 N bytes (written, read back) "
-                                     "are not counted"}
-    del packed
-    ms = timeit(lambda: ops.ht_spmv_staged(nx, ny, nz, keys, vals, dt, order, stage, u, out, fe=True), steps)
-    res["ht_two_arrays"] = {"ms": ms, "gbs": byt / ms / 1e6, "frac": byt / ms / 1e6 / peak,
-                            "table": "keys and values in two arrays (piro_ht_spmv_staged)"}
+                 "bytes_definition": "12 ts (keys and values, every slot) + 12 N (u, out, row order); the "
+                                     "stage's 64 N bytes (written, read back) are not counted"}
     del stage
     ms = timeit(lambda: ops.ht_spmv_ordered(nx, ny, nz, keys, vals, dt, order, u, out, fe=True), steps)
     res["ht_one_pass"] = {"ms": ms, "gbs": byt / ms / 1e6, "frac": byt / ms / 1e6 / peak}
@@ -1054,8 +1047,8 @@ def run_profile_case(args):
     matrix), `learned` two learned-preconditioner solves of the 128^3 step,
     `batched` two steps of a 64-member batch
     in each schedule (lockstep, then grouped), `train` four training steps of
-    the network on 8 crops of 34^3 cells, `ht` three staged hash-table steps on
-    the packed table, three on the two arrays and three one-pass ordered ones at 192^3, `fe160` the forward-Euler kernels one format at a time at 160^3
+    the network on 8 crops of 34^3 cells, `ht` three staged and three one-pass
+    ordered hash-table steps at 192^3, `fe160` the forward-Euler kernels one format at a time at 160^3
     (CSR, matrix-free, segmented COO, three launches each), three
     Laplacian assemblies and three v.grad merges (csrgeam3) of the upwind
     gradients, `lu` the scheme-27 band factorization and one solve at 24^3."""
@@ -1109,9 +1102,6 @@ def run_profile_case(args):
         u = torch.rand(N, device="cuda")
         out = torch.empty_like(u)
         stage = ops.ht_stage(N)
-        packed = ops.ht_pack(keys, vals)
-        for _ in range(3):
-            ops.ht_spmv_packed(n, n, n, packed, 0.01, order, stage, u, out, fe=True)
         for _ in range(3):
             ops.ht_spmv_staged(n, n, n, keys, vals, 0.01, order, stage, u, out, fe=True)
         for _ in range(3):

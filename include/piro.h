@@ -210,17 +210,6 @@ int piro_ht_stage_bytes(int64_t N, size_t *bytes);
 int piro_ht_spmv_staged(int nx, int ny, int nz, const int64_t *keys, const float *vals, int64_t ts, float dt, int fe,
                         const int32_t *order, void *stage, size_t stage_bytes, const float *u, float *out,
                         piro_stream_t stream);
-/* The table interleaved for that step: piro_ht_pack writes slot s of
- * (keys, vals) as 16 bytes {key low word, key high word, value bits, 0} into
- * packed (16*ts bytes, 16-byte aligned; once per table, like the row order),
- * and piro_ht_spmv_packed runs piro_ht_spmv_staged's two passes on it: a
- * probe reads its key and value with one 16-byte load.  Same results bit for
- * bit. */
-int piro_ht_pack(const int64_t *keys, const float *vals, int64_t ts, void *packed, size_t packed_bytes,
-                 piro_stream_t stream);
-int piro_ht_spmv_packed(int nx, int ny, int nz, const void *packed, int64_t ts, float dt, int fe,
-                        const int32_t *order, void *stage, size_t stage_bytes, const float *u, float *out,
-                        piro_stream_t stream);
 
 /* Scheme 27 (TIMESCHEME 12 + solver 27) on a table built by piro_ht_build
  * (int64 keys, -1 empty; -2 marks a deleted key).  piro_ht_lu_reference is

@@ -72,8 +72,6 @@ SIGNATURES = {
     "piro_ht_spmv_ordered": (i32, [i32, i32, i32, vp, vp, i64, f32, i32, vp, vp, vp, vp]),
     "piro_ht_stage_bytes": (i32, [i64, C.POINTER(sz)]),
     "piro_ht_spmv_staged": (i32, [i32, i32, i32, vp, vp, i64, f32, i32, vp, vp, sz, vp, vp, vp]),
-    "piro_ht_pack": (i32, [vp, vp, i64, vp, sz, vp]),
-    "piro_ht_spmv_packed": (i32, [i32, i32, i32, vp, i64, f32, i32, vp, vp, sz, vp, vp, vp]),
     "piro_dense_laplacian": (i32, [i32, i32, i32, i32, f32, vp, sz, vp]),
     "piro_dense_fe_step": (i32, [i64, vp, f32, vp, vp, vp]),
     "piro_dense_check": (i32, [vp]),

@@ -162,8 +162,7 @@ struct piro_ctx {
     float *ht_vals = nullptr;
     int64_t ht_ts = 0;
     int32_t *ht_order = nullptr;  // rows by the home slot of their keys (piro_ht_row_order)
-    float *ht_stage = nullptr;    // 32 bytes per row for the staged step
-    void *ht_packed = nullptr;    // the table as 16-byte slots (piro_ht_pack)
+    float *ht_stage = nullptr;    // 32 bytes per row for piro_ht_spmv_staged
     // scheme 27: factorized once (INIT::RHS_INIT, operatoroverload.cpp:68-81)
     bool lu_done = false;
     void *lu_band = nullptr;
@@ -537,7 +536,6 @@ extern "C" void piro_close(piro_ctx *c)
     cudaFree(c->ht_vals);
     cudaFree(c->ht_order);
     cudaFree(c->ht_stage);
-    cudaFree(c->ht_packed);
     cudaFree(c->lu_band);
     cudaFree(c->bc_idx);
     cudaFree(c->memD);
@@ -709,8 +707,6 @@ extern "C" int piro_laplacian(piro_ctx *c, const char *var, const char *coeff, p
             PK(piro_ht_row_order(N, ts, c->ht_order, c->work, c->work_bytes, c->stream));
             PK(piro_ht_stage_bytes(N, &wb));
             CK(cudaMalloc(&c->ht_stage, wb));
-            CK(cudaMalloc(&c->ht_packed, 16 * (size_t)ts));
-            PK(piro_ht_pack(c->ht_keys, c->ht_vals, ts, c->ht_packed, 16 * (size_t)ts, c->stream));
         }
     }
     c->lap_coeff = coef;
@@ -926,8 +922,8 @@ extern "C" int piro_assign(piro_ctx *c, piro_buf lhs, piro_op rhs, piro_buf *out
             PK(piro_dense_check(c->stream));
         } else if (c->datatype == 2) {
             if (!c->ht_keys) return fail(PIRO_ERR_STATE, "piro_assign: hash table not built");
-            PK(piro_ht_spmv_packed(c->nx, c->ny, c->nz, c->ht_packed, c->ht_ts, dt, 1, c->ht_order, c->ht_stage,
-                                   32 * (size_t)N, u, c->partD, c->stream));
+            PK(piro_ht_spmv_staged(c->nx, c->ny, c->nz, c->ht_keys, c->ht_vals, c->ht_ts, dt, 1, c->ht_order,
+                                   c->ht_stage, 32 * (size_t)N, u, c->partD, c->stream));
         } else if (c->datatype == 3) {
             if (!c->coo_rows) return fail(PIRO_ERR_STATE, "piro_assign: COO operator not assembled");
             PK(piro_coo_step_indexed(N, c->coo_rowstart, c->lap.col, c->lap.val, dt, 1, u, c->partD, c->stream));

@@ -395,54 +395,6 @@ __device__ __forceinline__ float ht_get_from(int64_t key, int64_t h, const int64
     return 0.0f;
 }
 
-// The table as the staged step reads it: two arrays (keys, values), or one
-// array of 16-byte slots {key low word, key high word, value bits, 0} built
-// from them by piro_ht_pack, where a probe is one 16-byte load (one L2 sector
-// request instead of two).
-struct HtSoA {
-    const int64_t *keys;
-    const float *vals;
-    __device__ __forceinline__ void load(int64_t h, int64_t &k, float &v) const
-    {
-        k = __ldg(keys + h);
-        v = __ldg(vals + h);
-    }
-};
-
-struct HtPacked {
-    const int4 *slots;
-    __device__ __forceinline__ void load(int64_t h, int64_t &k, float &v) const
-    {
-        const int4 s = __ldg(slots + h);
-        k = (int64_t)(((uint64_t)(uint32_t)s.y << 32) | (uint64_t)(uint32_t)s.x);
-        v = __int_as_float(s.z);
-    }
-};
-
-// ht_get_from over either layout.
-template <class Tab>
-__device__ __forceinline__ float ht_probe_from(int64_t key, int64_t h, const Tab &tab, int64_t ts)
-{
-    for (int64_t a = 0; a < ts; ++a) {
-        int64_t k;
-        float v;
-        tab.load(h, k, v);
-        if (k == key) return v;
-        if (k == -1) return 0.0f;
-        h = h + 1 == ts ? 0 : h + 1;
-    }
-    return 0.0f;
-}
-
-__global__ void k_ht_pack(int64_t ts, const int64_t *__restrict__ keys, const float *__restrict__ vals,
-                          int4 *__restrict__ slots)
-{
-    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < ts; s += (int64_t)gridDim.x * blockDim.x) {
-        const uint64_t k = (uint64_t)keys[s];
-        slots[s] = make_int4((int)(uint32_t)k, (int)(uint32_t)(k >> 32), __float_as_int(vals[s]), 0);
-    }
-}
-
 // Row i of the 7-point matrix (row order[j] of thread j when ordered): the
 // candidate columns c = i + off, off in
 // {-nx*ny, -nx, -1, 0, 1, nx, nx*ny}, in ascending order; absent keys give 0,
@@ -511,9 +463,9 @@ __global__ void __launch_bounds__(256, 4) k_ht_spmv(GridDiv g, int64_t N, const 
 // stores: whole sectors, no read-modify-write of a partly written sector).
 // Pass 2 (rows in index order) reads the records and u coalesced and writes
 // out coalesced.  The per-row arithmetic is the one above, term for term.
-template <class Tab>
-__global__ void __launch_bounds__(256, 5) k_ht_stage(GridDiv g, int64_t N, Tab tab, int64_t ts, ModU64 mts,
-                                                     const int32_t *__restrict__ order, float4 *__restrict__ stage)
+__global__ void __launch_bounds__(256, 4) k_ht_stage(GridDiv g, int64_t N, const int64_t *__restrict__ keys,
+                           const float *__restrict__ vals, int64_t ts, ModU64 mts, const int32_t *__restrict__ order,
+                           float4 *__restrict__ stage)
 {
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int64_t sxy = (int64_t)nx * ny;
@@ -540,7 +492,11 @@ __global__ void __launch_bounds__(256, 5) k_ht_stage(GridDiv g, int64_t N, Tab t
 #pragma unroll
         for (int t = 0; t < 7; ++t) {
             v[t] = 0.0f;
-            if (ok[t]) tab.load(home(t), k[t], v[t]);  // the value with the key: one round trip
+            if (ok[t]) {
+                const int64_t hh = home(t);
+                k[t] = __ldg(keys + hh);
+                v[t] = __ldg(vals + hh);  // with the key: one round trip
+            }
         }
 #pragma unroll
         for (int t = 0; t < 7; ++t) {
@@ -551,7 +507,7 @@ __global__ void __launch_bounds__(256, 5) k_ht_stage(GridDiv g, int64_t N, Tab t
                     v[t] = 0.0f;
                 } else {
                     const int64_t hh = home(t);
-                    v[t] = ht_probe_from(key, hh + 1 == ts ? 0 : hh + 1, tab, ts);
+                    v[t] = ht_get_from(key, hh + 1 == ts ? 0 : hh + 1, keys, vals, ts);
                 }
             }
         }
@@ -1245,41 +1201,7 @@ extern "C" int piro_ht_spmv_staged(int nx, int ny, int nz, const int64_t *keys, 
     cudaStream_t s = as_stream(stream);
     float4 *st = static_cast<float4 *>(stage);
     const GridDiv g(nx, ny, nz);
-    k_ht_stage<HtSoA><<<grid_for(N, 256, 8), 256, 0, s>>>(g, N, HtSoA{keys, vals}, ts, ModU64((uint64_t)ts), order,
-                                                          st);
-    PIRO_CHECK_LAUNCH("k_ht_stage");
-    k_ht_stage_apply<<<grid_for(N, 256, 8), 256, 0, s>>>(g, dt, fe, st, u, out);
-    PIRO_CHECK_LAUNCH("k_ht_stage_apply");
-    return PIRO_OK;
-}
-
-extern "C" int piro_ht_pack(const int64_t *keys, const float *vals, int64_t ts, void *packed, size_t packed_bytes,
-                            piro_stream_t stream)
-{
-    PIRO_ARG(keys && vals && packed && ts > 0, "piro_ht_pack: bad arguments");
-    PIRO_ARG(packed_bytes >= 16 * (size_t)ts && ((uintptr_t)packed & 15) == 0,
-             "piro_ht_pack: packed smaller than 16 bytes per slot or not 16-byte aligned");
-    k_ht_pack<<<grid_for(ts, 256, 8), 256, 0, as_stream(stream)>>>(ts, keys, vals, static_cast<int4 *>(packed));
-    PIRO_CHECK_LAUNCH("k_ht_pack");
-    return PIRO_OK;
-}
-
-extern "C" int piro_ht_spmv_packed(int nx, int ny, int nz, const void *packed, int64_t ts, float dt, int fe,
-                                   const int32_t *order, void *stage, size_t stage_bytes, const float *u, float *out,
-                                   piro_stream_t stream)
-{
-    PIRO_ARG(grid_ok(nx, ny, nz) && packed && ts > 0 && order && stage && u && out && u != out &&
-                 ((uintptr_t)packed & 15) == 0,
-             "piro_ht_spmv_packed: bad arguments");
-    const int64_t N = (int64_t)nx * ny * nz;
-    PIRO_ARG(N < INT32_MAX, "piro_ht_spmv_packed: more than 2^31 - 1 rows");
-    PIRO_ARG(stage_bytes >= 32 * (size_t)N && ((uintptr_t)stage & 15) == 0,
-             "piro_ht_spmv_packed: stage smaller than 32 bytes per row or not 16-byte aligned");
-    cudaStream_t s = as_stream(stream);
-    float4 *st = static_cast<float4 *>(stage);
-    const GridDiv g(nx, ny, nz);
-    k_ht_stage<HtPacked><<<grid_for(N, 256, 8), 256, 0, s>>>(g, N, HtPacked{static_cast<const int4 *>(packed)}, ts,
-                                                             ModU64((uint64_t)ts), order, st);
+    k_ht_stage<<<grid_for(N, 256, 8), 256, 0, s>>>(g, N, keys, vals, ts, ModU64((uint64_t)ts), order, st);
     PIRO_CHECK_LAUNCH("k_ht_stage");
     k_ht_stage_apply<<<grid_for(N, 256, 8), 256, 0, s>>>(g, dt, fe, st, u, out);
     PIRO_CHECK_LAUNCH("k_ht_stage_apply");

@@ -247,21 +247,6 @@ def ht_stage(N):
     return torch.empty(n.value // 4, dtype=torch.float32, device="cuda")
 
 
-def ht_pack(keys, vals):
-    """The table as 16-byte slots for ht_spmv_packed (once per table)."""
-    ts = keys.numel()
-    packed = torch.empty(4 * ts, dtype=i32, device="cuda")
-    check(lib().piro_ht_pack(_p(keys), _p(vals), ts, _p(packed), 16 * ts, _stream()), "piro_ht_pack")
-    return packed
-
-
-def ht_spmv_packed(nx, ny, nz, packed, dt, order, stage, u, out, fe=False):
-    check(lib().piro_ht_spmv_packed(nx, ny, nz, _p(packed), packed.numel() // 4, float(dt), int(fe), _p(order),
-                                    _p(stage), stage.numel() * stage.element_size(), _p(u), _p(out), _stream()),
-          "piro_ht_spmv_packed")
-    return out
-
-
 def ht_spmv_staged(nx, ny, nz, keys, vals, dt, order, stage, u, out, fe=False):
     check(lib().piro_ht_spmv_staged(nx, ny, nz, _p(keys), _p(vals), keys.numel(), float(dt), int(fe), _p(order),
                                     _p(stage), stage.numel() * stage.element_size(), _p(u), _p(out), _stream()),

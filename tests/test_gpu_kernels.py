@@ -121,9 +121,6 @@ def test_step_kernels_vs_golden(cuda, golden_grids):
             out2.fill_(float("nan"))
             ops.ht_spmv_staged(nx, ny, nz, keys, hv, 0.01, order, ops.ht_stage(N), u, out2)
             assert f32_bits_equal(h(out2), g[f"spmvht_{t}"])
-            out2.fill_(float("nan"))
-            ops.ht_spmv_packed(nx, ny, nz, ops.ht_pack(keys, hv), 0.01, order, ops.ht_stage(N), u, out2)
-            assert f32_bits_equal(h(out2), g[f"spmvht_{t}"])
             val = A[2].clone()
             ops.csr_rowscale(A[0], val, dev(torch, g[f"in_alpha_{t}"]))
             assert f32_bits_equal(h(val), g[f"spmdsm_{t}"])
@@ -348,13 +345,6 @@ def test_fe_steps_match_oracle(cuda, oracle, n):
     u = dev(torch, u0)
     for _ in range(3):
         ops.ht_spmv_staged(nx, ny, nz, keys, vals, dt, order, stage, u, out, fe=True)
-        ops.set_bc(idx, bc, out)
-        u, out = out, u
-    assert f32_bits_equal(h(u), ref_ht)
-    packed = ops.ht_pack(keys, vals)
-    u = dev(torch, u0)
-    for _ in range(3):
-        ops.ht_spmv_packed(nx, ny, nz, packed, dt, order, stage, u, out, fe=True)
         ops.set_bc(idx, bc, out)
         u, out = out, u
     assert f32_bits_equal(h(u), ref_ht)
