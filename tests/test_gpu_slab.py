@@ -111,14 +111,16 @@ def test_slab_advection_bitexact(cuda, world, scheme):
     assert np.array_equal(got[inter], ref[inter])
 
 
-@pytest.mark.parametrize("world,device_scalars", [(2, False), (3, False), (2, True), (3, True)])
-def test_slab_be_matches_single_grid(cuda, world, device_scalars):
+@pytest.mark.parametrize("world,device_scalars,n", [(2, False, 34), (3, False, 34), (2, True, 34), (3, True, 34),
+                                                    (2, True, 36), (3, False, 36)])
+def test_slab_be_matches_single_grid(cuda, world, device_scalars, n):
     """device_scalars: the CG scalars formed on the device from all-reduced
     sums (piro_slab_*_dev), the host looking at the done flag every 8
-    iterations."""
+    iterations.  n = 36 (nx % 4 == 0) takes the operator kernel's 16-byte
+    path, n = 34 its per-cell path; the update takes its 16-byte path in
+    both (nx * ny % 4 == 0)."""
     import torch
     from piro_b200 import learned, ops, slab
-    n = 34
     N, plane = n ** 3, n * n
     alpha, dt, b = learned.be_family(n, 204)
     a_t = torch.from_numpy(alpha).cuda()
