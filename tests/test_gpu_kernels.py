@@ -445,3 +445,38 @@ def test_fused_fe_step_with_bc(cuda, n):
     got.fill_(float("nan"))
     ops.csr_fe_step_bc(nx, ny, nz, A, 0.013, u, None, got)  # no [BC]: faces stay 0
     assert f32_bits_equal(h(got), h(ref))
+
+
+@pytest.mark.parametrize("n,load", [((40, 36, 30), 0.97), ((33, 17, 9), 0.5), ((3, 7, 64), 0.9)])
+def test_ht_ordered_and_staged_steps_on_crowded_tables(cuda, oracle, n, load):
+    """On tables with long probe runs (97% full), with deleted keys (-2, which
+    a lookup walks past) and with odd sizes, the home-slot-ordered and the
+    two-pass HT steps equal the row-major probing step bit for bit."""
+    import torch
+    from piro_b200 import ops
+    nx, ny, nz = n
+    N = nx * ny * nz
+    rng = np.random.default_rng(11)
+    A = ops.csr_laplacian(nx, ny, nz, 1, 1.0)
+    nnz = int(A[2].numel())
+    ts = int(nnz / load) | 1
+    keys, vals = ops.ht_build(N, *A, ts)
+    vals.copy_(torch.from_numpy(rng.standard_normal(ts).astype(np.float32)).cuda())
+    order = ops.ht_row_order(N, ts)
+    stage = ops.ht_stage(N)
+    u = dev(torch, rng.random(N, dtype=np.float32))
+    want = torch.empty_like(u)
+    got = torch.empty_like(u)
+    for trial in range(2):
+        if trial == 1:  # delete a tenth of the keys: every reader sees them as absent
+            kh = h(keys)
+            live = np.flatnonzero(kh >= 0)
+            kh[rng.choice(live, size=len(live) // 10, replace=False)] = -2
+            keys.copy_(torch.from_numpy(kh).cuda())
+        ops.ht_spmv(nx, ny, nz, keys, vals, 0.37, u, want, fe=True)
+        got.fill_(float("nan"))
+        ops.ht_spmv_ordered(nx, ny, nz, keys, vals, 0.37, order, u, got, fe=True)
+        assert f32_bits_equal(h(got), h(want)), trial
+        got.fill_(float("nan"))
+        ops.ht_spmv_staged(nx, ny, nz, keys, vals, 0.37, order, stage, u, got, fe=True)
+        assert f32_bits_equal(h(got), h(want)), trial
