@@ -774,19 +774,29 @@ struct Own {
     __device__ __forceinline__ int64_t g(int64_t v) const { return kRes ? v - (c0 >> 2) : v; }
 };
 
+// 1/a by PTX rcp.approx (max error about 1 ulp): for the weights 1/alpha of
+// the CG dot products, which need no correct rounding.
+__device__ __forceinline__ float rcp_approx(float a)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+
 // Phase A on groups of 4 x-adjacent cells (nx % 4 == 0: a group never spans
 // two x-lines, and every row offset keeps 16-byte alignment).  Per group:
 // 11 float4 loads + 4 scalar halo loads instead of 60 scalar loads.
-template <bool kRes>
+// kFlex (flexible CG): also <p, r/alpha> into pr, r read where the block keeps it.
+template <bool kRes, bool kFlex = false>
 __device__ __forceinline__ double cg_phase_a_vec(const PArgs &P, const Own<kRes> &O, const float *pold, float *pnew,
-                                                 float fb, int64_t v0, int64_t v1, int64_t dv)
+                                                 float fb, int64_t v0, int64_t v1, int64_t dv, double *pr = nullptr)
 {
     const GridDiv &g = P.g;
     const int64_t rx = g.nx >> 2, rxy = ((int64_t)g.nx * g.ny) >> 2;
     const float4 *Z = reinterpret_cast<const float4 *>(P.z);
     const float4 *Po = reinterpret_cast<const float4 *>(pold);
     const float4 *Al = reinterpret_cast<const float4 *>(P.alpha);
-    double pq = 0.0;
+    double pq = 0.0, prs = 0.0;
     for (int64_t v = v0; v < v1; v += dv) {
         const int64_t i = v << 2;
         int x0, y, z;
@@ -805,7 +815,12 @@ __device__ __forceinline__ double cg_phase_a_vec(const PArgs &P, const Own<kRes>
         const float zm[4] = {zzm.x + fb * pzm.x, zzm.y + fb * pzm.y, zzm.z + fb * pzm.z, zzm.w + fb * pzm.w};
         const float zp[4] = {zzp.x + fb * pzp.x, zzp.y + fb * pzp.y, zzp.z + fb * pzp.z, zzp.w + fb * pzp.w};
         const float a[4] = {al.x, al.y, al.z, al.w};
-        float pn[4], qv[4];
+        float pn[4], qv[4], rv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (kFlex) {
+            const float4 r4 = reinterpret_cast<const float4 *>(O.r)[O.g(v)];
+            rv[0] = r4.x; rv[1] = r4.y; rv[2] = r4.z; rv[3] = r4.w;
+        }
+        float pqf = 0.0f, prf = 0.0f;  // the group's dot terms in FP32 (CG scalars only), added in FP64
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int x = x0 + k;
@@ -814,45 +829,74 @@ __device__ __forceinline__ double cg_phase_a_vec(const PArgs &P, const Own<kRes>
                 const float co = __fmul_rn(P.mdt, __fmul_rn(a[k], P.vnb));
                 pn[k] = c[k + 1];
                 qv[k] = cd * c[k + 1] + co * (((c[k] + c[k + 2]) + (ym[k] + yp[k])) + (zm[k] + zp[k]));
-                pq += (double)pn[k] * (double)qv[k] / (double)a[k];
+                const float ia = rcp_approx(a[k]);
+                pqf += pn[k] * qv[k] * ia;
+                if (kFlex) prf += pn[k] * rv[k] * ia;
             } else {
                 pn[k] = 0.0f;
                 qv[k] = 0.0f;
             }
         }
+        pq += (double)pqf;
+        if (kFlex) prs += (double)prf;
         reinterpret_cast<float4 *>(pnew)[v] = make_float4(pn[0], pn[1], pn[2], pn[3]);
         reinterpret_cast<float4 *>(O.q)[O.g(v)] = make_float4(qv[0], qv[1], qv[2], qv[3]);
     }
+    if (kFlex) *pr = prs;
     return pq;
 }
 
 // Phase B on float4 groups (N % 4 == 0).  Boundary lanes carry p = q = r = 0
 // and dinv = 0, so the update leaves them at zero without a branch; only the
-// dot products are masked.
-template <bool kRes>
+// dot products are masked.  The dot products' terms are formed in FP32 (they
+// only steer CG; the FP64 residual decides convergence) and added in FP64,
+// 1/alpha by the approximate reciprocal: against FP64 products divided by
+// alpha in FP64, 0.784 -> 0.717 ms per 128^3 step on B200 (0.688 ms with
+// rcp.approx instead of the correctly rounded reciprocal), the same
+// iteration count.  Two groups per iteration with all their loads first
+// spilled registers and was slower (0.83 ms).
+struct PhaseBGroup {
+    float4 di, al, pp;  // the global loads; q, d, r are read when the group is finished
+};
+
+// kFlex (flexible CG): rzn takes <z, q/alpha> (the next direction's beta) instead of <r/alpha, z>.
+template <bool kRes, bool kFlex = false>
 __device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const Own<kRes> &O, const float *pnew, float fa,
                                                int64_t v0, int64_t v1, int64_t dv, double &rzn, double &rr)
 {
     float4 *D = reinterpret_cast<float4 *>(O.d), *R = reinterpret_cast<float4 *>(O.r);
     const float4 *Q = reinterpret_cast<const float4 *>(O.q);
-    for (int64_t v = v0; v < v1; v += dv) {
+    const float4 *Di = reinterpret_cast<const float4 *>(P.dinv), *Al = reinterpret_cast<const float4 *>(P.alpha);
+    const float4 *Pn = reinterpret_cast<const float4 *>(pnew);
+    auto load = [&](int64_t v, PhaseBGroup &G) {
         const int64_t o = O.g(v);
-        const float4 di = __ldg(reinterpret_cast<const float4 *>(P.dinv) + v);
-        const float4 al = __ldg(reinterpret_cast<const float4 *>(P.alpha) + v);
-        const float4 pp = ld_(reinterpret_cast<const float4 *>(pnew) + v);
+        G.di = __ldg(Di + v);
+        G.al = __ldg(Al + v);
+        G.pp = ld_(Pn + v);
+    };
+    auto finish = [&](int64_t v, const PhaseBGroup &G) {
+        const int64_t o = O.g(v);
         const float4 qq = Q[o];
-        float4 dd = D[o];
-        float4 r4 = R[o];
-        dd.x += fa * pp.x; dd.y += fa * pp.y; dd.z += fa * pp.z; dd.w += fa * pp.w;
+        float4 dd = D[o], r4 = R[o];
+        dd.x += fa * G.pp.x; dd.y += fa * G.pp.y; dd.z += fa * G.pp.z; dd.w += fa * G.pp.w;
         r4.x -= fa * qq.x; r4.y -= fa * qq.y; r4.z -= fa * qq.z; r4.w -= fa * qq.w;
-        const float4 z4 = make_float4(r4.x * di.x, r4.y * di.y, r4.z * di.z, r4.w * di.w);
+        const float4 z4 = make_float4(r4.x * G.di.x, r4.y * G.di.y, r4.z * G.di.z, r4.w * G.di.w);
         D[o] = dd;
         R[o] = r4;
         reinterpret_cast<float4 *>(P.z)[v] = z4;
-        if (di.x != 0.0f) { rzn += (double)r4.x / (double)al.x * (double)z4.x; rr += (double)r4.x * (double)r4.x; }
-        if (di.y != 0.0f) { rzn += (double)r4.y / (double)al.y * (double)z4.y; rr += (double)r4.y * (double)r4.y; }
-        if (di.z != 0.0f) { rzn += (double)r4.z / (double)al.z * (double)z4.z; rr += (double)r4.z * (double)r4.z; }
-        if (di.w != 0.0f) { rzn += (double)r4.w / (double)al.w * (double)z4.w; rr += (double)r4.w * (double)r4.w; }
+        const float4 w = kFlex ? qq : r4;  // <w/alpha, z>
+        float rz = 0.0f, r2 = 0.0f;
+        if (G.di.x != 0.0f) { rz += w.x * z4.x * rcp_approx(G.al.x); r2 += r4.x * r4.x; }
+        if (G.di.y != 0.0f) { rz += w.y * z4.y * rcp_approx(G.al.y); r2 += r4.y * r4.y; }
+        if (G.di.z != 0.0f) { rz += w.z * z4.z * rcp_approx(G.al.z); r2 += r4.z * r4.z; }
+        if (G.di.w != 0.0f) { rz += w.w * z4.w * rcp_approx(G.al.w); r2 += r4.w * r4.w; }
+        rzn += (double)rz;
+        rr += (double)r2;
+    };
+    for (int64_t v = v0; v < v1; v += dv) {
+        PhaseBGroup G0;
+        load(v, G0);
+        finish(v, G0);
     }
 }
 
@@ -1066,31 +1110,55 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
 //   z = D^-1 r, beta = -<z, S p_old> / <p_old, S p_old> (0 on a sweep's first
 //   iteration); A: p = z + beta p_old, q = A p, <p, S p>, <p, s>; a =
 //   <p, s> / <p, S p>; B: d += a p, r -= a q, z = D^-1 r, |r|^2, <z, S p>.
-// Global arrays only (the state lives in them between launches); barrier
-// waits bounded like k_be_persistent's.
-struct FArgs {
-    GridDiv g;
-    int64_t N;
-    float mdt, vself, vnb;
-    const float *alpha, *dinv;
-    float *r, *z, *q, *d, *p0, *p1;
-    double *partials;
-    DevState *st;
-    long long spin_limit;
-};
-
-__global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(FArgs F)
+// The state lives in the global arrays between launches.  As in
+// k_be_persistent, the phases run on float4 groups where the grid allows
+// (P.vec_a / P.vec_b), and the resident variant (kRes) keeps the block's own
+// r, d, q in shared memory for the launch, read from and written back to the
+// global arrays at its start and end.  Barrier waits bounded like
+// k_be_persistent's.
+template <bool kRes>
+__global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(PArgs P)
 {
     __shared__ double s_warp[32];
     __shared__ double s_red[4 * 32];
     __shared__ double s_b;
     __shared__ double s_bn[4];
     __shared__ int s_ok;
-    const GridDiv g = F.g;
-    const int64_t N = F.N, sxy = (int64_t)g.nx * g.ny;
-    const int64_t c_beg = (int64_t)blockIdx.x * kPT + threadIdx.x, c_step = (int64_t)gridDim.x * kPT;
-    DevState *st = F.st;
+    extern __shared__ float4 s_own[];
+    const GridDiv g = P.g;
+    const int64_t N = P.N, sxy = (int64_t)g.nx * g.ny;
+    DevState *st = P.st;
     if (*((volatile int *)&st->done)) return;  // the same in every block: written before this launch
+    int64_t c_beg, c_end, c_step, v_beg, v_end;
+    Own<kRes> O;
+    if (kRes) {
+        const int64_t c0 = (int64_t)blockIdx.x * P.own_cells, c1 = c0 + P.own_cells < N ? c0 + P.own_cells : N;
+        const int64_t G = P.own_cells >> 2;
+        c_beg = c0 + threadIdx.x;
+        c_end = c1;
+        c_step = kPT;
+        v_beg = (c0 >> 2) + threadIdx.x;
+        v_end = c1 >> 2;
+        O.r = reinterpret_cast<float *>(s_own);
+        O.d = reinterpret_cast<float *>(s_own + G);
+        O.q = reinterpret_cast<float *>(s_own + 2 * G);
+        O.c0 = c0;
+        for (int64_t i = c_beg; i < c_end; i += c_step) {
+            O.r[O.c(i)] = P.r[i];
+            O.d[O.c(i)] = P.d[i];
+            O.q[O.c(i)] = P.q[i];
+        }
+    } else {
+        c_beg = (int64_t)blockIdx.x * kPT + threadIdx.x;
+        c_end = N;
+        c_step = (int64_t)gridDim.x * kPT;
+        v_beg = c_beg;
+        v_end = N >> 2;
+        O.r = P.r;
+        O.d = P.d;
+        O.q = P.q;
+        O.c0 = 0;
+    }
     const int max_iters = st->max_iters;
     const double tol2 = st->tol2, rr0 = st->rr0;
     double t_pq = st->pq, t_rr = st->rr;
@@ -1101,54 +1169,58 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(FArgs F)
         g.coords((uint32_t)i, x, y, zc);
         return x > 0 && x < g.nx - 1 && y > 0 && y < g.ny - 1 && zc > 0 && zc < g.nz - 1;
     };
-    // z = D^-1 r and <z, S p_old> with S p_old = q / alpha
+    // z = D^-1 r and <z, S p_old> with S p_old = q / alpha (each thread its own cells, as copied above)
     double zq = 0.0;
-    for (int64_t i = c_beg; i < N; i += c_step) {
-        const float dv = __ldg(F.dinv + i);
-        const float zi = F.r[i] * dv;  // dinv = 0 on the boundary: z = 0 there
-        F.z[i] = zi;
-        if (dv != 0.0f) zq += (double)zi * (double)F.q[i] / (double)__ldg(F.alpha + i);
+    for (int64_t i = c_beg; i < c_end; i += c_step) {
+        const float dv = __ldg(P.dinv + i);
+        const float zi = O.r[O.c(i)] * dv;  // dinv = 0 on the boundary: z = 0 there
+        P.z[i] = zi;
+        if (dv != 0.0f) zq += (double)zi * (double)O.q[O.c(i)] / (double)__ldg(P.alpha + i);
     }
-    put_partial(F.partials, 0, zq, s_warp);
-    bool ok = grid_barrier(st, bar_target, F.spin_limit, &s_ok);
+    put_partial(P.partials, 0, zq, s_warp);
+    bool ok = grid_barrier(st, bar_target, P.spin_limit, &s_ok);
     double beta = 0.0, a = 0.0;
     bool broken = false;
     if (ok) {
-        const double t_zq = all_sum(F.partials, 0, s_warp, &s_b);
+        const double t_zq = all_sum(P.partials, 0, s_warp, &s_b);
         beta = iters == 0 ? 0.0 : -t_zq / t_pq;
         broken = !isfinite(beta);
     }
-    float *pold = F.p0, *pnew = F.p1;
+    float *pold = P.p0, *pnew = P.p1;
     while (ok && !broken) {
         // A: p = z + beta p_old, q = A p, <p, S p>, <p, s>
         const float fb = (float)beta;
         double pv[2] = {0.0, 0.0};
-        for (int64_t i = c_beg; i < N; i += c_step) {
-            if (!inter(i)) {
-                pnew[i] = 0.0f;
-                F.q[i] = 0.0f;
-                continue;
+        if (P.vec_a) {
+            pv[0] = cg_phase_a_vec<kRes, true>(P, O, pold, pnew, fb, v_beg, v_end, c_step, &pv[1]);
+        } else {
+            for (int64_t i = c_beg; i < c_end; i += c_step) {
+                if (!inter(i)) {
+                    pnew[i] = 0.0f;
+                    O.q[O.c(i)] = 0.0f;
+                    continue;
+                }
+                const float al = __ldg(P.alpha + i);
+                const float cur = ld_(P.z + i) + fb * ld_(pold + i);
+                const float xm = ld_(P.z + i - 1) + fb * ld_(pold + i - 1);
+                const float xp = ld_(P.z + i + 1) + fb * ld_(pold + i + 1);
+                const float ym = ld_(P.z + i - g.nx) + fb * ld_(pold + i - g.nx);
+                const float yp = ld_(P.z + i + g.nx) + fb * ld_(pold + i + g.nx);
+                const float zm = ld_(P.z + i - sxy) + fb * ld_(pold + i - sxy);
+                const float zp = ld_(P.z + i + sxy) + fb * ld_(pold + i + sxy);
+                const float cd = __fadd_rn(1.0f, __fmul_rn(P.mdt, __fmul_rn(al, P.vself)));
+                const float co = __fmul_rn(P.mdt, __fmul_rn(al, P.vnb));
+                const float qv = cd * cur + co * (((xm + xp) + (ym + yp)) + (zm + zp));
+                pnew[i] = cur;
+                O.q[O.c(i)] = qv;
+                pv[0] += (double)cur * (double)qv / (double)al;
+                pv[1] += (double)cur * (double)O.r[O.c(i)] / (double)al;
             }
-            const float al = __ldg(F.alpha + i);
-            const float cur = ld_(F.z + i) + fb * ld_(pold + i);
-            const float xm = ld_(F.z + i - 1) + fb * ld_(pold + i - 1);
-            const float xp = ld_(F.z + i + 1) + fb * ld_(pold + i + 1);
-            const float ym = ld_(F.z + i - g.nx) + fb * ld_(pold + i - g.nx);
-            const float yp = ld_(F.z + i + g.nx) + fb * ld_(pold + i + g.nx);
-            const float zm = ld_(F.z + i - sxy) + fb * ld_(pold + i - sxy);
-            const float zp = ld_(F.z + i + sxy) + fb * ld_(pold + i + sxy);
-            const float cd = __fadd_rn(1.0f, __fmul_rn(F.mdt, __fmul_rn(al, F.vself)));
-            const float co = __fmul_rn(F.mdt, __fmul_rn(al, F.vnb));
-            const float qv = cd * cur + co * (((xm + xp) + (ym + yp)) + (zm + zp));
-            pnew[i] = cur;
-            F.q[i] = qv;
-            pv[0] += (double)cur * (double)qv / (double)al;
-            pv[1] += (double)cur * (double)F.r[i] / (double)al;
         }
-        put_partials<2>(F.partials, 1, pv, s_red);
-        if (!(ok = grid_barrier(st, bar_target, F.spin_limit, &s_ok))) break;
+        put_partials<2>(P.partials, 1, pv, s_red);
+        if (!(ok = grid_barrier(st, bar_target, P.spin_limit, &s_ok))) break;
         double at[2];
-        all_sums<2>(F.partials, 1, at, s_red, s_bn);
+        all_sums<2>(P.partials, 1, at, s_red, s_bn);
         t_pq = at[0];
         a = at[1] / at[0];
         if (!isfinite(a) || at[0] <= 0.0) {
@@ -1158,22 +1230,26 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(FArgs F)
         // B: d += a p, r -= a q, z = D^-1 r, |r|^2, <z, S p>
         const float fa = (float)a;
         double bv[2] = {0.0, 0.0};
-        for (int64_t i = c_beg; i < N; i += c_step) {
-            const float dv = __ldg(F.dinv + i);
-            if (dv == 0.0f) continue;
-            const float qi = F.q[i];
-            F.d[i] += fa * pnew[i];
-            const float ri = F.r[i] - fa * qi;
-            const float zi = ri * dv;
-            F.r[i] = ri;
-            F.z[i] = zi;
-            bv[0] += (double)ri * (double)ri;
-            bv[1] += (double)zi * (double)qi / (double)__ldg(F.alpha + i);
+        if (P.vec_b) {
+            cg_phase_b_vec<kRes, true>(P, O, pnew, fa, v_beg, v_end, c_step, bv[1], bv[0]);
+        } else {
+            for (int64_t i = c_beg; i < c_end; i += c_step) {
+                const float dv = __ldg(P.dinv + i);
+                if (dv == 0.0f) continue;
+                const float qi = O.q[O.c(i)];
+                O.d[O.c(i)] += fa * pnew[i];
+                const float ri = O.r[O.c(i)] - fa * qi;
+                const float zi = ri * dv;
+                O.r[O.c(i)] = ri;
+                P.z[i] = zi;
+                bv[0] += (double)ri * (double)ri;
+                bv[1] += (double)zi * (double)qi / (double)__ldg(P.alpha + i);
+            }
         }
-        put_partials<2>(F.partials, 3, bv, s_red);
-        if (!(ok = grid_barrier(st, bar_target, F.spin_limit, &s_ok))) break;
+        put_partials<2>(P.partials, 3, bv, s_red);
+        if (!(ok = grid_barrier(st, bar_target, P.spin_limit, &s_ok))) break;
         double btot[2];
-        all_sums<2>(F.partials, 3, btot, s_red, s_bn);
+        all_sums<2>(P.partials, 3, btot, s_red, s_bn);
         t_rr = btot[0];
         beta = -btot[1] / t_pq;
         ++iters;
@@ -1185,6 +1261,14 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(FArgs F)
             break;
         }
         if (t_rr <= tol2 * rr0 || iters >= max_iters) break;
+    }
+    if (kRes) {  // the sweep's state back to the global arrays (d for the x update)
+        __syncthreads();
+        for (int64_t i = c_beg; i < c_end; i += c_step) {
+            P.r[i] = O.r[O.c(i)];
+            P.d[i] = O.d[O.c(i)];
+            P.q[i] = O.q[O.c(i)];
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         st->iters = iters;
@@ -1297,6 +1381,7 @@ struct piro_be_solver {
     float *ib_val;
     double *beff;
     unsigned grid_fp;   // k_fcg_persistent: co-resident blocks (0: use the graph-launched chunks)
+    int fcg_res;        // k_fcg_persistent<true> fits at grid_p blocks with res_smem
     int64_t res_cells;  // resident variant: cells per block, 0 if it does not fit
     size_t res_smem;
     cudaEvent_t pev0, pev1;
@@ -1499,9 +1584,10 @@ static int be_setup_persistent(piro_be_solver *s, bool allow_resident)
     s->grid_p = (unsigned)grid;
     s->persist = 1;
     int per_sm_f = 0;
-    PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_fcg_persistent, kPT, 0));
+    PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_fcg_persistent<false>, kPT, 0));
     const int64_t fgrid = (int64_t)nsm * per_sm_f;
     s->grid_fp = (unsigned)(fgrid < grid ? fgrid : grid);
+    s->fcg_res = 0;
     // resident variant: every block's r, d, q in shared memory, if they fit
     // with the same grid still co-resident
     s->res_cells = 0;
@@ -1513,6 +1599,8 @@ static int be_setup_persistent(piro_be_solver *s, bool allow_resident)
         int rc2 = device_once(once, dev, []() -> int {
             PIRO_CUDA(cudaFuncSetAttribute(k_be_persistent<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            kResSmemMax));
+            PIRO_CUDA(cudaFuncSetAttribute(k_fcg_persistent<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kResSmemMax));
             return PIRO_OK;
         });
         if (rc2) return rc2;
@@ -1521,6 +1609,9 @@ static int be_setup_persistent(piro_be_solver *s, bool allow_resident)
         if ((int64_t)per_sm_res * nsm >= grid) {
             s->res_cells = 4 * groups;
             s->res_smem = smem;
+            int per_sm_fres = 0;
+            PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_fres, k_fcg_persistent<true>, kPT, smem));
+            s->fcg_res = (int64_t)per_sm_fres * nsm >= grid ? 1 : 0;
         }
     }
     return PIRO_OK;
@@ -1866,7 +1957,7 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
             net_iters = false;
             if (learned && !with_net && s->persist && s->grid_fp > 0) {
                 // the rest of the sweep: Jacobi flexible CG in one cooperative launch
-                FArgs F;
+                PArgs F{};
                 F.g = GridDiv(s->nx, s->ny, s->nz);
                 F.N = N;
                 F.mdt = s->mdt;
@@ -1883,10 +1974,22 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
                 F.partials = s->partials;
                 F.st = s->st;
                 F.spin_limit = wait_limit(1ll << 22);
+                const uintptr_t al = reinterpret_cast<uintptr_t>(s->alpha) | reinterpret_cast<uintptr_t>(s->dinv) |
+                                     reinterpret_cast<uintptr_t>(s->r) | reinterpret_cast<uintptr_t>(s->z) |
+                                     reinterpret_cast<uintptr_t>(s->q) | reinterpret_cast<uintptr_t>(s->d) |
+                                     reinterpret_cast<uintptr_t>(s->p[0]) | reinterpret_cast<uintptr_t>(s->p[1]);
+                F.vec_b = (N % 4 == 0) && (al & 15) == 0;
+                F.vec_a = F.vec_b && (s->nx % 4 == 0);
+                const bool res = s->fcg_res && s->res_cells > 0 && F.vec_a;
+                F.own_cells = res ? s->res_cells : 0;
                 void *fargs[] = {&F};
                 PIRO_CUDA(cudaMemsetAsync(&s->st->bar_count, 0, 2 * sizeof(unsigned) + sizeof(int), st));
-                PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_fcg_persistent, dim3(s->grid_fp), dim3(kPT),
-                                                      fargs, 0, st));
+                if (res)
+                    PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_fcg_persistent<true>, dim3(s->grid_p),
+                                                          dim3(kPT), fargs, s->res_smem, st));
+                else
+                    PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_fcg_persistent<false>, dim3(s->grid_fp),
+                                                          dim3(kPT), fargs, 0, st));
                 s->kernel_launches += 1;
                 PIRO_CUDA(cudaMemcpyAsync(s->h_st, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, st));
                 PIRO_CUDA(cudaStreamSynchronize(st));
