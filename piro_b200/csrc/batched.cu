@@ -30,7 +30,8 @@
 //   S2   one warp per member: next beta, inner stop test, the count of
 //        members still active.
 // All sums are per-tile block reductions plus an in-order per-member sum, so
-// results do not depend on scheduling.  The grid barrier's waits are bounded:
+// results do not depend on scheduling.  The CG sums' terms are FP32 products
+// (they only steer CG) added in FP64; the residual norms are FP64 throughout.  The grid barrier's waits are bounded:
 // on timeout an error flag is raised and every block leaves.
 #include <algorithm>
 #include <cmath>
@@ -275,11 +276,12 @@ __global__ void __launch_bounds__(kThreads) k_batch_step(BArgs A)
                         c2 = pv(i2);
                         nb2 = ((pv(i2 - 1) + pv(i2 + 1)) + (pv(i2 - nx) + pv(i2 + nx))) + (pv(i2 - sxy) + pv(i2 + sxy));
                     }
+                    float pq = 0.0f;  // the two cells' <p, q> terms in FP32, added in FP64
                     if (in1) {
                         const float qv = m.cd * c1 + m.co * nb1;
                         pn[i] = c1;
                         qq[i] = qv;
-                        v0 += (double)c1 * (double)qv;
+                        pq = c1 * qv;
                     } else {
                         pn[i] = 0.0f;
                         qq[i] = 0.0f;
@@ -289,12 +291,13 @@ __global__ void __launch_bounds__(kThreads) k_batch_step(BArgs A)
                             const float qv = m.cd * c2 + m.co * nb2;
                             pn[i2] = c2;
                             qq[i2] = qv;
-                            v0 += (double)c2 * (double)qv;
+                            pq += c2 * qv;
                         } else {
                             pn[i2] = 0.0f;
                             qq[i2] = 0.0f;
                         }
                     }
+                    v0 += (double)pq;
                 }
             } else {
                 continue;
@@ -402,10 +405,9 @@ __global__ void __launch_bounds__(kThreads) k_batch_step(BArgs A)
                 auto upd = [&](float4 &d4, float4 &r4, const float4 p4, const float4 q4) {
                     d4.x += a * p4.x; d4.y += a * p4.y; d4.z += a * p4.z; d4.w += a * p4.w;
                     r4.x = r4.x - a * q4.x; r4.y = r4.y - a * q4.y; r4.z = r4.z - a * q4.z; r4.w = r4.w - a * q4.w;
-                    v0 += (double)r4.x * (double)(r4.x * m.dinv) + (double)r4.y * (double)(r4.y * m.dinv) +
-                          (double)r4.z * (double)(r4.z * m.dinv) + (double)r4.w * (double)(r4.w * m.dinv);
-                    v1 += (double)r4.x * (double)r4.x + (double)r4.y * (double)r4.y + (double)r4.z * (double)r4.z +
-                          (double)r4.w * (double)r4.w;
+                    const float r2 = ((r4.x * r4.x + r4.y * r4.y) + (r4.z * r4.z + r4.w * r4.w));
+                    v0 += (double)(r2 * m.dinv);  // <r, z> with z = r dinv (dinv uniform per member)
+                    v1 += (double)r2;
                 };
                 for (int64_t gi = g0 + threadIdx.x; gi < g1; gi += 2 * blockDim.x) {
                     const int64_t gj = gi + blockDim.x;
@@ -728,7 +730,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_batch_groups(GArgs A)
                     const float qv = m.cd * c + m.co * nb;
                     pn[i] = c;
                     qq[i] = qv;
-                    w[0] += (double)c * (double)qv;
+                    w[0] += (double)(c * qv);
                 }
                 if (!(ok = group_sums<1>(A, part, 4, q, G, count, target, w, s_red, s_tot, &s_ok))) break;
                 const double a = s.rz / w[0];
@@ -757,10 +759,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_batch_groups(GArgs A)
                     r4.x = r4.x - fa * q4.x; r4.y = r4.y - fa * q4.y; r4.z = r4.z - fa * q4.z; r4.w = r4.w - fa * q4.w;
                     reinterpret_cast<float4 *>(dd)[gi] = d4;
                     reinterpret_cast<float4 *>(rr)[gi] = r4;
-                    u2[0] += (double)r4.x * (double)(r4.x * m.dinv) + (double)r4.y * (double)(r4.y * m.dinv) +
-                             (double)r4.z * (double)(r4.z * m.dinv) + (double)r4.w * (double)(r4.w * m.dinv);
-                    u2[1] += (double)r4.x * (double)r4.x + (double)r4.y * (double)r4.y + (double)r4.z * (double)r4.z +
-                             (double)r4.w * (double)r4.w;
+                    const float r2 = ((r4.x * r4.x + r4.y * r4.y) + (r4.z * r4.z + r4.w * r4.w));
+                    u2[0] += (double)(r2 * m.dinv);
+                    u2[1] += (double)r2;
                 }
                 for (int64_t i = (g1 << 2) + threadIdx.x; i < c1; i += blockDim.x) {
                     dd[i] += fa * pn[i];

@@ -774,15 +774,6 @@ struct Own {
     __device__ __forceinline__ int64_t g(int64_t v) const { return kRes ? v - (c0 >> 2) : v; }
 };
 
-// 1/a by PTX rcp.approx (max error about 1 ulp): for the weights 1/alpha of
-// the CG dot products, which need no correct rounding.
-__device__ __forceinline__ float rcp_approx(float a)
-{
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
-    return r;
-}
-
 // Phase A on groups of 4 x-adjacent cells (nx % 4 == 0: a group never spans
 // two x-lines, and every row offset keeps 16-byte alignment).  Per group:
 // 11 float4 loads + 4 scalar halo loads instead of 60 scalar loads.

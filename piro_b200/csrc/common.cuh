@@ -167,6 +167,15 @@ __device__ __forceinline__ bool interior(int64_t i, int nx, int ny, int nz)
     return x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1;
 }
 
+// 1/a by PTX rcp.approx (max error about 1 ulp): for the weights 1/alpha of
+// CG dot products, which need no correct rounding.
+__device__ __forceinline__ float rcp_approx(float a)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+
 __device__ __forceinline__ double warp_sum(double v)
 {
 #pragma unroll

@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(kSlabThreads, 4) k_slab_cg_spmv(Slab S, float 
                 float cd, co;
                 coef(S, al[k], cd, co);
                 qo[k] = cd * pc[k] + co * (((xm + xp) + (ym + yp)) + (zm + zp));
-                v[0] += (double)pc[k] * (double)qo[k] / (double)al[k];
+                v[0] += (double)(pc[k] * qo[k] * rcp_approx(al[k]));  // FP32 term, FP64 sum
             }
             reinterpret_cast<float4 *>(q)[g4] = make_float4(qo[0], qo[1], qo[2], qo[3]);
         }
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kSlabThreads, 4) k_slab_cg_spmv(Slab S, float 
                              (pv(l - nx, y > 1) + pv(l + nx, y < S.g.ny - 2))) +
                             (pv(l - sxy, zc > 1) + pv(l + sxy, zc < S.g.nz - 2)));
         q[l] = qv;
-        v[0] += (double)pc * (double)qv / (double)a;
+        v[0] += (double)(pc * qv * rcp_approx(a));
     }
     block_partials(part, 1, v);
 }
@@ -229,8 +229,8 @@ __global__ void __launch_bounds__(kSlabThreads) k_slab_cg_update(Slab S, float a
         dv += a * pv;
         rv = rv - a * qv;
         zv = rv / cd;
-        v[0] += (double)rv / (double)al * (double)zv;
-        v[1] += (double)rv * (double)rv;
+        v[0] += (double)(rv * zv * rcp_approx(al));
+        v[1] += (double)(rv * rv);
     };
     const bool vec = ((S.own0 | S.own1) & 3) == 0 &&
                      ((reinterpret_cast<uintptr_t>(alpha) | reinterpret_cast<uintptr_t>(p) |
