@@ -67,7 +67,9 @@ __device__ __forceinline__ bool is_bnd(int x, int y, int z, const Grid &g)
     return x == 0 || x == g.nx - 1 || y == 0 || y == g.ny - 1 || z == 0 || z == g.nz - 1;
 }
 
-// One row of the Laplacian: columns, values and count, in push order.
+// One row of the Laplacian: columns, values and count, in push order.  c and
+// v point into the block's shared-memory stage (a thread-local array with a
+// run-time count would live in local memory).
 __device__ __forceinline__ int lap_row(int64_t i, const Grid &g, int scheme, float vself, float vnb, int32_t *c,
                                        float *v)
 {
@@ -148,14 +150,10 @@ __global__ void __launch_bounds__(kRowsPerBlock) k_laplacian(Grid g, int64_t N, 
             int x, y, z;
             coords(i, g, x, y, z);
             const int64_t p = lap_prefix(x, y, z, g);
-            int32_t c[kMaxPerRow];
-            float v[kMaxPerRow];
-            const int n = lap_row(i, g, scheme, vself, vnb, c, v);
             const int off = (int)(p - s_base) + sh;
-            for (int t = 0; t < n; ++t) {
-                s_col[off + t] = (int32_t)(c[t] - col_shift);
-                s_val[off + t] = v[t];
-            }
+            const int n = lap_row(i, g, scheme, vself, vnb, s_col + off, s_val + off);
+            if (col_shift)
+                for (int t = 0; t < n; ++t) s_col[off + t] -= (int32_t)col_shift;
             if (rows)
                 for (int t = 0; t < n; ++t) s_row[off + t] = (int32_t)(i - col_shift);
             if (rowptr) {

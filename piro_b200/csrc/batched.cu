@@ -165,7 +165,10 @@ __device__ __forceinline__ float a_apply32(const BMember &m, const float *v, int
     return m.cd * v[i] + m.co * (((v[i - 1] + v[i + 1]) + (v[i - nx] + v[i + nx])) + (v[i - sxy] + v[i + sxy]));
 }
 
-__global__ void __launch_bounds__(kThreads) k_batch_step(BArgs A)
+// kMinBlocks: the blocks per SM the registers are capped for (4: 64
+// registers; 6 and 8 cap them at 40 and 32 for more warps per SM).
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_batch_step(BArgs A)
 {
     __shared__ double s_warp[32];
     __shared__ double s_red[4 * 32];
@@ -955,6 +958,14 @@ static void batch_free_tiles(piro_batch *s)
 }
 
 // Cut the members into tiles of `tile` cells and size the cooperative grid.
+// The k_batch_step instance for a launch of blocks_per_sm blocks per SM.
+static const void *batch_kernel(int blocks_per_sm)
+{
+    if (blocks_per_sm >= 8) return (const void *)k_batch_step<8>;
+    if (blocks_per_sm >= 6) return (const void *)k_batch_step<6>;
+    return (const void *)k_batch_step<4>;
+}
+
 static int batch_tiles(piro_batch *s, int tile, int blocks_per_sm)
 {
     batch_free_tiles(s);
@@ -1001,7 +1012,7 @@ static int batch_tiles(piro_batch *s, int tile, int blocks_per_sm)
     int dev = 0, per_sm = 0, coop = 0;
     PIRO_CUDA(cudaGetDevice(&dev));
     PIRO_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-    PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step, kThreads, 0));
+    PIRO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel(blocks_per_sm), kThreads, 0));
     if (!coop || per_sm < 1) {
         set_error("piro_batch: cooperative launch is not available");
         return PIRO_ERR_CUDA;
@@ -1181,7 +1192,7 @@ static int batch_launch(piro_batch *s, const float *u, float *out, cudaStream_t 
     void *args[] = {&A};
     // a launch whose barrier wait gave up leaves count, gen and err behind
     PIRO_CUDA(cudaMemsetAsync(s->bar, 0, sizeof(BarrierState), st));
-    PIRO_CUDA(cudaLaunchCooperativeKernel((const void *)k_batch_step, dim3(s->grid), dim3(kThreads), args, 0, st));
+    PIRO_CUDA(cudaLaunchCooperativeKernel(batch_kernel(s->blocks_per_sm), dim3(s->grid), dim3(kThreads), args, 0, st));
     return PIRO_OK;
 }
 
@@ -1277,7 +1288,7 @@ extern "C" int piro_batch_autotune(piro_batch *s, double rtol, int *tile_out, in
     s->rtol = rtol;
     s->grouped = 0;  // the lockstep candidates first
     const int tiles[] = {2048, 4096, 8192, 16384};
-    const int bps[] = {1, 2, 4};
+    const int bps[] = {1, 2, 4, 6, 8};
     double best = INFINITY;
     int bt = s->tile, bb = s->blocks_per_sm;
     for (int t : tiles)
