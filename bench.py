@@ -529,9 +529,9 @@ def learned_section(torch, ops, cfg, A, alpha, plain_ms, plain_iters, steps, tfl
         "apply_frac_of_bf16_peak": round(alg_flops / avg_apply / 1e9 / tflops_peak, 4),
         "kernel_launches_per_step": launches / steps,
         "held_out": dict(LP.summary(held), seeds=[held_seeds[0], held_seeds[-1]]),
-        "note": "network applies on the tensor cores (tcgen05, 4 layers); the network preconditions the first 2 "
-                "flexible-CG iterations of each refinement sweep, Jacobi the rest; plain = Jacobi-PCG in the "
-                "persistent single-launch solver",
+        "note": "network applies on the tensor cores (tcgen05, 4 layers); the network preconditions the first "
+                "flexible-CG iteration of each refinement sweep, Jacobi the rest (in one persistent launch); "
+                "plain = Jacobi-PCG in the persistent single-launch solver",
     }
 
 

@@ -38,7 +38,11 @@ namespace {
 
 constexpr int kChunk = 8;       // CG iterations per graph launch (even: p buffers alternate)
 constexpr int kChunkF = 4;      // flexible-CG (Jacobi) iterations per graph launch (even)
-constexpr int kLearnedIters = 2;  // iterations per sweep preconditioned by the network (even)
+// Iterations per sweep preconditioned by the network.  Measured on the 128^3
+// configuration step (B200): one, 26.1 iterations in 1.30 ms; two, 19.9
+// iterations in 1.69 ms -- a network apply (0.43 ms) costs more than the
+// iterations a second one saves.
+constexpr int kLearnedIters = 1;
 constexpr int kRedCap = 4096;   // max blocks of a reducing kernel
 
 struct DevState {
@@ -1471,7 +1475,9 @@ static int be_capture_chunk(piro_be_solver *s)
 
 // Capture flexible-CG iterations: with the network (kLearnedIters of them,
 // events around each network apply give its live device time) or with the
-// Jacobi z (kChunkF).  Both start on p[0] and end on p[0].
+// Jacobi z (kChunkF, even).  The network iterations start on p[0] and leave
+// the last direction in p[kLearnedIters & 1], where the Jacobi chunks start
+// and end.
 static int be_capture_fcg(piro_be_solver *s, bool with_net)
 {
     const GridDiv g(s->nx, s->ny, s->nz);
@@ -1484,9 +1490,10 @@ static int be_capture_fcg(piro_be_solver *s, bool with_net)
         }
     PIRO_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     int rc = PIRO_OK;
+    const int par = with_net ? 0 : (kLearnedIters & 1);
     for (int it = 0; it < iters && rc == PIRO_OK; ++it) {
-        const float *p_old = s->p[it & 1];
-        float *p_new = s->p[(it + 1) & 1];
+        const float *p_old = s->p[(it + par) & 1];
+        float *p_new = s->p[(it + par + 1) & 1];
         if (with_net) {
             cudaEventRecordWithFlags(s->evf0[it], s->stream, cudaEventRecordExternal);
             rc = pcnet_apply(s->net, s->pc_work, g, s->N, s->r, s->feat, &s->st->rr, n_int, s->zt, &s->st->done,
@@ -1960,8 +1967,8 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
                 F.z = s->z;
                 F.q = s->q;
                 F.d = s->d;
-                F.p0 = s->p[0];
-                F.p1 = s->p[1];
+                F.p0 = s->p[kLearnedIters & 1];  // the direction the network iterations left
+                F.p1 = s->p[(kLearnedIters + 1) & 1];
                 F.partials = s->partials;
                 F.st = s->st;
                 F.spin_limit = wait_limit(1ll << 22);

@@ -240,3 +240,27 @@ def test_tensor_core_preconditioner_in_solver(cuda):
         sv.close()
     assert abs(its[0] - its[1]) <= 2, its
     net.close()
+
+
+def test_learned_solve_persistent_and_graph_launched_agree(cuda, monkeypatch):
+    """The Jacobi flexible-CG iterations that follow the network's run either
+    in one cooperative launch or as graph-launched chunks; both continue from
+    the direction the network iteration left and take the same iterations to
+    the same FP64 residual."""
+    import torch
+    from piro_b200 import ops
+    n = 32
+    a_t, b_t, A, dt = _family(n, 204)
+    net = ops.PCNet(seed=3)
+    its = []
+    for persist in ("1", "0"):
+        monkeypatch.setenv("PIRO_BE_PERSISTENT", persist)
+        sv = ops.BESolver(n, n, n, A, a_t, stencil=(float(dt), 1.0))
+        sv.set_preconditioner(net)
+        x = torch.empty_like(b_t)
+        info = sv.solve(b_t, x, rtol=1e-8)
+        assert info.status == 0 and info.rel_residual <= 1e-8 and info.fallbacks == 0
+        its.append(info.inner_iterations)
+        sv.close()
+    assert abs(its[0] - its[1]) <= 1, its
+    net.close()
