@@ -782,9 +782,10 @@ struct Own {
 // two x-lines, and every row offset keeps 16-byte alignment).  Per group:
 // 11 float4 loads + 4 scalar halo loads instead of 60 scalar loads.
 // kFlex (flexible CG): also <p, r/alpha> into pr, r read where the block keeps it.
-template <bool kRes, bool kFlex = false>
+template <bool kRes, bool kFlex = false, bool kDefer = false>
 __device__ __forceinline__ double cg_phase_a_vec(const PArgs &P, const Own<kRes> &O, const float *pold, float *pnew,
-                                                 float fb, int64_t v0, int64_t v1, int64_t dv, double *pr = nullptr)
+                                                 float fb, int64_t v0, int64_t v1, int64_t dv, double *pr = nullptr,
+                                                 float fa_prev = 0.0f)
 {
     const GridDiv &g = P.g;
     const int64_t rx = g.nx >> 2, rxy = ((int64_t)g.nx * g.ny) >> 2;
@@ -798,6 +799,12 @@ __device__ __forceinline__ double cg_phase_a_vec(const PArgs &P, const Own<kRes>
         g.coords((uint32_t)i, x0, y, z);
         if (!(y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1)) continue;  // boundary row: p, q stay 0
         const float4 zc = ld_(Z + v), pc = ld_(Po + v);
+        if (kDefer) {  // the previous iteration's d += a p, on this group's own p
+            float4 *D = reinterpret_cast<float4 *>(O.d);
+            float4 dd = D[O.g(v)];
+            dd.x += fa_prev * pc.x; dd.y += fa_prev * pc.y; dd.z += fa_prev * pc.z; dd.w += fa_prev * pc.w;
+            D[O.g(v)] = dd;
+        }
         const float4 zym = ld_(Z + v - rx), pym = ld_(Po + v - rx), zyp = ld_(Z + v + rx), pyp = ld_(Po + v + rx);
         const float4 zzm = ld_(Z + v - rxy), pzm = ld_(Po + v - rxy), zzp = ld_(Z + v + rxy), pzp = ld_(Po + v + rxy);
         const float zl = x0 > 0 ? ld_(P.z + i - 1) : 0.0f, pl = x0 > 0 ? ld_(pold + i - 1) : 0.0f;
@@ -855,7 +862,7 @@ struct PhaseBGroup {
 };
 
 // kFlex (flexible CG): rzn takes <z, q/alpha> (the next direction's beta) instead of <r/alpha, z>.
-template <bool kRes, bool kFlex = false>
+template <bool kRes, bool kFlex = false, bool kDefer = false>
 __device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const Own<kRes> &O, const float *pnew, float fa,
                                                int64_t v0, int64_t v1, int64_t dv, double &rzn, double &rr)
 {
@@ -867,16 +874,19 @@ __device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const Own<kRes> &
         const int64_t o = O.g(v);
         G.di = __ldg(Di + v);
         G.al = __ldg(Al + v);
-        G.pp = ld_(Pn + v);
+        if (!kDefer) G.pp = ld_(Pn + v);
     };
     auto finish = [&](int64_t v, const PhaseBGroup &G) {
         const int64_t o = O.g(v);
         const float4 qq = Q[o];
-        float4 dd = D[o], r4 = R[o];
-        dd.x += fa * G.pp.x; dd.y += fa * G.pp.y; dd.z += fa * G.pp.z; dd.w += fa * G.pp.w;
+        float4 r4 = R[o];
+        if (!kDefer) {
+            float4 dd = D[o];
+            dd.x += fa * G.pp.x; dd.y += fa * G.pp.y; dd.z += fa * G.pp.z; dd.w += fa * G.pp.w;
+            D[o] = dd;
+        }
         r4.x -= fa * qq.x; r4.y -= fa * qq.y; r4.z -= fa * qq.z; r4.w -= fa * qq.w;
         const float4 z4 = make_float4(r4.x * G.di.x, r4.y * G.di.y, r4.z * G.di.z, r4.w * G.di.w);
-        D[o] = dd;
         R[o] = r4;
         reinterpret_cast<float4 *>(P.z)[v] = z4;
         const float4 w = kFlex ? qq : r4;  // <w/alpha, z>
@@ -1012,12 +1022,16 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
         double beta = 0.0;
         float *pold = P.p0, *pnew = P.p1;
         bool broken = false;
+        // resident variant: d += a p rides on the next phase A (own cells only,
+        // so the block barrier below orders it before phase X)
+        const bool defer = kRes && P.vec_a;
+        float fa_prev = 0.0f;
         while (rr0 > 0.0) {
             // A: p = z + beta*p_old, q = A_II p, <p, q/alpha>
             const float fb = (float)beta;
             double pq = 0.0;
             if (P.vec_a) {
-                pq = cg_phase_a_vec<kRes>(P, O, pold, pnew, fb, v_beg, v_end, c_step);
+                pq = cg_phase_a_vec<kRes, false, kRes>(P, O, pold, pnew, fb, v_beg, v_end, c_step, nullptr, fa_prev);
             } else {
                 for (int64_t i = c_beg; i < c_end; i += c_step) {
                     if (!inter(i)) continue;
@@ -1046,7 +1060,8 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
             // B: d += a p, r -= a q, z = r / A_rr
             double bsum[2] = {0.0, 0.0};
             if (P.vec_b) {
-                cg_phase_b_vec<kRes>(P, O, pnew, fa, v_beg, v_end, c_step, bsum[0], bsum[1]);
+                cg_phase_b_vec<kRes, false, kRes>(P, O, pnew, fa, v_beg, v_end, c_step, bsum[0], bsum[1]);
+                fa_prev = fa;
             } else {
                 for (int64_t i = c_beg; i < c_end; i += c_step) {
                     const float dv = __ldg(P.dinv + i);
@@ -1076,6 +1091,17 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
         }
         if (!ok) break;
         if (broken) { status = PIRO_STATUS_STALLED; break; }
+        if (defer && fa_prev != 0.0f) {  // the last iteration's d += a p (its p is pold after the swap)
+            float4 *D = reinterpret_cast<float4 *>(O.d);
+            const float4 *Pl = reinterpret_cast<const float4 *>(pold);
+            for (int64_t v = v_beg; v < v_end; v += c_step) {
+                const float4 pp = ld_(Pl + v);
+                float4 dd = D[O.g(v)];
+                dd.x += fa_prev * pp.x; dd.y += fa_prev * pp.y; dd.z += fa_prev * pp.z; dd.w += fa_prev * pp.w;
+                D[O.g(v)] = dd;
+            }
+            __syncthreads();  // phase X reads d by cell, written here by group
+        }
         // X: x += d, d = 0
         for (int64_t i = c_beg; i < c_end; i += c_step) {
             const float dv = O.d[O.c(i)];
@@ -1182,12 +1208,13 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(PArgs P)
         broken = !isfinite(beta);
     }
     float *pold = P.p0, *pnew = P.p1;
+    float fa_prev = 0.0f;  // resident variant: d += a p rides on the next phase A, as in k_be_persistent
     while (ok && !broken) {
         // A: p = z + beta p_old, q = A p, <p, S p>, <p, s>
         const float fb = (float)beta;
         double pv[2] = {0.0, 0.0};
         if (P.vec_a) {
-            pv[0] = cg_phase_a_vec<kRes, true>(P, O, pold, pnew, fb, v_beg, v_end, c_step, &pv[1]);
+            pv[0] = cg_phase_a_vec<kRes, true, kRes>(P, O, pold, pnew, fb, v_beg, v_end, c_step, &pv[1], fa_prev);
         } else {
             for (int64_t i = c_beg; i < c_end; i += c_step) {
                 if (!inter(i)) {
@@ -1226,7 +1253,8 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(PArgs P)
         const float fa = (float)a;
         double bv[2] = {0.0, 0.0};
         if (P.vec_b) {
-            cg_phase_b_vec<kRes, true>(P, O, pnew, fa, v_beg, v_end, c_step, bv[1], bv[0]);
+            cg_phase_b_vec<kRes, true, kRes>(P, O, pnew, fa, v_beg, v_end, c_step, bv[1], bv[0]);
+            fa_prev = fa;
         } else {
             for (int64_t i = c_beg; i < c_end; i += c_step) {
                 const float dv = __ldg(P.dinv + i);
@@ -1258,6 +1286,16 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(PArgs P)
         if (t_rr <= tol2 * rr0 || iters >= max_iters) break;
     }
     if (kRes) {  // the sweep's state back to the global arrays (d for the x update)
+        if (ok && !broken && fa_prev != 0.0f) {  // the last iteration's d += a p (its p is pold after the swap)
+            float4 *D = reinterpret_cast<float4 *>(O.d);
+            const float4 *Pl = reinterpret_cast<const float4 *>(pold);
+            for (int64_t v = v_beg; v < v_end; v += c_step) {
+                const float4 pp = ld_(Pl + v);
+                float4 dd = D[O.g(v)];
+                dd.x += fa_prev * pp.x; dd.y += fa_prev * pp.y; dd.z += fa_prev * pp.z; dd.w += fa_prev * pp.w;
+                D[O.g(v)] = dd;
+            }
+        }
         __syncthreads();
         for (int64_t i = c_beg; i < c_end; i += c_step) {
             P.r[i] = O.r[O.c(i)];
