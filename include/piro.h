@@ -468,9 +468,11 @@ int piro_pcnet_destroy(piro_pcnet *n);
 /* Select the inner preconditioner of a stencil solver (piro_be_create_stencil):
  * PIRO_PRECOND_JACOBI, or PIRO_PRECOND_LEARNED with a network (not owned; it
  * must outlive the solver's use of it).  With the learned preconditioner the
- * inner solve is flexible CG (Notay's FCG(1)) on the graph-launched path; a
- * refinement sweep that stalls (FP64 residual not halved) or breaks down
- * reverts to Jacobi-PCG for the rest of the solve (piro_be_info.fallbacks). */
+ * inner solve is flexible CG (Notay's FCG(1)): the network preconditions the
+ * first iteration of each refinement sweep (graph-launched), Jacobi the rest
+ * (one cooperative launch where the device allows it); a refinement sweep
+ * that stalls (FP64 residual not halved) or breaks down reverts to
+ * Jacobi-PCG for the rest of the solve (piro_be_info.fallbacks). */
 int piro_be_set_preconditioner(piro_be_solver *s, int kind, piro_pcnet *net);
 /* Live timing of the learned preconditioner: network applies since the last
  * reset and their summed device time in ms (CUDA events around each apply). */
