@@ -137,6 +137,10 @@ struct ResidualRow {
     }
 };
 
+__device__ __forceinline__ void residual_finish(double rr64, double bb, double rz, double rr32,
+                                                double *__restrict__ partials, DevState *__restrict__ st, double rtol,
+                                                double inner_floor, double *s_warp, bool *s_last);
+
 __global__ void __launch_bounds__(kRowThreads) k_residual(GridDiv g, int64_t N,
                                                         const int32_t *__restrict__ rowptr,
                                                         const int32_t *__restrict__ col,
@@ -151,9 +155,18 @@ __global__ void __launch_bounds__(kRowThreads) k_residual(GridDiv g, int64_t N,
     __shared__ bool s_last;
     ResidualRow op{g, alpha, dinv, b, x, r, z, 0.0, 0.0, 0.0, 0.0, 0.0};
     csr_for_rows(N, rowptr, col, val, op);
-    double part[4] = {block_sum(op.rr64, s_warp), block_sum(op.bb, s_warp), block_sum(op.rz, s_warp),
-                      block_sum(op.rr32, s_warp)};
-    if (!publish_last(partials, kRedCap, 4, part, &st->ticket[0], &s_last)) return;
+    residual_finish(op.rr64, op.bb, op.rz, op.rr32, partials, st, rtol, inner_floor, s_warp, &s_last);
+}
+
+// The residual sweep's partial sums, and in the block that finishes last the
+// inner solve's set-up (the end of k_residual and k_residual_mf).
+__device__ __forceinline__ void residual_finish(double rr64, double bb, double rz, double rr32,
+                                                double *__restrict__ partials, DevState *__restrict__ st, double rtol,
+                                                double inner_floor, double *s_warp, bool *s_last)
+{
+    double part[4] = {block_sum(rr64, s_warp), block_sum(bb, s_warp), block_sum(rz, s_warp),
+                      block_sum(rr32, s_warp)};
+    if (!publish_last(partials, kRedCap, 4, part, &st->ticket[0], s_last)) return;
     double tot[4];
     for (int t = 0; t < 4; ++t) tot[t] = gather_sum(partials + t * kRedCap, s_warp);
     if (threadIdx.x == 0) {
@@ -175,6 +188,57 @@ __global__ void __launch_bounds__(kRowThreads) k_residual(GridDiv g, int64_t N,
         st->done = (tot[3] == 0.0 || rel <= rtol) ? 1 : 0;
         st->ticket[0] = 0u;
     }
+}
+
+// The residual sweep with the matrix-free operator of a stencil solver: per
+// interior row the 7-point stencil over its interior neighbours (the
+// coefficients fl(1 + fl(-dt fl(alpha vself))) and fl(-dt fl(alpha vnb))
+// that the solver checked against A) plus the row's interior-boundary
+// entries taken exactly from A (ib_*, PIRO's 10.0 values included), with x
+// holding b on the boundary: the same r = b - A x in FP64 as k_residual
+// (the terms summed in another order), without streaming A's 8 bytes per
+// nonzero.
+__global__ void __launch_bounds__(256) k_residual_mf(GridDiv g, int64_t N, float mdt, float vself, float vnb,
+                                                     const int32_t *__restrict__ ib_ptr,
+                                                     const int32_t *__restrict__ ib_col,
+                                                     const float *__restrict__ ib_val, const float *__restrict__ alpha,
+                                                     const float *__restrict__ dinv, const float *__restrict__ b,
+                                                     const double *__restrict__ x, float *__restrict__ r,
+                                                     float *__restrict__ z, double *__restrict__ partials,
+                                                     DevState *__restrict__ st, double rtol, double inner_floor)
+{
+    __shared__ double s_warp[32];
+    __shared__ bool s_last;
+    double rr64 = 0.0, bb = 0.0, rz = 0.0, rr32 = 0.0;
+    const int64_t sxy = (int64_t)g.nx * g.ny;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        int xc, y, zc;
+        g.coords((uint32_t)i, xc, y, zc);
+        if (!(xc > 0 && xc < g.nx - 1 && y > 0 && y < g.ny - 1 && zc > 0 && zc < g.nz - 1)) {
+            r[i] = 0.0f;
+            z[i] = 0.0f;
+            continue;
+        }
+        const float a = __ldg(alpha + i);
+        const double cd = (double)__fadd_rn(1.0f, __fmul_rn(mdt, __fmul_rn(a, vself)));
+        const double co = (double)__fmul_rn(mdt, __fmul_rn(a, vnb));
+        const double nb = ((xc > 1 ? x[i - 1] : 0.0) + (xc < g.nx - 2 ? x[i + 1] : 0.0)) +
+                          ((y > 1 ? x[i - g.nx] : 0.0) + (y < g.ny - 2 ? x[i + g.nx] : 0.0)) +
+                          ((zc > 1 ? x[i - sxy] : 0.0) + (zc < g.nz - 2 ? x[i + sxy] : 0.0));
+        double q = cd * x[i] + co * nb;
+        for (int32_t k = ib_ptr[i]; k < ib_ptr[i + 1]; ++k) q += (double)ib_val[k] * x[ib_col[k]];
+        const double bi = (double)b[i];
+        const double ri = bi - q;
+        const float rf = (float)ri;
+        const float zf = rf * dinv[i];
+        r[i] = rf;
+        z[i] = zf;
+        rr64 += ri * ri;
+        bb += bi * bi;
+        rz += (double)rf / (double)a * (double)zf;
+        rr32 += (double)rf * (double)rf;
+    }
+    residual_finish(rr64, bb, rz, rr32, partials, st, rtol, inner_floor, s_warp, &s_last);
 }
 
 // p = z + beta*p_old (interior; 0 on boundary), q = A p, partial <p, q/alpha>.
@@ -1962,10 +2026,16 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
     PIRO_CUDA(cudaMemsetAsync(s->d, 0, sizeof(float) * (size_t)N, st));
     double prev_rel = INFINITY;
     for (int outer = 0; outer <= max_outer; ++outer) {
-        k_residual<<<s->grid_tiles, kRowThreads, 0, st>>>(GridDiv(s->nx, s->ny, s->nz), N, s->rowptr,
-                                                                        s->col, s->val, s->alpha,
-                                                       s->dinv, b, s->x64, s->r, s->z, s->partials, s->st, rtol,
-                                                       s->inner_floor);
+        if (s->op_mf && s->ib_ptr)
+            k_residual_mf<<<(unsigned)std::min<int64_t>(cdiv(N, 256), (int64_t)kRedCap), 256, 0, st>>>(
+                                                              GridDiv(s->nx, s->ny, s->nz), N, s->mdt, s->vself,
+                                                              s->vnb, s->ib_ptr, s->ib_col, s->ib_val, s->alpha,
+                                                              s->dinv, b, s->x64, s->r, s->z, s->partials, s->st,
+                                                              rtol, s->inner_floor);
+        else
+            k_residual<<<s->grid_tiles, kRowThreads, 0, st>>>(GridDiv(s->nx, s->ny, s->nz), N, s->rowptr, s->col,
+                                                             s->val, s->alpha, s->dinv, b, s->x64, s->r, s->z,
+                                                             s->partials, s->st, rtol, s->inner_floor);
         PIRO_CHECK_LAUNCH("k_residual");
         s->kernel_launches += 1;
         // cap for this sweep

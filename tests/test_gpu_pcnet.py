@@ -264,3 +264,31 @@ def test_learned_solve_persistent_and_graph_launched_agree(cuda, monkeypatch):
         sv.close()
     assert abs(its[0] - its[1]) <= 1, its
     net.close()
+
+
+def test_learned_solution_matches_the_plain_solve(cuda, oracle):
+    """The learned solve judges convergence by its own FP64 residual sweep
+    (the matrix-free form with the solver's interior-boundary entries); its
+    solution must equal the plain persistent solve's, and the FP64 oracle's,
+    to the accuracy a 1e-8 residual allows."""
+    import torch
+    from piro_b200 import ops
+    n = 30
+    a_t, b_t, A, dt = _family(n, 205)
+    net = ops.PCNet(seed=3)
+    xs = []
+    for learned_pc in (False, True):
+        sv = ops.BESolver(n, n, n, A, a_t, stencil=(float(dt), 1.0))
+        if learned_pc:
+            sv.set_preconditioner(net)
+        x = torch.empty_like(b_t)
+        info = sv.solve(b_t, x, rtol=1e-8)
+        assert info.status == 0 and info.rel_residual <= 1e-8
+        xs.append(x.cpu().numpy().astype(np.float64))
+        sv.close()
+    Ah = tuple(t.cpu().numpy() for t in A)
+    ref, _, _ = oracle.be_cg_f64(n, n, n, Ah, a_t.cpu().numpy(), b_t.cpu().numpy(), rtol=1e-13)
+    scale = np.abs(ref).max()
+    assert np.abs(xs[1] - xs[0]).max() <= 1e-6 * scale
+    assert np.abs(xs[1] - ref).max() <= 1e-6 * scale
+    net.close()
