@@ -982,9 +982,10 @@ __device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const Own<kRes> &
 
 // kRes: the resident variant (P.own_cells > 0, float4 paths only): each block
 // works on its own contiguous cells and keeps their r, d and q in dynamic
-// shared memory (3 * own_cells floats), so phase B streams 16 instead of 36
-// bytes per cell through L2 and phase A stores no q.  Otherwise the grid
-// strides over all cells and r, d, q live in global memory.
+// shared memory (3 * own_cells floats), so that per CG iteration only z (read
+// at the neighbours), the block's own p, alpha and 1/A_rr cross L2, and d += a
+// p rides on the next phase A.  Otherwise the grid strides over all cells and
+// r, d, q live in global memory.
 template <bool kRes>
 __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
 {
