@@ -201,3 +201,31 @@ def test_reference_spmv_over_threads_equals_sequential(oracle):
     seq = R.spmvht(N, keys.astype(np.int32), vals, 0.01, u)
     par = R.spmv_par("ht", nx, ny, nz, (keys.astype(np.int32), vals), 0.01, u)
     assert np.array_equal(seq.view(np.uint32), par.view(np.uint32))
+
+
+@pytest.mark.parametrize("n,dt", [((12, 10, 9), 3.0), ((9, 14, 11), 40.0)])
+def test_fp64_cg_matches_direct_solve(oracle, n, dt):
+    """The oracle's FP64 Jacobi-PCG, the reference every backward-Euler result
+    is checked against, equals a direct sparse solve of the same system
+    (A = I - dt diag(alpha) L assembled by the oracle's own csrgeam2 and row
+    scale, interior unknowns, boundary held at b) to 1e-10."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    nx, ny, nz = n
+    N = nx * ny * nz
+    rng = np.random.default_rng(31)
+    alpha = np.exp(rng.standard_normal(N)).astype(np.float32) * np.float32(0.01)
+    L = oracle.laplacian(nx, ny, nz, 3, np.float32(1.0))
+    Ls = (L[0], L[1], oracle.csr_rowscale(N, L[0], L[2], alpha))
+    I = (np.arange(N + 1, dtype=np.int32), np.arange(N, dtype=np.int32), np.ones(N, np.float32))
+    A = oracle.csrgeam2(N, I, np.float32(-dt), Ls)
+    b = rng.random(N).astype(np.float32)
+    u, its, rel = oracle.be_cg_f64(nx, ny, nz, A, alpha, b, rtol=1e-13)
+    M = sp.csr_matrix((A[2].astype(np.float64), A[1], A[0]), shape=(N, N))
+    x, y, z = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    inter = ((x > 0) & (x < nx - 1) & (y > 0) & (y < ny - 1) & (z > 0) & (z < nz - 1)).transpose(2, 1, 0).reshape(-1)
+    bb = b.astype(np.float64)
+    want = bb.copy()
+    want[inter] = spla.spsolve(M[inter][:, inter].tocsc(), bb[inter] - M[inter][:, ~inter] @ bb[~inter])
+    assert rel <= 1e-13
+    assert np.abs(u - want).max() <= 1e-10 * np.abs(want).max()
