@@ -841,7 +841,7 @@ __device__ __forceinline__ void all_sums(const double *partials, int first, doub
 // at a neighbour, so only z and p have to go through global memory.
 template <bool kRes>
 struct Own {
-    float *r, *d, *q;
+    float *r, *d, *q, *p;  // p: the block's own directions (the r-free resident form keeps them here)
     int64_t c0;
     __device__ __forceinline__ int64_t c(int64_t i) const { return kRes ? i - c0 : i; }
     __device__ __forceinline__ int64_t g(int64_t v) const { return kRes ? v - (c0 >> 2) : v; }
@@ -859,7 +859,7 @@ struct Own {
 // Measured on the 128^3 step (B200): 0.681 -> 0.607 ms, the same 32.4
 // iterations and FP64 residuals.  kFlex (flexible CG): also <p, r/alpha>
 // into pr, r read where the block keeps it.
-template <bool kRes, bool kDefer, bool kFlex = false>
+template <bool kRes, bool kDefer, bool kFlex = false, bool kNoR = false>
 __device__ __forceinline__ double cg_phase_a_rec(const PArgs &P, const Own<kRes> &O, const float *pold, float *pnew,
                                                  float fb, int64_t v0, int64_t v1, int64_t dv, float fa_prev,
                                                  double *pr = nullptr)
@@ -876,7 +876,7 @@ __device__ __forceinline__ double cg_phase_a_rec(const PArgs &P, const Own<kRes>
         int x0, y, z;
         g.coords((uint32_t)i, x0, y, z);
         if (!(y > 0 && y < g.ny - 1 && z > 0 && z < g.nz - 1)) continue;  // boundary row: p, q stay 0
-        const float4 zc = ld_(Z + v), pc = ld_(Po + v);
+        const float4 zc = ld_(Z + v), pc = kNoR ? reinterpret_cast<const float4 *>(O.p)[O.g(v)] : ld_(Po + v);
         if (kDefer) {  // the previous iteration's d += a p, on this group's own p
             float4 *D = reinterpret_cast<float4 *>(O.d);
             float4 dd = D[O.g(v)];
@@ -916,7 +916,10 @@ __device__ __forceinline__ double cg_phase_a_rec(const PArgs &P, const Own<kRes>
         }
         pq += (double)pqf;
         if (kFlex) prs += (double)prf;
-        reinterpret_cast<float4 *>(pnew)[v] = make_float4(pn[0], pn[1], pn[2], pn[3]);
+        if (kNoR)
+            reinterpret_cast<float4 *>(O.p)[O.g(v)] = make_float4(pn[0], pn[1], pn[2], pn[3]);
+        else
+            reinterpret_cast<float4 *>(pnew)[v] = make_float4(pn[0], pn[1], pn[2], pn[3]);
         Q[O.g(v)] = make_float4(qv[0], qv[1], qv[2], qv[3]);
     }
     if (kFlex) *pr = prs;
@@ -933,11 +936,13 @@ __device__ __forceinline__ double cg_phase_a_rec(const PArgs &P, const Own<kRes>
 // iteration count.  Two groups per iteration with all their loads first
 // spilled registers and was slower (0.83 ms).
 struct PhaseBGroup {
-    float4 di, al, pp;  // the global loads; q, d, r are read when the group is finished
+    float4 di, al, pp, zo;  // the global loads; q, d, r are read when the group is finished
 };
 
 // kFlex (flexible CG): rzn takes <z, q/alpha> (the next direction's beta) instead of <r/alpha, z>.
-template <bool kRes, bool kFlex = false, bool kDefer = false>
+// kNoR (the r-free resident form): r is not stored; r = z A_rr is formed
+// from the group's z (global, its own) and the diagonal from alpha.
+template <bool kRes, bool kFlex = false, bool kDefer = false, bool kNoR = false>
 __device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const Own<kRes> &O, const float *pnew, float fa,
                                                int64_t v0, int64_t v1, int64_t dv, double &rzn, double &rr)
 {
@@ -950,11 +955,18 @@ __device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const Own<kRes> &
         G.di = __ldg(Di + v);
         G.al = __ldg(Al + v);
         if (!kDefer) G.pp = ld_(Pn + v);
+        if (kNoR) G.zo = ld_(reinterpret_cast<const float4 *>(P.z) + v);
     };
     auto finish = [&](int64_t v, const PhaseBGroup &G) {
         const int64_t o = O.g(v);
         const float4 qq = Q[o];
-        float4 r4 = R[o];
+        float4 r4;
+        if (kNoR) {  // r = z A_rr (z = 0 and q = 0 on boundary cells, so r stays 0 there)
+            auto dg = [&](float a) { return __fadd_rn(1.0f, __fmul_rn(P.mdt, __fmul_rn(a, P.vself))); };
+            r4 = make_float4(G.zo.x * dg(G.al.x), G.zo.y * dg(G.al.y), G.zo.z * dg(G.al.z), G.zo.w * dg(G.al.w));
+        } else {
+            r4 = R[o];
+        }
         if (!kDefer) {
             float4 dd = D[o];
             dd.x += fa * G.pp.x; dd.y += fa * G.pp.y; dd.z += fa * G.pp.z; dd.w += fa * G.pp.w;
@@ -962,7 +974,7 @@ __device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const Own<kRes> &
         }
         r4.x -= fa * qq.x; r4.y -= fa * qq.y; r4.z -= fa * qq.z; r4.w -= fa * qq.w;
         const float4 z4 = make_float4(r4.x * G.di.x, r4.y * G.di.y, r4.z * G.di.z, r4.w * G.di.w);
-        R[o] = r4;
+        if (!kNoR) R[o] = r4;
         reinterpret_cast<float4 *>(P.z)[v] = z4;
         const float4 w = kFlex ? qq : r4;  // <w/alpha, z>
         float rz = 0.0f, r2 = 0.0f;
@@ -981,11 +993,14 @@ __device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const Own<kRes> &
 }
 
 // kRes: the resident variant (P.own_cells > 0, float4 paths only): each block
-// works on its own contiguous cells and keeps their r, d and q in dynamic
-// shared memory (3 * own_cells floats), so that per CG iteration only z (read
-// at the neighbours), the block's own p, alpha and 1/A_rr cross L2, and d += a
-// p rides on the next phase A.  Otherwise the grid strides over all cells and
-// r, d, q live in global memory.
+// works on its own contiguous cells and keeps their p, d and q in dynamic
+// shared memory (3 * own_cells floats).  r is not stored at all: phase B forms
+// it as z A_rr from the block's own z, which the neighbours need in global
+// memory anyway.  Per CG iteration only z (at the neighbours and its own),
+// alpha and 1/A_rr cross L2, and d += a p rides on the next phase A
+// (measured on the 128^3 step, B200: 0.595 -> 0.571 ms against r in shared
+// memory and p in global memory).  Otherwise the grid strides over all cells
+// and r, d, q, p live in global memory.
 template <bool kRes>
 __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
 {
@@ -1009,7 +1024,8 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
         c_step = kPT;
         v_beg = (c0 >> 2) + threadIdx.x;
         v_end = c1 >> 2;
-        O.r = reinterpret_cast<float *>(s_own);
+        O.r = nullptr;  // r-free: r = z A_rr where a phase needs it
+        O.p = reinterpret_cast<float *>(s_own);
         O.d = reinterpret_cast<float *>(s_own + G);
         O.q = reinterpret_cast<float *>(s_own + 2 * G);
         O.c0 = c0;
@@ -1020,6 +1036,7 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
         v_beg = c_beg;
         v_end = N >> 2;
         O.r = P.r;
+        O.p = nullptr;
         O.d = P.d;
         O.q = P.q;
         O.c0 = 0;
@@ -1043,8 +1060,8 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
             P.beff[i] = 0.0;
         }
         O.d[O.c(i)] = 0.0f;
-        if (kRes) {  // the global r, q hold zeros on boundary cells from creation; shared memory does not
-            O.r[O.c(i)] = 0.0f;
+        if (kRes) {  // the global p, q hold zeros on boundary cells from creation; shared memory does not
+            O.p[O.c(i)] = 0.0f;
             O.q[O.c(i)] = 0.0f;
         }
         P.p0[i] = 0.0f;
@@ -1067,7 +1084,7 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
             const double ri = ld_(P.beff + i) - (cd * ld_(P.x64 + i) + co * nb);
             const float rf = (float)ri;
             const float zf = rf * __ldg(P.dinv + i);
-            O.r[O.c(i)] = rf;
+            if (!kRes) O.r[O.c(i)] = rf;
             P.z[i] = zf;
             const double bi = (double)P.b[i];
             rr64 += ri * ri;
@@ -1107,7 +1124,7 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
             const float fb = (float)beta;
             double pq = 0.0;
             if (P.vec_a) {
-                pq = cg_phase_a_rec<kRes, kRes>(P, O, pold, pnew, fb, v_beg, v_end, c_step, fa_prev);
+                pq = cg_phase_a_rec<kRes, kRes, false, kRes>(P, O, pold, pnew, fb, v_beg, v_end, c_step, fa_prev);
             } else {
                 for (int64_t i = c_beg; i < c_end; i += c_step) {
                     if (!inter(i)) continue;
@@ -1136,7 +1153,7 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
             // B: d += a p, r -= a q, z = r / A_rr
             double bsum[2] = {0.0, 0.0};
             if (P.vec_b) {
-                cg_phase_b_vec<kRes, false, kRes>(P, O, pnew, fa, v_beg, v_end, c_step, bsum[0], bsum[1]);
+                cg_phase_b_vec<kRes, false, kRes, kRes>(P, O, pnew, fa, v_beg, v_end, c_step, bsum[0], bsum[1]);
                 fa_prev = fa;
             } else {
                 for (int64_t i = c_beg; i < c_end; i += c_step) {
@@ -1167,9 +1184,10 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
         }
         if (!ok) break;
         if (broken) { status = PIRO_STATUS_STALLED; break; }
-        if (defer && fa_prev != 0.0f) {  // the last iteration's d += a p (its p is pold after the swap)
+        if (defer && fa_prev != 0.0f) {  // the last iteration's d += a p (the block's own p)
             float4 *D = reinterpret_cast<float4 *>(O.d);
-            const float4 *Pl = reinterpret_cast<const float4 *>(pold);
+            const float4 *Pl = kRes ? reinterpret_cast<const float4 *>(O.p) - (O.c0 >> 2)
+                                    : reinterpret_cast<const float4 *>(pold);
             for (int64_t v = v_beg; v < v_end; v += c_step) {
                 const float4 pp = ld_(Pl + v);
                 float4 dd = D[O.g(v)];
