@@ -951,8 +951,7 @@ __device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const Own<kRes> &
     const float4 *Di = reinterpret_cast<const float4 *>(P.dinv), *Al = reinterpret_cast<const float4 *>(P.alpha);
     const float4 *Pn = reinterpret_cast<const float4 *>(pnew);
     auto load = [&](int64_t v, PhaseBGroup &G) {
-        const int64_t o = O.g(v);
-        G.di = __ldg(Di + v);
+        if (!kNoR) G.di = __ldg(Di + v);
         G.al = __ldg(Al + v);
         if (!kDefer) G.pp = ld_(Pn + v);
         if (kNoR) G.zo = ld_(reinterpret_cast<const float4 *>(P.z) + v);
@@ -961,9 +960,12 @@ __device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const Own<kRes> &
         const int64_t o = O.g(v);
         const float4 qq = Q[o];
         float4 r4;
+        float4 di = G.di;
         if (kNoR) {  // r = z A_rr (z = 0 and q = 0 on boundary cells, so r stays 0 there)
             auto dg = [&](float a) { return __fadd_rn(1.0f, __fmul_rn(P.mdt, __fmul_rn(a, P.vself))); };
-            r4 = make_float4(G.zo.x * dg(G.al.x), G.zo.y * dg(G.al.y), G.zo.z * dg(G.al.z), G.zo.w * dg(G.al.w));
+            const float4 dd4 = make_float4(dg(G.al.x), dg(G.al.y), dg(G.al.z), dg(G.al.w));
+            r4 = make_float4(G.zo.x * dd4.x, G.zo.y * dd4.y, G.zo.z * dd4.z, G.zo.w * dd4.w);
+            di = make_float4(rcp_approx(dd4.x), rcp_approx(dd4.y), rcp_approx(dd4.z), rcp_approx(dd4.w));
         } else {
             r4 = R[o];
         }
@@ -973,15 +975,16 @@ __device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const Own<kRes> &
             D[o] = dd;
         }
         r4.x -= fa * qq.x; r4.y -= fa * qq.y; r4.z -= fa * qq.z; r4.w -= fa * qq.w;
-        const float4 z4 = make_float4(r4.x * G.di.x, r4.y * G.di.y, r4.z * G.di.z, r4.w * G.di.w);
+        const float4 z4 = make_float4(r4.x * di.x, r4.y * di.y, r4.z * di.z, r4.w * di.w);
         if (!kNoR) R[o] = r4;
         reinterpret_cast<float4 *>(P.z)[v] = z4;
         const float4 w = kFlex ? qq : r4;  // <w/alpha, z>
         float rz = 0.0f, r2 = 0.0f;
-        if (G.di.x != 0.0f) { rz += w.x * z4.x * rcp_approx(G.al.x); r2 += r4.x * r4.x; }
-        if (G.di.y != 0.0f) { rz += w.y * z4.y * rcp_approx(G.al.y); r2 += r4.y * r4.y; }
-        if (G.di.z != 0.0f) { rz += w.z * z4.z * rcp_approx(G.al.z); r2 += r4.z * r4.z; }
-        if (G.di.w != 0.0f) { rz += w.w * z4.w * rcp_approx(G.al.w); r2 += r4.w * r4.w; }
+        // boundary cells: r = z = q = 0 there, their terms are 0 (kNoR needs no mask)
+        if (kNoR || G.di.x != 0.0f) { rz += w.x * z4.x * rcp_approx(G.al.x); r2 += r4.x * r4.x; }
+        if (kNoR || G.di.y != 0.0f) { rz += w.y * z4.y * rcp_approx(G.al.y); r2 += r4.y * r4.y; }
+        if (kNoR || G.di.z != 0.0f) { rz += w.z * z4.z * rcp_approx(G.al.z); r2 += r4.z * r4.z; }
+        if (kNoR || G.di.w != 0.0f) { rz += w.w * z4.w * rcp_approx(G.al.w); r2 += r4.w * r4.w; }
         rzn += (double)rz;
         rr += (double)r2;
     };
@@ -999,8 +1002,11 @@ __device__ __forceinline__ void cg_phase_b_vec(const PArgs &P, const Own<kRes> &
 // memory anyway.  Per CG iteration only z (at the neighbours and its own),
 // alpha and 1/A_rr cross L2, and d += a p rides on the next phase A
 // (measured on the 128^3 step, B200: 0.595 -> 0.571 ms against r in shared
-// memory and p in global memory).  Otherwise the grid strides over all cells
-// and r, d, q, p live in global memory.
+// memory and p in global memory).  Phase B and the sweep's first z take
+// 1/A_rr by rcp.approx of the diagonal formed from alpha instead of loading
+// it (0.575 -> 0.554 ms; Jacobi with that reciprocal is the same fixed
+// preconditioner in every iteration).  Otherwise the grid strides over all
+// cells and r, d, q, p live in global memory.
 template <bool kRes>
 __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
 {
@@ -1083,7 +1089,9 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
                               (ld_(P.x64 + i - sxy) + ld_(P.x64 + i + sxy));
             const double ri = ld_(P.beff + i) - (cd * ld_(P.x64 + i) + co * nb);
             const float rf = (float)ri;
-            const float zf = rf * __ldg(P.dinv + i);
+            // the resident (r-free) variant forms 1/A_rr by rcp.approx in phase B; the sweep's first z uses the same
+            const float zf = kRes ? rf * rcp_approx(__fadd_rn(1.0f, __fmul_rn(P.mdt, __fmul_rn(a, P.vself))))
+                                  : rf * __ldg(P.dinv + i);
             if (!kRes) O.r[O.c(i)] = rf;
             P.z[i] = zf;
             const double bi = (double)P.b[i];
