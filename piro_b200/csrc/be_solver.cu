@@ -892,7 +892,7 @@ __device__ __forceinline__ double cg_phase_a_rec(const PArgs &P, const Own<kRes>
         const float zm[4] = {zzm.x, zzm.y, zzm.z, zzm.w}, zp[4] = {zzp.x, zzp.y, zzp.z, zzp.w};
         const float a[4] = {al.x, al.y, al.z, al.w}, po[4] = {pc.x, pc.y, pc.z, pc.w}, q0[4] = {qo.x, qo.y, qo.z, qo.w};
         float pn[4], qv[4], rv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-        if (kFlex) {
+        if (kFlex && !kNoR) {
             const float4 r4 = reinterpret_cast<const float4 *>(O.r)[O.g(v)];
             rv[0] = r4.x; rv[1] = r4.y; rv[2] = r4.z; rv[3] = r4.w;
         }
@@ -908,7 +908,7 @@ __device__ __forceinline__ double cg_phase_a_rec(const PArgs &P, const Own<kRes>
                 qv[k] = w + fb * q0[k];
                 const float ia = rcp_approx(a[k]);
                 pqf += pn[k] * qv[k] * ia;
-                if (kFlex) prf += pn[k] * rv[k] * ia;
+                if (kFlex) prf += pn[k] * (kNoR ? c[k + 1] * cd : rv[k]) * ia;  // r = z A_rr in the r-free form
             } else {
                 pn[k] = 0.0f;
                 qv[k] = 0.0f;
@@ -1262,12 +1262,15 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(PArgs P)
         c_step = kPT;
         v_beg = (c0 >> 2) + threadIdx.x;
         v_end = c1 >> 2;
-        O.r = reinterpret_cast<float *>(s_own);
+        // r-free, as k_be_persistent<1>: the block's p (the direction the
+        // network iteration left), d and q in shared memory; r only as z A_rr
+        O.r = nullptr;
+        O.p = reinterpret_cast<float *>(s_own);
         O.d = reinterpret_cast<float *>(s_own + G);
         O.q = reinterpret_cast<float *>(s_own + 2 * G);
         O.c0 = c0;
         for (int64_t i = c_beg; i < c_end; i += c_step) {
-            O.r[O.c(i)] = P.r[i];
+            O.p[O.c(i)] = P.p0[i];
             O.d[O.c(i)] = P.d[i];
             O.q[O.c(i)] = P.q[i];
         }
@@ -1278,6 +1281,7 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(PArgs P)
         v_beg = c_beg;
         v_end = N >> 2;
         O.r = P.r;
+        O.p = nullptr;
         O.d = P.d;
         O.q = P.q;
         O.c0 = 0;
@@ -1296,7 +1300,14 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(PArgs P)
     double zq = 0.0;
     for (int64_t i = c_beg; i < c_end; i += c_step) {
         const float dv = __ldg(P.dinv + i);
-        const float zi = O.r[O.c(i)] * dv;  // dinv = 0 on the boundary: z = 0 there
+        // dinv = 0 on the boundary: z = 0 there; the resident form takes 1/A_rr as its phase B does
+        float zi = 0.0f;
+        if (kRes) {
+            if (dv != 0.0f)
+                zi = P.r[i] * rcp_approx(__fadd_rn(1.0f, __fmul_rn(P.mdt, __fmul_rn(__ldg(P.alpha + i), P.vself))));
+        } else {
+            zi = O.r[O.c(i)] * dv;
+        }
         P.z[i] = zi;
         if (dv != 0.0f) zq += (double)zi * (double)O.q[O.c(i)] / (double)__ldg(P.alpha + i);
     }
@@ -1316,7 +1327,8 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(PArgs P)
         const float fb = (float)beta;
         double pv[2] = {0.0, 0.0};
         if (P.vec_a) {
-            pv[0] = cg_phase_a_rec<kRes, kRes, true>(P, O, pold, pnew, fb, v_beg, v_end, c_step, fa_prev, &pv[1]);
+            pv[0] = cg_phase_a_rec<kRes, kRes, true, kRes>(P, O, pold, pnew, fb, v_beg, v_end, c_step, fa_prev,
+                                                           &pv[1]);
         } else {
             for (int64_t i = c_beg; i < c_end; i += c_step) {
                 if (!inter(i)) {
@@ -1355,7 +1367,7 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(PArgs P)
         const float fa = (float)a;
         double bv[2] = {0.0, 0.0};
         if (P.vec_b) {
-            cg_phase_b_vec<kRes, true, kRes>(P, O, pnew, fa, v_beg, v_end, c_step, bv[1], bv[0]);
+            cg_phase_b_vec<kRes, true, kRes, kRes>(P, O, pnew, fa, v_beg, v_end, c_step, bv[1], bv[0]);
             fa_prev = fa;
         } else {
             for (int64_t i = c_beg; i < c_end; i += c_step) {
@@ -1388,9 +1400,9 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(PArgs P)
         if (t_rr <= tol2 * rr0 || iters >= max_iters) break;
     }
     if (kRes) {  // the sweep's state back to the global arrays (d for the x update)
-        if (ok && !broken && fa_prev != 0.0f) {  // the last iteration's d += a p (its p is pold after the swap)
+        if (ok && !broken && fa_prev != 0.0f) {  // the last iteration's d += a p (the block's own p)
             float4 *D = reinterpret_cast<float4 *>(O.d);
-            const float4 *Pl = reinterpret_cast<const float4 *>(pold);
+            const float4 *Pl = reinterpret_cast<const float4 *>(O.p) - (O.c0 >> 2);
             for (int64_t v = v_beg; v < v_end; v += c_step) {
                 const float4 pp = ld_(Pl + v);
                 float4 dd = D[O.g(v)];
@@ -1399,8 +1411,7 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(PArgs P)
             }
         }
         __syncthreads();
-        for (int64_t i = c_beg; i < c_end; i += c_step) {
-            P.r[i] = O.r[O.c(i)];
+        for (int64_t i = c_beg; i < c_end; i += c_step) {  // r is recomputed by the next sweep's residual
             P.d[i] = O.d[O.c(i)];
             P.q[i] = O.q[O.c(i)];
         }
