@@ -684,9 +684,10 @@ __global__ void k_pc_feature(GridDiv g, int64_t N, const float *__restrict__ alp
 // launch.  Phases are separated by a grid barrier; every block reduces the
 // per-block partials itself in the same fixed order, so all blocks hold
 // identical scalars and take identical branches.  Data written inside the
-// kernel by other blocks is read with ld.global.cg (L2), never through L1.
-// At 128^3 the working set (x64, beff, r, z, q, d, p0, p1, alpha, dinv: about
-// 90 MB) stays in the 126 MB L2.
+// kernel by other blocks is read with ordinary loads after the barrier's
+// acquire (the partial sums with ld.global.cg), never through the read-only
+// path.  At 128^3 the global working set (x64, beff, z, alpha, the side
+// matrix: about 60 MB) stays in the 126 MB L2.
 //
 // The interior-boundary coupling of A (including the 10.0 entries of
 // stencils.cpp:278-291) is taken exactly from the CSR into a small side matrix
