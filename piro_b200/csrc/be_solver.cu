@@ -1132,7 +1132,7 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
             // A: p = z + beta*p_old, q = A_II p, <p, q/alpha>
             const float fb = (float)beta;
             double pq = 0.0;
-            if (P.vec_a) {
+            if (kRes || P.vec_a) {  // the resident variant only runs with the float4 paths
                 pq = cg_phase_a_rec<kRes, kRes, false, kRes>(P, O, pold, pnew, fb, v_beg, v_end, c_step, fa_prev);
             } else {
                 for (int64_t i = c_beg; i < c_end; i += c_step) {
@@ -1161,7 +1161,7 @@ __global__ void __launch_bounds__(kPT, 2) k_be_persistent(PArgs P)
             const float fa = (float)alpha_k;
             // B: d += a p, r -= a q, z = r / A_rr
             double bsum[2] = {0.0, 0.0};
-            if (P.vec_b) {
+            if (kRes || P.vec_b) {
                 cg_phase_b_vec<kRes, false, kRes, kRes>(P, O, pnew, fa, v_beg, v_end, c_step, bsum[0], bsum[1]);
                 fa_prev = fa;
             } else {
@@ -1327,7 +1327,7 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(PArgs P)
         // A: p = z + beta p_old, q = A p, <p, S p>, <p, s>
         const float fb = (float)beta;
         double pv[2] = {0.0, 0.0};
-        if (P.vec_a) {
+        if (kRes || P.vec_a) {  // the resident variant only runs with the float4 paths
             pv[0] = cg_phase_a_rec<kRes, kRes, true, kRes>(P, O, pold, pnew, fb, v_beg, v_end, c_step, fa_prev,
                                                            &pv[1]);
         } else {
@@ -1367,7 +1367,7 @@ __global__ void __launch_bounds__(kPT, 2) k_fcg_persistent(PArgs P)
         // B: d += a p, r -= a q, z = D^-1 r, |r|^2, <z, S p>
         const float fa = (float)a;
         double bv[2] = {0.0, 0.0};
-        if (P.vec_b) {
+        if (kRes || P.vec_b) {
             cg_phase_b_vec<kRes, true, kRes, kRes>(P, O, pnew, fa, v_beg, v_end, c_step, bv[1], bv[0]);
             fa_prev = fa;
         } else {
