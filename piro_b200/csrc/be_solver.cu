@@ -2042,10 +2042,10 @@ extern "C" int piro_be_solve(piro_be_solver *s, const float *b, float *x, double
         if (cudaEventElapsedTime(&ms, s->pev0, s->pev1) == cudaSuccess) {
             s->persist_ms += ms;
             s->persist_launches += 1;
-            // algorithmic bytes: P0 32, residual sweep 32 + update 24, CG iteration 16 (phase A: z, own p,
-            // alpha, p out) + 12 (phase B: 1/A_rr, alpha, z out) bytes per cell
+            // algorithmic bytes: P0 32, residual sweep 32 + update 24, CG iteration 8 (phase A: z, alpha)
+            // + 12 (phase B: z, alpha in, z out) bytes per cell (the resident form; p, d, q stay on chip)
             const double n = (double)N;
-            s->persist_bytes += n * (32.0 + 56.0 * (s->h_st->p_outer + 1) + 28.0 * s->h_st->p_inner + 8.0);
+            s->persist_bytes += n * (32.0 + 56.0 * (s->h_st->p_outer + 1) + 20.0 * s->h_st->p_inner + 8.0);
         } else {
             (void)cudaGetLastError();
         }
