@@ -386,14 +386,17 @@ int piro_be_create(int nx, int ny, int nz, const int32_t *rowptr, const int32_t 
  * operator is then applied matrix-free (alpha, dt and norm instead of the
  * CSR stream: 20 instead of ~60 bytes per row) after a device check that A's
  * interior block holds exactly those coefficients; if it does not, the CSR
- * operator is used.  The FP64 residual always uses the CSR A. */
+ * operator is used.  The FP64 residual is always that of the assembled A:
+ * the CSR itself, or the checked stencil plus A's interior-boundary entries
+ * copied from the CSR. */
 int piro_be_create_stencil(int nx, int ny, int nz, const int32_t *rowptr, const int32_t *col, const float *val,
                            const float *alpha, float dt, float norm, piro_stream_t stream, piro_be_solver **out);
 /* Inner operator in use: 0 CSR SpMV (graph-launched CG), 1 matrix-free
  * 7-point stencil (graph-launched CG), 2 matrix-free stencil with the whole
  * solve in one persistent cooperative launch (FP64 refinement and CG phases
  * separated by a grid barrier whose waits are bounded), 3 the same launch
- * with each block's r, d, q resident in shared memory.  The environment
+ * with each block's p, d, q resident in shared memory (r formed from z where
+ * it is needed).  The environment
  * variable PIRO_BE_PERSISTENT, read at creation, forces kind <= 1 ("0") or
  * keeps kind 2 instead of 3 ("g"). */
 int piro_be_inner_operator(piro_be_solver *s, int *kind);
