@@ -113,3 +113,42 @@ def test_kernel_cg_form_converges_like_fp32_pcg(oracle):
     # the same error history, to FP32 rounding, while the error is above it
     for k in range(0, min(30, len(err[0]), len(err[1])), 5):
         assert abs(err[0][k] - err[1][k]) <= 1e-3 * err[0][k] + 1e-6, k
+
+
+@pytest.mark.parametrize("n,scheme", [((9, 8, 7), 3), ((12, 6, 10), 3)])
+def test_matrix_free_residual_with_side_matrix_equals_csr(oracle, n, scheme):
+    """The FP64 residual the stencil solver forms without streaming A: on
+    interior rows the 7-point stencil over interior neighbours with the
+    coefficients fl(1 + fl(-dt fl(alpha vself))) and fl(-dt fl(alpha vnb)),
+    plus the row's entries in boundary columns copied from A (PIRO's 10.0
+    values among them), with x = b on the boundary -- equals b - A x."""
+    nx, ny, nz = n
+    N = nx * ny * nz
+    rng = np.random.default_rng(43)
+    dt = np.float32(5.0)
+    alpha = (np.exp(rng.standard_normal(N)) * 0.01).astype(np.float32)
+    L = oracle.laplacian(nx, ny, nz, scheme, np.float32(1.0))
+    Ls = (L[0], L[1], oracle.csr_rowscale(N, L[0], L[2], alpha))
+    I = (np.arange(N + 1, dtype=np.int32), np.arange(N, dtype=np.int32), np.ones(N, np.float32))
+    A = oracle.csrgeam2(N, I, -dt, Ls)
+    M = sp.csr_matrix((A[2].astype(np.float64), A[1], A[0]), shape=(N, N))
+    x3, y3, z3 = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    to_flat = lambda a3: a3.transpose(2, 1, 0).reshape(-1)
+    X, Y, Z = to_flat(x3), to_flat(y3), to_flat(z3)
+    inter = (X > 0) & (X < nx - 1) & (Y > 0) & (Y < ny - 1) & (Z > 0) & (Z < nz - 1)
+    b = rng.random(N).astype(np.float32)
+    x = np.where(inter, rng.standard_normal(N), b.astype(np.float64))
+    want = b.astype(np.float64) - M @ x
+    # the side matrix: entries of interior rows in boundary columns, exactly A's
+    side = M.multiply(inter[:, None]).tocsr()
+    side = side[:, ~inter] @ x[~inter]
+    vself, vnb = np.float32(-6.0), np.float32(1.0)
+    cd = (np.float32(1.0) + (-dt) * (alpha * vself)).astype(np.float64)
+    co = ((-dt) * (alpha * vnb)).astype(np.float64)
+    sxy = nx * ny
+    nb = np.zeros(N)
+    for off, ok in ((-1, X > 1), (1, X < nx - 2), (-nx, Y > 1), (nx, Y < ny - 2), (-sxy, Z > 1), (sxy, Z < nz - 2)):
+        idx = np.arange(N) + off
+        nb += np.where(ok & inter, x[np.clip(idx, 0, N - 1)], 0.0)
+    got = b.astype(np.float64) - (cd * x + co * nb + side)
+    assert np.abs(got[inter] - want[inter]).max() <= 1e-12 * np.abs(want[inter]).max()
